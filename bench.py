@@ -1,0 +1,391 @@
+"""SSIMULACRA 2.1 throughput on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Workload: 64 pairs of 1920x1080 8-bit sRGB planar images (seeded synthetic
+textures with 32 uniform rectangles; each pair distorted by Gaussian noise,
+Gaussian blur or 8x8 block quantisation), resident in device memory. A step
+scores all 64 pairs through the batched path (one launch per stage over every
+pair). Reported beside it: the plain one-pair-per-call path on the same
+pairs, the end-to-end number through the public API from pinned host memory
+(H2D of every image and D2H of every result inside the timed region), the
+live roofline of the dominant kernel, the clocks seen during the timed
+region and a CPU baseline (the oracle on the host cores).
+
+Multi-GPU: one process per GPU (torchrun), each scoring its own 64 pairs;
+no data-path collective (the pairs are independent). Timings are CUDA events
+on the launching stream, max over ranks.
+
+`--impl reference` times the CPU implementation of the path (the FP32
+restatement of VQM's shaders in oracle/; VQM itself needs Vulkan, which this
+machine does not have) on all host threads, on bounded samples of the same
+workload, and prints the same JSON line with "impl": "reference".
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SSIMULACRA2 pairs/s 1080p+4K, plain vs batched/served; p50/p99 ms; % HBM peak"
+WIDTH, HEIGHT, PAIRS = 1920, 1080, 64
+SEED0 = 1000
+
+
+def rank_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def _gen(args):
+    w, h, seed = args
+    from vqm_b200 import synthetic
+    o, d, _ = synthetic.rgb_pair(w, h, seed)
+    return o.data, d.data
+
+
+def make_pairs(count, w, h, seed0, workers=None):
+    """Generates pairs in spawned worker processes (before any CUDA call)."""
+    from concurrent.futures import ProcessPoolExecutor
+    import multiprocessing as mp
+    from vqm_b200 import ss2
+    fmt = ss2.srgb8_format()
+    jobs = [(w, h, seed0 + i) for i in range(count)]
+    workers = workers or min(len(jobs), os.cpu_count() or 1, 16)
+    if workers > 1:
+        with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+            raw = list(ex.map(_gen, jobs))
+    else:
+        raw = [_gen(j) for j in jobs]
+    return [(ss2.Image(w, h, fmt, o), ss2.Image(w, h, fmt, d)) for o, d in raw]
+
+
+def alg_bytes(w, h):
+    """Algorithmic bytes of one pair: raw input read once, plus the FP32 XYB
+    pyramid of the kept channels written once and read once, both images.
+    Returns (prepare, blur, whole pair)."""
+    from oracle import binding as ob  # plan + pruning only
+    from vqm_b200 import ss2
+    plan = ss2.plan_scales(w, h)
+    kept = 0
+    for s, (lw, lh) in enumerate(plan):
+        for c in range(3):
+            if not ob.channel_pruned(c, s, len(plan)):
+                kept += lw * lh
+    inp = 2 * ss2.required_bytes(ss2.srgb8_format(), w, h)
+    pyramid = 2 * 4 * kept
+    return inp + pyramid, pyramid, inp + 2 * pyramid
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons of one GPU while running."""
+
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40,
+               "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
+
+    def __init__(self, device_index: int):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._h = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            import torch
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            if not uuid.startswith("GPU-"):
+                uuid = "GPU-" + uuid
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByUUID(uuid.encode())
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self._h = None
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _sample(self):
+        nv = self._nv
+        self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+        mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+        for name, bit in self.REASONS.items():
+            if mask & bit:
+                self.reasons.add(name)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self._sample()
+            except Exception:
+                return
+            self._stop.wait(0.02)
+
+    def __enter__(self):
+        if self._h is not None:
+            self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._h is not None:
+            self._t.join()
+            try:
+                self._sample()
+            except Exception:
+                pass
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch(stage):
+    """Per-launch DRAM bytes of `stage` from the committed ncu summary, if
+    one exists for this workload."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        t = json.load(f)
+    entry = t.get(f"{WIDTH}x{HEIGHT}x{PAIRS}", {}).get(stage)
+    return None if entry is None else entry.get("bytes_per_launch")
+
+
+def cpu_baseline(pairs, threads):
+    from oracle import binding as ob
+    from tests.helpers import to_oracle
+    op = [(to_oracle(o), to_oracle(d)) for o, d in pairs]
+    ob.compute_many(op[:threads], threads=threads)  # warm-up
+    t0 = time.perf_counter()
+    ob.compute_many(op, threads=threads)
+    dt = time.perf_counter() - t0
+    return len(op) / dt, dt
+
+
+def run_reference(args):
+    """The CPU implementation of the path on all host threads."""
+    rank, world, _ = rank_env()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    sample = max(4, threads)
+    pairs = make_pairs(sample, WIDTH, HEIGHT, SEED0)
+    from oracle import binding as ob
+    from tests.helpers import to_oracle
+    op = [(to_oracle(o), to_oracle(d)) for o, d in pairs]
+    for _ in range(args.warmup):
+        ob.compute_many(op, threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ob.compute_many(op, threads=threads)
+    dt = time.perf_counter() - t0
+    value = sample * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{PAIRS} pairs {WIDTH}x{HEIGHT} 8-bit sRGB planar, "
+                               f"sampled {sample} pairs per step",
+                   "pairs_per_step": sample},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "port",
+                         "sample": f"{sample} pairs of {WIDTH}x{HEIGHT} per step, "
+                                   f"{args.steps} steps, FP32 restatement of VQM's shaders"},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="vqm_b200", choices=["vqm_b200", "reference"])
+    ap.add_argument("--pairs", type=int, default=PAIRS)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-sample", type=int, default=32)
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    rank, world, local = rank_env()
+    pairs = make_pairs(args.pairs, WIDTH, HEIGHT, SEED0 + 100_000 * rank)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from vqm_b200 import ss2
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # Inputs resident in HBM.
+    dev = []
+    for o, d in pairs:
+        to = torch.from_numpy(o.data).cuda()
+        td = torch.from_numpy(d.data).cuda()
+        dev.append((ss2.DeviceImage.packed(WIDTH, HEIGHT, o.format, to.data_ptr(), to),
+                    ss2.DeviceImage.packed(WIDTH, HEIGHT, d.format, td.data_ptr(), td)))
+    stream = torch.cuda.Stream()
+    batch = ss2.Ssimulacra2Batch(max_pairs=args.pairs)
+    batch.set_stream(stream.cuda_stream)
+    batch.set_timing(True)
+
+    for _ in range(args.warmup):
+        batch.compute_many(dev)
+    barrier()
+    stage = np.zeros(3)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            results = batch.compute_many(dev)
+            stage += np.array(batch.stage_ms())
+        end.record(stream)
+        torch.cuda.synchronize()
+    elapsed_ms = max_over_ranks(start.elapsed_time(end))
+    barrier()
+    scores = [r.score() for r in results]
+    value = world * args.pairs * args.steps / (elapsed_ms / 1e3)
+
+    # Roofline of the dominant stage, from its live CUDA-event time.
+    prep_b, blur_b, pair_b = alg_bytes(WIDTH, HEIGHT)
+    avg = stage / args.steps  # ms per launch
+    names = ("prepare", "blur", "finalize")
+    dom = int(np.argmax(avg))
+    per_launch = {0: prep_b, 1: blur_b, 2: 0}[dom] * args.pairs
+    peak, peak_kind = peaks()
+    achieved = per_launch / (avg[dom] / 1e3) / 1e9
+    traffic = traffic_per_launch(names[dom])
+
+    # Plain path: one pair per call, same resident pairs.
+    pipe = ss2.Ssimulacra2Pipeline(WIDTH, HEIGHT)
+    pipe.set_stream(stream.cuda_stream)
+    for o, d in dev[:3]:
+        pipe.compute(o, d)
+    barrier()
+    ps, pe = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lat = []
+    ps.record(stream)
+    for o, d in dev:
+        t0 = time.perf_counter()
+        pipe.compute(o, d)
+        lat.append(1e3 * (time.perf_counter() - t0))
+    pe.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = max_over_ranks(ps.elapsed_time(pe))
+    plain_value = world * len(dev) / (plain_ms / 1e3)
+    pipe.close()
+
+    # End to end through the public API from pinned host memory.
+    host = []
+    h2d = 0
+    for o, d in pairs:
+        imgs = []
+        for img in (o, d):
+            buf = torch.empty(img.data.nbytes, dtype=torch.uint8, pin_memory=True).numpy()
+            buf[:] = img.data
+            imgs.append(ss2.Image(WIDTH, HEIGHT, img.format, buf))
+            h2d += img.data.nbytes
+        host.append(tuple(imgs))
+    batch.set_timing(False)
+    for _ in range(2):
+        batch.compute_many(host)
+    barrier()
+    es, ee = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    es.record(stream)
+    for _ in range(args.e2e_steps):
+        batch.compute_many(host)
+    ee.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(es.elapsed_time(ee))
+    e2e_value = world * args.pairs * args.e2e_steps / (e2e_ms / 1e3)
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.skip_cpu:
+            threads = os.cpu_count() or 1
+            sample = pairs[: max(1, min(args.cpu_sample, len(pairs)))]
+            cpu_value, cpu_s = cpu_baseline(sample, threads)
+            cpu = {"value": cpu_value, "unit": "pairs/s", "cores": threads, "kind": "port",
+                   "sample": f"{len(sample)} of the {WIDTH}x{HEIGHT} pairs, "
+                             f"{cpu_s:.1f} s wall on {threads} threads"}
+        line = {
+            "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.pairs} pairs {WIDTH}x{HEIGHT} 8-bit sRGB planar, "
+                                   "resident in HBM, batched path (one launch per stage)",
+                       "pairs_per_step_per_gpu": args.pairs, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (796 MB of images per step)"},
+            "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": 112 * 8 * args.pairs,
+                    "path": "Ssimulacra2Batch.compute_many on pinned host images"},
+            "plain": {"value": plain_value, "unit": "pairs/s",
+                      "path": "Ssimulacra2Pipeline.compute, one pair per call, resident",
+                      "latency_ms_p50": float(np.percentile(lat, 50)),
+                      "latency_ms_p99": float(np.percentile(lat, 99))},
+            "batched_over_plain": value / plain_value,
+            "stage_ms_per_step": {n: float(a) for n, a in zip(names, avg)},
+            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved,
+                         "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "alg_bytes_per_launch": per_launch},
+            "step_roofline": {"alg_bytes_per_pair": pair_b,
+                              "achieved_gbs": pair_b * value / world / 1e9,
+                              "frac": pair_b * value / world / 1e9 / peak},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+            "score_sample": scores[:3],
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,259 @@
+/*
+ * vqm_cu_ss2.h -- C ABI of the B200 SSIMULACRA 2.1 scorer.
+ *
+ * Drop-in boundary for VQM's SSIMULACRA 2 path (GreatValueCreamSoda/vqm):
+ * every entry point below replaces one member of the reference's C++ API
+ * (include/ssimulacra2.h, include/vqm_image.h, include/vqm_pool.h), cited
+ * per function. Plain pointers, sizes and POD structs only; CUDA device
+ * pointers take the place of VQM's Vulkan buffers, a cudaStream_t (passed as
+ * void*) the place of its queue. include/vqm_cuda.hpp restores the
+ * reference's C++ classes and exception types on top of this ABI.
+ *
+ * Errors: every function returns a status code (VQM_CU_OK = 0). The code
+ * names the exception the reference throws in the same situation
+ * (std::invalid_argument, std::logic_error, std::runtime_error,
+ * std::overflow_error); vqm_cu_last_error() returns that call's message on
+ * the calling thread. No function throws.
+ *
+ * Threading (include/ssimulacra2.h:66-70, 135-144): a pipeline is not
+ * thread-safe and holds at most one submission in flight; a batch scorer
+ * holds at most one batch in flight. Separate objects may be used from
+ * separate threads.
+ */
+#ifndef VQM_CU_SS2_H_
+#define VQM_CU_SS2_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VQM_CU_OK 0
+#define VQM_CU_INVALID_ARGUMENT 1 /* std::invalid_argument */
+#define VQM_CU_LOGIC_ERROR 2      /* std::logic_error */
+#define VQM_CU_RUNTIME_ERROR 3    /* std::runtime_error (device, CUDA) */
+#define VQM_CU_OVERFLOW_ERROR 4   /* std::overflow_error */
+
+#define VQM_CU_MEMORY_HOST 0   /* planes are host addresses */
+#define VQM_CU_MEMORY_DEVICE 1 /* planes are CUDA device addresses */
+
+/* Norms per scale and the largest result: Ssimulacra2Scale
+ * (include/ssimulacra2.h:18-25) flattened, avg_ssim[6] then avg_edgediff[12],
+ * scale-major, up to six scales. */
+#define VQM_CU_SS2_NORMS_PER_SCALE 18
+#define VQM_CU_SS2_MAX_NORMS 108
+
+/* vqm::ImageFormat (include/vqm_image.h:325-337), zimg numeric enum values. */
+typedef struct vqm_cu_format {
+    uint8_t type;            /* PixelType: 0 Byte, 1 Word, 2 Half, 3 Float */
+    uint8_t family;          /* ColorFamily: 0 Grey, 1 Rgb, 2 Yuv */
+    uint8_t alpha;           /* AlphaType: 0 None, 1 Straight, 2 Premultiplied */
+    uint8_t range;           /* PixelRange: 0 Limited, 1 Full */
+    uint8_t matrix;          /* MatrixCoefficients */
+    uint8_t transfer;        /* TransferCharacteristics */
+    uint8_t primaries;       /* ColorPrimaries */
+    uint8_t chroma_location; /* ChromaLocation */
+    uint8_t subsample_w;     /* log2, 0..2 */
+    uint8_t subsample_h;     /* log2, 0..2 */
+    uint8_t depth;           /* 0 = the pixel type's full depth */
+    uint8_t reserved;        /* must be 0 */
+} vqm_cu_format;
+
+/* One image: vqm::Image (packed, include/vqm_image.h:339-358), vqm::ImageView
+ * (strided host planes, include/vqm_views.h:18-24) or a caller-owned device
+ * buffer (the CUDA counterpart of VulkanBufferView, include/vqm_vulkan.h).
+ * planes[i] points at the first row of plane i (Y/R, U/G, V/B, alpha);
+ * strides[i] is its row stride in bytes, 0 meaning tightly packed. Absent
+ * planes are ignored. Device planes must stay unmodified until the
+ * submission that reads them is finished. */
+typedef struct vqm_cu_image {
+    uint32_t width;
+    uint32_t height;
+    vqm_cu_format format;
+    int32_t memory; /* VQM_CU_MEMORY_HOST or VQM_CU_MEMORY_DEVICE */
+    const void* planes[4];
+    size_t strides[4];
+} vqm_cu_image;
+
+/* Ssimulacra2Config (include/ssimulacra2.h:35-64). */
+typedef struct vqm_cu_ss2_config {
+    uint32_t width;
+    uint32_t height;
+    uint32_t gpu_resident_images; /* slots for upload(); default 2 */
+    uint32_t half_planes;         /* 1: FP16 pyramid planes */
+    uint32_t chroma_filter;       /* 0 bilinear, 1 bicubic, 2 lanczos */
+    uint32_t streaming_inputs;    /* 1: host-image submit overloads allowed */
+    uint64_t input_bytes;         /* pool for allocate_image(); 0 = none */
+    int32_t device;               /* CUDA ordinal; -1 = the current device */
+    uint32_t reserved;
+} vqm_cu_ss2_config;
+
+/* PipelineMemoryUsage (include/vqm_memory_types.h:24-33), device bytes. */
+typedef struct vqm_cu_memory_usage {
+    uint64_t pyramid_bytes;  /* XYB planes */
+    uint64_t resident_bytes; /* upload() slots */
+    uint64_t input_bytes;    /* allocate_image() pool + streaming inputs */
+    uint64_t scratch_bytes;  /* partials, tables, results */
+    uint64_t total_bytes;
+} vqm_cu_memory_usage;
+
+typedef struct vqm_cu_ss2_pipeline vqm_cu_ss2_pipeline;
+typedef struct vqm_cu_ss2_batch vqm_cu_ss2_batch;
+
+/* ---- library -------------------------------------------------------- */
+
+/* Message of the last failing call on this thread ("" after success). */
+const char* vqm_cu_last_error(void);
+/* ABI version: (major << 16) | minor. */
+uint32_t vqm_cu_version(void);
+
+/* ---- formats (src/input.cc) ----------------------------------------- */
+
+/* RequiredBytes (include/vqm_image.h:360-363; src/input.cc:244-255). */
+int vqm_cu_required_bytes(const vqm_cu_format* format, uint32_t width,
+                          uint32_t height, size_t* bytes);
+/* ValidateImage (src/input.cc:152-222): VQM_CU_INVALID_ARGUMENT with
+ * "<name>: <reason>" when the format/size pair is not decodable. */
+int vqm_cu_validate_format(const vqm_cu_format* format, uint32_t width,
+                           uint32_t height, const char* name);
+/* PlanSsimulacra2Scales (src/metrics/ssimulacra2/pipeline.cc:28-48): writes
+ * up to 6 (width, height) pairs into sizes12, the count into *scales. */
+int vqm_cu_ss2_plan_scales(uint32_t width, uint32_t height, uint32_t* sizes12,
+                           uint32_t* scales);
+/* Ssimulacra2Result::Score (src/metrics/ssimulacra2/score.cc:118-163), FP64,
+ * norms in the layout above. VQM_CU_INVALID_ARGUMENT for more than six
+ * scales or nonfinite norms, as the reference throws. */
+int vqm_cu_ss2_score(const double* norms, uint32_t scales, double* score);
+
+/* The decode constants this library derives for one format, as the 44
+ * words of VQM's per-image SourceDesc (src/vulkan/vulkan_support.h:104-120,
+ * built by src/vulkan/vulkan_source.cc:77-182) with plane offsets and row
+ * strides left 0. For inspection and tests. */
+int vqm_cu_ss2_source_constants(const vqm_cu_format* format,
+                                uint32_t chroma_filter, uint32_t* words44);
+
+/* ---- pipeline: one geometry, one pair in flight ---------------------- */
+/*      (class Ssimulacra2Pipeline, include/ssimulacra2.h:83-215)          */
+
+/* Ssimulacra2Pipeline(Ssimulacra2Config) (ssimulacra2.h:85-89): allocates
+ * all device memory for the geometry. INVALID_ARGUMENT below 8x8. */
+int vqm_cu_ss2_create(const vqm_cu_ss2_config* config,
+                      vqm_cu_ss2_pipeline** pipeline);
+/* ~Ssimulacra2Pipeline: waits for pending work, frees everything. */
+int vqm_cu_ss2_destroy(vqm_cu_ss2_pipeline* pipeline);
+/* The stream all of the pipeline's work is ordered on (cudaStream_t). The
+ * default is a stream the pipeline owns; a caller's stream replaces it. */
+int vqm_cu_ss2_set_stream(vqm_cu_ss2_pipeline* pipeline, void* stream);
+int vqm_cu_ss2_get_stream(vqm_cu_ss2_pipeline* pipeline, void** stream);
+
+/* Submit(Image/ImageView, Image/ImageView) (ssimulacra2.h:145-151) and the
+ * caller-owned device buffer form of Submit(VulkanBufferView, ...)
+ * (:192-195): host planes are copied to the device before this returns;
+ * device planes are read in place. LOGIC_ERROR while a submission is in
+ * flight. */
+int vqm_cu_ss2_submit(vqm_cu_ss2_pipeline* pipeline,
+                      const vqm_cu_image* original,
+                      const vqm_cu_image* distorted, float background,
+                      uint64_t* token);
+/* Submit(UploadedImage, UploadedImage) (ssimulacra2.h:152-155). */
+int vqm_cu_ss2_submit_resident(vqm_cu_ss2_pipeline* pipeline,
+                               uint64_t original, uint64_t distorted,
+                               float background, uint64_t* token);
+/* Submit(UploadedImage, Image) (ssimulacra2.h:156-159). */
+int vqm_cu_ss2_submit_resident_image(vqm_cu_ss2_pipeline* pipeline,
+                                     uint64_t original,
+                                     const vqm_cu_image* distorted,
+                                     float background, uint64_t* token);
+/* Submit(ImageBuffer, ImageBuffer) (ssimulacra2.h:181-184). */
+int vqm_cu_ss2_submit_buffers(vqm_cu_ss2_pipeline* pipeline,
+                              uint64_t original, uint64_t distorted,
+                              float background, uint64_t* token);
+/* Submit(..., VulkanSubmitSync) (ssimulacra2.h:198-201): the pipeline's
+ * stream first waits for every event in wait_events; after the pair's work
+ * it records every event in signal_events (cudaEvent_t, passed as void*). */
+int vqm_cu_ss2_submit_sync(vqm_cu_ss2_pipeline* pipeline,
+                           const vqm_cu_image* original,
+                           const vqm_cu_image* distorted,
+                           void* const* wait_events, uint32_t wait_count,
+                           void* const* signal_events, uint32_t signal_count,
+                           float background, uint64_t* token);
+/* Finish(token) (ssimulacra2.h:203): waits for the pair and writes its
+ * norms (18 per scale) and scale count. INVALID_ARGUMENT for an unknown or
+ * already finished token. */
+int vqm_cu_ss2_finish(vqm_cu_ss2_pipeline* pipeline, uint64_t token,
+                      double* norms108, uint32_t* scales);
+/* Compute (ssimulacra2.h:102-104) = submit + finish, plus the score. */
+int vqm_cu_ss2_compute(vqm_cu_ss2_pipeline* pipeline,
+                       const vqm_cu_image* original,
+                       const vqm_cu_image* distorted, float background,
+                       double* norms108, uint32_t* scales, double* score);
+
+/* Upload(Image) (ssimulacra2.h:115-118): copies into a resident slot and
+ * returns its handle (never 0). INVALID_ARGUMENT when every slot is used. */
+int vqm_cu_ss2_upload(vqm_cu_ss2_pipeline* pipeline, const vqm_cu_image* image,
+                      uint64_t* handle);
+/* Release(UploadedImage) (ssimulacra2.h:119-121): unknown or released
+ * handles are ignored. */
+int vqm_cu_ss2_release(vqm_cu_ss2_pipeline* pipeline, uint64_t handle);
+/* AllocateImage / MapImage / Release(ImageBuffer) (ssimulacra2.h:161-176):
+ * device memory carved from config.input_bytes, RequiredBytes(format) long,
+ * 64-byte aligned, in vqm::Image's packed layout. *device_ptr is a CUDA
+ * device address the caller fills (cudaMemcpy or its own kernels). */
+int vqm_cu_ss2_allocate_image(vqm_cu_ss2_pipeline* pipeline,
+                              const vqm_cu_format* format, uint64_t* handle,
+                              size_t* bytes);
+int vqm_cu_ss2_map_image(vqm_cu_ss2_pipeline* pipeline, uint64_t handle,
+                         void** device_ptr);
+int vqm_cu_ss2_release_image(vqm_cu_ss2_pipeline* pipeline, uint64_t handle);
+/* GetMemoryUsage (ssimulacra2.h:204-205). */
+int vqm_cu_ss2_memory_usage(vqm_cu_ss2_pipeline* pipeline,
+                            vqm_cu_memory_usage* usage);
+/* CUDA-graph replay of the pair's kernels (prepare, blur, finalize): on by
+ * default; 0 launches them one by one. */
+int vqm_cu_ss2_set_graphs(vqm_cu_ss2_pipeline* pipeline, int enabled);
+
+/* ---- batch: many pairs of any sizes and formats, one launch per stage --- */
+/*      (Ssimulacra2Pool::ComputeMany / ScoreMany, include/vqm_pool.h:51-87) */
+
+typedef struct vqm_cu_ss2_batch_config {
+    uint64_t max_pixels;   /* largest sum of W*H over one batch's pairs */
+    uint32_t max_pairs;    /* largest pair count of one batch */
+    uint32_t chroma_filter;
+    int32_t device;        /* CUDA ordinal; -1 = the current device */
+    uint32_t tile_w, tile_h; /* blur tile; 0 = the tuned default */
+    uint32_t reserved;
+} vqm_cu_ss2_batch_config;
+
+int vqm_cu_ss2_batch_create(const vqm_cu_ss2_batch_config* config,
+                            vqm_cu_ss2_batch** batch);
+int vqm_cu_ss2_batch_destroy(vqm_cu_ss2_batch* batch);
+int vqm_cu_ss2_batch_set_stream(vqm_cu_ss2_batch* batch, void* stream);
+/* Submits n pairs (host or device images; sizes may differ per pair, the
+ * two images of a pair must match). Host planes are copied before return. */
+int vqm_cu_ss2_batch_submit(vqm_cu_ss2_batch* batch, uint32_t n,
+                            const vqm_cu_image* originals,
+                            const vqm_cu_image* distorteds, float background,
+                            uint64_t* token);
+/* Waits and writes norms (n x 108, zero beyond each pair's scales), scale
+ * counts and scores (FP64, computed on the device). */
+int vqm_cu_ss2_batch_finish(vqm_cu_ss2_batch* batch, uint64_t token,
+                            double* norms, uint32_t* scales, double* scores);
+/* Opt-in stage timing, the CUDA counterpart of VQM's VQM_STAGE_TIMING
+ * (src/timing.h:18-112): CUDA events recorded on the batch's stream around
+ * the prepare, blur and finalize launches. After batch_finish, stage_ms3
+ * holds the last batch's device milliseconds of each stage. */
+int vqm_cu_ss2_batch_set_timing(vqm_cu_ss2_batch* batch, int enabled);
+int vqm_cu_ss2_batch_stage_ms(vqm_cu_ss2_batch* batch, float* stage_ms3);
+/* ComputeMany / ScoreMany = submit + finish. */
+int vqm_cu_ss2_batch_compute(vqm_cu_ss2_batch* batch, uint32_t n,
+                             const vqm_cu_image* originals,
+                             const vqm_cu_image* distorteds, float background,
+                             double* norms, uint32_t* scales, double* scores);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VQM_CU_SS2_H_ */

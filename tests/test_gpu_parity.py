@@ -1,0 +1,349 @@
+"""Parity of the CUDA scorer with the CPU oracle, through the C ABI.
+
+Bar: every one of the 108 features within 1e-4 relative (absolute floor
+1e-9) of the FP32 oracle, which the oracle tests pin to VQM's goldens;
+pruned features exactly 0; score within 1e-2; identity exactly 100; repeated
+calls bit-identical. The FP64 oracle error of each score is reported.
+"""
+
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+from tests import helpers
+from vqm_b200 import ss2, synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def check_parity(result, o, d, background=0.5, chroma_filter=0, label=""):
+    norms, score = helpers.oracle_compute(o, d, background, chroma_filter)
+    got = result.norms
+    assert got.shape == norms.shape, label
+    bad = helpers.feature_mismatch(got, norms)
+    assert not bad, (label, bad[:8])
+    mask = helpers.pruned_mask(got.shape[0])
+    assert np.all(got[mask] == 0.0), label
+    s = result.score()
+    assert abs(s - score) <= helpers.SCORE_TOL, (label, s, score)
+    _, score64 = helpers.oracle_compute(o, d, background, chroma_filter, precision=64)
+    print(f"{label}: cuda {s:.8f} oracle32 {score:.8f} oracle64 {score64:.8f} "
+          f"|d32| {abs(s - score):.2e} |d64| {abs(s - score64):.2e}")
+    return s
+
+
+@pytest.fixture(scope="module")
+def pipe32():
+    p = ss2.Ssimulacra2Pipeline(32, 32)
+    yield p
+    p.close()
+
+
+def test_vqm_gradient_goldens(pipe32):
+    # pipeline_test.cc:146-174.
+    o = helpers.gradient(0)
+    for v, gold in ((1, 93.17505696), (2, 92.12553218)):
+        d = helpers.gradient(v)
+        r = pipe32.compute(o, d)
+        assert len(r.scales) == 4
+        assert abs(r.score() - gold) <= 5e-3
+        check_parity(r, o, d, label=f"gradient 0/{v}")
+
+
+def test_identity_exactly_100(pipe32):
+    img = helpers.gradient(0)
+    r = pipe32.compute(img, img)
+    assert r.score() == 100.0
+    assert np.all(r.norms == 0.0)
+
+
+@pytest.mark.parametrize("w,h,scales", [(8, 8, 2), (13, 9, 2), (64, 64, 5), (65, 65, 5),
+                                        (129, 97, 5)])
+def test_small_geometries(w, h, scales):
+    # pipeline_test.cc:760-783: identity, scale count, repeatability.
+    img = helpers.ramp_image(w, h, False)
+    with ss2.Ssimulacra2Pipeline(w, h) as p:
+        first = p.compute(img, img)
+        assert len(first.scales) == scales
+        assert first.score() == 100.0
+        second = p.compute(img, img)
+        assert np.array_equal(first.norms, second.norms)
+        # A distorted ramp against the oracle at the same odd sizes.
+        d = helpers.ramp_image(w, h, False)
+        arr = d.data.view("<f4").copy()
+        arr[::7] = np.clip(arr[::7] * 0.9 + 0.03, 0, 1)
+        d.data = arr.view(np.uint8)
+        check_parity(p.compute(img, d), img, d, label=f"ramp {w}x{h}")
+
+
+def test_plain_256_pair():
+    o, d = helpers.plain_256_pair()
+    with ss2.Ssimulacra2Pipeline(256, 256) as p:
+        r = p.compute(o, d)
+        check_parity(r, o, d, label="256x256 noise+quant")
+        again = p.compute(o, d)
+        assert np.array_equal(r.norms, again.norms)
+
+
+@pytest.mark.parametrize("w,h", [(1920, 1080), (333, 187), (1001, 77), (640, 361)])
+def test_rgb8_sizes(w, h):
+    o, d, kind = synthetic.rgb_pair(w, h, seed=w * 7 + h)
+    with ss2.Ssimulacra2Pipeline(w, h) as p:
+        check_parity(p.compute(o, d), o, d, label=f"rgb8 {w}x{h} {kind}")
+
+
+@pytest.mark.parametrize("w,h", [(1920, 1080), (3840, 2160), (322, 182), (1278, 720)])
+def test_yuv420_10bit(w, h):
+    o, d, kind = synthetic.yuv_pair(w, h, seed=w + 3 * h)
+    with ss2.Ssimulacra2Pipeline(o.width, o.height) as p:
+        check_parity(p.compute(o, d), o, d, label=f"yuv420p10 {w}x{h} {kind}")
+
+
+def _variants():
+    F = ss2.ImageFormat
+    return {
+        "float": F(type=ss2.PixelType.Float),
+        "half": F(type=ss2.PixelType.Half),
+        "word16": F(type=ss2.PixelType.Word),
+        "word10_limited_rgb": F(type=ss2.PixelType.Word, depth=10, range=ss2.PixelRange.Limited),
+        "grey8": F(type=ss2.PixelType.Byte, family=ss2.ColorFamily.Grey,
+                   matrix=ss2.MatrixCoefficients.Unspecified),
+        "yuv444_bt2020": F(type=ss2.PixelType.Word, family=ss2.ColorFamily.Yuv, depth=10,
+                           range=ss2.PixelRange.Limited, matrix=ss2.MatrixCoefficients.Bt2020Ncl,
+                           transfer=ss2.TransferCharacteristics.Bt2020_10,
+                           primaries=ss2.ColorPrimaries.Bt2020),
+        "yuv422_bt601": F(type=ss2.PixelType.Byte, family=ss2.ColorFamily.Yuv,
+                          range=ss2.PixelRange.Limited, matrix=ss2.MatrixCoefficients.St170M,
+                          transfer=ss2.TransferCharacteristics.Bt601,
+                          primaries=ss2.ColorPrimaries.St170M, subsample_w=1),
+        "yuv420_pq": F(type=ss2.PixelType.Word, family=ss2.ColorFamily.Yuv, depth=10,
+                       range=ss2.PixelRange.Limited, matrix=ss2.MatrixCoefficients.Bt2020Ncl,
+                       transfer=ss2.TransferCharacteristics.St2084,
+                       primaries=ss2.ColorPrimaries.Bt2020, subsample_w=1, subsample_h=1,
+                       chroma_location=ss2.ChromaLocation.TopLeft),
+        "ictcp_hlg": F(type=ss2.PixelType.Word, family=ss2.ColorFamily.Yuv, depth=12,
+                       range=ss2.PixelRange.Limited, matrix=ss2.MatrixCoefficients.Bt2100ICtCp,
+                       transfer=ss2.TransferCharacteristics.AribB67,
+                       primaries=ss2.ColorPrimaries.Bt2020),
+        "cl_2020": F(type=ss2.PixelType.Word, family=ss2.ColorFamily.Yuv, depth=10,
+                     range=ss2.PixelRange.Limited, matrix=ss2.MatrixCoefficients.Bt2020Cl,
+                     transfer=ss2.TransferCharacteristics.Bt2020_10,
+                     primaries=ss2.ColorPrimaries.Bt2020),
+        "rgb8_alpha": F(type=ss2.PixelType.Byte, alpha=ss2.AlphaType.Straight),
+        "rgbf_premul": F(type=ss2.PixelType.Float, alpha=ss2.AlphaType.Premultiplied),
+        "xvycc": F(type=ss2.PixelType.Byte, family=ss2.ColorFamily.Yuv,
+                   range=ss2.PixelRange.Limited, matrix=ss2.MatrixCoefficients.Bt709,
+                   transfer=ss2.TransferCharacteristics.Iec61966_2_4,
+                   primaries=ss2.ColorPrimaries.Bt709),
+    }
+
+
+def _values(fmt, w, h, seed):
+    rng = np.random.default_rng(seed)
+    base = synthetic.texture(w, h, rng) / 255.0
+    layout = ss2.plane_layout(fmt, w, h)
+    vals = []
+    for p in range(4):
+        if layout[p] is None:
+            vals.append(None)
+            continue
+        _, pw, ph, _ = layout[p]
+        src = base[min(p, 2)]
+        if (pw, ph) != (w, h):
+            src = src[: ph * (h // ph): h // ph, : pw * (w // pw): w // pw][:ph, :pw]
+        if p in (1, 2) and fmt.family == ss2.ColorFamily.Yuv:
+            src = (src - 0.5) * 0.6
+        if p == 3:
+            src = 0.2 + 0.8 * src
+        vals.append(src)
+    return vals
+
+
+@pytest.mark.parametrize("name", list(_variants()))
+@pytest.mark.parametrize("chroma_filter", [0, 1, 2])
+def test_input_formats(name, chroma_filter):
+    fmt = _variants()[name]
+    sub = fmt.subsample_w or fmt.subsample_h
+    if chroma_filter and not sub:
+        pytest.skip("chroma filter only applies to subsampled chroma")
+    w, h = 96, 66
+    ov = _values(fmt, w, h, 11)
+    dv = [None if v is None else np.clip(v + np.random.default_rng(5).normal(0, 0.02, v.shape),
+                                         -0.5 if i in (1, 2) and fmt.family == 2 else 0, 1)
+          for i, v in enumerate(ov)]
+    o = helpers.pack_planes(fmt, w, h, ov)
+    d = helpers.pack_planes(fmt, w, h, dv)
+    with ss2.Ssimulacra2Pipeline(w, h, chroma_filter=chroma_filter) as p:
+        for bg in ((0.1, 0.9) if fmt.alpha else (0.5,)):
+            check_parity(p.compute(o, d, bg), o, d, bg, chroma_filter,
+                         label=f"{name} filter {chroma_filter} bg {bg}")
+
+
+def test_mixed_format_pair():
+    o, _, _ = synthetic.rgb_pair(320, 180, seed=1)
+    _, d, _ = synthetic.yuv_pair(320, 180, seed=1)
+    with ss2.Ssimulacra2Pipeline(320, 180) as p:
+        check_parity(p.compute(o, d), o, d, label="rgb8 vs yuv420p10")
+
+
+def test_batch_matches_pipeline_bitwise():
+    pairs = [synthetic.rgb_pair(333, 187, 1)[:2], synthetic.yuv_pair(640, 360, 2)[:2],
+             synthetic.rgb_pair(8, 8, 3)[:2], synthetic.rgb_pair(1920, 1080, 4)[:2],
+             synthetic.yuv_pair(1000, 563, 5)[:2], helpers.plain_256_pair()]
+    b = ss2.Ssimulacra2Batch()
+    results = b.compute_many(pairs)
+    for (o, d), r in zip(pairs, results):
+        with ss2.Ssimulacra2Pipeline(o.width, o.height) as p:
+            single = p.compute(o, d)
+        assert np.array_equal(single.norms, r.norms)
+        assert abs(r.device_score - r.score()) <= 1e-9
+        check_parity(r, o, d, label=f"batch {o.width}x{o.height}")
+    # A second, smaller batch on the same scorer reuses its memory.
+    again = b.compute_many(pairs[:2])
+    assert np.array_equal(again[1].norms, results[1].norms)
+
+
+def test_pool_score_many_in_order():
+    pairs = [synthetic.rgb_pair(200 + 10 * i, 120, i)[:2] for i in range(5)]
+    pool = ss2.Ssimulacra2Pool(workers=2, chunk=2)
+    scores = pool.score_many(pairs)
+    for (o, d), s in zip(pairs, scores):
+        _, want = helpers.oracle_compute(o, d)
+        assert abs(s - want) <= helpers.SCORE_TOL
+
+
+def test_resident_and_streaming_agree_bitwise():
+    o, d = helpers.plain_256_pair()
+    with ss2.Ssimulacra2Pipeline(256, 256, gpu_resident_images=2) as p:
+        streamed = p.compute(o, d)
+        a, b = p.upload(o), p.upload(d)
+        assert np.array_equal(p.compute(a, b).norms, streamed.norms)
+        assert np.array_equal(p.compute(a, d).norms, streamed.norms)
+        with pytest.raises(ss2.InvalidArgument):
+            p.upload(o)  # both slots in use
+        p.release(a)
+        with pytest.raises(ss2.InvalidArgument, match="not a live resident image"):
+            p.compute(a, b)
+        p.release(a)  # stale release is ignored
+        c = p.upload(d)
+        assert c.slot != a.slot
+        assert p.compute(c, b).score() == 100.0
+
+
+def test_submit_finish_contracts():
+    o, d = helpers.plain_256_pair()
+    with ss2.Ssimulacra2Pipeline(256, 256) as p:
+        expected = p.compute(o, d)
+        tok = p.submit(o, d)
+        with pytest.raises(ss2.LogicError):
+            p.submit(o, o)
+        with pytest.raises(ss2.LogicError):
+            p.upload(o)
+        r = p.finish(tok)
+        assert np.array_equal(r.norms, expected.norms)
+        with pytest.raises(ss2.InvalidArgument):
+            p.finish(tok)
+        short = ss2.Image(256, 256, o.format, o.data[:-1])
+        with pytest.raises(ss2.InvalidArgument):
+            p.compute(short, d)
+        wrong = synthetic.rgb_pair(128, 256, 0)[0]
+        with pytest.raises(ss2.InvalidArgument, match="geometry"):
+            p.compute(wrong, d)
+
+
+def test_streaming_disabled():
+    o, d = helpers.plain_256_pair()
+    with ss2.Ssimulacra2Pipeline(256, 256, streaming_inputs=False) as p:
+        with pytest.raises(ss2.InvalidArgument):
+            p.compute(o, d)
+        a, b = p.upload(o), p.upload(d)
+        _, want = helpers.oracle_compute(o, d)
+        assert abs(p.compute(a, b).score() - want) <= helpers.SCORE_TOL
+
+
+def _cudart():
+    for name in ("libcudart.so.12", "libcudart.so"):
+        try:
+            return ctypes.CDLL(name)
+        except OSError:
+            continue
+    import torch  # the torch wheel ships a cudart
+    import glob
+    import os
+    libs = glob.glob(os.path.join(os.path.dirname(torch.__file__), "..", "nvidia",
+                                  "cuda_runtime", "lib", "libcudart.so*"))
+    return ctypes.CDLL(libs[0])
+
+
+def test_device_buffers_and_caller_pool():
+    import torch
+    o, d = helpers.plain_256_pair()
+    nbytes = o.data.nbytes
+    with ss2.Ssimulacra2Pipeline(256, 256, input_bytes=2 * ((nbytes + 63) // 64 * 64)) as p:
+        want = p.compute(o, d)
+        # Caller-owned device memory read in place.
+        to = torch.from_numpy(o.data).cuda()
+        td = torch.from_numpy(d.data).cuda()
+        do = ss2.DeviceImage.packed(256, 256, o.format, to.data_ptr(), to)
+        dd = ss2.DeviceImage.packed(256, 256, d.format, td.data_ptr(), td)
+        assert np.array_equal(p.compute(do, dd).norms, want.norms)
+        # AllocateImage / MapImage pool.
+        a = p.allocate_image(o.format)
+        b = p.allocate_image(d.format)
+        assert a.bytes == nbytes and b.bytes == nbytes
+        with pytest.raises(ss2.InvalidArgument):
+            p.allocate_image(o.format)  # pool full
+        rt = _cudart()
+        for buf, t in ((a, to), (b, td)):
+            assert rt.cudaMemcpy(ctypes.c_void_p(p.map_image(buf)), ctypes.c_void_p(t.data_ptr()),
+                                 ctypes.c_size_t(nbytes), 3) == 0
+        assert np.array_equal(p.compute(a, b).norms, want.norms)
+        tok = p.submit(a, b)
+        with pytest.raises(ss2.LogicError):
+            p.release(a)
+        with pytest.raises(ss2.LogicError):
+            p.map_image(a)
+        p.finish(tok)
+        p.release(a)
+        with pytest.raises(ss2.InvalidArgument):
+            p.compute(a, b)
+        c = p.allocate_image(o.format)
+        assert c.slot != a.slot
+
+
+def test_strided_host_planes():
+    o, d = helpers.plain_256_pair()
+    pad = 37
+    views = []
+    for img in (o, d):
+        planes = []
+        for p in range(3):
+            off = p * 256 * 256
+            plane = img.data[off:off + 256 * 256].reshape(256, 256)
+            padded = np.zeros((256, 256 + pad), dtype=np.uint8)
+            padded[:, :256] = plane
+            planes.append(padded)
+        views.append(ss2.HostImage(256, 256, img.format, planes + [None],
+                                   (256 + pad, 256 + pad, 256 + pad, 0)))
+    with ss2.Ssimulacra2Pipeline(256, 256) as p:
+        assert np.array_equal(p.compute(*views).norms, p.compute(o, d).norms)
+
+
+def test_graphs_on_and_off_agree():
+    o, d = helpers.plain_256_pair()
+    with ss2.Ssimulacra2Pipeline(256, 256) as p:
+        a = p.compute(o, d)
+        p.set_graphs(False)
+        b = p.compute(o, d)
+        p.set_graphs(True)
+        c = p.compute(o, d)
+    assert np.array_equal(a.norms, b.norms) and np.array_equal(a.norms, c.norms)
+
+
+def test_identity_at_4k():
+    o, _, _ = synthetic.yuv_pair(3840, 2160, seed=9)
+    with ss2.Ssimulacra2Pipeline(3840, 2160) as p:
+        r = p.compute(o, o)
+    assert r.score() == 100.0 and np.all(r.norms == 0.0)

@@ -1,0 +1,218 @@
+"""The CPU oracle, pinned before it is trusted: against the reference test
+suite's own golden scores and rules (tests/metrics/ssimulacra2/*.cc of
+GreatValueCreamSoda/vqm) and against the reference's score.cc / input.cc
+compiled from source (oracle/_ref)."""
+
+import ctypes
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle import binding as ob
+from tests import helpers
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def goldens():
+    with open(os.path.join(GOLDEN, "goldens.json")) as f:
+        return json.load(f)
+
+
+def test_gradient_fixtures_match_definition():
+    for v in range(3):
+        stored = np.load(os.path.join(GOLDEN, f"gradient_{v}.npy"))
+        assert np.array_equal(stored, helpers.gradient(v).data)
+
+
+@pytest.mark.parametrize("pin", goldens()["vqm_pins"]["gradient_scores"])
+def test_oracle_matches_vqm_gradient_goldens(pin):
+    # pipeline_test.cc:146-174: 93.17505696 / 92.12553218 within 5e-3.
+    o = helpers.gradient(pin["original"])
+    d = helpers.gradient(pin["distorted"])
+    norms, score = helpers.oracle_compute(o, d)
+    assert norms.shape == (4, 18)
+    assert abs(score - pin["score"]) <= pin["tolerance"]
+    # The FP64 restatement agrees within the same allowance.
+    _, score64 = helpers.oracle_compute(o, d, precision=64)
+    assert abs(score64 - pin["score"]) <= pin["tolerance"]
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_oracle_identity_is_exactly_100(precision):
+    # pipeline_test.cc:120-144: equal inputs cancel exactly in the maps.
+    for img in (helpers.gradient(0), helpers.ramp_image(65, 33, False),
+                helpers.plain_256_pair()[0]):
+        norms, score = helpers.oracle_compute(img, img, precision=precision)
+        assert score == 100.0
+        assert np.all(norms == 0.0)
+
+
+@pytest.mark.parametrize("w,h,scales", goldens()["vqm_pins"]["scale_counts"])
+def test_scale_counts(w, h, scales):
+    # pipeline_test.cc:760-783.
+    assert len(ob.plan_scales(w, h)) == scales
+    img = helpers.ramp_image(w, h, False)
+    norms, score = helpers.oracle_compute(img, img)
+    assert norms.shape[0] == scales and score == 100.0
+
+
+def test_plan_rejects_below_8x8():
+    with pytest.raises(ob.OracleError, match="8x8"):
+        ob.plan_scales(4, 8)
+
+
+def test_1080p_plan_and_pruning():
+    assert ob.plan_scales(1920, 1080) == [(1920, 1080), (960, 540), (480, 270),
+                                           (240, 135), (120, 68), (60, 34)]
+    kept = {s: [c for c in range(3) if not ob.channel_pruned(c, s, 6)] for s in range(6)}
+    assert kept == {0: [1], 1: [0, 1], 2: [0, 1], 3: [0, 1, 2], 4: [0, 1, 2], 5: []}
+    # pipeline_test.cc:163-169: at four scales X@1:1, Y@1:2, B@1:32 go.
+    pruned4 = {(c, s) for s in range(4) for c in range(3) if ob.channel_pruned(c, s, 4)}
+    assert pruned4 == {(0, 0), (1, 1), (2, 3)}
+
+
+def test_pruned_features_are_exact_zeros():
+    o, d = helpers.plain_256_pair()
+    norms, _ = helpers.oracle_compute(o, d)
+    mask = helpers.pruned_mask(norms.shape[0])
+    assert np.all(norms[mask] == 0.0)
+    assert np.all(norms[~mask] >= 0.0)
+
+
+def test_oracle_regression_pins():
+    g = goldens()["oracle"]
+    o, d = helpers.plain_256_pair()
+    import hashlib
+    assert hashlib.sha256(o.data.tobytes() + d.data.tobytes()).hexdigest() == \
+        g["plain_256_f32"]["sha256"]
+    for prec in (32, 64):
+        norms, score = helpers.oracle_compute(o, d, precision=prec)
+        assert score == g[f"plain_256_f{prec}"]["score"]
+        assert np.array_equal(norms, np.array(g[f"plain_256_f{prec}"]["norms"]))
+
+
+def test_fp32_vs_fp64_error_is_small():
+    o, d = helpers.plain_256_pair()
+    n32, s32 = helpers.oracle_compute(o, d)
+    n64, s64 = helpers.oracle_compute(o, d, precision=64)
+    assert abs(s32 - s64) < 1e-3
+    assert not helpers.feature_mismatch(n32, n64, rtol=1e-3, atol=1e-7)
+
+
+# --- score KATs (score_test.cc:11-46) ---------------------------------------
+
+
+def test_score_kats():
+    empty = np.zeros(0)
+    assert ob.score(empty, 0) == 100.0
+    six = np.zeros((6, 18))
+    assert ob.score(six, 6) == 100.0
+    for bad in (math.inf, -math.inf, math.nan):
+        for k in range(108):
+            n = np.zeros(108)
+            n[k] = bad
+            with pytest.raises(ob.OracleError):
+                ob.score(n, 6)
+    n = np.zeros(108)
+    n[3] = np.finfo(np.float64).max
+    with pytest.raises(ob.OracleError):
+        ob.score(n, 6)
+    n[3] = 1e200
+    with pytest.raises(ob.OracleError):
+        ob.score(n, 6)
+    n[3] = 100.0
+    s = ob.score(n, 6)
+    assert math.isfinite(s) and s < 0.0
+    with pytest.raises(ob.OracleError):
+        ob.score(np.zeros(126), 7)
+
+
+# --- against the reference's own host code (oracle/_ref) --------------------
+
+
+ref = ob.ref()
+needs_ref = pytest.mark.skipif(ref is None, reason="reference checkout not built")
+
+
+@needs_ref
+def test_score_bit_exact_against_reference_score_cc():
+    rng = np.random.default_rng(7)
+    for scales in range(0, 7):
+        for _ in range(50):
+            n = np.zeros(108)
+            n[: 18 * scales] = rng.uniform(0, 0.3, size=18 * scales) ** rng.uniform(1, 4)
+            out = ctypes.c_double()
+            assert ref.vqmref_score(n.ctypes.data_as(ctypes.c_void_p), scales,
+                                    ctypes.byref(out)) == 0
+            assert ob.score(n, scales) == out.value
+
+
+@needs_ref
+def test_pruning_matches_reference():
+    for scales in range(1, 7):
+        for s in range(scales):
+            for c in range(3):
+                assert ob.channel_pruned(c, s, scales) == bool(
+                    ref.vqmref_channel_pruned(c, s, scales))
+
+
+def _formats():
+    F = ob.Format
+    out = []
+    for family, matrix, sub in ((1, 0, (0, 0)), (0, 1, (0, 0)), (2, 1, (1, 1)), (2, 1, (1, 0)),
+                                (2, 9, (1, 1)), (2, 5, (0, 0)), (2, 8, (1, 1)), (2, 12, (1, 1)),
+                                (2, 10, (1, 1)), (2, 13, (0, 0))):
+        for t, depth in ((0, 0), (1, 10), (1, 12), (1, 0), (2, 0), (3, 0)):
+            for rng in (0, 1):
+                if rng == 0 and t >= 2:
+                    continue
+                for transfer in (13, 1, 8, 16, 18):
+                    for prim in (1, 9, 5):
+                        f = F()
+                        f.type, f.family, f.range, f.matrix = t, family, rng, matrix
+                        f.transfer, f.primaries, f.depth = transfer, prim, depth
+                        f.subsample_w, f.subsample_h = sub
+                        out.append(f)
+    ict = F()
+    ict.type, ict.family, ict.range, ict.matrix, ict.transfer, ict.primaries = 1, 2, 0, 14, 16, 9
+    ict.depth = 10
+    out.append(ict)
+    hlg = F()
+    hlg.type, hlg.family, hlg.range, hlg.matrix, hlg.transfer, hlg.primaries = 1, 2, 0, 14, 18, 9
+    hlg.depth = 10
+    out.append(hlg)
+    return out
+
+
+@needs_ref
+def test_decode_constants_bit_exact_against_reference_input_cc():
+    checked = 0
+    for f in _formats():
+        if ref.vqmref_validate(ctypes.c_char_p(bytes(f)), 64, 64) != 0:
+            continue
+        want = np.zeros(44, dtype=np.uint32)
+        assert ref.vqmref_source_desc(ctypes.c_char_p(bytes(f)), 0,
+                                      want.ctypes.data_as(ctypes.c_void_p)) == 0
+        got = ob.source_desc(f, 0)
+        # Words 34/35 (chroma siting) come from vulkan_source.cc, which has
+        # no standalone build; every other word must match bit for bit.
+        mask = np.ones(44, dtype=bool)
+        mask[[34, 35]] = False
+        assert np.array_equal(got[mask], want[mask]), (bytes(f), got, want)
+        checked += 1
+    assert checked > 100
+
+
+@needs_ref
+def test_required_bytes_matches_reference():
+    for f in _formats():
+        for w, h in ((33, 17), (8, 8), (64, 30), (1920, 1080)):
+            out = ctypes.c_size_t()
+            status = ref.vqmref_required_bytes(ctypes.c_char_p(bytes(f)), w, h,
+                                               ctypes.byref(out))
+            assert status == 0
+            assert ob.required_bytes(f, w, h) == out.value

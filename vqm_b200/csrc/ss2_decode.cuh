@@ -1,0 +1,332 @@
+// Input decode on the device: one image's raw samples to linear Rec.709 RGB.
+//
+// The arithmetic follows VQM's input chain (src/vulkan/shaders/color.glsl,
+// with the host constants of src/input.cc): raw sample times scale plus
+// offset, chroma upsampling, the matrix / constant-luminance / ICtCp step,
+// alpha, the transfer function and the primaries matrix. Every multiply-add
+// the reference's shader compiler would contract is an explicit __fmaf_rn;
+// the library is compiled with -fmad=false so nothing else is contracted.
+//
+// The 8-bit RGB / grey formats without alpha decode through a 256-entry table
+// built on the host per image (transfer(code * scale + offset)): the table
+// holds exactly the per-sample values, so both paths round identically.
+#pragma once
+
+#include <cuda_fp16.h>
+
+#include "ss2_device.cuh"
+
+namespace vqm_b200 {
+
+struct SrcView {
+    const DevSource* s;  // decode constants (shared memory copy)
+};
+
+__device__ __forceinline__ float RawSample(const DevSource& s, int plane,
+                                           uint32_t x, uint32_t y) {
+    const uint8_t* row = s.plane[plane] + static_cast<size_t>(y) * s.row_bytes[plane];
+    float v;
+    switch (s.type) {
+        case 0: v = static_cast<float>(row[x]); break;
+        case 1: v = static_cast<float>(reinterpret_cast<const uint16_t*>(row)[x]); break;
+        case 2: v = __half2float(reinterpret_cast<const __half*>(row)[x]); break;
+        default: v = reinterpret_cast<const float*>(row)[x]; break;
+    }
+    // color.glsl:86-89: class 0 luma/R (and RGB's G, B), 1 YUV chroma, 2 alpha.
+    const int cls = plane == 3 ? 2 : (plane != 0 && s.family == 2 ? 1 : 0);
+    return __fmaf_rn(v, s.scale[cls], s.offset[cls]);
+}
+
+// color.glsl:117-179.
+__device__ __forceinline__ float Rec709InvOetf(float x) {
+    x = fmaxf(x, 0.0f);
+    const float alpha = 1.09929682680944f, beta = 0.018053968510807f;
+    return x < __fmul_rn(4.5f, beta)
+               ? __fdiv_rn(x, 4.5f)
+               : powf(__fdiv_rn(__fadd_rn(x, __fsub_rn(alpha, 1.0f)), alpha),
+                      __fdiv_rn(1.0f, 0.45f));
+}
+__device__ __forceinline__ float SrgbEotf(float v) {
+    return v <= 0.04045f ? __fdiv_rn(v, 12.92f)
+                         : powf(__fdiv_rn(__fadd_rn(v, 0.055f), 1.055f), 2.4f);
+}
+__device__ __forceinline__ float St2084Eotf(float x) {
+    if (x <= 0.0f) return 0.0f;
+    const float xp = powf(x, __fdiv_rn(1.0f, 78.84375f));
+    const float num = fmaxf(__fsub_rn(xp, 0.8359375f), 0.0f);
+    const float den = fmaxf(__fsub_rn(18.8515625f, __fmul_rn(18.6875f, xp)),
+                            1.17549435e-38f);
+    return powf(__fdiv_rn(num, den), __fdiv_rn(1.0f, 0.1593017578125f));
+}
+__device__ __forceinline__ float AribInvOetf(float x) {
+    x = fmaxf(x, 0.0f);
+    return x <= 0.5f ? __fmul_rn(__fmul_rn(x, x), __fdiv_rn(1.0f, 3.0f))
+                     : __fdiv_rn(__fadd_rn(expf(__fdiv_rn(__fsub_rn(x, 0.55991073f),
+                                                         0.17883277f)),
+                                           0.28466892f),
+                                 12.0f);
+}
+__device__ __forceinline__ float TransferDecode(const DevSource& s, float v) {
+    switch (s.transfer) {
+        case 0: return v;
+        case 1: return v < 0.0f ? 0.0f : powf(v, 2.4f);
+        case 2: return v < 0.0f ? 0.0f : powf(v, 2.2f);
+        case 3: return v < 0.0f ? 0.0f : powf(v, 2.8f);
+        case 4: return SrgbEotf(v);
+        case 5: return v <= 0.0f ? 0.01f : powf(10.0f, __fmul_rn(2.0f, __fsub_rn(v, 1.0f)));
+        case 6:
+            return v <= 0.0f ? 0.00316227766f
+                             : powf(10.0f, __fmul_rn(2.5f, __fsub_rn(v, 1.0f)));
+        case 7:
+            return v >= 0.0f && v <= 1.0f
+                       ? powf(v, 2.4f)
+                       : (v < 0.0f ? -Rec709InvOetf(-v) : Rec709InvOetf(v));
+        case 8:
+            if (v >= 0.0f && v <= 1.0f) return powf(v, 2.4f);
+            return v >= 0.0f ? Rec709InvOetf(v)
+                             : __fdiv_rn(-Rec709InvOetf(__fmul_rn(-4.0f, v)), 4.0f);
+        case 9: return __fmul_rn(s.to_linear, St2084Eotf(v));
+        case 10:
+            return v < 0.0f ? 0.0f
+                            : __fmul_rn(__fdiv_rn(52.37f, 48.0f), powf(v, 2.6f));
+    }
+    return v;
+}
+// color.glsl:181-205.
+__device__ __forceinline__ void TransferRgb(const DevSource& s, float c[3]) {
+    if (s.transfer == 11) {
+        for (int i = 0; i < 3; ++i) c[i] = AribInvOetf(c[i]);
+        const float luma =
+            fmaxf(__fmaf_rn(s.kb, c[2], __fmaf_rn(s.kg, c[1], __fmul_rn(s.kr, c[0]))),
+                  1.17549435e-38f);
+        const float f = __fmul_rn(powf(luma, 0.2f), s.to_linear);
+        for (int i = 0; i < 3; ++i) c[i] = __fmul_rn(c[i], f);
+        return;
+    }
+    for (int i = 0; i < 3; ++i) c[i] = TransferDecode(s, c[i]);
+}
+// color.glsl:209-218.
+__device__ __forceinline__ void ApplyMatrix(const float* m, float v[3]) {
+    float r[3];
+    for (int row = 0; row < 3; ++row)
+        r[row] = __fmaf_rn(m[row * 3 + 2], v[2],
+                           __fmaf_rn(m[row * 3 + 1], v[1], __fmul_rn(m[row * 3], v[0])));
+    v[0] = r[0];
+    v[1] = r[1];
+    v[2] = r[2];
+}
+// color.glsl:223-236.
+__device__ __forceinline__ void ClToRgb(const DevSource& s, float e[3]) {
+    const float u = e[1], v = e[2];
+    const float kbv = u < 0.0f ? s.cl[0] : s.cl[1];
+    const float krv = v < 0.0f ? s.cl[2] : s.cl[3];
+    const float b = Rec709InvOetf(__fmaf_rn(__fmul_rn(u, 2.0f), kbv, e[0]));
+    const float r = Rec709InvOetf(__fmaf_rn(__fmul_rn(v, 2.0f), krv, e[0]));
+    const float luma = Rec709InvOetf(e[0]);
+    const float g = __fdiv_rn(__fmaf_rn(-s.kb, b, __fmaf_rn(-s.kr, r, luma)), s.kg);
+    e[0] = r;
+    e[1] = g;
+    e[2] = b;
+}
+
+// color.glsl:271-283.
+__device__ __forceinline__ float RoundHalfup(float x) {
+    return x < 0.0f ? floorf(__fadd_rn(x, 0.5f)) : floorf(__fadd_rn(x, 0.49999997f));
+}
+__device__ __forceinline__ int MirrorIndex(float xpos, uint32_t dim) {
+    const float extent = static_cast<float>(dim);
+    const float m = xpos < 0.0f ? -xpos
+                                : (xpos >= extent ? __fsub_rn(__fmul_rn(2.0f, extent), xpos)
+                                                  : xpos);
+    return static_cast<int>(fminf(fmaxf(m, 0.0f), __fsub_rn(extent, 1.0f)));
+}
+__device__ __forceinline__ float FilterKernel(int filter, float x) {
+    x = fabsf(x);
+    if (filter == 0) return fmaxf(__fsub_rn(1.0f, x), 0.0f);
+    if (filter == 1) {
+        if (x < 1.0f)
+            return __fmaf_rn(__fmul_rn(x, x), __fmaf_rn(x, 1.5f, -2.5f), 1.0f);
+        if (x < 2.0f)
+            return __fmaf_rn(x, __fmaf_rn(x, __fmaf_rn(-0.5f, x, 2.5f), -4.0f), 2.0f);
+        return 0.0f;
+    }
+    const float pi = 3.14159265358979323846f;
+    if (!(x < 3.0f)) return 0.0f;
+    const float a = x == 0.0f ? 1.0f : __fdiv_rn(sinf(__fmul_rn(pi, x)), __fmul_rn(pi, x));
+    const float x3 = __fdiv_rn(x, 3.0f);
+    const float b = x3 == 0.0f ? 1.0f : __fdiv_rn(sinf(__fmul_rn(pi, x3)), __fmul_rn(pi, x3));
+    return __fmul_rn(a, b);
+}
+
+// color.glsl:288-299.
+__device__ __forceinline__ void BilinearPhase(uint32_t out_pos, float scale, float shift,
+                                              int centre, int& s0, int& s1, float& w0,
+                                              float& w1) {
+    const float pos =
+        __fadd_rn(__fdiv_rn(__fadd_rn(static_cast<float>(out_pos), 0.5f), scale), shift);
+    const float base = __fadd_rn(RoundHalfup(__fsub_rn(pos, 1.0f)), 0.5f);
+    const float t = __fsub_rn(pos, base);
+    s0 = static_cast<int>(floorf(base)) - centre + 1;
+    s1 = s0 + 1;
+    w0 = __fsub_rn(1.0f, t);
+    w1 = t;
+}
+
+// color.glsl:324-367: bilinear chroma of the block's four samples.
+__device__ void ChromaBilinear(const DevSource& s, int plane, const uint32_t px[4],
+                               const uint32_t py[4], float out[4]) {
+    const uint32_t dx = s.plane_w[plane], dy = s.plane_h[plane];
+    const int cx = static_cast<int>(px[0] >> s.sub_w);
+    const int cy = static_cast<int>(py[0] >> s.sub_h);
+    float win[9];
+    const bool interior =
+        cx > 0 && cx + 1 < static_cast<int>(dx) && cy > 0 && cy + 1 < static_cast<int>(dy);
+#pragma unroll
+    for (int j = -1; j <= 1; ++j)
+#pragma unroll
+        for (int i = -1; i <= 1; ++i) {
+            uint32_t sx, sy;
+            if (interior) {
+                sx = static_cast<uint32_t>(cx + i);
+                sy = static_cast<uint32_t>(cy + j);
+            } else {
+                sx = static_cast<uint32_t>(
+                    MirrorIndex(__fadd_rn(static_cast<float>(cx + i), 0.5f), dx));
+                sy = static_cast<uint32_t>(
+                    MirrorIndex(__fadd_rn(static_cast<float>(cy + j), 0.5f), dy));
+            }
+            win[(j + 1) * 3 + (i + 1)] = RawSample(s, plane, sx, sy);
+        }
+    const float scx = static_cast<float>(1u << s.sub_w);
+    const float scy = static_cast<float>(1u << s.sub_h);
+    int xa0, xa1, xb0, xb1, ya0, ya1, yb0, yb1;
+    float xwa0, xwa1, xwb0, xwb1, ywa0, ywa1, ywb0, ywb1;
+    BilinearPhase(px[0], scx, s.shift_x, cx, xa0, xa1, xwa0, xwa1);
+    BilinearPhase(px[1], scx, s.shift_x, cx, xb0, xb1, xwb0, xwb1);
+    BilinearPhase(py[0], scy, s.shift_y, cy, ya0, ya1, ywa0, ywa1);
+    BilinearPhase(py[2], scy, s.shift_y, cy, yb0, yb1, ywb0, ywb1);
+    auto window = [&](int xa, int xb, int ya, int yb, float xwa, float xwb, float ywa,
+                      float ywb) {
+        const float w00 = __fmul_rn(xwa, ywa), w10 = __fmul_rn(xwb, ywa);
+        const float w01 = __fmul_rn(xwa, ywb), w11 = __fmul_rn(xwb, ywb);
+        return __fmaf_rn(w11, win[yb * 3 + xb],
+                         __fmaf_rn(w01, win[yb * 3 + xa],
+                                   __fmaf_rn(w10, win[ya * 3 + xb],
+                                             __fmul_rn(w00, win[ya * 3 + xa]))));
+    };
+    out[0] = window(xa0, xa1, ya0, ya1, xwa0, xwa1, ywa0, ywa1);
+    out[1] = window(xb0, xb1, ya0, ya1, xwb0, xwb1, ywa0, ywa1);
+    out[2] = window(xa0, xa1, yb0, yb1, xwa0, xwa1, ywb0, ywb1);
+    out[3] = window(xb0, xb1, yb0, yb1, xwb0, xwb1, ywb0, ywb1);
+}
+
+// color.glsl:371-432: bicubic (4 taps) or Lanczos-3 (6 taps) chroma.
+__device__ void AxisTaps(const DevSource& s, uint32_t out_pos, float scale, float shift,
+                         uint32_t dim, int taps, float* w, int* idx) {
+    const float pos =
+        __fadd_rn(__fdiv_rn(__fadd_rn(static_cast<float>(out_pos), 0.5f), scale), shift);
+    const float base =
+        __fadd_rn(RoundHalfup(__fsub_rn(pos, __fdiv_rn(static_cast<float>(taps), 2.0f))), 0.5f);
+    float total = 0.0f;
+    for (int j = 0; j < taps; ++j)
+        total = __fadd_rn(total, FilterKernel(s.filter,
+                                              __fsub_rn(__fadd_rn(base, static_cast<float>(j)), pos)));
+    for (int j = 0; j < taps; ++j) {
+        w[j] = __fdiv_rn(
+            FilterKernel(s.filter, __fsub_rn(__fadd_rn(base, static_cast<float>(j)), pos)),
+            total);
+        idx[j] = MirrorIndex(__fadd_rn(base, static_cast<float>(j)), dim);
+    }
+}
+__device__ void ChromaTaps(const DevSource& s, int plane, const uint32_t px[4],
+                           const uint32_t py[4], float out[4]) {
+    const int taps = s.filter == 1 ? 4 : 6;
+    const float scx = static_cast<float>(1u << s.sub_w);
+    const float scy = static_cast<float>(1u << s.sub_h);
+    float wx0[6], wx1[6], wy0[6], wy1[6];
+    int ix0[6], ix1[6], iy0[6], iy1[6];
+    AxisTaps(s, px[0], scx, s.shift_x, s.plane_w[plane], taps, wx0, ix0);
+    AxisTaps(s, px[1], scx, s.shift_x, s.plane_w[plane], taps, wx1, ix1);
+    AxisTaps(s, py[0], scy, s.shift_y, s.plane_h[plane], taps, wy0, iy0);
+    AxisTaps(s, py[2], scy, s.shift_y, s.plane_h[plane], taps, wy1, iy1);
+    auto taps2d = [&](const float* wx, const int* ix, const float* wy, const int* iy) {
+        float sum = 0.0f;
+        for (int j = 0; j < taps; ++j) {
+            float row = 0.0f;
+            for (int k = 0; k < taps; ++k)
+                row = __fmaf_rn(wx[k],
+                                RawSample(s, plane, static_cast<uint32_t>(ix[k]),
+                                          static_cast<uint32_t>(iy[j])),
+                                row);
+            sum = __fmaf_rn(wy[j], row, sum);
+        }
+        return sum;
+    };
+    out[0] = taps2d(wx0, ix0, wy0, iy0);
+    out[1] = taps2d(wx1, ix1, wy0, iy0);
+    out[2] = taps2d(wx0, ix0, wy1, iy1);
+    out[3] = taps2d(wx1, ix1, wy1, iy1);
+}
+
+// color.glsl:447-541: the block's four samples, linear Rec.709, in
+// (0,0), (1,0), (0,1), (1,1) order. The generic path: any format. Kept out
+// of line so its registers do not weigh on the table-driven fast path.
+__device__ __noinline__ void BlockLinearGeneric(const DevSource& s, uint32_t bx, uint32_t by,
+                                   float rgb[4][3]) {
+    const uint32_t lx = s.width - 1, ly = s.height - 1;
+    const uint32_t px[4] = {min(2 * bx, lx), min(2 * bx + 1, lx), min(2 * bx, lx),
+                            min(2 * bx + 1, lx)};
+    const uint32_t py[4] = {min(2 * by, ly), min(2 * by, ly), min(2 * by + 1, ly),
+                            min(2 * by + 1, ly)};
+    float cu[4] = {0, 0, 0, 0}, cv[4] = {0, 0, 0, 0};
+    const bool sub = s.chroma_variant && s.family == 2;
+    if (sub) {
+        if (s.filter == 0) {
+            ChromaBilinear(s, 1, px, py, cu);
+            ChromaBilinear(s, 2, px, py, cv);
+        } else {
+            ChromaTaps(s, 1, px, py, cu);
+            ChromaTaps(s, 2, px, py, cv);
+        }
+    }
+    const bool has_alpha = s.alpha != 0;
+    const bool premul = s.alpha == 2;
+    for (int i = 0; i < 4; ++i) {
+        const float alpha = has_alpha ? RawSample(s, 3, px[i], py[i]) : 1.0f;
+        float e[3];
+        e[0] = e[1] = e[2] = RawSample(s, 0, px[i], py[i]);
+        if (s.family != 0) {
+            if (sub) {
+                e[1] = cu[i];
+                e[2] = cv[i];
+            } else {
+                e[1] = RawSample(s, 1, px[i], py[i]);
+                e[2] = RawSample(s, 2, px[i], py[i]);
+            }
+        }
+        if (s.mode == 1) {
+            ClToRgb(s, e);
+        } else if (!s.identity1) {
+            ApplyMatrix(s.m1, e);
+        }
+        if (premul) {
+            const float cl = fminf(fmaxf(alpha, 0.0f), 1.0f);
+            if (cl == 0.0f) {
+                e[0] = e[1] = e[2] = 0.0f;
+            } else {
+                for (int k = 0; k < 3; ++k) e[k] = __fdiv_rn(e[k], cl);
+            }
+        }
+        if (has_alpha) {
+            const float target = __fmul_rn(__fsub_rn(1.0f, alpha), s.background);
+            for (int k = 0; k < 3; ++k) e[k] = __fmaf_rn(alpha, e[k], target);
+        }
+        if (s.mode != 1) TransferRgb(s, e);
+        if (!s.identity2) ApplyMatrix(s.m2, e);
+        rgb[i][0] = e[0];
+        rgb[i][1] = e[1];
+        rgb[i][2] = e[2];
+    }
+}
+
+}  // namespace vqm_b200

@@ -1,0 +1,110 @@
+// Device-side data layout of the SSIMULACRA 2.1 scorer: what the host
+// runtime writes into device memory once per batch shape and the kernels read.
+//
+// A "batch" is any list of image pairs, of any sizes and formats: a plain
+// one-pair call is a batch of one. Work is flattened into three launch
+// spaces so that every kernel covers every pair of the batch in one grid:
+//
+//   prepare  one CTA per (pair, image, 32x32 base tile): decode, linear RGB,
+//            XYB, and the whole 6-level 2x2 box pyramid of that tile
+//            (reference: src/metrics/ssimulacra2/shaders/prepare.comp).
+//   blur     one CTA per (pair, level, kept channel, output tile): the five
+//            13-tap blurs, the SSIM' and edge maps and the six norm partials
+//            (reference: shaders/scale.comp).
+//   finalize one CTA per (pair, level, kept channel) segment: the FP64 sum of
+//            the tile partials; the last segment of a pair to finish turns
+//            the 18 x levels sums into the 108 norms and the score
+//            (reference: shaders/reduce.comp, vulkan.cc:545-583 ReadResult,
+//            score.cc:118-163 Score).
+//
+// Pyramid planes are FP32, row pitch a multiple of 32 floats (128 bytes), so
+// every row starts on a 128-byte boundary and float4 accesses are aligned.
+#pragma once
+
+#include <cstdint>
+
+namespace vqm_b200 {
+
+constexpr int kMaxLevels = 6;
+constexpr int kChannels = 3;
+constexpr int kTaps = 13;
+constexpr int kRadius = 6;
+constexpr int kNormsPerChannel = 6;
+constexpr int kSumsPerLevel = 18;
+// Per pair result block: 108 norms, the score, the scale count, a status.
+constexpr int kResultDoubles = 112;
+constexpr int kResultScore = 108;
+constexpr int kResultScales = 109;
+constexpr int kResultStatus = 110;
+
+// One input image as the decode reads it: the per-image constants of VQM's
+// SourceDesc (src/vulkan/vulkan_support.h:104-120) with device pointers and
+// byte strides in place of arena word offsets, so caller-owned padded device
+// buffers are read in place.
+struct DevSource {
+    const uint8_t* plane[4];   // device address of each plane's first row
+    uint32_t row_bytes[4];     // row stride of each plane, bytes
+    uint32_t plane_w[4];       // samples per row of each plane
+    uint32_t plane_h[4];       // rows of each plane
+    uint32_t width, height;    // the image (plane 0) size
+    uint8_t type;              // 0 Byte, 1 Word, 2 Half, 3 Float
+    uint8_t family;            // 0 Grey, 1 Rgb, 2 Yuv
+    uint8_t alpha;             // 0 None, 1 Straight, 2 Premultiplied
+    uint8_t sub_w, sub_h;      // log2 chroma subsampling
+    uint8_t transfer;          // transfer id 0..11 (input.cc:664-698)
+    uint8_t mode;              // 0 matrix, 1 constant luminance, 2 ICtCp
+    uint8_t filter;            // chroma filter 0 bilinear, 1 bicubic, 2 lanczos
+    uint8_t identity1, identity2;
+    uint8_t chroma_variant;    // subsampled chroma planes present
+    uint8_t lut;               // 1: 8-bit RGB, no alpha: decode by table
+    float scale[3], offset[3]; // luma, chroma, alpha
+    float m1[9], m2[9];        // encoded->RGB (or ICtCp->LMS), primaries->709
+    float kr, kg, kb, to_linear;
+    float shift_x, shift_y;
+    float cl[4];               // constant-luminance corner values
+    float background;          // alpha blend target
+    float srgb_lut[256];       // transfer(raw * scale + offset) per byte code
+};
+
+// One pair of a batch.
+struct DevPair {
+    DevSource src[2];
+    uint32_t levels;
+    uint32_t w[kMaxLevels], h[kMaxLevels], pitch[kMaxLevels];
+    uint32_t mask[kMaxLevels];          // kept channels per level, bit c
+    // Float offset, from `pyramid`, of plane [level][channel] of image 0;
+    // image 1's plane follows at + image_stride. Pruned planes are absent.
+    uint64_t plane_off[kMaxLevels][kChannels];
+    uint64_t image_stride;
+    float* pyramid;
+    uint32_t prep_tiles_x, prep_tiles_y;  // 32x32 base tiles per image
+    uint32_t seg_first, seg_count;        // this pair's blur segments
+    double* result;                       // kResultDoubles per pair
+};
+
+// One (pair, level, channel) of the blur stage.
+struct DevSegment {
+    uint32_t pair;
+    uint32_t level;
+    uint32_t channel;
+    uint32_t tiles_x;
+    uint32_t tiles;
+    uint32_t partial_first;  // index of this segment's first tile partial
+};
+
+struct DevBatch {
+    uint32_t pairs;
+    uint32_t segments;
+    uint32_t prep_blocks;    // sum over pairs of 2 * prep tiles
+    uint32_t blur_blocks;    // sum over segments of tiles
+    const DevPair* pair;
+    const DevSegment* seg;
+    const uint32_t* prep_start;  // pairs + 1 prefix offsets
+    const uint32_t* blur_start;  // segments + 1 prefix offsets
+    double* partials;            // 6 doubles per blur tile
+    double* seg_sums;            // 6 doubles per segment
+    uint32_t* pair_done;         // per pair: segments finalized so far
+    uint32_t* status;            // nonzero: a kernel found bad input
+};
+
+}  // namespace vqm_b200

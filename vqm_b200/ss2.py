@@ -1,0 +1,624 @@
+"""SSIMULACRA 2.1 on B200: Python mirror of VQM's metric API over the C ABI.
+
+The classes follow the reference's C++ interface (include/ssimulacra2.h,
+include/vqm_pool.h) name for name: ``Ssimulacra2Pipeline`` with
+``compute`` / ``submit`` / ``finish`` / ``upload`` / ``release`` /
+``allocate_image`` / ``map_image`` / ``get_memory_usage``,
+``Ssimulacra2Result.score()``, and ``Ssimulacra2Pool.compute_many`` /
+``score_many``. The reference's exception types map to ``InvalidArgument``
+(std::invalid_argument, a ValueError), ``LogicError`` (std::logic_error),
+``CudaError`` (std::runtime_error) and ``OverflowError``.
+
+Every call goes through libvqm_ss2.so (include/vqm_cu_ss2.h). There is no
+CPU fallback: without the compiled extension, importing this module fails.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import Iterable, Sequence
+
+import numpy as np
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libvqm_ss2.so")
+
+if not os.path.exists(_LIB_PATH):
+    raise ImportError(
+        f"vqm_b200: the CUDA extension {_LIB_PATH} is not built; run "
+        "`python -m vqm_b200.build` (needs nvcc). There is no CPU fallback.")
+
+_lib = ctypes.CDLL(_LIB_PATH)
+
+# ---------------------------------------------------------------------------
+# Enums (include/vqm_image.h:243-316, zimg numeric values)
+# ---------------------------------------------------------------------------
+
+
+class PixelType:
+    Byte, Word, Half, Float = 0, 1, 2, 3
+
+
+class PixelRange:
+    Limited, Full = 0, 1
+
+
+class ColorFamily:
+    Grey, Rgb, Yuv = 0, 1, 2
+
+
+class AlphaType:
+    None_, Straight, Premultiplied = 0, 1, 2
+
+
+class ChromaLocation:
+    Left, Center, TopLeft, Top, BottomLeft, Bottom = 0, 1, 2, 3, 4, 5
+
+
+class MatrixCoefficients:
+    Rgb, Bt709, Unspecified = 0, 1, 2
+    Fcc, Bt470Bg, St170M, St240M, YCgCo = 4, 5, 6, 7, 8
+    Bt2020Ncl, Bt2020Cl, St2085YDzDx = 9, 10, 11
+    ChromaticityDerivedNcl, ChromaticityDerivedCl, Bt2100ICtCp = 12, 13, 14
+    St2128IptC2, YCgCoRe, YCgCoRo = 15, 16, 17
+
+
+class TransferCharacteristics:
+    Bt709, Unspecified, Bt470M, Bt470Bg, Bt601, St240M, Linear = 1, 2, 4, 5, 6, 7, 8
+    Log100, Log316, Iec61966_2_4, Bt1361, Srgb = 9, 10, 11, 12, 13
+    Bt2020_10, Bt2020_12, St2084, St428, AribB67 = 14, 15, 16, 17, 18
+
+
+class ColorPrimaries:
+    Bt709, Unspecified, Bt470M, Bt470Bg, St170M, St240M, Film = 1, 2, 4, 5, 6, 7, 8
+    Bt2020, St428, St431_2, St432_1, Ebu3213E = 9, 10, 11, 12, 22
+
+
+class ChromaFilter:
+    Bilinear, Bicubic, Lanczos = 0, 1, 2
+
+
+# ---------------------------------------------------------------------------
+# C structs (include/vqm_cu_ss2.h)
+# ---------------------------------------------------------------------------
+
+
+class ImageFormat(ctypes.Structure):
+    """vqm::ImageFormat; the defaults are the reference's (8-bit needs type)."""
+
+    _fields_ = [(n, ctypes.c_uint8) for n in (
+        "type", "family", "alpha", "range", "matrix", "transfer", "primaries",
+        "chroma_location", "subsample_w", "subsample_h", "depth", "reserved")]
+
+    def __init__(self, type=PixelType.Float, family=ColorFamily.Rgb,
+                 alpha=AlphaType.None_, range=PixelRange.Full,
+                 matrix=MatrixCoefficients.Rgb,
+                 transfer=TransferCharacteristics.Srgb,
+                 primaries=ColorPrimaries.Bt709,
+                 chroma_location=ChromaLocation.Left, subsample_w=0,
+                 subsample_h=0, depth=0):
+        super().__init__(type, family, alpha, range, matrix, transfer,
+                         primaries, chroma_location, subsample_w, subsample_h,
+                         depth, 0)
+
+    def copy(self, **changes) -> "ImageFormat":
+        values = {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
+        values.update(changes)
+        return ImageFormat(**values)
+
+
+def srgb8_format() -> ImageFormat:
+    """The format the reference's CLI decoders pin for 8-bit sRGB input."""
+    return ImageFormat(type=PixelType.Byte)
+
+
+def yuv420_10bit_bt709_format() -> ImageFormat:
+    """10-bit 4:2:0 BT.709 limited range, Word samples, left chroma siting."""
+    return ImageFormat(type=PixelType.Word, family=ColorFamily.Yuv,
+                       range=PixelRange.Limited, matrix=MatrixCoefficients.Bt709,
+                       transfer=TransferCharacteristics.Bt709,
+                       primaries=ColorPrimaries.Bt709, subsample_w=1,
+                       subsample_h=1, depth=10)
+
+
+class _CImage(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_uint32),
+        ("height", ctypes.c_uint32),
+        ("format", ImageFormat),
+        ("memory", ctypes.c_int32),
+        ("planes", ctypes.c_void_p * 4),
+        ("strides", ctypes.c_size_t * 4),
+    ]
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_uint32),
+        ("height", ctypes.c_uint32),
+        ("gpu_resident_images", ctypes.c_uint32),
+        ("half_planes", ctypes.c_uint32),
+        ("chroma_filter", ctypes.c_uint32),
+        ("streaming_inputs", ctypes.c_uint32),
+        ("input_bytes", ctypes.c_uint64),
+        ("device", ctypes.c_int32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
+class _BatchConfig(ctypes.Structure):
+    _fields_ = [
+        ("max_pixels", ctypes.c_uint64),
+        ("max_pairs", ctypes.c_uint32),
+        ("chroma_filter", ctypes.c_uint32),
+        ("device", ctypes.c_int32),
+        ("tile_w", ctypes.c_uint32),
+        ("tile_h", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
+class MemoryUsage(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "pyramid_bytes", "resident_bytes", "input_bytes", "scratch_bytes",
+        "total_bytes")]
+
+
+_P = ctypes.c_void_p
+_U64P = ctypes.POINTER(ctypes.c_uint64)
+_SIGS = {
+    "vqm_cu_last_error": ([], ctypes.c_char_p),
+    "vqm_cu_version": ([], ctypes.c_uint32),
+    "vqm_cu_required_bytes": ([_P, ctypes.c_uint32, ctypes.c_uint32, _P], ctypes.c_int),
+    "vqm_cu_validate_format": ([_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p], ctypes.c_int),
+    "vqm_cu_ss2_plan_scales": ([ctypes.c_uint32, ctypes.c_uint32, _P, _P], ctypes.c_int),
+    "vqm_cu_ss2_score": ([_P, ctypes.c_uint32, _P], ctypes.c_int),
+    "vqm_cu_ss2_source_constants": ([_P, ctypes.c_uint32, _P], ctypes.c_int),
+    "vqm_cu_ss2_create": ([_P, _P], ctypes.c_int),
+    "vqm_cu_ss2_destroy": ([_P], ctypes.c_int),
+    "vqm_cu_ss2_set_stream": ([_P, _P], ctypes.c_int),
+    "vqm_cu_ss2_get_stream": ([_P, _P], ctypes.c_int),
+    "vqm_cu_ss2_set_graphs": ([_P, ctypes.c_int], ctypes.c_int),
+    "vqm_cu_ss2_submit": ([_P, _P, _P, ctypes.c_float, _P], ctypes.c_int),
+    "vqm_cu_ss2_submit_resident": ([_P, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float, _P], ctypes.c_int),
+    "vqm_cu_ss2_submit_resident_image": ([_P, ctypes.c_uint64, _P, ctypes.c_float, _P], ctypes.c_int),
+    "vqm_cu_ss2_submit_buffers": ([_P, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float, _P], ctypes.c_int),
+    "vqm_cu_ss2_submit_sync": ([_P, _P, _P, _P, ctypes.c_uint32, _P, ctypes.c_uint32, ctypes.c_float, _P], ctypes.c_int),
+    "vqm_cu_ss2_finish": ([_P, ctypes.c_uint64, _P, _P], ctypes.c_int),
+    "vqm_cu_ss2_compute": ([_P, _P, _P, ctypes.c_float, _P, _P, _P], ctypes.c_int),
+    "vqm_cu_ss2_upload": ([_P, _P, _P], ctypes.c_int),
+    "vqm_cu_ss2_release": ([_P, ctypes.c_uint64], ctypes.c_int),
+    "vqm_cu_ss2_allocate_image": ([_P, _P, _P, _P], ctypes.c_int),
+    "vqm_cu_ss2_map_image": ([_P, ctypes.c_uint64, _P], ctypes.c_int),
+    "vqm_cu_ss2_release_image": ([_P, ctypes.c_uint64], ctypes.c_int),
+    "vqm_cu_ss2_memory_usage": ([_P, _P], ctypes.c_int),
+    "vqm_cu_ss2_batch_create": ([_P, _P], ctypes.c_int),
+    "vqm_cu_ss2_batch_destroy": ([_P], ctypes.c_int),
+    "vqm_cu_ss2_batch_set_stream": ([_P, _P], ctypes.c_int),
+    "vqm_cu_ss2_batch_submit": ([_P, ctypes.c_uint32, _P, _P, ctypes.c_float, _P], ctypes.c_int),
+    "vqm_cu_ss2_batch_finish": ([_P, ctypes.c_uint64, _P, _P, _P], ctypes.c_int),
+    "vqm_cu_ss2_batch_set_timing": ([_P, ctypes.c_int], ctypes.c_int),
+    "vqm_cu_ss2_batch_stage_ms": ([_P, _P], ctypes.c_int),
+    "vqm_cu_ss2_batch_compute": ([_P, ctypes.c_uint32, _P, _P, ctypes.c_float, _P, _P, _P], ctypes.c_int),
+}
+for _name, (_args, _res) in _SIGS.items():
+    _fn = getattr(_lib, _name)
+    _fn.argtypes = _args
+    _fn.restype = _res
+
+EXPORTED_SYMBOLS = tuple(_SIGS)
+
+
+def library_path() -> str:
+    return _LIB_PATH
+
+
+# ---------------------------------------------------------------------------
+# Errors
+# ---------------------------------------------------------------------------
+
+
+class InvalidArgument(ValueError):
+    """std::invalid_argument."""
+
+
+class LogicError(RuntimeError):
+    """std::logic_error."""
+
+
+class CudaError(RuntimeError):
+    """std::runtime_error: no device, allocation or CUDA failure."""
+
+
+_ERRORS = {1: InvalidArgument, 2: LogicError, 3: CudaError, 4: OverflowError}
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        msg = _lib.vqm_cu_last_error().decode()
+        raise _ERRORS.get(status, CudaError)(msg)
+
+
+# ---------------------------------------------------------------------------
+# Images
+# ---------------------------------------------------------------------------
+
+
+def required_bytes(fmt: ImageFormat, width: int, height: int) -> int:
+    """RequiredBytes (include/vqm_image.h:360-363)."""
+    out = ctypes.c_size_t()
+    _check(_lib.vqm_cu_required_bytes(ctypes.byref(fmt), width, height, ctypes.byref(out)))
+    return out.value
+
+
+def validate_format(fmt: ImageFormat, width: int, height: int, name: str = "image") -> None:
+    _check(_lib.vqm_cu_validate_format(ctypes.byref(fmt), width, height, name.encode()))
+
+
+def plane_layout(fmt: ImageFormat, width: int, height: int):
+    """[(offset, width, height, sample_bytes) or None] for planes 0..3
+    (src/input.cc:114-145)."""
+    sb = {0: 1, 1: 2, 2: 2, 3: 4}[fmt.type]
+    cw, ch = width >> fmt.subsample_w, height >> fmt.subsample_h
+    out, cursor = [], 0
+    for p in range(4):
+        chroma = p in (1, 2)
+        present = p == 0 or (chroma and fmt.family != 0) or (p == 3 and fmt.alpha != 0)
+        if not present:
+            out.append(None)
+            continue
+        w, h = (cw, ch) if chroma else (width, height)
+        out.append((cursor, w, h, sb))
+        cursor = (cursor + w * h * sb + 3) // 4 * 4
+    return out
+
+
+@dataclass
+class Image:
+    """vqm::Image: packed planes (Y/R, U/G, V/B, alpha) in one byte buffer."""
+
+    width: int
+    height: int
+    format: ImageFormat
+    data: np.ndarray
+
+    @property
+    def size(self):
+        return (self.width, self.height)
+
+    def _c(self) -> _CImage:
+        self.data = np.ascontiguousarray(self.data, dtype=np.uint8)
+        expected = required_bytes(self.format, self.width, self.height)
+        if self.data.nbytes != expected:
+            raise InvalidArgument(
+                f"image: data size does not match the image format (expected {expected} bytes)")
+        c = _CImage(self.width, self.height, self.format, 0)
+        base = self.data.ctypes.data
+        for p, geo in enumerate(plane_layout(self.format, self.width, self.height)):
+            if geo is not None:
+                c.planes[p] = base + geo[0]
+        return c
+
+
+@dataclass
+class DeviceImage:
+    """A caller-owned device buffer (the CUDA counterpart of VulkanBufferView):
+    plane device addresses and byte strides (0 = packed rows)."""
+
+    width: int
+    height: int
+    format: ImageFormat
+    planes: Sequence[int]
+    strides: Sequence[int] = (0, 0, 0, 0)
+    owner: object = None  # keeps the memory alive (e.g. a torch tensor)
+
+    @staticmethod
+    def packed(width: int, height: int, fmt: ImageFormat, base_ptr: int, owner=None):
+        planes = [0, 0, 0, 0]
+        for p, geo in enumerate(plane_layout(fmt, width, height)):
+            if geo is not None:
+                planes[p] = base_ptr + geo[0]
+        return DeviceImage(width, height, fmt, planes, (0, 0, 0, 0), owner)
+
+    def _c(self) -> _CImage:
+        c = _CImage(self.width, self.height, self.format, 1)
+        for p in range(4):
+            c.planes[p] = int(self.planes[p]) if self.planes[p] else None
+            c.strides[p] = int(self.strides[p])
+        return c
+
+
+@dataclass
+class HostImage:
+    """vqm::ImageView: separately allocated, optionally padded host planes."""
+
+    width: int
+    height: int
+    format: ImageFormat
+    planes: Sequence[np.ndarray | None]
+    strides: Sequence[int] = (0, 0, 0, 0)
+
+    def _c(self) -> _CImage:
+        c = _CImage(self.width, self.height, self.format, 0)
+        for p in range(4):
+            arr = self.planes[p] if p < len(self.planes) else None
+            if arr is not None:
+                c.planes[p] = arr.ctypes.data
+                c.strides[p] = int(self.strides[p])
+        return c
+
+
+# ---------------------------------------------------------------------------
+# Results
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class Ssimulacra2Scale:
+    """18 norms of one scale (include/ssimulacra2.h:18-25)."""
+
+    avg_ssim: np.ndarray      # [channel * 2 + norm]
+    avg_edgediff: np.ndarray  # [channel * 4 + n]: ringing 0, 1; blurring 2, 3
+
+
+@dataclass
+class Ssimulacra2Result:
+    norms: np.ndarray  # [scales, 18]
+    device_score: float | None = None
+    scales: list = field(init=False)
+
+    def __post_init__(self):
+        self.scales = [Ssimulacra2Scale(r[:6].copy(), r[6:].copy()) for r in self.norms]
+
+    def score(self) -> float:
+        """Ssimulacra2Result::Score (score.cc:118-163), FP64 on the host."""
+        return score(self.norms)
+
+
+def score(norms: np.ndarray) -> float:
+    norms = np.asarray(norms, dtype=np.float64)
+    scales = norms.shape[0] if norms.ndim == 2 else norms.size // 18
+    buf = np.zeros(max(108, norms.size), dtype=np.float64)
+    buf[: norms.size] = norms.reshape(-1)
+    out = ctypes.c_double()
+    _check(_lib.vqm_cu_ss2_score(buf.ctypes.data, scales, ctypes.byref(out)))
+    return out.value
+
+
+def source_constants(fmt: ImageFormat, chroma_filter: int = 0) -> np.ndarray:
+    """The 44 SourceDesc words this library derives for `fmt`."""
+    words = np.zeros(44, dtype=np.uint32)
+    _check(_lib.vqm_cu_ss2_source_constants(ctypes.byref(fmt), chroma_filter, words.ctypes.data))
+    return words
+
+
+def plan_scales(width: int, height: int):
+    sizes = (ctypes.c_uint32 * 12)()
+    n = ctypes.c_uint32()
+    _check(_lib.vqm_cu_ss2_plan_scales(width, height, sizes, ctypes.byref(n)))
+    return [(sizes[2 * i], sizes[2 * i + 1]) for i in range(n.value)]
+
+
+# ---------------------------------------------------------------------------
+# Pipeline
+# ---------------------------------------------------------------------------
+
+
+def _handle_of(h) -> int:
+    return int(getattr(h, "slot", h))
+
+
+@dataclass(frozen=True)
+class UploadedImage:
+    slot: int
+    size: tuple
+
+
+@dataclass(frozen=True)
+class ImageBuffer:
+    slot: int
+    size: tuple
+    bytes: int
+
+
+class Ssimulacra2Pipeline:
+    """Ssimulacra2Pipeline (include/ssimulacra2.h:83-215) on a CUDA device."""
+
+    def __init__(self, width: int, height: int, gpu_resident_images: int = 2,
+                 half_planes: bool = False, chroma_filter: int = 0,
+                 input_bytes: int = 0, streaming_inputs: bool = True,
+                 device: int = -1):
+        cfg = _Config(width, height, gpu_resident_images, int(half_planes),
+                      chroma_filter, int(streaming_inputs), input_bytes, device, 0)
+        self._p = ctypes.c_void_p()
+        _check(_lib.vqm_cu_ss2_create(ctypes.byref(cfg), ctypes.byref(self._p)))
+        self.size = (width, height)
+
+    def close(self):
+        if getattr(self, "_p", None) and self._p.value:
+            _check(_lib.vqm_cu_ss2_destroy(self._p))
+            self._p = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> int:
+        return self._p.value
+
+    def set_stream(self, stream: int | None):
+        _check(_lib.vqm_cu_ss2_set_stream(self._p, stream or None))
+
+    def set_graphs(self, enabled: bool):
+        _check(_lib.vqm_cu_ss2_set_graphs(self._p, int(enabled)))
+
+    def submit(self, original, distorted, background: float = 0.5) -> int:
+        tok = ctypes.c_uint64()
+        if isinstance(original, UploadedImage) and isinstance(distorted, UploadedImage):
+            _check(_lib.vqm_cu_ss2_submit_resident(self._p, original.slot, distorted.slot,
+                                                   background, ctypes.byref(tok)))
+        elif isinstance(original, UploadedImage):
+            d = distorted._c()
+            _check(_lib.vqm_cu_ss2_submit_resident_image(self._p, original.slot, ctypes.byref(d),
+                                                         background, ctypes.byref(tok)))
+        elif isinstance(original, ImageBuffer) and isinstance(distorted, ImageBuffer):
+            _check(_lib.vqm_cu_ss2_submit_buffers(self._p, original.slot, distorted.slot,
+                                                  background, ctypes.byref(tok)))
+        else:
+            o, d = original._c(), distorted._c()
+            _check(_lib.vqm_cu_ss2_submit(self._p, ctypes.byref(o), ctypes.byref(d),
+                                          background, ctypes.byref(tok)))
+        return tok.value
+
+    def finish(self, token: int) -> Ssimulacra2Result:
+        norms = np.zeros(108, dtype=np.float64)
+        n = ctypes.c_uint32()
+        _check(_lib.vqm_cu_ss2_finish(self._p, token, norms.ctypes.data, ctypes.byref(n)))
+        return Ssimulacra2Result(norms[: 18 * n.value].reshape(n.value, 18).copy())
+
+    def compute(self, original, distorted, background: float = 0.5) -> Ssimulacra2Result:
+        return self.finish(self.submit(original, distorted, background))
+
+    def upload(self, image) -> UploadedImage:
+        c = image._c()
+        h = ctypes.c_uint64()
+        _check(_lib.vqm_cu_ss2_upload(self._p, ctypes.byref(c), ctypes.byref(h)))
+        return UploadedImage(h.value, (image.width, image.height))
+
+    def release(self, handle) -> None:
+        if isinstance(handle, ImageBuffer):
+            _check(_lib.vqm_cu_ss2_release_image(self._p, handle.slot))
+        else:
+            _check(_lib.vqm_cu_ss2_release(self._p, _handle_of(handle)))
+
+    def allocate_image(self, fmt: ImageFormat) -> ImageBuffer:
+        h = ctypes.c_uint64()
+        b = ctypes.c_size_t()
+        _check(_lib.vqm_cu_ss2_allocate_image(self._p, ctypes.byref(fmt), ctypes.byref(h),
+                                              ctypes.byref(b)))
+        return ImageBuffer(h.value, self.size, b.value)
+
+    def map_image(self, buffer: ImageBuffer) -> int:
+        """Device address of the buffer (fill it with cudaMemcpy or a kernel)."""
+        ptr = ctypes.c_void_p()
+        _check(_lib.vqm_cu_ss2_map_image(self._p, buffer.slot, ctypes.byref(ptr)))
+        return ptr.value
+
+    def get_memory_usage(self) -> MemoryUsage:
+        u = MemoryUsage()
+        _check(_lib.vqm_cu_ss2_memory_usage(self._p, ctypes.byref(u)))
+        return u
+
+
+# ---------------------------------------------------------------------------
+# Batched scoring
+# ---------------------------------------------------------------------------
+
+
+class Ssimulacra2Batch:
+    """Many pairs of any sizes, scored by one launch per stage."""
+
+    def __init__(self, max_pairs: int = 0, max_pixels: int = 0, chroma_filter: int = 0,
+                 device: int = -1, tile: tuple[int, int] | None = None):
+        tw, th = tile if tile else (0, 0)
+        cfg = _BatchConfig(max_pixels, max_pairs, chroma_filter, device, tw, th, 0)
+        self._b = ctypes.c_void_p()
+        _check(_lib.vqm_cu_ss2_batch_create(ctypes.byref(cfg), ctypes.byref(self._b)))
+
+    def close(self):
+        if getattr(self, "_b", None) and self._b.value:
+            _check(_lib.vqm_cu_ss2_batch_destroy(self._b))
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> int:
+        return self._b.value
+
+    def set_stream(self, stream: int | None):
+        _check(_lib.vqm_cu_ss2_batch_set_stream(self._b, stream or None))
+
+    def set_timing(self, enabled: bool):
+        """Record CUDA events around each stage of every batch."""
+        _check(_lib.vqm_cu_ss2_batch_set_timing(self._b, int(enabled)))
+
+    def stage_ms(self):
+        """(prepare, blur, finalize) device milliseconds of the last batch."""
+        ms = (ctypes.c_float * 3)()
+        _check(_lib.vqm_cu_ss2_batch_stage_ms(self._b, ms))
+        return tuple(ms)
+
+    @staticmethod
+    def _arrays(pairs):
+        n = len(pairs)
+        origs = (_CImage * n)(*[p[0]._c() for p in pairs])
+        dists = (_CImage * n)(*[p[1]._c() for p in pairs])
+        return n, origs, dists
+
+    def submit(self, pairs, background: float = 0.5) -> int:
+        n, origs, dists = self._arrays(pairs)
+        self._pending = n
+        tok = ctypes.c_uint64()
+        _check(_lib.vqm_cu_ss2_batch_submit(self._b, n, origs, dists, background,
+                                            ctypes.byref(tok)))
+        return tok.value
+
+    def finish(self, token: int):
+        n = self._pending
+        norms = np.zeros((n, 108), dtype=np.float64)
+        scales = np.zeros(n, dtype=np.uint32)
+        scores = np.zeros(n, dtype=np.float64)
+        _check(_lib.vqm_cu_ss2_batch_finish(self._b, token, norms.ctypes.data,
+                                            scales.ctypes.data, scores.ctypes.data))
+        return [Ssimulacra2Result(norms[i, : 18 * scales[i]].reshape(scales[i], 18).copy(),
+                                  float(scores[i])) for i in range(n)]
+
+    def compute_many(self, pairs, background: float = 0.5):
+        return self.finish(self.submit(pairs, background))
+
+    def score_many(self, pairs, background: float = 0.5):
+        return [r.score() for r in self.compute_many(pairs, background)]
+
+
+class Ssimulacra2Pool:
+    """Ssimulacra2Pool (include/vqm_pool.h:51-87): results in input order.
+
+    The reference round-robins pairs over ``workers`` one-in-flight
+    pipelines; here one batch scorer takes the pairs ``chunk`` at a time,
+    each chunk one launch per stage."""
+
+    def __init__(self, workers: int = 1, chunk: int = 64, chroma_filter: int = 0,
+                 device: int = -1):
+        if workers == 0:
+            raise InvalidArgument("pool needs at least one worker")
+        self._workers = workers
+        self._chunk = max(1, chunk)
+        self._batch = Ssimulacra2Batch(chroma_filter=chroma_filter, device=device)
+
+    def workers(self) -> int:
+        return self._workers
+
+    def compute_many(self, pairs: Iterable, background: float = 0.5):
+        pairs = list(pairs)
+        out = []
+        for i in range(0, len(pairs), self._chunk):
+            out.extend(self._batch.compute_many(pairs[i:i + self._chunk], background))
+        return out
+
+    def score_many(self, pairs: Iterable, background: float = 0.5):
+        return [r.score() for r in self.compute_many(pairs, background)]

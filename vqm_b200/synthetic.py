@@ -1,0 +1,219 @@
+"""Seeded synthetic image pairs with the shapes, formats and distortions of
+the benchmark workloads. No corpus ships with the reference for this path
+(its bench pairs are ffmpeg testsrc2 renders that are not in the repository),
+so these stand in for it.
+
+Textures: per channel, a sum of 8 plane waves (random orientation and phase,
+period uniform in [4, 64] px) plus a linear gradient, min-max scaled to
+0..255. Distortions: Gaussian noise, Gaussian blur, or 8x8 block
+quantisation. The block quantisation keeps every pixel's offset from its
+8x8 block mean and rounds the block mean itself to a multiple of the step
+(a DC-only quantiser), so it produces blocking without flattening texture.
+
+10-bit 4:2:0 inputs are BT.709 Y'CbCr in limited range (Y 64..940,
+C 64..960): the RGB texture's normalised code values go through the BT.709
+matrix, chroma is the mean of each 2x2 block. 4:2:0 needs even sizes (the
+reference rejects odd ones, src/input.cc:176-179), so odd sizes drawn for
+those pairs are rounded up to even; odd geometries are exercised with 8-bit
+RGB pairs instead.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+try:  # scipy is in the image; only the blur distortion needs it
+    from scipy.ndimage import gaussian_filter
+except Exception:  # pragma: no cover
+    gaussian_filter = None
+
+from . import ss2
+
+
+def _waves(w: int, h: int, rng: np.random.Generator) -> np.ndarray:
+    x = np.arange(w, dtype=np.float64)
+    y = np.arange(h, dtype=np.float64)
+    out = np.zeros((h, w), dtype=np.float32)
+    for _ in range(8):
+        theta = rng.uniform(0, math.pi)
+        period = rng.uniform(4, 64)
+        phase = rng.uniform(0, 2 * math.pi)
+        amp = rng.uniform(0.3, 1.0)
+        k = 2 * math.pi / period
+        a = k * math.cos(theta) * x            # along x
+        b = k * math.sin(theta) * y + phase    # along y
+        # sin(a + b) = sin a cos b + cos a sin b, as two outer products.
+        sa, ca = (amp * np.sin(a)).astype(np.float32), (amp * np.cos(a)).astype(np.float32)
+        out += np.outer(np.cos(b).astype(np.float32), sa)
+        out += np.outer(np.sin(b).astype(np.float32), ca)
+    gx, gy = rng.uniform(-1, 1, size=2)
+    g = rng.uniform(1, 4)
+    out += (g * gx * x / max(w - 1, 1)).astype(np.float32)[None, :]
+    out += (g * gy * y / max(h - 1, 1)).astype(np.float32)[:, None]
+    return out
+
+
+def texture(w: int, h: int, rng: np.random.Generator, offset=(0, 0)) -> np.ndarray:
+    """[3, h, w] float64 in 0..255. `offset` shifts the texture (video)."""
+    ox, oy = offset
+    planes = []
+    for _ in range(3):
+        big = _waves(w + ox, h + oy, rng)[oy:, ox:]
+        lo, hi = float(big.min()), float(big.max())
+        planes.append((big - lo) * np.float32(255.0 / max(hi - lo, 1e-9)))
+    return np.stack(planes)
+
+
+def add_rectangles(img: np.ndarray, rng: np.random.Generator, count: int = 32) -> np.ndarray:
+    _, h, w = img.shape
+    img = img.copy()
+    for _ in range(count):
+        rw = int(rng.integers(max(2, w // 40), max(3, w // 6)))
+        rh = int(rng.integers(max(2, h // 40), max(3, h // 6)))
+        x0 = int(rng.integers(0, max(1, w - rw)))
+        y0 = int(rng.integers(0, max(1, h - rh)))
+        img[:, y0:y0 + rh, x0:x0 + rw] = rng.uniform(0, 255, size=3)[:, None, None]
+    return img
+
+
+def block_quantise(img: np.ndarray, step: float, block: int = 8) -> np.ndarray:
+    """Round each 8x8 block mean to a multiple of `step`, keep the residual."""
+    c, h, w = img.shape
+    hp, wp = (h + block - 1) // block * block, (w + block - 1) // block * block
+    pad = np.pad(img, ((0, 0), (0, hp - h), (0, wp - w)), mode="edge")
+    blocks = pad.reshape(c, hp // block, block, wp // block, block)
+    mean = blocks.mean(axis=(2, 4), keepdims=True)
+    q = blocks - mean + step * np.round(mean / step)
+    return q.reshape(c, hp, wp)[:, :h, :w]
+
+
+def blur(img: np.ndarray, sigma: float) -> np.ndarray:
+    if gaussian_filter is None:
+        raise RuntimeError("scipy is needed for the blur distortion")
+    return np.stack([gaussian_filter(p, sigma, mode="nearest") for p in img])
+
+
+def to_u8(img: np.ndarray) -> np.ndarray:
+    return np.clip(np.rint(img), 0, 255).astype(np.uint8)
+
+
+def rgb8_image(planes_u8: np.ndarray) -> ss2.Image:
+    _, h, w = planes_u8.shape
+    fmt = ss2.srgb8_format()
+    data = np.zeros(ss2.required_bytes(fmt, w, h), dtype=np.uint8)
+    layout = ss2.plane_layout(fmt, w, h)
+    for p in range(3):
+        off = layout[p][0]
+        data[off:off + w * h] = planes_u8[p].reshape(-1)
+    return ss2.Image(w, h, fmt, data)
+
+
+def yuv420_10bit_image(rgb: np.ndarray) -> ss2.Image:
+    """RGB code values (0..255 floats) -> BT.709 limited 10-bit 4:2:0."""
+    _, h, w = rgb.shape
+    if w % 2 or h % 2:
+        raise ValueError("4:2:0 needs even dimensions")
+    r, g, b = (np.clip(rgb, 0, 255) / 255.0)
+    kr, kb = 0.2126, 0.0722
+    kg = 1 - kr - kb
+    y = kr * r + kg * g + kb * b
+    cb = (b - y) / (2 - 2 * kb)
+    cr = (r - y) / (2 - 2 * kr)
+
+    def sub(p):
+        return p.reshape(h // 2, 2, w // 2, 2).mean(axis=(1, 3))
+
+    yc = np.clip(np.rint(64 + 876 * y), 64, 940)
+    cbc = np.clip(np.rint(512 + 896 * sub(cb)), 64, 960)
+    crc = np.clip(np.rint(512 + 896 * sub(cr)), 64, 960)
+    fmt = ss2.yuv420_10bit_bt709_format()
+    data = np.zeros(ss2.required_bytes(fmt, w, h), dtype=np.uint8)
+    layout = ss2.plane_layout(fmt, w, h)
+    for p, arr in enumerate((yc, cbc, crc)):
+        off, pw, ph, _ = layout[p]
+        data[off:off + pw * ph * 2] = arr.astype("<u2").reshape(-1).view(np.uint8)
+    return ss2.Image(w, h, fmt, data)
+
+
+# --- workloads --------------------------------------------------------------
+
+
+def pair_plain_256(seed: int = 0):
+    """One 256x256 8-bit sRGB pair: noise sigma 4, then 8x8 quantisation
+    step 16, clipped to 8 bits."""
+    rng = np.random.default_rng(seed)
+    ref = texture(256, 256, rng)
+    dist = ref + rng.normal(0, 4, size=ref.shape)
+    dist = block_quantise(dist, 16)
+    return rgb8_image(to_u8(ref)), rgb8_image(to_u8(dist))
+
+
+def distort(ref: np.ndarray, rng: np.random.Generator) -> tuple[np.ndarray, str]:
+    kind = int(rng.integers(0, 3))
+    if kind == 0:
+        s = rng.uniform(1, 8)
+        return ref + rng.normal(0, s, size=ref.shape).astype(np.float32), f"noise{s:.2f}"
+    if kind == 1:
+        s = rng.uniform(0.5, 3)
+        return blur(ref, s), f"blur{s:.2f}"
+    s = rng.uniform(4, 32)
+    return block_quantise(ref, s), f"quant{s:.2f}"
+
+
+def rgb_pair(w: int, h: int, seed: int):
+    """8-bit sRGB pair: texture + 32 rectangles, one random distortion."""
+    rng = np.random.default_rng(seed)
+    ref = add_rectangles(texture(w, h, rng), rng)
+    dist, kind = distort(ref, rng)
+    return rgb8_image(to_u8(ref)), rgb8_image(to_u8(dist)), kind
+
+
+def yuv_pair(w: int, h: int, seed: int):
+    """10-bit 4:2:0 pair of the same content model (sizes rounded to even)."""
+    w += w % 2
+    h += h % 2
+    rng = np.random.default_rng(seed)
+    ref = add_rectangles(texture(w, h, rng), rng)
+    dist, kind = distort(ref, rng)
+    return yuv420_10bit_image(ref), yuv420_10bit_image(np.clip(dist, 0, 255)), kind
+
+
+def plain_1080p(count: int = 64, seed0: int = 1000, width: int = 1920, height: int = 1080):
+    return [rgb_pair(width, height, seed0 + i)[:2] for i in range(count)]
+
+
+def uneven_batch(count: int = 128, seed0: int = 2000, odd_rgb: int = 8):
+    """`count` 10-bit 4:2:0 pairs of sizes W in [320, 3840], H in [180, 2160]
+    (rounded to even), plus `odd_rgb` 8-bit RGB pairs keeping odd sizes."""
+    rng = np.random.default_rng(seed0)
+    pairs = []
+    for i in range(count):
+        w = int(rng.integers(320, 3841))
+        h = int(rng.integers(180, 2161))
+        pairs.append(yuv_pair(w, h, seed0 + 1 + i)[:2])
+    for i in range(odd_rgb):
+        w = int(rng.integers(320, 3841)) | 1
+        h = int(rng.integers(180, 2161)) | 1
+        pairs.append(rgb_pair(w, h, seed0 + 10_000 + i)[:2])
+    return pairs
+
+
+def video_frames(count: int = 240, width: int = 3840, height: int = 2160, seed: int = 4000):
+    """Frame pairs of a texture translating 1-3 px per frame; the distorted
+    stream is 8x8 quantised with a step drifting 8 -> 48 plus noise sigma 2
+    (8-bit units). Yields (original, distorted) 10-bit 4:2:0 images."""
+    rng = np.random.default_rng(seed)
+    total_shift = 3 * count + 4
+    base_rng = np.random.default_rng(seed + 1)
+    big = add_rectangles(texture(width + total_shift, height + total_shift, base_rng), base_rng)
+    x = y = 0
+    for f in range(count):
+        x += int(rng.integers(1, 4))
+        y += int(rng.integers(0, 2))
+        x, y = min(x, total_shift - 1), min(y, total_shift - 1)
+        ref = big[:, y:y + height, x:x + width]
+        step = 8 + (48 - 8) * f / max(count - 1, 1)
+        dist = block_quantise(ref, step) + rng.normal(0, 2, size=ref.shape)
+        yield yuv420_10bit_image(ref), yuv420_10bit_image(np.clip(dist, 0, 255))
