@@ -210,6 +210,11 @@ int vqm_cu_ss2_release_image(vqm_cu_ss2_pipeline* pipeline, uint64_t handle);
 /* GetMemoryUsage (ssimulacra2.h:204-205). */
 int vqm_cu_ss2_memory_usage(vqm_cu_ss2_pipeline* pipeline,
                             vqm_cu_memory_usage* usage);
+/* Diagnostic: copies the XYB plane (level, channel) of image 0 (original) or
+ * 1 (distorted) written by the last finished pair into out (width_l *
+ * height_l floats, row-major). INVALID_ARGUMENT for a pruned channel. */
+int vqm_cu_ss2_debug_plane(vqm_cu_ss2_pipeline* pipeline, uint32_t image,
+                           uint32_t level, uint32_t channel, float* out);
 /* CUDA-graph replay of the pair's kernels (prepare, blur, finalize): on by
  * default; 0 launches them one by one. */
 int vqm_cu_ss2_set_graphs(vqm_cu_ss2_pipeline* pipeline, int enabled);

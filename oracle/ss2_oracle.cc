@@ -20,6 +20,11 @@
 
 #include "ss2_oracle.h"
 
+// pow, cube root, exp and sin(pi x) of the FP32 path: the deterministic
+// functions the CUDA kernels evaluate too (pinned to double-precision libm by
+// tests/test_detmath.py). The FP64 path uses libm itself.
+#include "../vqm_b200/csrc/ss2_detmath.h"
+
 #include <algorithm>
 #include <array>
 #include <atomic>
@@ -645,7 +650,25 @@ float HalfToFloat(uint16_t h) {
 // Decode to linear Rec.709 (color.glsl).
 // ---------------------------------------------------------------------------
 
-template <class T> T Pow(T a, T b) { return std::pow(a, b); }
+template <class T> T Pow(T a, T b);
+template <> float Pow<float>(float a, float b) { return ss2dm::pow(a, b); }
+template <> double Pow<double>(double a, double b) { return std::pow(a, b); }
+template <class T> T Exp(T a);
+template <> float Exp<float>(float a) { return ss2dm::exp(a); }
+template <> double Exp<double>(double a) { return std::exp(a); }
+template <class T> T Cbrt(T a);
+template <> float Cbrt<float>(float a) { return ss2dm::cbrt(a); }
+template <> double Cbrt<double>(double a) { return std::cbrt(a); }
+// sin(pi v) / (pi v) with the reference's float pi in the denominator.
+template <class T> T Sinc(T v);
+template <> float Sinc<float>(float v) {
+    const float pi = 3.14159265358979323846f;
+    return v == 0.0f ? 1.0f : ss2dm::sinpi(v) / (pi * v);
+}
+template <> double Sinc<double>(double v) {
+    const double pi = 3.14159265358979323846;
+    return v == 0.0 ? 1.0 : std::sin(pi * v) / (pi * v);
+}
 
 template <class T>
 struct Decoder {
@@ -719,7 +742,7 @@ struct Decoder {
         x = std::max(x, T(0));
         return x <= T(0.5)
                    ? (x * x) * (T(1) / T(3))
-                   : (std::exp((x - T(0.55991073)) / T(0.17883277)) +
+                   : (Exp<T>((x - T(0.55991073)) / T(0.17883277)) +
                       T(0.28466892)) / T(12);
     }
     T Transfer(int id, T v) const {
@@ -802,11 +825,7 @@ struct Decoder {
                                 T(2));
             return T(0);
         }
-        const T pi = T(3.14159265358979323846);
-        auto sinc = [pi](T v) {
-            return v == T(0) ? T(1) : std::sin(pi * v) / (pi * v);
-        };
-        return x < T(3) ? sinc(x) * sinc(x / T(3)) : T(0);
+        return x < T(3) ? Sinc<T>(x) * Sinc<T>(x / T(3)) : T(0);
     }
 
     // color.glsl:288-367: bilinear chroma of the four samples of a block.
@@ -973,10 +992,11 @@ void Xyb(const T lin[3], T out[3]) {
     m0 = std::max(m0, T(0));
     m1 = std::max(m1, T(0));
     m2 = std::max(m2, T(0));
-    const T third = T(1) / T(3);
-    const T c0 = Pow<T>(m0, third) - cbias;
-    const T c1 = Pow<T>(m1, third) - cbias;
-    const T c2 = Pow<T>(m2, third) - cbias;
+    // prepare.comp:78 evaluates pow(v, 1/3); the cube root here is that value
+    // in exact arithmetic, rounded to the working type.
+    const T c0 = Cbrt<T>(m0) - cbias;
+    const T c1 = Cbrt<T>(m1) - cbias;
+    const T c2 = Cbrt<T>(m2) - cbias;
     out[0] = std::fma(T(0.5) * (c0 - c1), T(14), T(0.42));
     out[1] = std::fma(T(0.5), c0 + c1, T(0.01));
     out[2] = std::fma(T(-0.5), c0 + c1, c2) + T(0.55);
@@ -1440,6 +1460,19 @@ int ss2o_level_sums(const ss2o_image* original, const ss2o_image* distorted,
     } catch (const std::exception& e) {
         return Fail(e);
     }
+}
+
+int ss2o_detmath(int fn, const float* x, float y, float* out, size_t n) {
+    for (size_t i = 0; i < n; ++i) {
+        switch (fn) {
+            case 0: out[i] = ss2dm::cbrt(x[i]); break;
+            case 1: out[i] = ss2dm::pow(x[i], y); break;
+            case 2: out[i] = ss2dm::exp(x[i]); break;
+            case 3: out[i] = ss2dm::sinpi(x[i]); break;
+            default: g_error = "unknown function"; return SS2O_INVALID;
+        }
+    }
+    return SS2O_OK;
 }
 
 const char* ss2o_last_error(void) { return g_error.c_str(); }

@@ -96,6 +96,9 @@ int ss2o_pyramid(const ss2o_image* image, float background, int chroma_filter,
 int ss2o_level_sums(const ss2o_image* original, const ss2o_image* distorted,
                     float background, int chroma_filter, float* sums,
                     uint32_t* scales);
+/* The shared deterministic functions, for their accuracy tests: fn 0 cube
+ * root, 1 pow(x, y), 2 exp, 3 sin(pi x). */
+int ss2o_detmath(int fn, const float* x, float y, float* out, size_t n);
 const char* ss2o_last_error(void);
 
 #ifdef __cplusplus

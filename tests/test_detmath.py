@@ -1,0 +1,83 @@
+"""Accuracy of the deterministic pow / cube root / exp / sin(pi x) that the
+kernels, the host decode tables and the oracle share
+(vqm_b200/csrc/ss2_detmath.h), against double-precision libm.
+
+Each function evaluates in double and rounds once, so it must land on the
+correctly rounded float in all but a tiny fraction of cases, and never more
+than one ulp away."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import binding as ob
+
+
+def det(fn, x, y=0.0):
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty_like(x)
+    assert ob.lib().ss2o_detmath(fn, x.ctypes.data_as(ctypes.c_void_p), ctypes.c_float(y),
+                                 out.ctypes.data_as(ctypes.c_void_p), x.size) == 0
+    return out
+
+
+def ulps(a, b):
+    ai = a.view(np.int32).astype(np.int64)
+    bi = b.view(np.int32).astype(np.int64)
+    return np.abs(ai - bi)
+
+
+def check(got, exact64, max_bad_frac=1e-5):
+    want = exact64.astype(np.float32)
+    d = ulps(got, want)
+    assert d.max() <= 1, (d.max(), got[d.argmax()], exact64[d.argmax()])
+    assert (d > 0).mean() <= max_bad_frac
+
+
+def samples(lo, hi, n=2_000_000, seed=0):
+    rng = np.random.default_rng(seed)
+    x = np.exp(rng.uniform(np.log(lo), np.log(hi), n)).astype(np.float32)
+    return x
+
+
+def test_cbrt():
+    x = np.concatenate([samples(1e-38, 1e30), samples(0.0037, 1.2),
+                        np.float32([1, 8, 27, 0.125, 1e-45, 3e38])])
+    check(det(0, x), np.cbrt(x.astype(np.float64)))
+    assert det(0, np.float32([0.0, -1.0]))[0] == 0.0
+
+
+@pytest.mark.parametrize("y", [2.4, 2.2, 2.8, 2.6, 1 / 0.45, 0.2, 1 / 78.84375,
+                               1 / 0.1593017578125])
+def test_pow(y):
+    yf = np.float32(y)
+    x = samples(1e-6, 1.5)
+    check(det(1, x, yf), np.power(x.astype(np.float64), np.float64(yf)))
+    assert det(1, np.float32([0.0, 1.0]), yf).tolist() == [0.0, 1.0]
+
+
+def test_pow_base10():
+    # 10^(2 (v - 1)) and 10^(2.5 (v - 1)) of the log transfers.
+    e = np.random.default_rng(1).uniform(-5, 0, 200_000).astype(np.float32)
+    x = np.full_like(e, 10.0)
+    out = np.array([det(1, x[i:i + 1], float(e[i]))[0] for i in range(0, 2000)])
+    check(out, np.power(10.0, e[:2000].astype(np.float64)), max_bad_frac=1e-3)
+
+
+def test_exp():
+    x = np.random.default_rng(2).uniform(-20, 20, 1_000_000).astype(np.float32)
+    check(det(2, x), np.exp(x.astype(np.float64)))
+
+
+def test_sinpi():
+    x = np.random.default_rng(3).uniform(0, 3, 1_000_000).astype(np.float32)
+    x = np.concatenate([x, np.float32([0.0, 1.0, 2.0, 1e-7, 2.0000002])])
+    got = det(3, x)
+    exact = np.sin(np.pi * x.astype(np.float64))
+    # sin(pi x) has zeros at integers; compare with an absolute floor there.
+    want = exact.astype(np.float32)
+    d = ulps(got, want)
+    near_zero = np.abs(exact) < 1e-6
+    assert d[~near_zero].max() <= 1
+    assert np.abs(got[near_zero] - exact[near_zero]).max() < 1e-12

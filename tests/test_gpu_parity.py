@@ -78,6 +78,36 @@ def test_small_geometries(w, h, scales):
         check_parity(p.compute(img, d), img, d, label=f"ramp {w}x{h}")
 
 
+def _pyramid_cases():
+    return {
+        "rgb8_256": lambda: helpers.plain_256_pair(),
+        "rgb8_odd": lambda: synthetic.rgb_pair(333, 187, 5)[:2],
+        "yuv420p10": lambda: synthetic.yuv_pair(322, 182, 6)[:2],
+        "float_ramp": lambda: (helpers.ramp_image(65, 33, False), helpers.ramp_image(65, 33, False)),
+        "rgb8_alpha": lambda: (helpers.ramp_image(40, 24, True, ss2.PixelType.Byte),) * 2,
+    }
+
+
+@pytest.mark.parametrize("case", list(_pyramid_cases()))
+def test_pyramid_planes_bit_exact(case):
+    """The XYB planes equal the oracle's bit for bit: decode, transfer, cube
+    root and the box pyramid all round identically on both sides."""
+    from oracle import binding as ob
+    o, d = _pyramid_cases()[case]()
+    with ss2.Ssimulacra2Pipeline(o.width, o.height) as p:
+        p.compute(o, d, 0.3)
+        scales = len(ss2.plan_scales(o.width, o.height))
+        for image, img in enumerate((o, d)):
+            want = ob.pyramid(helpers.to_oracle(img), 0.3)
+            for level in range(scales):
+                for c in range(3):
+                    if ob.channel_pruned(c, level, scales):
+                        continue
+                    got = p.debug_plane(image, level, c)
+                    assert np.array_equal(got.view(np.uint32), want[level][c].view(np.uint32)), \
+                        (case, image, level, c, np.abs(got - want[level][c]).max())
+
+
 def test_plain_256_pair():
     o, d = helpers.plain_256_pair()
     with ss2.Ssimulacra2Pipeline(256, 256) as p:

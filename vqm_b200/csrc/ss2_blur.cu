@@ -1,6 +1,7 @@
-// SSIMULACRA 2.1 kernels for sm_100a: prepare (decode + XYB pyramid), blur
-// (five 13-tap blurs, maps, compensated norm partials) and finalize (FP64
-// reduction, norms, score). See ss2_device.cuh for the batch layout.
+// Blur and finalize stages for sm_100a: the five 13-tap blurs, the maps and
+// compensated norm partials of every (pair, level, kept channel) tile, then
+// the FP64 reduction to norms and score. See ss2_device.cuh for the batch
+// layout.
 //
 // Rounding contract: the library is compiled with -fmad=false; every fused
 // multiply-add is an explicit __fmaf_rn placed where VQM's shaders accumulate
@@ -12,7 +13,6 @@
 
 #include <cstdint>
 
-#include "ss2_decode.cuh"
 #include "ss2_device.cuh"
 #include "ss2_kernels.h"
 
@@ -35,174 +35,6 @@ __device__ __forceinline__ uint32_t FindSlot(const uint32_t* __restrict__ start,
         else hi = mid;
     }
     return lo;
-}
-
-// ---------------------------------------------------------------------------
-// XYB (prepare.comp:40-98).
-// ---------------------------------------------------------------------------
-
-struct XybConst {
-    static constexpr float m00 = 0.30f, m02 = 0.078f, m01 = static_cast<float>(1.0 - 0.078 - 0.30);
-    static constexpr float m10 = 0.23f, m12 = 0.078f, m11 = static_cast<float>(1.0 - 0.078 - 0.23);
-    static constexpr float m20 = 0.24342268924547819f, m21 = 0.20476744424496821f;
-    static constexpr float m22 =
-        static_cast<float>(1.0 - 0.24342268924547819 - 0.20476744424496821);
-    static constexpr float bias = 0.0037930732552754493f;
-    static constexpr float cbias = 0.15595419704914093f;
-};
-
-// pow(v, 1/3) as the reference computes its cube root (prepare.comp:78).
-__device__ __forceinline__ float CubeRoot(float v) {
-    return powf(v, __fdiv_rn(1.0f, 3.0f));
-}
-
-// XYB of one linear sample; only the channels in `mask` are meaningful
-// (c2's cube root is skipped when B is not stored).
-__device__ __forceinline__ void Xyb(float r, float g, float b, uint32_t mask, float out[3]) {
-    using X = XybConst;
-    float m0 = __fmaf_rn(X::m00, r, __fmaf_rn(X::m01, g, __fmaf_rn(X::m02, b, X::bias)));
-    float m1 = __fmaf_rn(X::m10, r, __fmaf_rn(X::m11, g, __fmaf_rn(X::m12, b, X::bias)));
-    m0 = fmaxf(m0, 0.0f);
-    m1 = fmaxf(m1, 0.0f);
-    const float c0 = __fsub_rn(CubeRoot(m0), X::cbias);
-    const float c1 = __fsub_rn(CubeRoot(m1), X::cbias);
-    const float sum = __fadd_rn(c0, c1);
-    out[0] = __fmaf_rn(__fmul_rn(0.5f, __fsub_rn(c0, c1)), 14.0f, 0.42f);
-    out[1] = __fmaf_rn(0.5f, sum, 0.01f);
-    out[2] = 0.0f;
-    if (mask & 4u) {
-        float m2 = __fmaf_rn(X::m20, r, __fmaf_rn(X::m21, g, __fmaf_rn(X::m22, b, X::bias)));
-        m2 = fmaxf(m2, 0.0f);
-        const float c2 = __fsub_rn(CubeRoot(m2), X::cbias);
-        out[2] = __fadd_rn(__fmaf_rn(-0.5f, sum, c2), 0.55f);
-    }
-}
-
-// prepare.comp:103-111.
-__device__ __forceinline__ float BoxAverage(float a, float b, float c, float d) {
-    return __fmul_rn(__fadd_rn(__fadd_rn(__fadd_rn(a, b), c), d), 0.25f);
-}
-
-// ---------------------------------------------------------------------------
-// Prepare: one CTA of 16x16 threads per 32x32 base tile of one image; each
-// thread owns one 2x2 block and the CTA builds the tile's whole sub-pyramid
-// (levels 0 and 1 in registers, 2+ through a shared-memory ladder).
-// ---------------------------------------------------------------------------
-
-constexpr int kPrepThreads = 256;
-
-__device__ __forceinline__ void StoreXyb(const DevPair& P, int image, int level,
-                                         uint32_t x, uint32_t y, float r, float g,
-                                         float b) {
-    const uint32_t mask = P.mask[level];
-    if (mask == 0u) return;
-    float v[3];
-    Xyb(r, g, b, mask, v);
-    float* base = P.pyramid + static_cast<size_t>(image) * P.image_stride;
-    const size_t at = static_cast<size_t>(y) * P.pitch[level] + x;
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-        if (mask & (1u << c)) base[P.plane_off[level][c] + at] = v[c];
-}
-
-__global__ void __launch_bounds__(kPrepThreads)
-    Ss2PrepareKernel(DevBatch batch) {
-    __shared__ float ladder[2][256 * 3];
-    __shared__ float lut[256];
-    __shared__ DevSource src_s;
-    const uint32_t tid = threadIdx.x;
-    const uint32_t blk = blockIdx.x;
-    const uint32_t p = FindSlot(batch.prep_start, batch.pairs, blk);
-    const DevPair& P = batch.pair[p];
-    const uint32_t rem = blk - __ldg(&batch.prep_start[p]);
-    const uint32_t tiles = P.prep_tiles_x * P.prep_tiles_y;
-    const int image = rem >= tiles ? 1 : 0;
-    const uint32_t t = rem - static_cast<uint32_t>(image) * tiles;
-    const uint32_t gx = t % P.prep_tiles_x;
-    const uint32_t gy = t / P.prep_tiles_x;
-
-    // Stage this image's decode constants (and its table) in shared memory.
-    {
-        const uint32_t* from = reinterpret_cast<const uint32_t*>(&P.src[image]);
-        uint32_t* to = reinterpret_cast<uint32_t*>(&src_s);
-        constexpr uint32_t words = (offsetof(DevSource, srgb_lut)) / 4;
-        for (uint32_t i = tid; i < words; i += kPrepThreads) to[i] = from[i];
-        lut[tid] = P.src[image].srgb_lut[tid];
-    }
-    __syncthreads();
-    const DevSource& s = src_s;
-    const uint32_t levels = P.levels;
-    const uint32_t width = s.width, height = s.height;
-    const uint32_t bx = gx * 16 + (tid & 15);
-    const uint32_t by = gy * 16 + (tid >> 4);
-    const bool in_block = bx < (width + 1) / 2 && by < (height + 1) / 2;
-
-    float lin[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    if (in_block) {
-        if (s.lut) {
-            const uint32_t lx = width - 1, ly = height - 1;
-            const uint32_t x0 = min(2 * bx, lx), x1 = min(2 * bx + 1, lx);
-            const uint32_t y0 = min(2 * by, ly), y1 = min(2 * by + 1, ly);
-            const int planes = s.family == 0 ? 1 : 3;
-            for (int c = 0; c < 3; ++c) {
-                const int pl = planes == 1 ? 0 : c;
-                const uint8_t* r0 = s.plane[pl] + static_cast<size_t>(y0) * s.row_bytes[pl];
-                const uint8_t* r1 = s.plane[pl] + static_cast<size_t>(y1) * s.row_bytes[pl];
-                lin[0][c] = lut[r0[x0]];
-                lin[1][c] = lut[r0[x1]];
-                lin[2][c] = lut[r1[x0]];
-                lin[3][c] = lut[r1[x1]];
-            }
-            if (!s.identity2)
-                for (int i = 0; i < 4; ++i) ApplyMatrix(s.m2, lin[i]);
-        } else {
-            BlockLinearGeneric(s, bx, by, lin);
-        }
-        for (int i = 0; i < 4; ++i) {
-            const uint32_t x = min(2 * bx + (i & 1), width - 1);
-            const uint32_t y = min(2 * by + (i >> 1), height - 1);
-            StoreXyb(P, image, 0, x, y, lin[i][0], lin[i][1], lin[i][2]);
-        }
-    }
-
-    for (uint32_t level = 1; level < levels; ++level) {
-        const uint32_t side = 32u >> level;
-        const uint32_t jx = tid % side;
-        const uint32_t jy = tid / side;
-        const bool in_tile = tid < side * side;
-        float v[3] = {0.0f, 0.0f, 0.0f};
-        if (in_tile) {
-            if (level == 1) {
-                for (int c = 0; c < 3; ++c)
-                    v[c] = BoxAverage(lin[0][c], lin[1][c], lin[2][c], lin[3][c]);
-            } else {
-                // prepare.comp:149-168: the previous level's 2x2 block,
-                // clamped to its last column and row.
-                const uint32_t slot = (level - 1) & 1u;
-                const uint32_t prev_side = side * 2;
-                const uint32_t pw = P.w[level - 1], ph = P.h[level - 1];
-                const uint32_t ox = min(gx * prev_side, pw - 1);
-                const uint32_t oy = min(gy * prev_side, ph - 1);
-                const uint32_t lx = pw - 1 - ox, ly = ph - 1 - oy;
-                const uint32_t cx0 = min(2 * jx, lx), cx1 = min(2 * jx + 1, lx);
-                const uint32_t cy0 = min(2 * jy, ly), cy1 = min(2 * jy + 1, ly);
-                for (int c = 0; c < 3; ++c)
-                    v[c] = BoxAverage(ladder[slot][(cy0 * prev_side + cx0) * 3 + c],
-                                      ladder[slot][(cy0 * prev_side + cx1) * 3 + c],
-                                      ladder[slot][(cy1 * prev_side + cx0) * 3 + c],
-                                      ladder[slot][(cy1 * prev_side + cx1) * 3 + c]);
-            }
-        }
-        const uint32_t x = gx * side + jx;
-        const uint32_t y = gy * side + jy;
-        if (in_tile && x < P.w[level] && y < P.h[level])
-            StoreXyb(P, image, level, x, y, v[0], v[1], v[2]);
-        if (level + 1 < levels) {
-            if (in_tile)
-                for (int c = 0; c < 3; ++c) ladder[level & 1u][(jy * side + jx) * 3 + c] = v[c];
-            __syncthreads();
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -487,12 +319,6 @@ cudaError_t SetConstants(const float* taps13, const double* weights108) {
     cudaError_t e = cudaMemcpyToSymbol(c_taps, taps13, sizeof(float) * kTaps);
     if (e != cudaSuccess) return e;
     return cudaMemcpyToSymbol(c_weights, weights108, sizeof(double) * 108);
-}
-
-cudaError_t LaunchPrepare(const DevBatch& b, cudaStream_t stream) {
-    if (b.prep_blocks == 0) return cudaSuccess;
-    Ss2PrepareKernel<<<b.prep_blocks, kPrepThreads, 0, stream>>>(b);
-    return cudaGetLastError();
 }
 
 cudaError_t LaunchBlur(const DevBatch& b, int tile_w, int tile_h, cudaStream_t stream) {

@@ -14,13 +14,10 @@
 
 #include <cuda_fp16.h>
 
+#include "ss2_detmath.h"
 #include "ss2_device.cuh"
 
 namespace vqm_b200 {
-
-struct SrcView {
-    const DevSource* s;  // decode constants (shared memory copy)
-};
 
 __device__ __forceinline__ float RawSample(const DevSource& s, int plane,
                                            uint32_t x, uint32_t y) {
@@ -43,25 +40,25 @@ __device__ __forceinline__ float Rec709InvOetf(float x) {
     const float alpha = 1.09929682680944f, beta = 0.018053968510807f;
     return x < __fmul_rn(4.5f, beta)
                ? __fdiv_rn(x, 4.5f)
-               : powf(__fdiv_rn(__fadd_rn(x, __fsub_rn(alpha, 1.0f)), alpha),
+               : ss2dm::pow(__fdiv_rn(__fadd_rn(x, __fsub_rn(alpha, 1.0f)), alpha),
                       __fdiv_rn(1.0f, 0.45f));
 }
 __device__ __forceinline__ float SrgbEotf(float v) {
     return v <= 0.04045f ? __fdiv_rn(v, 12.92f)
-                         : powf(__fdiv_rn(__fadd_rn(v, 0.055f), 1.055f), 2.4f);
+                         : ss2dm::pow(__fdiv_rn(__fadd_rn(v, 0.055f), 1.055f), 2.4f);
 }
 __device__ __forceinline__ float St2084Eotf(float x) {
     if (x <= 0.0f) return 0.0f;
-    const float xp = powf(x, __fdiv_rn(1.0f, 78.84375f));
+    const float xp = ss2dm::pow(x, __fdiv_rn(1.0f, 78.84375f));
     const float num = fmaxf(__fsub_rn(xp, 0.8359375f), 0.0f);
     const float den = fmaxf(__fsub_rn(18.8515625f, __fmul_rn(18.6875f, xp)),
                             1.17549435e-38f);
-    return powf(__fdiv_rn(num, den), __fdiv_rn(1.0f, 0.1593017578125f));
+    return ss2dm::pow(__fdiv_rn(num, den), __fdiv_rn(1.0f, 0.1593017578125f));
 }
 __device__ __forceinline__ float AribInvOetf(float x) {
     x = fmaxf(x, 0.0f);
     return x <= 0.5f ? __fmul_rn(__fmul_rn(x, x), __fdiv_rn(1.0f, 3.0f))
-                     : __fdiv_rn(__fadd_rn(expf(__fdiv_rn(__fsub_rn(x, 0.55991073f),
+                     : __fdiv_rn(__fadd_rn(ss2dm::exp(__fdiv_rn(__fsub_rn(x, 0.55991073f),
                                                          0.17883277f)),
                                            0.28466892f),
                                  12.0f);
@@ -69,26 +66,26 @@ __device__ __forceinline__ float AribInvOetf(float x) {
 __device__ __forceinline__ float TransferDecode(const DevSource& s, float v) {
     switch (s.transfer) {
         case 0: return v;
-        case 1: return v < 0.0f ? 0.0f : powf(v, 2.4f);
-        case 2: return v < 0.0f ? 0.0f : powf(v, 2.2f);
-        case 3: return v < 0.0f ? 0.0f : powf(v, 2.8f);
+        case 1: return v < 0.0f ? 0.0f : ss2dm::pow(v, 2.4f);
+        case 2: return v < 0.0f ? 0.0f : ss2dm::pow(v, 2.2f);
+        case 3: return v < 0.0f ? 0.0f : ss2dm::pow(v, 2.8f);
         case 4: return SrgbEotf(v);
-        case 5: return v <= 0.0f ? 0.01f : powf(10.0f, __fmul_rn(2.0f, __fsub_rn(v, 1.0f)));
+        case 5: return v <= 0.0f ? 0.01f : ss2dm::pow(10.0f, __fmul_rn(2.0f, __fsub_rn(v, 1.0f)));
         case 6:
             return v <= 0.0f ? 0.00316227766f
-                             : powf(10.0f, __fmul_rn(2.5f, __fsub_rn(v, 1.0f)));
+                             : ss2dm::pow(10.0f, __fmul_rn(2.5f, __fsub_rn(v, 1.0f)));
         case 7:
             return v >= 0.0f && v <= 1.0f
-                       ? powf(v, 2.4f)
+                       ? ss2dm::pow(v, 2.4f)
                        : (v < 0.0f ? -Rec709InvOetf(-v) : Rec709InvOetf(v));
         case 8:
-            if (v >= 0.0f && v <= 1.0f) return powf(v, 2.4f);
+            if (v >= 0.0f && v <= 1.0f) return ss2dm::pow(v, 2.4f);
             return v >= 0.0f ? Rec709InvOetf(v)
                              : __fdiv_rn(-Rec709InvOetf(__fmul_rn(-4.0f, v)), 4.0f);
         case 9: return __fmul_rn(s.to_linear, St2084Eotf(v));
         case 10:
             return v < 0.0f ? 0.0f
-                            : __fmul_rn(__fdiv_rn(52.37f, 48.0f), powf(v, 2.6f));
+                            : __fmul_rn(__fdiv_rn(52.37f, 48.0f), ss2dm::pow(v, 2.6f));
     }
     return v;
 }
@@ -99,7 +96,7 @@ __device__ __forceinline__ void TransferRgb(const DevSource& s, float c[3]) {
         const float luma =
             fmaxf(__fmaf_rn(s.kb, c[2], __fmaf_rn(s.kg, c[1], __fmul_rn(s.kr, c[0]))),
                   1.17549435e-38f);
-        const float f = __fmul_rn(powf(luma, 0.2f), s.to_linear);
+        const float f = __fmul_rn(ss2dm::pow(luma, 0.2f), s.to_linear);
         for (int i = 0; i < 3; ++i) c[i] = __fmul_rn(c[i], f);
         return;
     }
@@ -150,11 +147,13 @@ __device__ __forceinline__ float FilterKernel(int filter, float x) {
             return __fmaf_rn(x, __fmaf_rn(x, __fmaf_rn(-0.5f, x, 2.5f), -4.0f), 2.0f);
         return 0.0f;
     }
+    // sin(pi v) / (pi v), the sine from the shared deterministic functions,
+    // the denominator with the reference's float pi.
     const float pi = 3.14159265358979323846f;
     if (!(x < 3.0f)) return 0.0f;
-    const float a = x == 0.0f ? 1.0f : __fdiv_rn(sinf(__fmul_rn(pi, x)), __fmul_rn(pi, x));
+    const float a = x == 0.0f ? 1.0f : __fdiv_rn(ss2dm::sinpi(x), __fmul_rn(pi, x));
     const float x3 = __fdiv_rn(x, 3.0f);
-    const float b = x3 == 0.0f ? 1.0f : __fdiv_rn(sinf(__fmul_rn(pi, x3)), __fmul_rn(pi, x3));
+    const float b = x3 == 0.0f ? 1.0f : __fdiv_rn(ss2dm::sinpi(x3), __fmul_rn(pi, x3));
     return __fmul_rn(a, b);
 }
 
@@ -269,9 +268,8 @@ __device__ void ChromaTaps(const DevSource& s, int plane, const uint32_t px[4],
 }
 
 // color.glsl:447-541: the block's four samples, linear Rec.709, in
-// (0,0), (1,0), (0,1), (1,1) order. The generic path: any format. Kept out
-// of line so its registers do not weigh on the table-driven fast path.
-__device__ __noinline__ void BlockLinearGeneric(const DevSource& s, uint32_t bx, uint32_t by,
+// (0,0), (1,0), (0,1), (1,1) order. The generic path: any format.
+__device__ __forceinline__ void BlockLinearGeneric(const DevSource& s, uint32_t bx, uint32_t by,
                                    float rgb[4][3]) {
     const uint32_t lx = s.width - 1, ly = s.height - 1;
     const uint32_t px[4] = {min(2 * bx, lx), min(2 * bx + 1, lx), min(2 * bx, lx),

@@ -1,0 +1,222 @@
+// Deterministic transcendental functions for the SSIMULACRA 2.1 path.
+//
+// VQM computes its cube root as pow(v, 1/3) and its transfer functions with
+// pow/exp/sin in 32-bit float (src/metrics/ssimulacra2/shaders/prepare.comp:78,
+// src/vulkan/shaders/color.glsl:117-205); the precision of those built-ins is
+// left to each device's shader compiler. The metric's small 1-norms are
+// sensitive to single-ulp changes in the XYB planes, so this file pins the
+// functions down: each is built only from IEEE-754 basic operations
+// (add, multiply, fused multiply-add, divide, conversions, integer bit
+// manipulation), which round identically on every conforming CPU and GPU.
+// The CUDA kernels, the host-side 8-bit decode tables and the CPU checker all
+// evaluate these same functions, so the pyramid planes agree bit for bit.
+//
+// Accuracy (checked by tests/test_detmath.py against double-precision libm):
+// every function evaluates in double with relative error below 1e-13 and
+// rounds once to float, so the float result is the correctly rounded value
+// except in the rare cases where the exact value lies within that error of a
+// rounding boundary.
+//
+// Compiled as host C++ (g++, -ffp-contract=off) or as CUDA (nvcc,
+// -fmad=false): no expression below may be contracted differently.
+#pragma once
+
+#include <cstdint>
+#include <cstring>
+
+#if defined(__CUDACC__)
+#define SS2_DM __host__ __device__ __forceinline__
+#else
+#define SS2_DM inline
+#include <cmath>
+#endif
+
+namespace ss2dm {
+
+SS2_DM double fmad(double a, double b, double c) {
+#if defined(__CUDA_ARCH__)
+    return __fma_rn(a, b, c);
+#else
+    return std::fma(a, b, c);
+#endif
+}
+SS2_DM float fmaf_(float a, float b, float c) {
+#if defined(__CUDA_ARCH__)
+    return __fmaf_rn(a, b, c);
+#else
+    return std::fma(a, b, c);
+#endif
+}
+SS2_DM uint32_t bits(float f) {
+#if defined(__CUDA_ARCH__)
+    return __float_as_uint(f);
+#else
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+#endif
+}
+SS2_DM float from_bits(uint32_t u) {
+#if defined(__CUDA_ARCH__)
+    return __uint_as_float(u);
+#else
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+#endif
+}
+SS2_DM uint64_t bits(double f) {
+#if defined(__CUDA_ARCH__)
+    return static_cast<uint64_t>(__double_as_longlong(f));
+#else
+    uint64_t u;
+    std::memcpy(&u, &f, 8);
+    return u;
+#endif
+}
+SS2_DM double from_bits64(uint64_t u) {
+#if defined(__CUDA_ARCH__)
+    return __longlong_as_double(static_cast<long long>(u));
+#else
+    double f;
+    std::memcpy(&f, &u, 8);
+    return f;
+#endif
+}
+
+SS2_DM double floord(double x) {
+#if defined(__CUDA_ARCH__)
+    return ::floor(x);
+#else
+    return std::floor(x);
+#endif
+}
+
+// 2^n for integer n in [-1022, 1023].
+SS2_DM double pow2i(int n) {
+    return from_bits64(static_cast<uint64_t>(n + 1023) << 52);
+}
+
+// Cube root of x >= 0, evaluated as x * r^2 with r = x^(-1/3): a bit-level
+// seed, three single-precision Newton steps on r (each roughly squares the
+// relative error: 0.04 -> 3e-3 -> 2e-5 -> ~1e-7) and one double-precision
+// step (-> ~1e-13). Returns 0 for x <= 0 and x for infinities and NaN.
+SS2_DM float cbrt(float x) {
+    if (!(x > 0.0f) || !(x < 3.402823466e38f)) return x > 0.0f ? x : 0.0f;
+    // Bring subnormal and tiny inputs into the normal range: cbrt(x * 2^90) =
+    // cbrt(x) * 2^30.
+    float scale = 1.0f;
+    if (x < 1.0e-30f) {
+        x = x * 1.237940039285380274899e27f;  // 2^90
+        scale = 9.313225746154785156e-10f;    // 2^-30
+    }
+    // x^(-1/3) seed from the exponent and mantissa bits (log-linear).
+    const uint32_t i = bits(x);
+    float r = from_bits(0x54a21d2au - i / 3u);
+    const float third = 0.333333343267440796f;
+    for (int k = 0; k < 3; ++k) {
+        const float r3 = r * r * r;
+        const float t = fmaf_(-x, r3, 1.0f);
+        r = fmaf_(r * t, third, r);
+    }
+    const double xd = static_cast<double>(x);
+    double rd = static_cast<double>(r);
+    const double t = fmad(-xd, rd * rd * rd, 1.0);
+    rd = fmad(rd * t, 0.33333333333333331483, rd);
+    return static_cast<float>(xd * rd * rd) * scale;
+}
+
+// log2 of a finite x > 0 in double: x = m 2^e with m in [sqrt(1/2), sqrt(2)),
+// ln m = 2 atanh(s), s = (m - 1) / (m + 1), |s| <= 0.1716, ten odd terms.
+SS2_DM double log2d(double x) {
+    uint64_t u = bits(x);
+    int e = static_cast<int>((u >> 52) & 0x7ff);
+    if (e == 0) {  // subnormal: normalise
+        x = x * 18014398509481984.0;  // 2^54
+        u = bits(x);
+        e = static_cast<int>((u >> 52) & 0x7ff) - 54;
+    }
+    e -= 1023;
+    double m = from_bits64((u & 0x000fffffffffffffull) | 0x3ff0000000000000ull);  // [1, 2)
+    if (m > 1.4142135623730951) {
+        m = m * 0.5;
+        e += 1;
+    }
+    const double s = (m - 1.0) / (m + 1.0);
+    const double s2 = s * s;
+    double p = 1.0 / 21.0;
+    p = fmad(p, s2, 1.0 / 19.0);
+    p = fmad(p, s2, 1.0 / 17.0);
+    p = fmad(p, s2, 1.0 / 15.0);
+    p = fmad(p, s2, 1.0 / 13.0);
+    p = fmad(p, s2, 1.0 / 11.0);
+    p = fmad(p, s2, 1.0 / 9.0);
+    p = fmad(p, s2, 1.0 / 7.0);
+    p = fmad(p, s2, 1.0 / 5.0);
+    p = fmad(p, s2, 1.0 / 3.0);
+    const double ln_m = 2.0 * fmad(s * s2, p, s);
+    return static_cast<double>(e) + ln_m * 1.4426950408889634074;  // 1/ln 2
+}
+
+// 2^t in double for |t| < 1000: t = n + f, f in [-1/2, 1/2], e^(f ln 2) by a
+// degree-13 Taylor polynomial.
+SS2_DM double exp2d(double t) {
+    if (t > 1000.0) t = 1000.0;
+    if (t < -1000.0) return 0.0;
+    const double nf = floord(t + 0.5);
+    const double f = t - nf;
+    const double z = f * 0.69314718055994530942;
+    double p = 1.0 / 6227020800.0;  // 1/13!
+    p = fmad(p, z, 1.0 / 479001600.0);
+    p = fmad(p, z, 1.0 / 39916800.0);
+    p = fmad(p, z, 1.0 / 3628800.0);
+    p = fmad(p, z, 1.0 / 362880.0);
+    p = fmad(p, z, 1.0 / 40320.0);
+    p = fmad(p, z, 1.0 / 5040.0);
+    p = fmad(p, z, 1.0 / 720.0);
+    p = fmad(p, z, 1.0 / 120.0);
+    p = fmad(p, z, 1.0 / 24.0);
+    p = fmad(p, z, 1.0 / 6.0);
+    p = fmad(p, z, 0.5);
+    p = fmad(p, z, 1.0);
+    p = fmad(p, z, 1.0);
+    int n = static_cast<int>(nf);
+    // Split the scale so every factor stays a normal double.
+    if (n > 1000) n = 1000;
+    const int n1 = n / 2, n2 = n - n1;
+    return p * pow2i(n1) * pow2i(n2);
+}
+
+// x^y for float x > 0 (0 for x == 0 and y > 0), both as float values.
+SS2_DM float pow(float x, float y) {
+    if (x == 1.0f || y == 0.0f) return 1.0f;
+    if (!(x > 0.0f)) return x == 0.0f ? (y > 0.0f ? 0.0f : 3.402823466e38f * 10.0f) : x - x;
+    return static_cast<float>(exp2d(static_cast<double>(y) * log2d(static_cast<double>(x))));
+}
+
+// e^x for float x.
+SS2_DM float exp(float x) {
+    return static_cast<float>(exp2d(static_cast<double>(x) * 1.4426950408889634074));
+}
+
+// sin(pi x) for float x in [0, 8): reduced to [-1/2, 1/2] around the
+// nearest integer, Taylor polynomial in double.
+SS2_DM float sinpi(float xf) {
+    const double x = static_cast<double>(xf);
+    const double k = floord(x + 0.5);  // nearest integer
+    const double f = x - k;             // [-1/2, 1/2]
+    const double z = f * 3.14159265358979323846;
+    const double z2 = z * z;
+    double p = -1.0 / 1307674368000.0;  // -1/15!
+    p = fmad(p, z2, 1.0 / 6227020800.0);
+    p = fmad(p, z2, -1.0 / 39916800.0);
+    p = fmad(p, z2, 1.0 / 362880.0);
+    p = fmad(p, z2, -1.0 / 5040.0);
+    p = fmad(p, z2, 1.0 / 120.0);
+    p = fmad(p, z2, -1.0 / 6.0);
+    const double s = fmad(z * z2, p, z);
+    const long long ki = static_cast<long long>(k);
+    return static_cast<float>((ki & 1) ? -s : s);
+}
+
+}  // namespace ss2dm

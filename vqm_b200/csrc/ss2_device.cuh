@@ -92,14 +92,27 @@ struct DevSegment {
     uint32_t partial_first;  // index of this segment's first tile partial
 };
 
+// One image of one pair for the prepare stage. Images decoded through the
+// 8-bit table come first in the list, the rest (generic decode) after them,
+// each group with its own prefix offsets, so each group is one launch of its
+// own specialised kernel.
+struct DevPrepItem {
+    uint32_t pair;
+    uint32_t image;
+};
+
 struct DevBatch {
     uint32_t pairs;
     uint32_t segments;
-    uint32_t prep_blocks;    // sum over pairs of 2 * prep tiles
-    uint32_t blur_blocks;    // sum over segments of tiles
+    uint32_t prep_items[2];   // table-decoded images, generic images
+    uint32_t prep_blocks[2];  // 32x32 base tiles in each group
+    uint32_t blur_blocks;     // sum over segments of tiles
     const DevPair* pair;
     const DevSegment* seg;
-    const uint32_t* prep_start;  // pairs + 1 prefix offsets
+    const DevPrepItem* prep_item;  // group 0 then group 1
+    // Prefix tile offsets: group 0 (prep_items[0] + 1 entries) then group 1
+    // (prep_items[1] + 1 entries).
+    const uint32_t* prep_start;
     const uint32_t* blur_start;  // segments + 1 prefix offsets
     double* partials;            // 6 doubles per blur tile
     double* seg_sums;            // 6 doubles per segment

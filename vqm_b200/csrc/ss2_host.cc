@@ -6,6 +6,8 @@
 
 #include "ss2_host.h"
 
+#include "ss2_detmath.h"
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -292,7 +294,7 @@ void LumaWeights(const vqm_cu_format& f, double& kr, double& kg, double& kb) {
 
 // The per-channel transfer decode in float, for the 8-bit table: the same
 // formulas and rounding as the device path (ss2_decode.cuh) and color.glsl.
-float HostPow(float a, float b) { return std::pow(a, b); }
+float HostPow(float a, float b) { return ss2dm::pow(a, b); }
 float Rec709InvOetfF(float x) {
     x = std::max(x, 0.0f);
     const float alpha = 1.09929682680944f, beta = 0.018053968510807f;

@@ -177,7 +177,10 @@ struct BlurShape {
 struct Tables {
     std::vector<DevPair> pairs;
     std::vector<DevSegment> segs;
-    std::vector<uint32_t> prep_start, blur_start;
+    std::vector<DevPrepItem> prep_items;  // table-decoded images, then generic
+    std::vector<uint32_t> prep_start;     // both groups' prefix offsets
+    uint32_t prep_count[2] = {0, 0}, prep_blocks[2] = {0, 0};
+    std::vector<uint32_t> blur_start;
     std::vector<size_t> pyramid_first;  // float offset of each pair's planes
     size_t pyramid_floats = 0;
     size_t partials = 0;  // tile partial count
@@ -188,7 +191,6 @@ struct Tables {
 Tables BuildTables(const std::vector<std::pair<uint32_t, uint32_t>>& sizes, BlurShape shape) {
     Tables t;
     t.pairs.resize(sizes.size());
-    t.prep_start.push_back(0);
     t.blur_start.push_back(0);
     uint64_t prep = 0, blur = 0;
     for (size_t i = 0; i < sizes.size(); ++i) {
@@ -214,7 +216,6 @@ Tables BuildTables(const std::vector<std::pair<uint32_t, uint32_t>>& sizes, Blur
         P.prep_tiles_x = (((sizes[i].first + 1) / 2) + 15) / 16;
         P.prep_tiles_y = (((sizes[i].second + 1) / 2) + 15) / 16;
         prep += 2ull * P.prep_tiles_x * P.prep_tiles_y;
-        t.prep_start.push_back(static_cast<uint32_t>(prep));
         P.seg_first = static_cast<uint32_t>(t.segs.size());
         for (int l = 0; l < plan.count; ++l)
             for (int c = 0; c < 3; ++c) {
@@ -236,7 +237,35 @@ Tables BuildTables(const std::vector<std::pair<uint32_t, uint32_t>>& sizes, Blur
     }
     if (prep > 0x7fffffffull || blur > 0x7fffffffull)
         throw std::invalid_argument("cuda: batch too large for one launch");
+    t.prep_items.resize(2 * sizes.size());
+    t.prep_start.resize(2 * sizes.size() + 2);
     return t;
+}
+
+// Splits the images into the table-decoded group and the generic group
+// (table[i][k]: image k of pair i decodes by table) and lays out each
+// group's prefix tile offsets. The list sizes do not depend on the split.
+void BuildPrepLists(Tables& t, const std::vector<std::array<bool, 2>>& table) {
+    uint32_t n[2] = {0, 0};
+    for (size_t i = 0; i < t.pairs.size(); ++i)
+        for (int k = 0; k < 2; ++k) ++n[table[i][k] ? 0 : 1];
+    uint32_t at[2] = {0, n[0]};
+    uint32_t* start[2] = {t.prep_start.data(), t.prep_start.data() + n[0] + 1};
+    uint32_t blocks[2] = {0, 0};
+    start[0][0] = 0;
+    start[1][0] = 0;
+    for (size_t i = 0; i < t.pairs.size(); ++i)
+        for (uint32_t k = 0; k < 2; ++k) {
+            const int g = table[i][k] ? 0 : 1;
+            const uint32_t idx = at[g]++;
+            t.prep_items[idx] = DevPrepItem{static_cast<uint32_t>(i), k};
+            blocks[g] += t.pairs[i].prep_tiles_x * t.pairs[i].prep_tiles_y;
+            start[g][idx - (g ? n[0] : 0) + 1] = blocks[g];
+        }
+    t.prep_count[0] = n[0];
+    t.prep_count[1] = n[1];
+    t.prep_blocks[0] = blocks[0];
+    t.prep_blocks[1] = blocks[1];
 }
 
 // The device tables of one batch: one table allocation, its pinned mirror,
@@ -244,7 +273,11 @@ Tables BuildTables(const std::vector<std::pair<uint32_t, uint32_t>>& sizes, Blur
 struct BatchMemory {
     DeviceBuffer table, pyramid, partials, seg_sums, pair_done, results;
     PinnedBuffer table_host, results_host;
-    size_t off_pairs = 0, off_segs = 0, off_prep = 0, off_blur = 0, table_bytes = 0;
+    // Table layout: [pairs | prep items | prep starts | segments | blur
+    // starts]. Everything a call can change (pair records, which images take
+    // the table path) sits in the first `head_bytes`.
+    size_t off_pairs = 0, off_items = 0, off_prep = 0, off_segs = 0, off_blur = 0;
+    size_t head_bytes = 0, table_bytes = 0;
     DevBatch dev{};
     uint32_t pair_count = 0;
 
@@ -252,9 +285,11 @@ struct BatchMemory {
     bool Layout(const Tables& t) {
         bool moved = false;
         off_pairs = 0;
-        off_segs = AlignUp(off_pairs + sizeof(DevPair) * t.pairs.size(), 256);
-        off_prep = AlignUp(off_segs + sizeof(DevSegment) * t.segs.size(), 256);
-        off_blur = AlignUp(off_prep + sizeof(uint32_t) * t.prep_start.size(), 256);
+        off_items = AlignUp(off_pairs + sizeof(DevPair) * t.pairs.size(), 16);
+        off_prep = AlignUp(off_items + sizeof(DevPrepItem) * t.prep_items.size(), 16);
+        head_bytes = AlignUp(off_prep + sizeof(uint32_t) * t.prep_start.size(), 256);
+        off_segs = head_bytes;
+        off_blur = AlignUp(off_segs + sizeof(DevSegment) * t.segs.size(), 256);
         table_bytes = AlignUp(off_blur + sizeof(uint32_t) * t.blur_start.size(), 256);
         moved |= table.ensure(table_bytes);
         moved |= table_host.ensure(table_bytes);
@@ -271,10 +306,10 @@ struct BatchMemory {
         uint8_t* base = table.as<uint8_t>();
         dev.pairs = static_cast<uint32_t>(t.pairs.size());
         dev.segments = static_cast<uint32_t>(t.segs.size());
-        dev.prep_blocks = t.prep_start.back();
         dev.blur_blocks = t.blur_start.back();
         dev.pair = reinterpret_cast<const DevPair*>(base + off_pairs);
         dev.seg = reinterpret_cast<const DevSegment*>(base + off_segs);
+        dev.prep_item = reinterpret_cast<const DevPrepItem*>(base + off_items);
         dev.prep_start = reinterpret_cast<const uint32_t*>(base + off_prep);
         dev.blur_start = reinterpret_cast<const uint32_t*>(base + off_blur);
         dev.partials = partials.as<double>();
@@ -293,8 +328,19 @@ struct BatchMemory {
         uint8_t* h = table_host.as<uint8_t>();
         std::memcpy(h + off_pairs, t.pairs.data(), sizeof(DevPair) * t.pairs.size());
         std::memcpy(h + off_segs, t.segs.data(), sizeof(DevSegment) * t.segs.size());
-        std::memcpy(h + off_prep, t.prep_start.data(), sizeof(uint32_t) * t.prep_start.size());
         std::memcpy(h + off_blur, t.blur_start.data(), sizeof(uint32_t) * t.blur_start.size());
+        StagePrep(t);
+    }
+    // The prepare lists (after BuildPrepLists) into the host mirror and the
+    // kernel parameters.
+    void StagePrep(const Tables& t) {
+        uint8_t* h = table_host.as<uint8_t>();
+        std::memcpy(h + off_items, t.prep_items.data(), sizeof(DevPrepItem) * t.prep_items.size());
+        std::memcpy(h + off_prep, t.prep_start.data(), sizeof(uint32_t) * t.prep_start.size());
+        for (int g = 0; g < 2; ++g) {
+            dev.prep_items[g] = t.prep_count[g];
+            dev.prep_blocks[g] = t.prep_blocks[g];
+        }
     }
     DevPair* HostPair(size_t i) {
         return reinterpret_cast<DevPair*>(table_host.as<uint8_t>() + off_pairs) + i;
@@ -421,6 +467,7 @@ public:
         VQM_CK(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming));
         VQM_CK(cudaEventCreateWithFlags(&copied_, cudaEventDisableTiming));
         tables_ = BuildTables({{cfg.width, cfg.height}}, shape_);
+        BuildPrepLists(tables_, {{true, true}});
         mem_.Layout(tables_);
         mem_.Stage(tables_);
         VQM_CK(cudaMemcpy(mem_.table.as<void>(), mem_.table_host.as<void>(), mem_.table_bytes,
@@ -431,7 +478,8 @@ public:
     ~Pipeline() {
         cudaSetDevice(device_);
         if (stream_) cudaStreamSynchronize(stream_);
-        if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+        for (auto& g : graph_exec_)
+            if (g) cudaGraphExecDestroy(g);
         if (done_) cudaEventDestroy(done_);
         if (copied_) cudaEventDestroy(copied_);
         if (own_stream_) cudaStreamDestroy(own_stream_);
@@ -681,6 +729,20 @@ public:
         a.live = false;
     }
 
+    void DebugPlane(uint32_t image, uint32_t level, uint32_t channel, float* out) {
+        RequireIdle("debug_plane");
+        if (image > 1 || level >= static_cast<uint32_t>(plan_.count) || channel > 2)
+            throw std::invalid_argument("cuda: no such plane");
+        if (!(plan_.mask[level] & (1u << channel)))
+            throw std::invalid_argument("cuda: the channel is pruned at this level");
+        const DevPair& P = tables_.pairs[0];
+        const float* src = mem_.pyramid.as<float>() + tables_.pyramid_first[0] +
+                           image * P.image_stride + P.plane_off[level][channel];
+        VQM_CK(cudaSetDevice(device_));
+        VQM_CK(cudaMemcpy2D(out, P.w[level] * sizeof(float), src, P.pitch[level] * sizeof(float),
+                            P.w[level] * sizeof(float), P.h[level], cudaMemcpyDeviceToHost));
+    }
+
     void Usage(vqm_cu_memory_usage* u) const {
         std::memset(u, 0, sizeof(*u));
         u->pyramid_bytes = mem_.pyramid.bytes();
@@ -719,11 +781,18 @@ private:
     // [upload the pair record, prepare, blur, finalize, read back], as one
     // graph replay when graphs are on.
     uint64_t Launch() {
-        const size_t upload = sizeof(DevPair);  // the pair record is first
+        // Which images decode by table decides the two prepare launches; one
+        // graph per combination.
+        const DevPair* hp = mem_.HostPair(0);
+        const int key = (hp->src[0].lut ? 1 : 0) | (hp->src[1].lut ? 2 : 0);
+        BuildPrepLists(tables_, {{hp->src[0].lut != 0, hp->src[1].lut != 0}});
+        mem_.StagePrep(tables_);
+        const size_t upload = mem_.head_bytes;
         // Stream capture needs a real stream; the legacy default stream runs
         // the same work launch by launch.
         if (graphs_ && stream_ != nullptr) {
-            if (!graph_exec_) {
+            cudaGraphExec_t& exec = graph_exec_[key];
+            if (!exec) {
                 cudaGraph_t graph = nullptr;
                 VQM_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
                 try {
@@ -736,11 +805,11 @@ private:
                     throw;
                 }
                 VQM_CK(cudaStreamEndCapture(stream_, &graph));
-                const cudaError_t e = cudaGraphInstantiate(&graph_exec_, graph, 0);
+                const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
                 cudaGraphDestroy(graph);
                 Check(e, "cudaGraphInstantiate");
             }
-            VQM_CK(cudaGraphLaunch(graph_exec_, stream_));
+            VQM_CK(cudaGraphLaunch(exec, stream_));
         } else {
             mem_.EnqueueUpload(upload, stream_);
             mem_.EnqueueKernels(shape_, stream_);
@@ -758,7 +827,7 @@ private:
     int device_ = 0;
     cudaStream_t own_stream_ = nullptr, stream_ = nullptr;
     cudaEvent_t done_ = nullptr, copied_ = nullptr;
-    cudaGraphExec_t graph_exec_ = nullptr;
+    cudaGraphExec_t graph_exec_[4] = {nullptr, nullptr, nullptr, nullptr};
     bool graphs_ = true;
     Tables tables_;
     BatchMemory mem_;
@@ -860,6 +929,10 @@ public:
                 }
             }
         }
+        std::vector<std::array<bool, 2>> table(n);
+        for (uint32_t i = 0; i < n; ++i)
+            table[i] = {t.pairs[i].src[0].lut != 0, t.pairs[i].src[1].lut != 0};
+        BuildPrepLists(t, table);
         mem_.Stage(t);
         if (host_bytes) VQM_CK(cudaEventRecord(copied_, stream_));
         mem_.EnqueueUpload(mem_.table_bytes, stream_);
@@ -1188,6 +1261,15 @@ int vqm_cu_ss2_release_image(vqm_cu_ss2_pipeline* p, uint64_t handle) {
     return Guard([&] {
         NotNull(p, "pipeline");
         p->impl.ReleaseImage(handle);
+    });
+}
+
+int vqm_cu_ss2_debug_plane(vqm_cu_ss2_pipeline* p, uint32_t image, uint32_t level,
+                           uint32_t channel, float* out) {
+    return Guard([&] {
+        NotNull(p, "pipeline");
+        NotNull(out, "out");
+        p->impl.DebugPlane(image, level, channel, out);
     });
 }
 

@@ -193,6 +193,7 @@ _SIGS = {
     "vqm_cu_ss2_map_image": ([_P, ctypes.c_uint64, _P], ctypes.c_int),
     "vqm_cu_ss2_release_image": ([_P, ctypes.c_uint64], ctypes.c_int),
     "vqm_cu_ss2_memory_usage": ([_P, _P], ctypes.c_int),
+    "vqm_cu_ss2_debug_plane": ([_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_create": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_destroy": ([_P], ctypes.c_int),
     "vqm_cu_ss2_batch_set_stream": ([_P, _P], ctypes.c_int),
@@ -513,6 +514,13 @@ class Ssimulacra2Pipeline:
         ptr = ctypes.c_void_p()
         _check(_lib.vqm_cu_ss2_map_image(self._p, buffer.slot, ctypes.byref(ptr)))
         return ptr.value
+
+    def debug_plane(self, image: int, level: int, channel: int) -> np.ndarray:
+        """The XYB plane the last finished pair wrote (diagnostic)."""
+        w, h = plan_scales(*self.size)[level]
+        out = np.empty((h, w), dtype=np.float32)
+        _check(_lib.vqm_cu_ss2_debug_plane(self._p, image, level, channel, out.ctypes.data))
+        return out
 
     def get_memory_usage(self) -> MemoryUsage:
         u = MemoryUsage()
