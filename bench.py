@@ -226,6 +226,8 @@ def main(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-sample", type=int, default=32)
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="time the batched path only (for profiler runs)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
@@ -296,6 +298,16 @@ def main(argv=None):
     peak, peak_kind = peaks()
     achieved = per_launch / (avg[dom] / 1e3) / 1e9
     traffic = traffic_per_launch(names[dom])
+
+    if args.batched_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "pairs/s",
+                              "stage_ms_per_step": dict(zip(("prepare", "blur", "finalize"),
+                                                            map(float, stage / args.steps))),
+                              "pairs": args.pairs, "steps": args.steps}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
 
     # Plain path: one pair per call, same resident pairs.
     pipe = ss2.Ssimulacra2Pipeline(WIDTH, HEIGHT)
