@@ -219,6 +219,29 @@ int vqm_cu_ss2_debug_plane(vqm_cu_ss2_pipeline* pipeline, uint32_t image,
  * default; 0 launches them one by one. */
 int vqm_cu_ss2_set_graphs(vqm_cu_ss2_pipeline* pipeline, int enabled);
 
+/* ---- scoring without allocation --------------------------------------- */
+
+/* No counterpart in the reference. For callers that cannot let a library
+ * allocate device memory (their own allocator owns all of it, or a
+ * cudaMalloc/cudaFree would stall their real-time streams): scores one pair
+ * of device images (memory == VQM_CU_MEMORY_DEVICE) on `stream` without any
+ * allocation, with all scratch in one fixed 32 MiB device array that the
+ * library reserves on every GPU that loads it, held until exit. Pairs whose
+ * scratch exceeds it (above about 2.4 megapixels: 1920x1080 and 2048x1200
+ * fit, 2560x1440 does not) return INVALID_ARGUMENT.
+ * Returns once the work is queued; result_device (caller-owned device
+ * memory, VQM_CU_SS2_RESULT_DOUBLES doubles) then receives 108 norms (18 per
+ * scale, zero past the pair's scales), the FP64 score, the scale count and
+ * a status word 0. All calls share the array and it keeps the last call's
+ * contents, so calls whose work overlaps on the GPU race: serialize them.
+ * The first call on a device sets up that device (symbol address lookup,
+ * constant upload) and should come before any stream capture. */
+#define VQM_CU_SS2_RESULT_DOUBLES 112
+int vqm_cu_ss2_compute_noalloc(const vqm_cu_image* original,
+                               const vqm_cu_image* distorted,
+                               float background, uint32_t chroma_filter,
+                               void* stream, double* result_device);
+
 /* ---- batch: many pairs of any sizes and formats, one launch per stage --- */
 /*      (Ssimulacra2Pool::ComputeMany / ScoreMany, include/vqm_pool.h:51-87) */
 

@@ -50,4 +50,7 @@ const double* ScoreWeights();
 // score.cc:118-163; throws std::invalid_argument like the reference.
 double Score(const double* norms, int scales);
 
+// Sets the calling thread's vqm_cu_last_error() message.
+void SetLastErrorMessage(const char* message);
+
 }  // namespace vqm_b200

@@ -1024,6 +1024,11 @@ void NotNull(const void* p, const char* what) {
 }
 
 }  // namespace
+
+// The message vqm_cu_last_error() returns on this thread, for entry points
+// defined in other translation units.
+void SetLastErrorMessage(const char* message) { g_last_error = message ? message : ""; }
+
 }  // namespace vqm_b200
 
 using vqm_b200::Guard;

@@ -194,6 +194,7 @@ _SIGS = {
     "vqm_cu_ss2_release_image": ([_P, ctypes.c_uint64], ctypes.c_int),
     "vqm_cu_ss2_memory_usage": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_debug_plane": ([_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _P], ctypes.c_int),
+    "vqm_cu_ss2_compute_noalloc": ([_P, _P, ctypes.c_float, ctypes.c_uint32, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_create": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_destroy": ([_P], ctypes.c_int),
     "vqm_cu_ss2_batch_set_stream": ([_P, _P], ctypes.c_int),
