@@ -251,8 +251,14 @@ typedef struct vqm_cu_ss2_batch_config {
     uint32_t chroma_filter;
     int32_t device;        /* CUDA ordinal; -1 = the current device */
     uint32_t tile_w, tile_h; /* blur tile; 0 = the tuned default */
-    uint32_t reserved;
+    uint32_t variant;      /* blur kernel: 0 = by tile (or the tuned
+                              default), k = compiled variant k - 1 */
 } vqm_cu_ss2_batch_config;
+
+/* The blur kernels compiled into the library, for tuning: *count variants,
+ * and for each (if `shapes` is not null) its tile width, tile height and
+ * threads per CTA, 3 words per variant. */
+int vqm_cu_ss2_blur_variants(uint32_t* count, uint32_t* shapes);
 
 int vqm_cu_ss2_batch_create(const vqm_cu_ss2_batch_config* config,
                             vqm_cu_ss2_batch** batch);

@@ -235,6 +235,19 @@ def test_batch_matches_pipeline_bitwise():
     assert np.array_equal(again[1].norms, results[1].norms)
 
 
+@pytest.mark.parametrize("variant", range(len(ss2.blur_variants())))
+def test_every_blur_variant(variant):
+    """Every compiled blur kernel gives the oracle's features; they differ
+    from each other only in how tile partials group the sums."""
+    pairs = [synthetic.rgb_pair(333, 187, 41)[:2], synthetic.yuv_pair(1280, 720, 42)[:2],
+             synthetic.rgb_pair(8, 8, 43)[:2], synthetic.rgb_pair(97, 2000, 44)[:2]]
+    b = ss2.Ssimulacra2Batch(variant=variant)
+    ref = ss2.Ssimulacra2Batch(variant=0).compute_many(pairs)
+    for (o, d), r, r0 in zip(pairs, b.compute_many(pairs), ref):
+        check_parity(r, o, d, label=f"variant {variant} {o.width}x{o.height}")
+        assert not helpers.feature_mismatch(r.norms, r0.norms, rtol=1e-6, atol=1e-12)
+
+
 def test_pool_score_many_in_order():
     pairs = [synthetic.rgb_pair(200 + 10 * i, 120, i)[:2] for i in range(5)]
     pool = ss2.Ssimulacra2Pool(workers=2, chunk=2)

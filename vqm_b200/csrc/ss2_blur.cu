@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "ss2_device.cuh"
 #include "ss2_kernels.h"
@@ -219,6 +220,233 @@ __global__ void __launch_bounds__(BlurTile<TW, TH>::kThreads)
 }
 
 // ---------------------------------------------------------------------------
+// Blur with packed FP32 (Blackwell FFMA2: two fused multiply-adds per
+// instruction). Same arithmetic per output as above -- every output is still
+// w0*s0 followed by fused ascending taps -- but two outputs share each
+// instruction:
+//   * the source tile is stored as row pairs, element (r, c) at
+//     src[image][r / 2][c].{x: r even, y: r odd}, so one 64-bit shared load
+//     gives the same column of two rows and the horizontal pass accumulates
+//     rows (2p, 2p+1) together, four output columns per task;
+//   * the horizontal results go to row-major planes, so the vertical pass
+//     reads columns (c, c+1) as one 64-bit load and accumulates that column
+//     pair over four output rows per task;
+//   * the maps run on the column pair, packed wherever the arithmetic is a
+//     multiply, add or fused multiply-add.
+// ---------------------------------------------------------------------------
+
+template <int TW, int TH, int NT>
+struct Blur2Tile {
+    static constexpr int SW = TW + 2 * kRadius;  // source columns
+    static constexpr int SH = TH + 2 * kRadius;  // source rows
+    static constexpr int RP = SH / 2;            // source row pairs
+    static constexpr int KH = 4;                 // output columns per horizontal task
+    static constexpr int HT = RP * (TW / KH);    // horizontal tasks
+    static constexpr int RV = 4;                 // output rows per vertical task
+    static constexpr int VT = (TW / 2) * (TH / RV);
+    static constexpr int kWarps = NT / 32;
+    // Dynamic shared memory: the row-pair source tiles of both images, then
+    // the five horizontal-pass planes.
+    static constexpr size_t kSrcBytes = sizeof(float2) * 2 * RP * SW;
+    static constexpr size_t kSmemBytes = kSrcBytes + sizeof(float) * 5 * SH * TW;
+    static_assert(TW % KH == 0 && TH % RV == 0 && SH % 2 == 0, "tile shape");
+    static_assert(NT % 32 == 0, "whole warps");
+    static_assert(kSrcBytes % 16 == 0, "plane alignment");
+};
+
+__device__ __forceinline__ float2 Pack(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 Neg(float2 v) { return make_float2(-v.x, -v.y); }
+
+template <int TW, int TH, int NT>
+__global__ void __launch_bounds__(NT) Ss2Blur2Kernel(DevBatch batch) {
+    using T = Blur2Tile<TW, TH, NT>;
+    constexpr int SW = T::SW, SH = T::SH, RP = T::RP;
+    extern __shared__ __align__(16) unsigned char smem[];
+    auto src = reinterpret_cast<float2 (*)[RP][SW]>(smem);
+    auto hq = reinterpret_cast<float (*)[SH][TW]>(smem + T::kSrcBytes);
+    __shared__ float red[T::kWarps][12];
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const uint32_t blk = blockIdx.x;
+    const uint32_t si = FindSlot(batch.blur_start, batch.segments, blk);
+    const DevSegment seg = batch.seg[si];
+    const uint32_t tile = blk - __ldg(&batch.blur_start[si]);
+    const DevPair& P = batch.pair[seg.pair];
+    const int w = static_cast<int>(P.w[seg.level]), h = static_cast<int>(P.h[seg.level]);
+    const size_t pitch = P.pitch[seg.level];
+    const float* __restrict__ pa = P.pyramid + P.plane_off[seg.level][seg.channel];
+    const float* __restrict__ pb = pa + P.image_stride;
+    const int x0 = static_cast<int>((tile % seg.tiles_x) * TW);
+    const int y0 = static_cast<int>((tile / seg.tiles_x) * TH);
+
+    // Zero-padded source tiles (scale.comp:107-124), as row pairs.
+    for (int rp = warp; rp < RP; rp += T::kWarps) {
+        const int gy0 = y0 - kRadius + 2 * rp, gy1 = gy0 + 1;
+        const bool in0 = gy0 >= 0 && gy0 < h, in1 = gy1 >= 0 && gy1 < h;
+        for (int c = lane; c < SW; c += 32) {
+            const int gx = x0 - kRadius + c;
+            const bool inx = gx >= 0 && gx < w;
+            float a0 = 0.0f, a1 = 0.0f, b0 = 0.0f, b1 = 0.0f;
+            if (inx && in0) {
+                a0 = __ldg(pa + static_cast<size_t>(gy0) * pitch + gx);
+                b0 = __ldg(pb + static_cast<size_t>(gy0) * pitch + gx);
+            }
+            if (inx && in1) {
+                a1 = __ldg(pa + static_cast<size_t>(gy1) * pitch + gx);
+                b1 = __ldg(pb + static_cast<size_t>(gy1) * pitch + gx);
+            }
+            src[0][rp][c] = make_float2(a0, a1);
+            src[1][rp][c] = make_float2(b0, b1);
+        }
+    }
+    __syncthreads();
+
+    // Horizontal pass (scale.comp:149-207): row pair rp, columns c0..c0+3.
+    for (int task = tid; task < T::HT; task += NT) {
+        const int rp = task / (TW / T::KH);
+        const int c0 = (task % (TW / T::KH)) * T::KH;
+        float2 A[T::KH + 12], B[T::KH + 12];
+#pragma unroll
+        for (int j = 0; j < T::KH + 12; j += 2) {
+            const float4 va = *reinterpret_cast<const float4*>(&src[0][rp][c0 + j]);
+            const float4 vb = *reinterpret_cast<const float4*>(&src[1][rp][c0 + j]);
+            A[j] = make_float2(va.x, va.y);
+            A[j + 1] = make_float2(va.z, va.w);
+            B[j] = make_float2(vb.x, vb.y);
+            B[j + 1] = make_float2(vb.z, vb.w);
+        }
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            float2 S[T::KH + 12];
+#pragma unroll
+            for (int j = 0; j < T::KH + 12; ++j)
+                S[j] = q == 0 ? A[j]
+                     : q == 1 ? B[j]
+                     : q == 2 ? __fmul2_rn(A[j], A[j])
+                     : q == 3 ? __fmul2_rn(B[j], B[j])
+                              : __fmul2_rn(A[j], B[j]);
+            float2 acc[T::KH];
+#pragma unroll
+            for (int k = 0; k < T::KH; ++k) acc[k] = __fmul2_rn(Pack(c_taps[0]), S[k]);
+#pragma unroll
+            for (int t = 1; t < kTaps; ++t) {
+                const float2 wt = Pack(c_taps[t]);
+#pragma unroll
+                for (int k = 0; k < T::KH; ++k) acc[k] = __ffma2_rn(wt, S[k + t], acc[k]);
+            }
+            *reinterpret_cast<float4*>(&hq[q][2 * rp][c0]) =
+                make_float4(acc[0].x, acc[1].x, acc[2].x, acc[3].x);
+            *reinterpret_cast<float4*>(&hq[q][2 * rp + 1][c0]) =
+                make_float4(acc[0].y, acc[1].y, acc[2].y, acc[3].y);
+        }
+    }
+    __syncthreads();
+
+    float2 sum[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) sum[k] = make_float2(0.0f, 0.0f);
+
+    // Vertical pass (scale.comp:211-301) on column pair (c, c+1), rows
+    // r0..r0+3, then the maps (scale.comp:305-333) of those eight pixels.
+    for (int task = tid; task < T::VT; task += NT) {
+        const int c = (task % (TW / 2)) * 2;
+        const int r0 = (task / (TW / 2)) * T::RV;
+        float2 V[5][T::RV];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            float2 M[T::RV + 12];
+#pragma unroll
+            for (int i = 0; i < T::RV + 12; ++i)
+                M[i] = *reinterpret_cast<const float2*>(&hq[q][r0 + i][c]);
+#pragma unroll
+            for (int j = 0; j < T::RV; ++j) {
+                float2 acc = __fmul2_rn(Pack(c_taps[0]), M[j]);
+#pragma unroll
+                for (int t = 1; t < kTaps; ++t) acc = __ffma2_rn(Pack(c_taps[t]), M[j + t], acc);
+                V[q][j] = acc;
+            }
+        }
+        const int out_x = x0 + c;
+#pragma unroll
+        for (int j = 0; j < T::RV; ++j) {
+            const int out_y = y0 + r0 + j;
+            if (out_y >= h || out_x >= w) continue;
+            const bool second = out_x + 1 < w;
+            const float2 mu1 = V[0][j], mu2 = V[1][j];
+            const float2 dm = __fadd2_rn(mu1, Neg(mu2));
+            const float2 num_m = __ffma2_rn(Neg(dm), dm, Pack(1.0f));
+            const float2 num_s =
+                __ffma2_rn(Pack(2.0f), __ffma2_rn(Neg(mu1), mu2, V[4][j]), Pack(0.0009f));
+            const float2 denom = __fadd2_rn(
+                __fadd2_rn(__ffma2_rn(Neg(mu1), mu1, V[2][j]), __ffma2_rn(Neg(mu2), mu2, V[3][j])),
+                Pack(0.0009f));
+            const float2 numer = __ffma2_rn(Neg(num_m), num_s, denom);
+            float2 d;
+            d.x = fmaxf(__fdiv_rn(numer.x, denom.x), 0.0f);
+            d.y = second ? fmaxf(__fdiv_rn(numer.y, denom.y), 0.0f) : 0.0f;
+            const float2 dd = __fmul2_rn(d, d);
+            // The raw XYB value is the centre of the source tile.
+            const int rr = r0 + j + kRadius;
+            const float2 s1a = src[0][rr >> 1][c + kRadius], s1b = src[0][rr >> 1][c + kRadius + 1];
+            const float2 s2a = src[1][rr >> 1][c + kRadius], s2b = src[1][rr >> 1][c + kRadius + 1];
+            const float2 img1 = (rr & 1) ? make_float2(s1a.y, s1b.y) : make_float2(s1a.x, s1b.x);
+            const float2 img2 = (rr & 1) ? make_float2(s2a.y, s2b.y) : make_float2(s2a.x, s2b.x);
+            float2 e2 = __fadd2_rn(img2, Neg(mu2));
+            float2 e1 = __fadd2_rn(img1, Neg(mu1));
+            e2 = make_float2(fabsf(e2.x), fabsf(e2.y));
+            e1 = make_float2(fabsf(e1.x), fabsf(e1.y));
+            const float2 dist = __fadd2_rn(Pack(1.0f), e2);
+            const float2 orig = __fadd2_rn(Pack(1.0f), e1);
+            const float2 diff = __fadd2_rn(dist, Neg(orig));
+            float2 d1;
+            d1.x = __fdiv_rn(diff.x, orig.x);
+            d1.y = second ? __fdiv_rn(diff.y, orig.y) : 0.0f;
+            const float2 ring = make_float2(fmaxf(d1.x, 0.0f), fmaxf(d1.y, 0.0f));
+            const float2 blur = make_float2(fmaxf(-d1.x, 0.0f), fmaxf(-d1.y, 0.0f));
+            const float2 r2 = __fmul2_rn(ring, ring), b2 = __fmul2_rn(blur, blur);
+            sum[0] = __fadd2_rn(sum[0], d);
+            sum[1] = __fadd2_rn(sum[1], __fmul2_rn(dd, dd));
+            sum[2] = __fadd2_rn(sum[2], ring);
+            sum[3] = __fadd2_rn(sum[3], __fmul2_rn(r2, r2));
+            sum[4] = __fadd2_rn(sum[4], blur);
+            sum[5] = __fadd2_rn(sum[5], __fmul2_rn(b2, b2));
+        }
+    }
+
+    // Compensated block reduction: the column pair's two sums, warp tree,
+    // then across warps.
+    float s[6], comp[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        s[k] = sum[k].x;
+        comp[k] = 0.0f;
+        TwoSumAdd(s[k], comp[k], sum[k].y, 0.0f);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const float s2 = __shfl_xor_sync(0xffffffffu, s[k], off);
+            const float c2 = __shfl_xor_sync(0xffffffffu, comp[k], off);
+            TwoSumAdd(s[k], comp[k], s2, c2);
+        }
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            red[warp][k] = s[k];
+            red[warp][6 + k] = comp[k];
+        }
+    __syncthreads();
+    if (tid < 6) {
+        float a = red[0][tid], cc = red[0][6 + tid];
+        for (int wi = 1; wi < T::kWarps; ++wi) TwoSumAdd(a, cc, red[wi][tid], red[wi][6 + tid]);
+        batch.partials[(static_cast<size_t>(seg.partial_first) + tile) * 6 + tid] =
+            static_cast<double>(a) + static_cast<double>(cc);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Finalize: one CTA per segment sums its tile partials in FP64 (fixed order,
 // so results repeat bit for bit); the last segment of a pair to finish writes
 // the pair's 108 norms (vulkan.cc:545-583) and score (score.cc:118-163).
@@ -321,21 +549,60 @@ cudaError_t SetConstants(const float* taps13, const double* weights108) {
     return cudaMemcpyToSymbol(c_weights, weights108, sizeof(double) * 108);
 }
 
-cudaError_t LaunchBlur(const DevBatch& b, int tile_w, int tile_h, cudaStream_t stream) {
-    if (b.blur_blocks == 0) return cudaSuccess;
-    if (tile_w == 32 && tile_h == 32) {
-        Ss2BlurKernel<32, 32><<<b.blur_blocks, BlurTile<32, 32>::kThreads, 0, stream>>>(b);
-    } else {
-        return cudaErrorInvalidValue;
+// The blur variants compiled in: {tile width, tile height, threads, packed}.
+// Variant 0 is the scalar kernel; the rest use packed FP32.
+struct BlurVariant {
+    int w, h, threads, packed;
+};
+constexpr BlurVariant kBlurVariants[] = {
+    {32, 32, 256, 0}, {32, 32, 128, 1}, {64, 32, 256, 1}, {32, 52, 128, 1}, {64, 20, 256, 1},
+};
+constexpr int kBlurVariantCount = sizeof(kBlurVariants) / sizeof(kBlurVariants[0]);
+
+// Launches one packed variant, raising its dynamic shared-memory limit the
+// first time on each device.
+template <int TW, int TH, int NT>
+cudaError_t LaunchPacked(const DevBatch& b, cudaStream_t stream) {
+    using T = Blur2Tile<TW, TH, NT>;
+    static std::mutex mu;
+    static uint64_t ready = 0;  // bit per device ordinal
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (device >= 64) return cudaErrorInvalidDevice;
+        if (!(ready & (1ull << device))) {
+            e = cudaFuncSetAttribute(Ss2Blur2Kernel<TW, TH, NT>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(T::kSmemBytes));
+            if (e != cudaSuccess) return e;
+            ready |= 1ull << device;
+        }
     }
+    Ss2Blur2Kernel<TW, TH, NT><<<b.blur_blocks, NT, T::kSmemBytes, stream>>>(b);
     return cudaGetLastError();
 }
 
-int BlurTileCount() { return 1; }
+cudaError_t LaunchBlur(const DevBatch& b, int variant, cudaStream_t stream) {
+    if (b.blur_blocks == 0) return cudaSuccess;
+    switch (variant) {
+        case 0:
+            Ss2BlurKernel<32, 32><<<b.blur_blocks, 256, 0, stream>>>(b);
+            return cudaGetLastError();
+        case 1: return LaunchPacked<32, 32, 128>(b, stream);
+        case 2: return LaunchPacked<64, 32, 256>(b, stream);
+        case 3: return LaunchPacked<32, 52, 128>(b, stream);
+        case 4: return LaunchPacked<64, 20, 256>(b, stream);
+    }
+    return cudaErrorInvalidValue;
+}
+
+int BlurTileCount() { return kBlurVariantCount; }
+int BlurTileThreads(int index) { return kBlurVariants[index].threads; }
 void BlurTileShape(int index, int* w, int* h) {
-    (void)index;
-    *w = 32;
-    *h = 32;
+    *w = kBlurVariants[index].w;
+    *h = kBlurVariants[index].h;
 }
 
 cudaError_t LaunchFinalize(const DevBatch& b, cudaStream_t stream) {

@@ -11,6 +11,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 namespace vqm_b200 {
 namespace {
@@ -501,10 +503,28 @@ void BuildSourceConstants(const vqm_cu_format& f, uint32_t chroma_filter, float 
              tid != 11)
                 ? 1
                 : 0;
-    for (int v = 0; v < 256; ++v)
-        d.srgb_lut[v] = d.lut ? TransferF(tid, tls, std::fma(static_cast<float>(v), d.scale[0],
-                                                             d.offset[0]))
-                              : 0.0f;
+    if (!d.lut) {
+        std::memset(d.srgb_lut, 0, sizeof(d.srgb_lut));
+        return;
+    }
+    // The table depends only on the transfer and the luma scale and offset;
+    // it is built once per distinct triple and reused.
+    static std::mutex mu;
+    static std::map<std::array<uint32_t, 4>, std::array<float, 256>> cache;
+    uint32_t sb, ob, tb;
+    std::memcpy(&sb, &d.scale[0], 4);
+    std::memcpy(&ob, &d.offset[0], 4);
+    std::memcpy(&tb, &tls, 4);
+    const std::array<uint32_t, 4> key{static_cast<uint32_t>(tid), sb, ob, tb};
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it == cache.end()) {
+        std::array<float, 256> table{};
+        for (int v = 0; v < 256; ++v)
+            table[v] = TransferF(tid, tls, std::fma(static_cast<float>(v), d.scale[0], d.offset[0]));
+        it = cache.emplace(key, table).first;
+    }
+    std::memcpy(d.srgb_lut, it->second.data(), sizeof(d.srgb_lut));
 }
 
 bool ChannelPruned(int channel, int scale, int scales) {

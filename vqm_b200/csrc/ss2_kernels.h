@@ -12,12 +12,16 @@ namespace vqm_b200 {
 cudaError_t SetConstants(const float* taps13, const double* weights108);
 
 cudaError_t LaunchPrepare(const DevBatch& batch, cudaStream_t stream);
-cudaError_t LaunchBlur(const DevBatch& batch, int tile_w, int tile_h,
-                       cudaStream_t stream);
+// `variant` indexes the blur kernels compiled in (BlurTileShape gives each
+// one's output tile); the batch's segments must have been tiled with it.
+cudaError_t LaunchBlur(const DevBatch& batch, int variant, cudaStream_t stream);
 cudaError_t LaunchFinalize(const DevBatch& batch, cudaStream_t stream);
 
-// Blur tile shapes compiled into the library, as (w, h) pairs.
+// The blur variants compiled into the library and their output tiles.
 int BlurTileCount();
 void BlurTileShape(int index, int* w, int* h);
+int BlurTileThreads(int index);
+// The variant used when a caller does not choose one.
+constexpr int kDefaultBlurVariant = 1;
 
 }  // namespace vqm_b200

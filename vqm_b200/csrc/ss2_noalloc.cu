@@ -46,7 +46,6 @@ namespace vqm_b200 {
 namespace {
 
 constexpr size_t kScratchBytes = size_t(32) << 20;
-constexpr int kTile = 32;  // the blur tile the library launches
 constexpr int kMaxSegments = kMaxLevels * kChannels;
 
 // The scratch itself. Host code must never dereference or pass this symbol:
@@ -143,6 +142,9 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
     ValidateFormat(o->format, o->width, o->height, "original");
     ValidateFormat(d->format, d->width, d->height, "distorted");
     const ScalePlan plan = PlanScales(o->width, o->height);
+    int tile_w = 0, tile_h = 0;  // the output tile of the blur kernel used
+    BlurTileShape(kDefaultBlurVariant, &tile_w, &tile_h);
+    const uint32_t tw = static_cast<uint32_t>(tile_w), th = static_cast<uint32_t>(tile_h);
 
     PairTables t;
     std::memset(static_cast<void*>(&t), 0, sizeof(t));
@@ -164,8 +166,8 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
             s.pair = 0;
             s.level = static_cast<uint32_t>(l);
             s.channel = static_cast<uint32_t>(c);
-            s.tiles_x = (plan.w[l] + kTile - 1) / kTile;
-            s.tiles = s.tiles_x * ((plan.h[l] + kTile - 1) / kTile);
+            s.tiles_x = (plan.w[l] + tw - 1) / tw;
+            s.tiles = s.tiles_x * ((plan.h[l] + th - 1) / th);
             s.partial_first = tiles;
             tiles += s.tiles;
             ++nseg;
@@ -248,7 +250,7 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
     StageTablesKernel<<<1, 256, 0, stream>>>(t, dev_tables, pair_done);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = LaunchPrepare(b, stream);
-    if (e == cudaSuccess) e = LaunchBlur(b, kTile, kTile, stream);
+    if (e == cudaSuccess) e = LaunchBlur(b, kDefaultBlurVariant, stream);
     if (e == cudaSuccess) e = LaunchFinalize(b, stream);
     if (e != cudaSuccess)
         throw std::runtime_error(std::string("cuda: launch: ") + cudaGetErrorString(e));

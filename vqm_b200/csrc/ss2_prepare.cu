@@ -199,9 +199,9 @@ __global__ void __launch_bounds__(kThreads) PrepareKernel(DevBatch batch) {
     }
 
     for (uint32_t level = 1; level < levels; ++level) {
-        const uint32_t side = 32u >> level;
-        const uint32_t jx = tid % side;
-        const uint32_t jy = tid / side;
+        const uint32_t side = 32u >> level;  // a power of two: shifts, not divisions
+        const uint32_t jx = tid & (side - 1);
+        const uint32_t jy = tid >> (5 - level);
         const bool in_tile = tid < side * side;
         float v[3] = {0.0f, 0.0f, 0.0f};
         if (in_tile) {

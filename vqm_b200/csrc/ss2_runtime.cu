@@ -170,8 +170,17 @@ size_t AlignUp(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // Batch tables: pyramid plane offsets, work segments and prefix offsets.
 // ---------------------------------------------------------------------------
 
+// The blur kernel variant and its output tile.
 struct BlurShape {
+    int variant = kDefaultBlurVariant;
     int w = 32, h = 32;
+    static BlurShape Of(int variant) {
+        BlurShape s;
+        s.variant = variant;
+        BlurTileShape(variant, &s.w, &s.h);
+        return s;
+    }
+    BlurShape() { BlurTileShape(variant, &w, &h); }
 };
 
 struct Tables {
@@ -356,7 +365,7 @@ struct BatchMemory {
         if (ev) VQM_CK(cudaEventRecord(ev[0], s));
         VQM_CK(LaunchPrepare(dev, s));
         if (ev) VQM_CK(cudaEventRecord(ev[1], s));
-        VQM_CK(LaunchBlur(dev, shape.w, shape.h, s));
+        VQM_CK(LaunchBlur(dev, shape.variant, s));
         if (ev) VQM_CK(cudaEventRecord(ev[2], s));
         VQM_CK(LaunchFinalize(dev, s));
         if (ev) VQM_CK(cudaEventRecord(ev[3], s));
@@ -847,16 +856,21 @@ class Batch {
 public:
     explicit Batch(const vqm_cu_ss2_batch_config& cfg) : cfg_(cfg) {
         if (cfg.chroma_filter > 2) throw std::invalid_argument("invalid chroma filter");
-        if (cfg.tile_w || cfg.tile_h) {
-            shape_.w = static_cast<int>(cfg.tile_w);
-            shape_.h = static_cast<int>(cfg.tile_h);
-            bool known = false;
+        if (cfg.variant) {
+            if (cfg.variant > static_cast<uint32_t>(BlurTileCount()))
+                throw std::invalid_argument("cuda: no such blur variant");
+            shape_ = BlurShape::Of(static_cast<int>(cfg.variant) - 1);
+        } else if (cfg.tile_w || cfg.tile_h) {
+            // The last compiled variant with that tile (the packed ones come
+            // after the scalar one).
+            int found = -1;
             for (int i = 0; i < BlurTileCount(); ++i) {
                 int w, h;
                 BlurTileShape(i, &w, &h);
-                known |= (w == shape_.w && h == shape_.h);
+                if (w == static_cast<int>(cfg.tile_w) && h == static_cast<int>(cfg.tile_h)) found = i;
             }
-            if (!known) throw std::invalid_argument("cuda: blur tile shape is not compiled in");
+            if (found < 0) throw std::invalid_argument("cuda: blur tile shape is not compiled in");
+            shape_ = BlurShape::Of(found);
         }
         device_ = ResolveDevice(cfg.device);
         EnsureDevice(device_);
@@ -1324,6 +1338,21 @@ int vqm_cu_ss2_batch_finish(vqm_cu_ss2_batch* b, uint64_t token, double* norms, 
     return Guard([&] {
         NotNull(b, "batch");
         b->impl.Finish(token, norms, scales, scores);
+    });
+}
+
+int vqm_cu_ss2_blur_variants(uint32_t* count, uint32_t* shapes) {
+    return Guard([&] {
+        NotNull(count, "count");
+        *count = static_cast<uint32_t>(vqm_b200::BlurTileCount());
+        if (shapes)
+            for (int i = 0; i < vqm_b200::BlurTileCount(); ++i) {
+                int w, h;
+                vqm_b200::BlurTileShape(i, &w, &h);
+                shapes[3 * i] = static_cast<uint32_t>(w);
+                shapes[3 * i + 1] = static_cast<uint32_t>(h);
+                shapes[3 * i + 2] = static_cast<uint32_t>(vqm_b200::BlurTileThreads(i));
+            }
     });
 }
 

@@ -155,7 +155,7 @@ class _BatchConfig(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("tile_w", ctypes.c_uint32),
         ("tile_h", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("variant", ctypes.c_uint32),
     ]
 
 
@@ -201,6 +201,7 @@ _SIGS = {
     "vqm_cu_ss2_batch_submit": ([_P, ctypes.c_uint32, _P, _P, ctypes.c_float, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_finish": ([_P, ctypes.c_uint64, _P, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_set_timing": ([_P, ctypes.c_int], ctypes.c_int),
+    "vqm_cu_ss2_blur_variants": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_stage_ms": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_compute": ([_P, ctypes.c_uint32, _P, _P, ctypes.c_float, _P, _P, _P], ctypes.c_int),
 }
@@ -534,13 +535,26 @@ class Ssimulacra2Pipeline:
 # ---------------------------------------------------------------------------
 
 
+def blur_variants():
+    """[(tile_w, tile_h, threads)] of the blur kernels compiled in."""
+    n = ctypes.c_uint32()
+    _check(_lib.vqm_cu_ss2_blur_variants(ctypes.byref(n), None))
+    shapes = (ctypes.c_uint32 * (3 * n.value))()
+    _check(_lib.vqm_cu_ss2_blur_variants(ctypes.byref(n), shapes))
+    return [tuple(shapes[3 * i:3 * i + 3]) for i in range(n.value)]
+
+
 class Ssimulacra2Batch:
     """Many pairs of any sizes, scored by one launch per stage."""
 
     def __init__(self, max_pairs: int = 0, max_pixels: int = 0, chroma_filter: int = 0,
-                 device: int = -1, tile: tuple[int, int] | None = None):
+                 device: int = -1, tile: tuple[int, int] | None = None,
+                 variant: int | None = None):
+        """`variant` picks a compiled blur kernel (see blur_variants());
+        `tile` picks one by its output tile; neither: the tuned default."""
         tw, th = tile if tile else (0, 0)
-        cfg = _BatchConfig(max_pixels, max_pairs, chroma_filter, device, tw, th, 0)
+        v = 0 if variant is None else variant + 1
+        cfg = _BatchConfig(max_pixels, max_pairs, chroma_filter, device, tw, th, v)
         self._b = ctypes.c_void_p()
         _check(_lib.vqm_cu_ss2_batch_create(ctypes.byref(cfg), ctypes.byref(self._b)))
 
