@@ -198,40 +198,64 @@ __global__ void __launch_bounds__(kThreads) PrepareKernel(DevBatch batch) {
         }
     }
 
-    for (uint32_t level = 1; level < levels; ++level) {
+    // Levels past the deepest one that stores a channel are not computed:
+    // nothing reads them (at six scales level 5 keeps no channel).
+    uint32_t last = 0;
+    for (uint32_t l = 1; l < levels; ++l)
+        if (lv.mask[l]) last = l;
+
+    // Level 1: every thread, from its own four samples.
+    if (last >= 1) {
+        float v[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = BoxAverage(lin[0][c], lin[1][c], lin[2][c], lin[3][c]);
+        const uint32_t x = gx * 16 + (tid & 15), y = gy * 16 + (tid >> 4);
+        const uint32_t mask = lv.mask[1];
+        if (mask && x < lv.w[1] && y < lv.h[1]) {
+            float xyb[3];
+            Xyb(v[0], v[1], v[2], mask, xyb);
+            const size_t at = static_cast<size_t>(y) * lv.pitch[1] + x;
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                if (mask & (1u << c)) lv.plane[1][c][at] = xyb[c];
+        }
+        if (last >= 2) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) ladder[1][tid * 3 + c] = v[c];
+        }
+    }
+    if (last < 2) return;
+    __syncthreads();
+
+    // Levels 2..last: the first side^2 threads (64, 16, 4, 1) average the
+    // previous level's 2x2 blocks from the ladder (prepare.comp:149-168,
+    // clamped to the previous level's last column and row); threads that no
+    // longer take part leave, and the rest meet at a barrier of their own.
+    for (uint32_t level = 2; level <= last; ++level) {
         const uint32_t side = 32u >> level;  // a power of two: shifts, not divisions
+        const uint32_t active = side * side;
+        if (tid >= active) return;
         const uint32_t jx = tid & (side - 1);
         const uint32_t jy = tid >> (5 - level);
-        const bool in_tile = tid < side * side;
-        float v[3] = {0.0f, 0.0f, 0.0f};
-        if (in_tile) {
-            if (level == 1) {
+        const uint32_t slot = (level - 1) & 1u;
+        const uint32_t prev_side = side * 2;
+        const uint32_t pw = lv.w[level - 1], ph = lv.h[level - 1];
+        const uint32_t ox = min(gx * prev_side, pw - 1);
+        const uint32_t oy = min(gy * prev_side, ph - 1);
+        const uint32_t lx = pw - 1 - ox, ly = ph - 1 - oy;
+        const uint32_t cx0 = min(2 * jx, lx), cx1 = min(2 * jx + 1, lx);
+        const uint32_t cy0 = min(2 * jy, ly), cy1 = min(2 * jy + 1, ly);
+        float v[3];
 #pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    v[c] = BoxAverage(lin[0][c], lin[1][c], lin[2][c], lin[3][c]);
-            } else {
-                // prepare.comp:149-168: the previous level's 2x2 block,
-                // clamped to its last column and row.
-                const uint32_t slot = (level - 1) & 1u;
-                const uint32_t prev_side = side * 2;
-                const uint32_t pw = lv.w[level - 1], ph = lv.h[level - 1];
-                const uint32_t ox = min(gx * prev_side, pw - 1);
-                const uint32_t oy = min(gy * prev_side, ph - 1);
-                const uint32_t lx = pw - 1 - ox, ly = ph - 1 - oy;
-                const uint32_t cx0 = min(2 * jx, lx), cx1 = min(2 * jx + 1, lx);
-                const uint32_t cy0 = min(2 * jy, ly), cy1 = min(2 * jy + 1, ly);
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    v[c] = BoxAverage(ladder[slot][(cy0 * prev_side + cx0) * 3 + c],
-                                      ladder[slot][(cy0 * prev_side + cx1) * 3 + c],
-                                      ladder[slot][(cy1 * prev_side + cx0) * 3 + c],
-                                      ladder[slot][(cy1 * prev_side + cx1) * 3 + c]);
-            }
-        }
+        for (int c = 0; c < 3; ++c)
+            v[c] = BoxAverage(ladder[slot][(cy0 * prev_side + cx0) * 3 + c],
+                              ladder[slot][(cy0 * prev_side + cx1) * 3 + c],
+                              ladder[slot][(cy1 * prev_side + cx0) * 3 + c],
+                              ladder[slot][(cy1 * prev_side + cx1) * 3 + c]);
         const uint32_t x = gx * side + jx;
         const uint32_t y = gy * side + jy;
         const uint32_t mask = lv.mask[level];
-        if (mask && in_tile && x < lv.w[level] && y < lv.h[level]) {
+        if (mask && x < lv.w[level] && y < lv.h[level]) {
             float xyb[3];
             Xyb(v[0], v[1], v[2], mask, xyb);
             const size_t at = static_cast<size_t>(y) * lv.pitch[level] + x;
@@ -239,12 +263,15 @@ __global__ void __launch_bounds__(kThreads) PrepareKernel(DevBatch batch) {
             for (int c = 0; c < 3; ++c)
                 if (mask & (1u << c)) lv.plane[level][c][at] = xyb[c];
         }
-        if (level + 1 < levels) {
-            if (in_tile) {
+        if (level < last) {
 #pragma unroll
-                for (int c = 0; c < 3; ++c) ladder[level & 1u][(jy * side + jx) * 3 + c] = v[c];
+            for (int c = 0; c < 3; ++c) ladder[level & 1u][tid * 3 + c] = v[c];
+            if (active > 32) {
+                // Level 2's 64 threads are warps 0 and 1, whole.
+                asm volatile("bar.sync 1, %0;" ::"r"(active) : "memory");
+            } else {
+                __syncwarp((1u << active) - 1u);
             }
-            __syncthreads();
         }
     }
 }
