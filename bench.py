@@ -230,7 +230,7 @@ def main(argv=None):
                     help="time the batched path only (for profiler runs)")
     ap.add_argument("--variant", type=int, default=None,
                     help="blur kernel variant; default: chosen by the autotuner")
-    ap.add_argument("--streams", type=int, default=2, choices=[1, 2],
+    ap.add_argument("--streams", type=int, default=1, choices=[1, 2],
                     help="streams for the two alternating batch scorers")
     args = ap.parse_args(argv)
     if args.warmup < 3:

@@ -1,0 +1,558 @@
+// vqm_cuda.hpp -- VQM's SSIMULACRA 2 C++ API on the B200 scorer.
+//
+// Header-only C++ layer over the C ABI in vqm_cu_ss2.h: the classes, member
+// functions, argument meanings and exception types of the reference's
+// include/ssimulacra2.h, include/vqm_image.h, include/vqm_views.h and
+// include/vqm_pool.h (GreatValueCreamSoda/vqm), with CUDA device buffers
+// (CudaBufferView) in place of Vulkan buffers. A VQM caller switches by
+// including this header and linking libvqm_ss2.so; every call crosses into
+// CUDA through the C ABI only.
+//
+// Status codes map back to the reference's exceptions:
+//   VQM_CU_INVALID_ARGUMENT -> std::invalid_argument
+//   VQM_CU_LOGIC_ERROR      -> std::logic_error
+//   VQM_CU_OVERFLOW_ERROR   -> std::overflow_error
+//   VQM_CU_RUNTIME_ERROR    -> std::runtime_error
+#pragma once
+
+#include <array>
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <span>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "vqm_cu_ss2.h"
+
+namespace vqm::cuda {
+
+// ---- vqm_image.h ------------------------------------------------------------
+
+struct Size {
+    std::size_t width = 0;
+    std::size_t height = 0;
+    constexpr bool operator==(const Size&) const noexcept = default;
+};
+
+enum class PixelType : std::uint8_t { Byte = 0, Word = 1, Half = 2, Float = 3 };
+enum class PixelRange : std::uint8_t { Limited = 0, Full = 1 };
+enum class ColorFamily : std::uint8_t { Grey = 0, Rgb = 1, Yuv = 2 };
+enum class AlphaType : std::uint8_t { None = 0, Straight = 1, Premultiplied = 2 };
+enum class ChromaLocation : std::uint8_t {
+    Left = 0, Center = 1, TopLeft = 2, Top = 3, BottomLeft = 4, Bottom = 5
+};
+enum class MatrixCoefficients : std::uint8_t {
+    Rgb = 0, Bt709 = 1, Unspecified = 2, Fcc = 4, Bt470Bg = 5, St170M = 6, St240M = 7,
+    YCgCo = 8, Bt2020Ncl = 9, Bt2020Cl = 10, St2085YDzDx = 11, ChromaticityDerivedNcl = 12,
+    ChromaticityDerivedCl = 13, Bt2100ICtCp = 14, St2128IptC2 = 15, YCgCoRe = 16, YCgCoRo = 17
+};
+enum class TransferCharacteristics : std::uint8_t {
+    Bt709 = 1, Unspecified = 2, Bt470M = 4, Bt470Bg = 5, Bt601 = 6, St240M = 7, Linear = 8,
+    Log100 = 9, Log316 = 10, Iec61966_2_4 = 11, Bt1361 = 12, Srgb = 13, Bt2020_10 = 14,
+    Bt2020_12 = 15, St2084 = 16, St428 = 17, AribB67 = 18
+};
+enum class ColorPrimaries : std::uint8_t {
+    Bt709 = 1, Unspecified = 2, Bt470M = 4, Bt470Bg = 5, St170M = 6, St240M = 7, Film = 8,
+    Bt2020 = 9, St428 = 10, St431_2 = 11, St432_1 = 12, Ebu3213E = 22
+};
+enum class ChromaFilter : std::uint8_t { Bilinear = 0, Bicubic = 1, Lanczos = 2 };
+
+struct ImageFormat {
+    PixelType type = PixelType::Float;
+    ColorFamily family = ColorFamily::Rgb;
+    AlphaType alpha = AlphaType::None;
+    PixelRange range = PixelRange::Full;
+    MatrixCoefficients matrix = MatrixCoefficients::Rgb;
+    TransferCharacteristics transfer = TransferCharacteristics::Srgb;
+    ColorPrimaries primaries = ColorPrimaries::Bt709;
+    ChromaLocation chroma_location = ChromaLocation::Left;
+    std::uint8_t subsample_w = 0;
+    std::uint8_t subsample_h = 0;
+    std::uint8_t depth = 0;
+};
+
+// Packed planes (Y/R, U/G, V/B, alpha), each on a 4-byte boundary.
+struct Image {
+    Size size;
+    ImageFormat format;
+    std::vector<std::uint8_t> data;
+    [[nodiscard]] bool HasAlpha() const noexcept { return format.alpha != AlphaType::None; }
+};
+
+struct UploadedImage {
+    std::uint64_t slot = 0;  // 0 == invalid
+    Size size;
+};
+
+struct ImageBuffer {
+    std::uint64_t slot = 0;  // 0 == invalid
+    Size size;
+    std::size_t bytes = 0;
+};
+
+// ---- vqm_views.h --------------------------------------------------------------
+
+struct PlaneView {
+    const std::byte* data = nullptr;
+    std::size_t stride_bytes = 0;
+};
+
+struct ImageView {
+    Size size;
+    ImageFormat format;
+    std::array<PlaneView, 4> planes{};
+};
+
+// The CUDA counterpart of VulkanBufferView (include/vqm_vulkan.h): planes in
+// caller-owned device memory, read in place; 0 strides mean packed rows.
+struct CudaBufferView {
+    Size size;
+    ImageFormat format;
+    std::array<const void*, 4> planes{};
+    std::array<std::size_t, 4> strides{};
+};
+
+// The counterpart of VulkanSubmitSync: events the pair's work waits for
+// before it starts and records when it is done (cudaEvent_t as void*).
+struct CudaSubmitSync {
+    std::vector<void*> wait_events;
+    std::vector<void*> signal_events;
+};
+
+namespace detail {
+
+inline void Check(int status) {
+    if (status == VQM_CU_OK) return;
+    const std::string message = vqm_cu_last_error();
+    switch (status) {
+        case VQM_CU_INVALID_ARGUMENT: throw std::invalid_argument(message);
+        case VQM_CU_LOGIC_ERROR: throw std::logic_error(message);
+        case VQM_CU_OVERFLOW_ERROR: throw std::overflow_error(message);
+        default: throw std::runtime_error(message);
+    }
+}
+
+inline vqm_cu_format ToC(const ImageFormat& f) {
+    vqm_cu_format c{};
+    c.type = static_cast<std::uint8_t>(f.type);
+    c.family = static_cast<std::uint8_t>(f.family);
+    c.alpha = static_cast<std::uint8_t>(f.alpha);
+    c.range = static_cast<std::uint8_t>(f.range);
+    c.matrix = static_cast<std::uint8_t>(f.matrix);
+    c.transfer = static_cast<std::uint8_t>(f.transfer);
+    c.primaries = static_cast<std::uint8_t>(f.primaries);
+    c.chroma_location = static_cast<std::uint8_t>(f.chroma_location);
+    c.subsample_w = f.subsample_w;
+    c.subsample_h = f.subsample_h;
+    c.depth = f.depth;
+    return c;
+}
+
+inline std::uint32_t Dim(std::size_t v) {
+    if (v > 0xffffffffull) throw std::overflow_error("image dimension exceeds 32 bits");
+    return static_cast<std::uint32_t>(v);
+}
+
+}  // namespace detail
+
+// RequiredBytes (include/vqm_image.h:360-363).
+[[nodiscard]] inline std::size_t RequiredBytes(const ImageFormat& format, Size size) {
+    std::size_t bytes = 0;
+    const vqm_cu_format f = detail::ToC(format);
+    detail::Check(vqm_cu_required_bytes(&f, detail::Dim(size.width), detail::Dim(size.height),
+                                        &bytes));
+    return bytes;
+}
+
+// ValidateFormat (src/input.cc): throws std::invalid_argument with the
+// reference's message, prefixed by `name`.
+inline void ValidateFormat(const ImageFormat& format, Size size, const char* name) {
+    const vqm_cu_format f = detail::ToC(format);
+    detail::Check(vqm_cu_validate_format(&f, detail::Dim(size.width), detail::Dim(size.height),
+                                         name));
+}
+
+namespace detail {
+
+// Plane addresses of a packed Image (input.cc:114-145 layout).
+inline vqm_cu_image ToC(const Image& img, const char* name) {
+    const std::size_t expected = RequiredBytes(img.format, img.size);
+    if (img.data.size() != expected)
+        throw std::invalid_argument(std::string(name) +
+                                    ": data size does not match the image format (expected " +
+                                    std::to_string(expected) + " bytes)");
+    vqm_cu_image c{};
+    c.width = Dim(img.size.width);
+    c.height = Dim(img.size.height);
+    c.format = ToC(img.format);
+    c.memory = VQM_CU_MEMORY_HOST;
+    const std::size_t sb = img.format.type == PixelType::Byte ? 1
+                         : img.format.type == PixelType::Float ? 4 : 2;
+    const std::size_t cw = img.size.width >> img.format.subsample_w;
+    const std::size_t ch = img.size.height >> img.format.subsample_h;
+    std::size_t cursor = 0;
+    for (int p = 0; p < 4; ++p) {
+        const bool chroma = p == 1 || p == 2;
+        const bool present = p == 0 || (chroma && img.format.family != ColorFamily::Grey) ||
+                             (p == 3 && img.format.alpha != AlphaType::None);
+        if (!present) continue;
+        c.planes[p] = img.data.data() + cursor;
+        const std::size_t n = chroma ? cw * ch : img.size.width * img.size.height;
+        cursor = (cursor + n * sb + 3) / 4 * 4;
+    }
+    return c;
+}
+
+inline vqm_cu_image ToC(const ImageView& v) {
+    vqm_cu_image c{};
+    c.width = Dim(v.size.width);
+    c.height = Dim(v.size.height);
+    c.format = ToC(v.format);
+    c.memory = VQM_CU_MEMORY_HOST;
+    for (int p = 0; p < 4; ++p) {
+        c.planes[p] = v.planes[p].data;
+        c.strides[p] = v.planes[p].stride_bytes;
+    }
+    return c;
+}
+
+inline vqm_cu_image ToC(const CudaBufferView& v) {
+    vqm_cu_image c{};
+    c.width = Dim(v.size.width);
+    c.height = Dim(v.size.height);
+    c.format = ToC(v.format);
+    c.memory = VQM_CU_MEMORY_DEVICE;
+    for (int p = 0; p < 4; ++p) {
+        c.planes[p] = v.planes[p];
+        c.strides[p] = v.strides[p];
+    }
+    return c;
+}
+
+}  // namespace detail
+
+// ---- ssimulacra2.h ----------------------------------------------------------
+
+struct Ssimulacra2Scale {
+    static constexpr std::size_t kSsimNormCount = 6;
+    static constexpr std::size_t kEdgeNormCount = 12;
+    std::array<double, kSsimNormCount> avg_ssim{};     // [channel * 2 + norm]
+    std::array<double, kEdgeNormCount> avg_edgediff{}; // [channel * 4 + n]
+};
+
+struct Ssimulacra2Result {
+    std::vector<Ssimulacra2Scale> scales;
+    // Ssimulacra2Result::Score (score.cc:118-163): throws
+    // std::invalid_argument for more than six scales, nonfinite norms or an
+    // overflowing mapping.
+    [[nodiscard]] double Score() const {
+        std::vector<double> flat(std::max<std::size_t>(scales.size(), 1) * 18, 0.0);
+        for (std::size_t s = 0; s < scales.size(); ++s) {
+            for (int k = 0; k < 6; ++k) flat[s * 18 + k] = scales[s].avg_ssim[k];
+            for (int k = 0; k < 12; ++k) flat[s * 18 + 6 + k] = scales[s].avg_edgediff[k];
+        }
+        double score = 0.0;
+        detail::Check(vqm_cu_ss2_score(flat.data(), static_cast<std::uint32_t>(scales.size()),
+                                       &score));
+        return score;
+    }
+
+    static Ssimulacra2Result FromNorms(const double* norms, std::uint32_t count) {
+        Ssimulacra2Result r;
+        r.scales.resize(count);
+        for (std::uint32_t s = 0; s < count; ++s) {
+            for (int k = 0; k < 6; ++k) r.scales[s].avg_ssim[k] = norms[s * 18 + k];
+            for (int k = 0; k < 12; ++k) r.scales[s].avg_edgediff[k] = norms[s * 18 + 6 + k];
+        }
+        return r;
+    }
+};
+
+struct Ssimulacra2Config {
+    Size size;
+    std::size_t gpu_resident_images = 2;
+    bool half_planes = false;
+    ChromaFilter chroma_filter = ChromaFilter::Bilinear;
+    std::size_t input_bytes = 0;
+    bool streaming_inputs = true;
+    int device = -1;  // CUDA ordinal; -1 = the current device
+};
+
+// Memory the pipeline holds on the device (PipelineMemoryUsage's role).
+using PipelineMemoryUsage = vqm_cu_memory_usage;
+
+class Ssimulacra2Pipeline {
+public:
+    explicit Ssimulacra2Pipeline(Ssimulacra2Config config) : config_(config) {
+        vqm_cu_ss2_config c{};
+        c.width = detail::Dim(config.size.width);
+        c.height = detail::Dim(config.size.height);
+        if (config.gpu_resident_images > 0xffffffffull)
+            throw std::invalid_argument("gpu_resident_images is limited to 4095 slots");
+        c.gpu_resident_images = static_cast<std::uint32_t>(config.gpu_resident_images);
+        c.half_planes = config.half_planes ? 1 : 0;
+        c.chroma_filter = static_cast<std::uint32_t>(config.chroma_filter);
+        c.streaming_inputs = config.streaming_inputs ? 1 : 0;
+        c.input_bytes = config.input_bytes;
+        c.device = config.device;
+        vqm_cu_ss2_pipeline* p = nullptr;
+        detail::Check(vqm_cu_ss2_create(&c, &p));
+        p_.reset(p);
+    }
+    Ssimulacra2Pipeline(Ssimulacra2Pipeline&&) noexcept = default;
+    Ssimulacra2Pipeline& operator=(Ssimulacra2Pipeline&&) noexcept = default;
+
+    [[nodiscard]] Ssimulacra2Result Compute(const Image& o, const Image& d, float background = 0.5f) {
+        return Finish(Submit(o, d, background));
+    }
+    [[nodiscard]] Ssimulacra2Result Compute(const ImageView& o, const ImageView& d,
+                                            float background = 0.5f) {
+        return Finish(Submit(o, d, background));
+    }
+    [[nodiscard]] Ssimulacra2Result Compute(const UploadedImage& o, const UploadedImage& d,
+                                            float background = 0.5f) {
+        return Finish(Submit(o, d, background));
+    }
+    [[nodiscard]] Ssimulacra2Result Compute(const UploadedImage& o, const Image& d,
+                                            float background = 0.5f) {
+        return Finish(Submit(o, d, background));
+    }
+    [[nodiscard]] Ssimulacra2Result Compute(const ImageBuffer& o, const ImageBuffer& d,
+                                            float background = 0.5f) {
+        return Finish(Submit(o, d, background));
+    }
+    [[nodiscard]] Ssimulacra2Result Compute(const CudaBufferView& o, const CudaBufferView& d,
+                                            float background = 0.5f) {
+        return Finish(Submit(o, d, background));
+    }
+
+    [[nodiscard]] std::uint64_t Submit(const Image& o, const Image& d, float background = 0.5f) {
+        Geometry(o.size, "original");
+        Geometry(d.size, "distorted");
+        const vqm_cu_image a = detail::ToC(o, "original"), b = detail::ToC(d, "distorted");
+        return SubmitC(a, b, background);
+    }
+    [[nodiscard]] std::uint64_t Submit(const ImageView& o, const ImageView& d,
+                                       float background = 0.5f) {
+        return SubmitC(detail::ToC(o), detail::ToC(d), background);
+    }
+    [[nodiscard]] std::uint64_t Submit(const UploadedImage& o, const UploadedImage& d,
+                                       float background = 0.5f) {
+        std::uint64_t token = 0;
+        detail::Check(vqm_cu_ss2_submit_resident(p_.get(), o.slot, d.slot, background, &token));
+        return token;
+    }
+    [[nodiscard]] std::uint64_t Submit(const UploadedImage& o, const Image& d,
+                                       float background = 0.5f) {
+        Geometry(d.size, "distorted");
+        const vqm_cu_image b = detail::ToC(d, "distorted");
+        std::uint64_t token = 0;
+        detail::Check(vqm_cu_ss2_submit_resident_image(p_.get(), o.slot, &b, background, &token));
+        return token;
+    }
+    [[nodiscard]] std::uint64_t Submit(const ImageBuffer& o, const ImageBuffer& d,
+                                       float background = 0.5f) {
+        std::uint64_t token = 0;
+        detail::Check(vqm_cu_ss2_submit_buffers(p_.get(), o.slot, d.slot, background, &token));
+        return token;
+    }
+    [[nodiscard]] std::uint64_t Submit(const CudaBufferView& o, const CudaBufferView& d,
+                                       float background = 0.5f) {
+        return SubmitC(detail::ToC(o), detail::ToC(d), background);
+    }
+    [[nodiscard]] std::uint64_t Submit(const CudaBufferView& o, const CudaBufferView& d,
+                                       const CudaSubmitSync& sync, float background = 0.5f) {
+        const vqm_cu_image a = detail::ToC(o), b = detail::ToC(d);
+        std::uint64_t token = 0;
+        detail::Check(vqm_cu_ss2_submit_sync(
+            p_.get(), &a, &b, sync.wait_events.data(),
+            static_cast<std::uint32_t>(sync.wait_events.size()), sync.signal_events.data(),
+            static_cast<std::uint32_t>(sync.signal_events.size()), background, &token));
+        return token;
+    }
+
+    [[nodiscard]] Ssimulacra2Result Finish(std::uint64_t token) {
+        double norms[VQM_CU_SS2_MAX_NORMS];
+        std::uint32_t scales = 0;
+        detail::Check(vqm_cu_ss2_finish(p_.get(), token, norms, &scales));
+        return Ssimulacra2Result::FromNorms(norms, scales);
+    }
+
+    [[nodiscard]] UploadedImage Upload(const Image& image) {
+        Geometry(image.size, "image");
+        const vqm_cu_image c = detail::ToC(image, "image");
+        std::uint64_t handle = 0;
+        detail::Check(vqm_cu_ss2_upload(p_.get(), &c, &handle));
+        return UploadedImage{handle, image.size};
+    }
+    void Release(UploadedImage image) { detail::Check(vqm_cu_ss2_release(p_.get(), image.slot)); }
+
+    [[nodiscard]] ImageBuffer AllocateImage(const ImageFormat& format) {
+        const vqm_cu_format f = detail::ToC(format);
+        std::uint64_t handle = 0;
+        std::size_t bytes = 0;
+        detail::Check(vqm_cu_ss2_allocate_image(p_.get(), &f, &handle, &bytes));
+        return ImageBuffer{handle, config_.size, bytes};
+    }
+    // A CUDA device address (fill it with cudaMemcpy or a kernel).
+    [[nodiscard]] void* MapImage(ImageBuffer buffer) {
+        void* ptr = nullptr;
+        detail::Check(vqm_cu_ss2_map_image(p_.get(), buffer.slot, &ptr));
+        return ptr;
+    }
+    void Release(ImageBuffer buffer) {
+        detail::Check(vqm_cu_ss2_release_image(p_.get(), buffer.slot));
+    }
+
+    [[nodiscard]] PipelineMemoryUsage GetMemoryUsage() const {
+        PipelineMemoryUsage u{};
+        detail::Check(vqm_cu_ss2_memory_usage(p_.get(), &u));
+        return u;
+    }
+    void SetStream(void* stream) { detail::Check(vqm_cu_ss2_set_stream(p_.get(), stream)); }
+
+private:
+    struct Deleter {
+        void operator()(vqm_cu_ss2_pipeline* p) const noexcept { vqm_cu_ss2_destroy(p); }
+    };
+    void Geometry(Size s, const char* name) const {
+        if (!(s == config_.size))
+            throw std::invalid_argument(std::string(name) +
+                                        ": image size does not match the pipeline geometry");
+    }
+    std::uint64_t SubmitC(const vqm_cu_image& a, const vqm_cu_image& b, float background) {
+        std::uint64_t token = 0;
+        detail::Check(vqm_cu_ss2_submit(p_.get(), &a, &b, background, &token));
+        return token;
+    }
+    Ssimulacra2Config config_;
+    std::unique_ptr<vqm_cu_ss2_pipeline, Deleter> p_;
+};
+
+// ---- vqm_pool.h ---------------------------------------------------------------
+
+struct ImagePair {
+    const Image& original;
+    const Image& distorted;
+};
+struct ImageViewPair {
+    const ImageView& original;
+    const ImageView& distorted;
+};
+struct CudaBufferPair {
+    const CudaBufferView& original;
+    const CudaBufferView& distorted;
+};
+
+// Ssimulacra2Pool (include/vqm_pool.h:51-87): results in input order. The
+// reference round-robins pairs over `workers` one-in-flight pipelines of one
+// geometry; here every `chunk` pairs (any sizes) are one batched submission,
+// one launch per stage over all of them, with `workers` batch scorers in
+// flight at once.
+class Ssimulacra2Pool {
+public:
+    Ssimulacra2Pool(Ssimulacra2Config config, std::size_t workers, std::size_t chunk = 64)
+        : chroma_filter_(config.chroma_filter), chunk_(chunk ? chunk : 1) {
+        if (workers == 0) throw std::invalid_argument("pool needs at least one worker");
+        for (std::size_t i = 0; i < workers; ++i) {
+            vqm_cu_ss2_batch_config c{};
+            c.chroma_filter = static_cast<std::uint32_t>(config.chroma_filter);
+            c.device = config.device;
+            c.max_pairs = static_cast<std::uint32_t>(chunk_);
+            vqm_cu_ss2_batch* b = nullptr;
+            detail::Check(vqm_cu_ss2_batch_create(&c, &b));
+            batches_.emplace_back(b);
+        }
+    }
+    [[nodiscard]] std::size_t Workers() const noexcept { return batches_.size(); }
+
+    [[nodiscard]] std::vector<Ssimulacra2Result> ComputeMany(std::span<const ImagePair> pairs,
+                                                             float background = 0.5f) {
+        std::vector<vqm_cu_image> o, d;
+        for (const auto& p : pairs) {
+            o.push_back(detail::ToC(p.original, "original"));
+            d.push_back(detail::ToC(p.distorted, "distorted"));
+        }
+        return Run(o, d, background);
+    }
+    [[nodiscard]] std::vector<Ssimulacra2Result> ComputeMany(std::span<const ImageViewPair> pairs,
+                                                             float background = 0.5f) {
+        std::vector<vqm_cu_image> o, d;
+        for (const auto& p : pairs) {
+            o.push_back(detail::ToC(p.original));
+            d.push_back(detail::ToC(p.distorted));
+        }
+        return Run(o, d, background);
+    }
+    [[nodiscard]] std::vector<Ssimulacra2Result> ComputeMany(std::span<const CudaBufferPair> pairs,
+                                                             float background = 0.5f) {
+        std::vector<vqm_cu_image> o, d;
+        for (const auto& p : pairs) {
+            o.push_back(detail::ToC(p.original));
+            d.push_back(detail::ToC(p.distorted));
+        }
+        return Run(o, d, background);
+    }
+    template <class Pairs>
+    [[nodiscard]] std::vector<double> ScoreMany(const Pairs& pairs, float background = 0.5f) {
+        std::vector<double> scores;
+        for (const auto& r : ComputeMany(pairs, background)) scores.push_back(r.Score());
+        return scores;
+    }
+
+private:
+    struct Deleter {
+        void operator()(vqm_cu_ss2_batch* b) const noexcept { vqm_cu_ss2_batch_destroy(b); }
+    };
+    std::vector<Ssimulacra2Result> Run(const std::vector<vqm_cu_image>& o,
+                                       const std::vector<vqm_cu_image>& d, float background) {
+        const std::size_t n = o.size();
+        std::vector<Ssimulacra2Result> out(n);
+        std::vector<std::pair<std::uint64_t, std::size_t>> pending(batches_.size(), {0, 0});
+        std::vector<std::size_t> first(batches_.size(), 0);
+        std::vector<double> norms(chunk_ * VQM_CU_SS2_MAX_NORMS);
+        std::vector<std::uint32_t> scales(chunk_);
+        auto drain = [&](std::size_t w) {
+            if (!pending[w].second) return;
+            detail::Check(vqm_cu_ss2_batch_finish(batches_[w].get(), pending[w].first,
+                                                  norms.data(), scales.data(), nullptr));
+            for (std::size_t i = 0; i < pending[w].second; ++i)
+                out[first[w] + i] = Ssimulacra2Result::FromNorms(
+                    norms.data() + i * VQM_CU_SS2_MAX_NORMS, scales[i]);
+            pending[w].second = 0;
+        };
+        std::size_t w = 0;
+        try {
+            for (std::size_t at = 0; at < n; at += chunk_, w = (w + 1) % batches_.size()) {
+                drain(w);
+                const std::size_t count = std::min(chunk_, n - at);
+                std::uint64_t token = 0;
+                detail::Check(vqm_cu_ss2_batch_submit(batches_[w].get(),
+                                                      static_cast<std::uint32_t>(count),
+                                                      o.data() + at, d.data() + at, background,
+                                                      &token));
+                pending[w] = {token, count};
+                first[w] = at;
+            }
+            for (std::size_t k = 0; k < batches_.size(); ++k) drain(k);
+        } catch (...) {
+            // Drain what was submitted before rethrowing (pool.cc:64-112).
+            for (std::size_t k = 0; k < batches_.size(); ++k) {
+                if (!pending[k].second) continue;
+                vqm_cu_ss2_batch_finish(batches_[k].get(), pending[k].first, nullptr, nullptr,
+                                        nullptr);
+                pending[k].second = 0;
+            }
+            throw;
+        }
+        return out;
+    }
+    ChromaFilter chroma_filter_;
+    std::size_t chunk_;
+    std::vector<std::unique_ptr<vqm_cu_ss2_batch, Deleter>> batches_;
+};
+
+}  // namespace vqm::cuda

@@ -1,0 +1,152 @@
+// Exercises include/vqm_cuda.hpp the way a VQM C++ caller would.
+//
+//   facade_check host   checks that need no device (sizes, Score, errors)
+//   facade_check gpu    scores the 32x32 gradient pairs (tests/support.h
+//                       MakeGradient) through Pipeline, Upload and Pool and
+//                       prints one JSON object per result on stdout
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "vqm_cuda.hpp"
+
+namespace v = vqm::cuda;
+
+namespace {
+
+int failures = 0;
+
+void Expect(bool ok, const char* what) {
+    if (!ok) {
+        std::fprintf(stderr, "FAIL: %s\n", what);
+        ++failures;
+    }
+}
+
+template <class E, class F>
+void ExpectThrow(F&& f, const char* what) {
+    try {
+        f();
+    } catch (const E&) {
+        return;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "FAIL: %s threw the wrong type: %s\n", what, e.what());
+        ++failures;
+        return;
+    }
+    std::fprintf(stderr, "FAIL: %s did not throw\n", what);
+    ++failures;
+}
+
+v::ImageFormat Srgb8() {
+    v::ImageFormat f;
+    f.type = v::PixelType::Byte;
+    return f;
+}
+
+// MakeGradient (tests/support.h:259-289): 0 gradient, 1 checkerboard +16
+// red, 2 3-bit truncation.
+v::Image Gradient(int variant) {
+    const int side = 32;
+    v::Image img;
+    img.size = {side, side};
+    img.format = Srgb8();
+    img.data.resize(3 * side * side);
+    for (int y = 0; y < side; ++y)
+        for (int x = 0; x < side; ++x) {
+            int r = x * 255 / (side - 1), g = y * 255 / (side - 1);
+            int b = ((x * 7 + y * 11) * 13) & 255;
+            if (variant == 1 && ((x + y) & 1) == 0) r = std::min(r + 16, 255);
+            if (variant == 2) { r &= 0xF8; g &= 0xF8; b &= 0xF8; }
+            const int i = y * side + x;
+            img.data[i] = static_cast<std::uint8_t>(r);
+            img.data[side * side + i] = static_cast<std::uint8_t>(g);
+            img.data[2 * side * side + i] = static_cast<std::uint8_t>(b);
+        }
+    return img;
+}
+
+void Print(const char* path, int variant, const v::Ssimulacra2Result& r) {
+    std::printf("{\"path\": \"%s\", \"variant\": %d, \"score\": %.17g, \"norms\": [", path,
+                variant, r.Score());
+    bool first = true;
+    for (const auto& s : r.scales) {
+        for (double n : s.avg_ssim) { std::printf(first ? "%.17g" : ", %.17g", n); first = false; }
+        for (double n : s.avg_edgediff) std::printf(", %.17g", n);
+    }
+    std::printf("]}\n");
+}
+
+void Host() {
+    Expect(v::RequiredBytes(Srgb8(), {32, 32}) == 3 * 32 * 32, "RequiredBytes srgb8");
+    v::ImageFormat yuv;
+    yuv.type = v::PixelType::Word;
+    yuv.family = v::ColorFamily::Yuv;
+    yuv.range = v::PixelRange::Limited;
+    yuv.matrix = v::MatrixCoefficients::Bt709;
+    yuv.transfer = v::TransferCharacteristics::Bt709;
+    yuv.subsample_w = yuv.subsample_h = 1;
+    yuv.depth = 10;
+    Expect(v::RequiredBytes(yuv, {64, 32}) == 64 * 32 * 2 + 2 * 32 * 16 * 2,
+           "RequiredBytes yuv420 10-bit");
+    ExpectThrow<std::invalid_argument>([&] { v::ValidateFormat(yuv, {63, 32}, "original"); },
+                                       "odd width with 4:2:0");
+
+    v::Ssimulacra2Result perfect;
+    perfect.scales.resize(6);
+    Expect(perfect.Score() == 100.0, "all-zero norms score 100");
+    v::Ssimulacra2Result seven;
+    seven.scales.resize(7);
+    ExpectThrow<std::invalid_argument>([&] { (void)seven.Score(); }, "seven scales");
+    v::Ssimulacra2Result bad;
+    bad.scales.resize(1);
+    bad.scales[0].avg_ssim[0] = NAN;
+    ExpectThrow<std::invalid_argument>([&] { (void)bad.Score(); }, "nonfinite norm");
+}
+
+void Gpu() {
+    v::Ssimulacra2Config config;
+    config.size = {32, 32};
+    v::Ssimulacra2Pipeline pipeline(config);
+    const v::Image base = Gradient(0);
+    for (int variant = 0; variant < 3; ++variant) {
+        const v::Image dist = Gradient(variant);
+        Print("pipeline", variant, pipeline.Compute(base, dist));
+    }
+    const v::UploadedImage up = pipeline.Upload(base);
+    Print("uploaded", 1, pipeline.Compute(up, Gradient(1)));
+    pipeline.Release(up);
+    v::Image small = Gradient(0);
+    small.size = {16, 16};
+    small.data.resize(3 * 16 * 16);
+    ExpectThrow<std::invalid_argument>([&] { (void)pipeline.Compute(base, small); },
+                                       "size mismatch");
+    ExpectThrow<std::invalid_argument>([&] { (void)pipeline.Finish(12345); }, "unknown token");
+
+    v::Ssimulacra2Pool pool(config, 2, 2);
+    const v::Image d1 = Gradient(1), d2 = Gradient(2);
+    const std::vector<v::ImagePair> pairs{{base, base}, {base, d1}, {base, d2}};
+    const auto results = pool.ComputeMany(std::span<const v::ImagePair>(pairs));
+    for (std::size_t i = 0; i < results.size(); ++i) Print("pool", static_cast<int>(i), results[i]);
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    const std::string mode = argc > 1 ? argv[1] : "host";
+    try {
+        if (mode == "host") Host();
+        else if (mode == "gpu") Gpu();
+        else {
+            std::fprintf(stderr, "usage: facade_check host|gpu\n");
+            return 2;
+        }
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "FAIL: unexpected exception: %s\n", e.what());
+        return 1;
+    }
+    return failures ? 1 : 0;
+}
