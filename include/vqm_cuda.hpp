@@ -2,8 +2,9 @@
 //
 // Header-only C++ layer over the C ABI in vqm_cu_ss2.h: the classes, member
 // functions, argument meanings and exception types of the reference's
-// include/ssimulacra2.h, include/vqm_image.h, include/vqm_views.h and
-// include/vqm_pool.h (GreatValueCreamSoda/vqm), with CUDA device buffers
+// include/ssimulacra2.h, include/vqm_image.h, include/vqm_views.h,
+// include/vqm_pool.h and, for SSIMULACRA 2, include/vqm_metrics.h
+// (GreatValueCreamSoda/vqm), with CUDA device buffers
 // (CudaBufferView) in place of Vulkan buffers. A VQM caller switches by
 // including this header and linking libvqm_ss2.so; every call crosses into
 // CUDA through the C ABI only.
@@ -18,7 +19,9 @@
 #include <array>
 #include <cstddef>
 #include <cstdint>
+#include <cstring>
 #include <memory>
+#include <optional>
 #include <span>
 #include <stdexcept>
 #include <string>
@@ -553,6 +556,164 @@ private:
     ChromaFilter chroma_filter_;
     std::size_t chunk_;
     std::vector<std::unique_ptr<vqm_cu_ss2_batch, Deleter>> batches_;
+};
+
+// ---- vqm_metrics.h (SSIMULACRA 2 only) ---------------------------------------
+
+struct MetricsConfig {
+    Size size;
+    ImageFormat original_format{};
+    ImageFormat distorted_format{};
+    bool streaming_inputs = true;
+    float background = 0.5f;
+    // The one metric this library computes; leaving it empty is the
+    // reference's "select at least one metric" error.
+    std::optional<Ssimulacra2Config> ssimulacra2 = std::nullopt;
+};
+
+struct MetricsResult {
+    std::uint64_t frame_index = 0;
+    std::optional<double> ssimulacra2;
+};
+
+struct MetricsFinalResult {
+    std::optional<MetricsResult> last_frame;
+    std::uint64_t frames = 0;
+    std::optional<MetricsResult> penultimate_frame;
+};
+
+// Metrics (include/vqm_metrics.h:147-217, src/metrics/metrics.cc:83-396) with
+// SSIMULACRA 2 as the selected metric. SSIMULACRA 2 has no lookahead, so
+// Compute returns each frame's result at once and Flush returns nothing; the
+// sequence rules are the reference's: after a failed call only Reset helps,
+// after Flush/Finalize the sequence is finished until Reset, and ComputeImage
+// needs a fresh sequence and resets it afterwards.
+class Metrics {
+public:
+    explicit Metrics(MetricsConfig config) : config_(config) {
+        if (!config_.ssimulacra2)
+            throw std::invalid_argument("metrics: select at least one metric");
+        Ssimulacra2Config c = *config_.ssimulacra2;
+        c.size = config_.size;
+        c.streaming_inputs = config_.streaming_inputs;
+        c.gpu_resident_images = 0;
+        c.input_bytes = 0;
+        pipeline_.emplace(c);
+    }
+
+    [[nodiscard]] std::optional<MetricsResult> Compute(const Image& o, const Image& d) {
+        return Run([&] { return pipeline_->Compute(o, d, config_.background); }, o.size,
+                   o.format, d.size, d.format, true);
+    }
+    [[nodiscard]] std::optional<MetricsResult> Compute(const ImageView& o, const ImageView& d) {
+        return Run([&] { return pipeline_->Compute(o, d, config_.background); }, o.size,
+                   o.format, d.size, d.format, true);
+    }
+    // Tightly packed planes in the configured formats, exactly RequiredBytes
+    // each.
+    [[nodiscard]] std::optional<MetricsResult> Compute(std::span<const std::byte> o,
+                                                       std::span<const std::byte> d) {
+        const Image a = Packed(o, config_.original_format, "original");
+        const Image b = Packed(d, config_.distorted_format, "distorted");
+        return Compute(a, b);
+    }
+    [[nodiscard]] std::optional<MetricsResult> Compute(const CudaBufferView& o,
+                                                       const CudaBufferView& d) {
+        return Run([&] { return pipeline_->Compute(o, d, config_.background); }, o.size,
+                   o.format, d.size, d.format, false);
+    }
+
+    [[nodiscard]] MetricsResult ComputeImage(const Image& o, const Image& d) {
+        return Still([&] { return Compute(o, d); });
+    }
+    [[nodiscard]] MetricsResult ComputeImage(const ImageView& o, const ImageView& d) {
+        return Still([&] { return Compute(o, d); });
+    }
+    [[nodiscard]] MetricsResult ComputeImage(std::span<const std::byte> o,
+                                             std::span<const std::byte> d) {
+        return Still([&] { return Compute(o, d); });
+    }
+    [[nodiscard]] MetricsResult ComputeImage(const CudaBufferView& o, const CudaBufferView& d) {
+        return Still([&] { return Compute(o, d); });
+    }
+
+    [[nodiscard]] std::optional<MetricsResult> Flush() {
+        if (failed_) throw std::logic_error("metrics: previous call failed; call Reset");
+        finished_ = true;
+        return std::nullopt;
+    }
+    [[nodiscard]] MetricsFinalResult Finalize() {
+        (void)Flush();
+        MetricsFinalResult r;
+        r.frames = next_index_;
+        return r;
+    }
+    void Reset() {
+        next_index_ = 0;
+        failed_ = false;
+        finished_ = false;
+    }
+    [[nodiscard]] PipelineMemoryUsage GetMemoryUsage() const { return pipeline_->GetMemoryUsage(); }
+
+private:
+    static bool SameFormat(const ImageFormat& a, const ImageFormat& b) {
+        return a.type == b.type && a.family == b.family && a.alpha == b.alpha &&
+               a.range == b.range && a.matrix == b.matrix && a.transfer == b.transfer &&
+               a.primaries == b.primaries && a.chroma_location == b.chroma_location &&
+               a.subsample_w == b.subsample_w && a.subsample_h == b.subsample_h &&
+               a.depth == b.depth;
+    }
+    Image Packed(std::span<const std::byte> bytes, const ImageFormat& f, const char* name) const {
+        if (bytes.size() != RequiredBytes(f, config_.size))
+            throw std::invalid_argument(std::string(name) +
+                                        ": data size does not match the image format");
+        Image img;
+        img.size = config_.size;
+        img.format = f;
+        img.data.resize(bytes.size());
+        std::memcpy(img.data.data(), bytes.data(), bytes.size());
+        return img;
+    }
+    template <class F>
+    std::optional<MetricsResult> Run(F&& compute, Size os, const ImageFormat& of, Size ds,
+                                     const ImageFormat& df, bool host) {
+        if (failed_) throw std::logic_error("metrics: previous call failed; call Reset");
+        if (finished_) throw std::logic_error("metrics: sequence finished; call Reset");
+        if (next_index_ == ~std::uint64_t{0})
+            throw std::overflow_error("metrics: too many frames");
+        if (!(os == config_.size) || !(ds == config_.size))
+            throw std::invalid_argument("metrics: image size differs from configured size");
+        if (!SameFormat(of, config_.original_format) || !SameFormat(df, config_.distorted_format))
+            throw std::invalid_argument("metrics: image format differs from configured format");
+        if (host && !config_.streaming_inputs)
+            throw std::invalid_argument("metrics: streaming inputs are disabled");
+        try {
+            MetricsResult r;
+            r.frame_index = next_index_;
+            r.ssimulacra2 = compute().Score();
+            ++next_index_;
+            return r;
+        } catch (...) {
+            failed_ = true;
+            throw;
+        }
+    }
+    template <class F>
+    MetricsResult Still(F&& first) {
+        if (failed_) throw std::logic_error("metrics: previous call failed; call Reset");
+        if (finished_) throw std::logic_error("metrics: sequence finished; call Reset");
+        if (next_index_ != 0)
+            throw std::logic_error("metrics: reset the active sequence before ComputeImage");
+        std::optional<MetricsResult> r = first();
+        Reset();
+        return *r;
+    }
+
+    MetricsConfig config_;
+    std::optional<Ssimulacra2Pipeline> pipeline_;
+    std::uint64_t next_index_ = 0;
+    bool failed_ = false;
+    bool finished_ = false;
 };
 
 }  // namespace vqm::cuda

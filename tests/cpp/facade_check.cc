@@ -105,6 +105,42 @@ void Host() {
     bad.scales.resize(1);
     bad.scales[0].avg_ssim[0] = NAN;
     ExpectThrow<std::invalid_argument>([&] { (void)bad.Score(); }, "nonfinite norm");
+
+    v::MetricsConfig none;
+    none.size = {32, 32};
+    ExpectThrow<std::invalid_argument>([&] { v::Metrics m(none); }, "no metric selected");
+}
+
+void GpuMetrics() {
+    v::MetricsConfig mc;
+    mc.size = {32, 32};
+    mc.original_format = mc.distorted_format = Srgb8();
+    mc.ssimulacra2 = v::Ssimulacra2Config{};
+    v::Metrics metrics(mc);
+    const v::Image base = Gradient(0);
+    for (int variant = 0; variant < 3; ++variant) {
+        const auto r = metrics.Compute(base, Gradient(variant));
+        Expect(r.has_value() && r->frame_index == static_cast<std::uint64_t>(variant),
+               "frame index");
+        std::printf("{\"path\": \"metrics\", \"variant\": %d, \"score\": %.17g}\n", variant,
+                    *r->ssimulacra2);
+    }
+    ExpectThrow<std::logic_error>([&] { (void)metrics.ComputeImage(base, base); },
+                                  "ComputeImage inside a sequence");
+    const v::MetricsFinalResult fin = metrics.Finalize();
+    Expect(fin.frames == 3 && !fin.last_frame, "Finalize frames");
+    ExpectThrow<std::logic_error>([&] { (void)metrics.Compute(base, base); },
+                                  "Compute after Finalize");
+    metrics.Reset();
+    const v::MetricsResult still = metrics.ComputeImage(base, Gradient(1));
+    Expect(still.frame_index == 0, "still frame index");
+    std::printf("{\"path\": \"metrics_image\", \"variant\": 1, \"score\": %.17g}\n",
+                *still.ssimulacra2);
+    v::Image grey = Gradient(0);
+    grey.format.family = v::ColorFamily::Grey;
+    grey.data.resize(32 * 32);
+    ExpectThrow<std::invalid_argument>([&] { (void)metrics.Compute(grey, grey); },
+                                       "format differs from configured");
 }
 
 void Gpu() {
@@ -139,7 +175,10 @@ int main(int argc, char** argv) {
     const std::string mode = argc > 1 ? argv[1] : "host";
     try {
         if (mode == "host") Host();
-        else if (mode == "gpu") Gpu();
+        else if (mode == "gpu") {
+            Gpu();
+            GpuMetrics();
+        }
         else {
             std::fprintf(stderr, "usage: facade_check host|gpu\n");
             return 2;

@@ -45,7 +45,8 @@ def test_facade_scores_match_oracle(facade_binary):
     r = subprocess.run([facade_binary, "gpu"], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     results = [json.loads(line) for line in r.stdout.splitlines() if line.startswith("{")]
-    assert [x["path"] for x in results] == ["pipeline"] * 3 + ["uploaded"] + ["pool"] * 3
+    assert [x["path"] for x in results] == (["pipeline"] * 3 + ["uploaded"] + ["pool"] * 3 +
+                                            ["metrics"] * 3 + ["metrics_image"])
     base = helpers.gradient(0)
     expected = {}
     for v in range(3):
@@ -53,9 +54,14 @@ def test_facade_scores_match_oracle(facade_binary):
     # Pool pairs are (base, base), (base, 1), (base, 2).
     for x in results:
         norms, score = expected[x["variant"]]
-        got = np.asarray(x["norms"], dtype=np.float64).reshape(norms.shape)
-        bad = helpers.feature_mismatch(got, norms)
-        assert not bad, (x["path"], x["variant"], bad[:6])
+        if "norms" in x:
+            got = np.asarray(x["norms"], dtype=np.float64).reshape(norms.shape)
+            bad = helpers.feature_mismatch(got, norms)
+            assert not bad, (x["path"], x["variant"], bad[:6])
         assert abs(x["score"] - score) <= helpers.SCORE_TOL, (x["path"], x["score"], score)
+    # The unified facade returns the pipeline's score bit for bit.
+    for k in range(3):
+        assert results[7 + k]["score"] == results[k]["score"]
+    assert results[10]["score"] == results[1]["score"]
     assert results[0]["score"] == 100.0
     assert results[4]["score"] == 100.0
