@@ -7,8 +7,9 @@ workload by timing every compiled variant on it.
 
 The timing is the blur stage's device time from the batch scorer's CUDA
 events (vqm_cu_ss2_batch_stage_ms), median of `repeats` runs after one
-warm-up. Results are cached per device name and size class (the pixel count
-of the largest pair rounded to a power of two) in a JSON file, by default
+warm-up. Results are cached per device name, size class (the pixel count
+of the largest pair rounded to a power of two) and compiled variant list in a
+JSON file, by default
 ~/.cache/vqm_b200/blur_variants.json or $VQM_B200_TUNE_CACHE.
 """
 
@@ -71,7 +72,10 @@ def tune(pairs, repeats: int = 3, use_cache: bool = True, stream: int | None = N
          variants=None) -> TuneResult:
     """Times every blur variant on `pairs` and returns the fastest."""
     shapes = ss2.blur_variants()
-    key = f"{_device_name()}|{_size_class(pairs)}"
+    # The compiled variant list is part of the key: a library with other
+    # variants (or another order) never reuses an index tuned for this one.
+    signature = ";".join(",".join(str(v) for v in shape) for shape in shapes)
+    key = f"{_device_name()}|{_size_class(pairs)}|{signature}"
     if use_cache and variants is None:
         hit = _load().get(key)
         if hit is not None and hit["variant"] < len(shapes):

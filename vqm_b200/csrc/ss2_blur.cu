@@ -7,13 +7,23 @@
 // (scale.comp:149-333): each blurred value is w0*s0 followed by fused
 // ascending taps, horizontal pass first. So the blurred quantities and map
 // values are bit-identical to the CPU checker's FP32 path for bit-identical
-// pyramid planes, whichever kernel variant below computes them.
+// pyramid planes, whichever tile shape below computes them.
 //
-// Variants (kBlurVariants): the scalar kernel (ss2_blur_scalar.cuh), packed
-// kernels that issue Blackwell's two-lane FP32 instructions (FFMA2) with one
-// output tile per CTA, and persistent packed kernels that keep each CTA
-// resident and prefetch its next tile with cp.async while computing the
-// current one.
+// One CTA computes a TW x TH output tile:
+//   1. cp.async copies the (TW+12) x (TH+12) source window of both images in
+//      16-byte chunks (2 columns x 2 rows of the row-pair planes, see
+//      ss2_layout.h); chunks outside the plane are zero-filled, which is the
+//      zero padding of scale.comp:107-124.
+//   2. Horizontal pass: a thread takes one row pair and four output columns
+//      and accumulates both rows at once with Blackwell's two-lane FP32
+//      instructions (FFMA2); the five results go to row-major planes.
+//   3. Vertical pass: a thread takes a column pair and four output rows,
+//      again two lanes per instruction, then evaluates the maps of its eight
+//      pixels and keeps six running sums.
+//   4. The CTA's six sums are combined with two-sum compensation into one
+//      partial per tile; the finalize kernel adds the partials in FP64.
+// A persistent form keeps each CTA resident and copies its next tile's
+// window into a second buffer while it computes the current one.
 
 #include <cuda_runtime.h>
 
@@ -22,6 +32,7 @@
 
 #include "ss2_device.cuh"
 #include "ss2_kernels.h"
+#include "ss2_layout.h"
 
 namespace vqm_b200 {
 namespace {
@@ -49,46 +60,36 @@ __device__ __forceinline__ void TwoSumAdd(float& s, float& c, float s2, float c2
     c = __fadd_rn(__fadd_rn(c, c2), e);
 }
 
-#include "ss2_blur_scalar.cuh"
-
-// ---------------------------------------------------------------------------
-// Packed tiles.
-//
-//   * The source tile is stored as row pairs: element (r, c) of image i at
-//     src[i][r / 2][c].{x: r even, y: r odd}. One 64-bit shared load gives
-//     one column of two rows, so the horizontal pass accumulates rows
-//     (2p, 2p+1) together, four output columns per task.
-//   * The horizontal results go to row-major planes, so the vertical pass
-//     reads columns (c, c+1) as one 64-bit load and accumulates that column
-//     pair over four output rows per task.
-//   * The maps run on the column pair, packed wherever the arithmetic is a
-//     multiply, add or fused multiply-add.
-// ---------------------------------------------------------------------------
-
 template <int TW, int TH, int NT>
-struct PackedTile {
+struct Tile {
     static constexpr int SW = TW + 2 * kRadius;  // source columns
     static constexpr int SH = TH + 2 * kRadius;  // source rows
     static constexpr int RP = SH / 2;            // source row pairs
-    static constexpr int KH = 4;                 // output columns per horizontal task
-    static constexpr int HT = RP * (TW / KH);    // horizontal tasks
-    static constexpr int RV = 4;                 // output rows per vertical task
+    static constexpr int CP = SW / 2;            // 16-byte chunks per source row pair
+    // Floats per source row pair: 2 * SW plus 4 of padding, so that the row
+    // pair stride is 28 banks mod 32 (see HorizontalPass).
+    static constexpr int SRS = 2 * SW + 4;
+    static constexpr int IMG = RP * SRS;  // floats per source image
+    static constexpr int KH = 4;          // output columns per horizontal task
+    static constexpr int NG = TW / KH;    // column groups per row pair
+    static constexpr int HT = RP * NG;    // horizontal tasks
+    static constexpr int RV = 4;          // output rows per vertical task
     static constexpr int VT = (TW / 2) * (TH / RV);
-    static constexpr int kWarps = NT / 32;
-    // One source buffer (both images) and the five horizontal-pass planes.
-    static constexpr size_t kSrcBytes = sizeof(float2) * 2 * RP * SW;
+    static constexpr size_t kSrcBytes = sizeof(float) * 2 * IMG;
     static constexpr size_t kHqBytes = sizeof(float) * 5 * SH * TW;
-    static_assert(TW % KH == 0 && TH % RV == 0 && SH % 2 == 0, "tile shape");
-    static_assert(NT % 32 == 0, "whole warps");
-    static_assert(kSrcBytes % 16 == 0, "plane alignment");
+    static_assert(TW % 32 == 0, "the store swizzle flips 16-float column blocks");
+    static_assert(TH % RV == 0 && RP % 2 == 0 && NG % 4 == 0, "tile shape");
+    static_assert(SRS % 32 == 28, "bank spread of the horizontal loads");
+    static_assert(NT % 32 == 0 && NT >= 96, "whole warps, 16 lanes per sum");
+    static_assert(kSrcBytes >= sizeof(float) * 12 * NT, "the reduction reuses the source buffer");
 };
 
 // Where one output tile's planes, geometry and partial slot are.
 struct TileRef {
     const float* pa;
     const float* pb;
-    size_t pitch;
-    size_t partial;
+    uint32_t pitch;    // floats per row pair
+    uint32_t partial;  // index of the tile's partial
     int w, h, x0, y0;
 };
 
@@ -104,18 +105,18 @@ __device__ __forceinline__ TileRef LocateTile(const DevBatch& batch, uint32_t bl
     t.pitch = P.pitch[seg.level];
     t.w = static_cast<int>(P.w[seg.level]);
     t.h = static_cast<int>(P.h[seg.level]);
-    t.x0 = static_cast<int>((tile % seg.tiles_x) * TW);
-    t.y0 = static_cast<int>((tile / seg.tiles_x) * TH);
-    t.partial = (static_cast<size_t>(seg.partial_first) + tile) * 6;
+    const uint32_t ty = tile / seg.tiles_x;
+    t.x0 = static_cast<int>((tile - ty * seg.tiles_x) * TW);
+    t.y0 = static_cast<int>(ty * TH);
+    t.partial = seg.partial_first + tile;
     return t;
 }
 
-// Asynchronous 4-byte global-to-shared copy; a source size of 0 writes zero
-// and reads nothing (the zero padding of scale.comp:107-124).
-__device__ __forceinline__ void CpAsync4(float* dst, const float* src, bool valid) {
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    const int n = valid ? 4 : 0;
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(src), "r"(n)
+// Asynchronous 16-byte global-to-shared copy; a source size of 0 writes
+// zeros and reads nothing.
+__device__ __forceinline__ void CpAsync16(uint32_t dst, const float* src, bool valid) {
+    const int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(n)
                  : "memory");
 }
 __device__ __forceinline__ void CpAsyncCommit() {
@@ -126,51 +127,60 @@ __device__ __forceinline__ void CpAsyncWait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// Issues the copies of one tile's two source tiles into `buf` (row pairs).
+// Issues the copies of one tile's two source windows into `buf`: chunk
+// (rp, cp) of the window is the 2x2 block at window column 2cp, row 2rp.
 template <int TW, int TH, int NT>
 __device__ __forceinline__ void IssueTileLoads(float* buf, const TileRef& t) {
-    using T = PackedTile<TW, TH, NT>;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float* bufb = buf + 2 * T::RP * T::SW;
-    for (int r = warp; r < T::SH; r += T::kWarps) {
-        const int gy = t.y0 - kRadius + r;
-        const bool iny = gy >= 0 && gy < t.h;
-        const size_t row = iny ? static_cast<size_t>(gy) * t.pitch : 0;
-        const int e0 = (r >> 1) * T::SW * 2 + (r & 1);
-        for (int c = lane; c < T::SW; c += 32) {
-            const int gx = t.x0 - kRadius + c;
-            const bool in = iny && gx >= 0 && gx < t.w;
-            const size_t off = in ? row + static_cast<size_t>(gx) : 0;
-            CpAsync4(buf + e0 + 2 * c, t.pa + off, in);
-            CpAsync4(bufb + e0 + 2 * c, t.pb + off, in);
-        }
+    using T = Tile<TW, TH, NT>;
+    const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(buf));
+    const uint32_t wp = static_cast<uint32_t>(t.w + 1) >> 1;  // chunks per row pair
+    const uint32_t hp = static_cast<uint32_t>(t.h + 1) >> 1;  // row pairs
+    const int cx0 = (t.x0 >> 1) - kRadius / 2, ry0 = (t.y0 >> 1) - kRadius / 2;
+    for (int k = threadIdx.x; k < T::RP * T::CP; k += NT) {
+        const int rp = k / T::CP, cp = k - rp * T::CP;
+        const int gy = ry0 + rp, gx = cx0 + cp;
+        const bool in = static_cast<uint32_t>(gy) < hp && static_cast<uint32_t>(gx) < wp;
+        const uint32_t off = in ? static_cast<uint32_t>(gy) * t.pitch + 4u * static_cast<uint32_t>(gx)
+                                : 0u;
+        const uint32_t dst = base + 4u * static_cast<uint32_t>(rp * T::SRS + 4 * cp);
+        CpAsync16(dst, t.pa + off, in);
+        CpAsync16(dst + 4u * T::IMG, t.pb + off, in);
     }
 }
 
 __device__ __forceinline__ float2 Pack(float v) { return make_float2(v, v); }
 __device__ __forceinline__ float2 Neg(float2 v) { return make_float2(-v.x, -v.y); }
 
-// Horizontal pass (scale.comp:149-207): row pair rp, columns c0..c0+3, all
-// five quantities.
+// Horizontal pass (scale.comp:149-207): row pair rp, output columns
+// c0..c0+3, all five quantities, both rows per instruction.
+//
+// Task -> (rp, column group): within every 8 lanes, lanes 0-3 take four
+// column groups of row pair rp and lanes 4-7 the same groups of rp + 1. The
+// source row pair stride is 28 banks mod 32, so the quarter warp's eight
+// 16-byte loads cover all 32 banks once. The results are stored with the
+// 16-byte column block index XORed with 4 on rows whose (row >> 1) is odd,
+// so the quarter warp's stores (rows 2rp and 2rp + 2) do not collide either.
 template <int TW, int TH, int NT>
-__device__ __forceinline__ void HorizontalPass(const float2* src, float* hq) {
-    using T = PackedTile<TW, TH, NT>;
-    constexpr int SW = T::SW, KH = T::KH;
-    const float2* srca = src;
-    const float2* srcb = src + T::RP * SW;
+__device__ __forceinline__ void HorizontalPass(const float* src, float* hq) {
+    using T = Tile<TW, TH, NT>;
+    constexpr int KH = T::KH;
     for (int task = threadIdx.x; task < T::HT; task += NT) {
-        const int rp = task / (TW / KH);
-        const int c0 = (task % (TW / KH)) * KH;
+        const int cg_lo = task & 3, rp_lo = (task >> 2) & 1, rest = task >> 3;
+        const int cg = (rest % (T::NG / 4)) * 4 + cg_lo;
+        const int rp = (rest / (T::NG / 4)) * 2 + rp_lo;
+        const float* ra = src + rp * T::SRS + 2 * KH * cg;
+        const float* rb = ra + T::IMG;
         float2 A[KH + 12], B[KH + 12];
 #pragma unroll
         for (int j = 0; j < KH + 12; j += 2) {
-            const float4 va = *reinterpret_cast<const float4*>(&srca[rp * SW + c0 + j]);
-            const float4 vb = *reinterpret_cast<const float4*>(&srcb[rp * SW + c0 + j]);
+            const float4 va = *reinterpret_cast<const float4*>(ra + 2 * j);
+            const float4 vb = *reinterpret_cast<const float4*>(rb + 2 * j);
             A[j] = make_float2(va.x, va.y);
             A[j + 1] = make_float2(va.z, va.w);
             B[j] = make_float2(vb.x, vb.y);
             B[j + 1] = make_float2(vb.z, vb.w);
         }
+        float* out = hq + (2 * rp) * TW + ((cg ^ ((rp & 1) << 2)) << 2);
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             float2 S[KH + 12];
@@ -185,49 +195,42 @@ __device__ __forceinline__ void HorizontalPass(const float2* src, float* hq) {
 #pragma unroll
             for (int k = 0; k < KH; ++k) acc[k] = __fmul2_rn(Pack(c_taps[0]), S[k]);
 #pragma unroll
-            for (int t = 1; t < kTaps; ++t) {
-                const float2 wt = Pack(c_taps[t]);
+            for (int tap = 1; tap < kTaps; ++tap) {
+                const float2 wt = Pack(c_taps[tap]);
 #pragma unroll
-                for (int k = 0; k < KH; ++k) acc[k] = __ffma2_rn(wt, S[k + t], acc[k]);
+                for (int k = 0; k < KH; ++k) acc[k] = __ffma2_rn(wt, S[k + tap], acc[k]);
             }
-            float* plane = hq + q * T::SH * TW;
-            *reinterpret_cast<float4*>(&plane[(2 * rp) * TW + c0]) =
-                make_float4(acc[0].x, acc[1].x, acc[2].x, acc[3].x);
-            *reinterpret_cast<float4*>(&plane[(2 * rp + 1) * TW + c0]) =
+            float* plane = out + q * T::SH * TW;
+            *reinterpret_cast<float4*>(plane) = make_float4(acc[0].x, acc[1].x, acc[2].x, acc[3].x);
+            *reinterpret_cast<float4*>(plane + TW) =
                 make_float4(acc[0].y, acc[1].y, acc[2].y, acc[3].y);
         }
     }
 }
 
-// Vertical pass (scale.comp:211-301) on column pairs, the maps
-// (scale.comp:305-333) of each task's eight pixels, and the block's
-// compensated reduction to six partials (scale.comp:395-436, with two-sum
-// compensation in place of the plain ladder). Ends with the partial written
-// and a barrier, so src and hq may be reused afterwards.
-template <int TW, int TH, int NT>
-__device__ __forceinline__ void VerticalMapsReduce(const float2* src, const float* hq,
-                                                   const TileRef& t, double* partials,
-                                                   float (*red)[12]) {
-    using T = PackedTile<TW, TH, NT>;
-    constexpr int SW = T::SW, RV = T::RV;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const float2* srca = src;
-    const float2* srcb = src + T::RP * SW;
-    float2 sum[6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) sum[k] = make_float2(0.0f, 0.0f);
-
-    for (int task = tid; task < T::VT; task += NT) {
+// Vertical pass (scale.comp:211-301) on column pairs and the maps
+// (scale.comp:305-333) of each task's eight pixels, added into `sum`. With
+// kEdge, pixels outside the level contribute 0 (their inputs are the zero
+// padding, so every map value is finite before it is dropped).
+template <int TW, int TH, int NT, bool kEdge>
+__device__ __forceinline__ void VerticalMaps(const float* src, const float* hq, const TileRef& t,
+                                             float2 (&sum)[6]) {
+    using T = Tile<TW, TH, NT>;
+    constexpr int RV = T::RV;
+    for (int task = threadIdx.x; task < T::VT; task += NT) {
         const int c = (task % (TW / 2)) * 2;
         const int r0 = (task / (TW / 2)) * RV;
+        // Row r0 + i holds column c at c ^ 16 when ((r0 + i) >> 1) is odd,
+        // i.e. when (i >> 1) is odd, r0 being a multiple of 4.
+        const int cols[2] = {c, c ^ 16};
         float2 V[5][RV];
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
-            const float* plane = hq + q * T::SH * TW;
+            const float* plane = hq + q * T::SH * TW + r0 * TW;
             float2 M[RV + 12];
 #pragma unroll
             for (int i = 0; i < RV + 12; ++i)
-                M[i] = *reinterpret_cast<const float2*>(&plane[(r0 + i) * TW + c]);
+                M[i] = *reinterpret_cast<const float2*>(plane + i * TW + cols[(i >> 1) & 1]);
 #pragma unroll
             for (int j = 0; j < RV; ++j) {
                 float2 acc = __fmul2_rn(Pack(c_taps[0]), M[j]);
@@ -236,12 +239,18 @@ __device__ __forceinline__ void VerticalMapsReduce(const float2* src, const floa
                 V[q][j] = acc;
             }
         }
+        // The raw values of rows r0 + 6 .. r0 + 9, columns c + 6 and c + 7:
+        // one 16-byte load per row pair and image.
+        float4 raw1[RV / 2], raw2[RV / 2];
+#pragma unroll
+        for (int p = 0; p < RV / 2; ++p) {
+            const float* at = src + ((r0 + kRadius) / 2 + p) * T::SRS + 2 * (c + kRadius);
+            raw1[p] = *reinterpret_cast<const float4*>(at);
+            raw2[p] = *reinterpret_cast<const float4*>(at + T::IMG);
+        }
         const int out_x = t.x0 + c;
 #pragma unroll
         for (int j = 0; j < RV; ++j) {
-            const int out_y = t.y0 + r0 + j;
-            if (out_y >= t.h || out_x >= t.w) continue;
-            const bool second = out_x + 1 < t.w;
             const float2 mu1 = V[0][j], mu2 = V[1][j];
             const float2 dm = __fadd2_rn(mu1, Neg(mu2));
             const float2 num_m = __ffma2_rn(Neg(dm), dm, Pack(1.0f));
@@ -251,18 +260,11 @@ __device__ __forceinline__ void VerticalMapsReduce(const float2* src, const floa
                 __fadd2_rn(__ffma2_rn(Neg(mu1), mu1, V[2][j]), __ffma2_rn(Neg(mu2), mu2, V[3][j])),
                 Pack(0.0009f));
             const float2 numer = __ffma2_rn(Neg(num_m), num_s, denom);
-            float2 d;
-            d.x = fmaxf(__fdiv_rn(numer.x, denom.x), 0.0f);
-            d.y = second ? fmaxf(__fdiv_rn(numer.y, denom.y), 0.0f) : 0.0f;
-            const float2 dd = __fmul2_rn(d, d);
-            // The raw XYB values are the centre of the source tile.
-            const int rr = r0 + j + kRadius;
-            const float2 s1a = srca[(rr >> 1) * SW + c + kRadius];
-            const float2 s1b = srca[(rr >> 1) * SW + c + kRadius + 1];
-            const float2 s2a = srcb[(rr >> 1) * SW + c + kRadius];
-            const float2 s2b = srcb[(rr >> 1) * SW + c + kRadius + 1];
-            const float2 img1 = (rr & 1) ? make_float2(s1a.y, s1b.y) : make_float2(s1a.x, s1b.x);
-            const float2 img2 = (rr & 1) ? make_float2(s2a.y, s2b.y) : make_float2(s2a.x, s2b.x);
+            float2 d = make_float2(fmaxf(__fdiv_rn(numer.x, denom.x), 0.0f),
+                                   fmaxf(__fdiv_rn(numer.y, denom.y), 0.0f));
+            const float4 r1 = raw1[j >> 1], r2v = raw2[j >> 1];
+            const float2 img1 = (j & 1) ? make_float2(r1.y, r1.w) : make_float2(r1.x, r1.z);
+            const float2 img2 = (j & 1) ? make_float2(r2v.y, r2v.w) : make_float2(r2v.x, r2v.z);
             float2 e2 = __fadd2_rn(img2, Neg(mu2));
             float2 e1 = __fadd2_rn(img1, Neg(mu1));
             e2 = make_float2(fabsf(e2.x), fabsf(e2.y));
@@ -270,79 +272,102 @@ __device__ __forceinline__ void VerticalMapsReduce(const float2* src, const floa
             const float2 dist = __fadd2_rn(Pack(1.0f), e2);
             const float2 orig = __fadd2_rn(Pack(1.0f), e1);
             const float2 diff = __fadd2_rn(dist, Neg(orig));
-            float2 d1;
-            d1.x = __fdiv_rn(diff.x, orig.x);
-            d1.y = second ? __fdiv_rn(diff.y, orig.y) : 0.0f;
-            const float2 ring = make_float2(fmaxf(d1.x, 0.0f), fmaxf(d1.y, 0.0f));
-            const float2 blur = make_float2(fmaxf(-d1.x, 0.0f), fmaxf(-d1.y, 0.0f));
-            const float2 r2 = __fmul2_rn(ring, ring), b2 = __fmul2_rn(blur, blur);
+            const float2 d1 = make_float2(__fdiv_rn(diff.x, orig.x), __fdiv_rn(diff.y, orig.y));
+            float2 ring = make_float2(fmaxf(d1.x, 0.0f), fmaxf(d1.y, 0.0f));
+            float2 blur = make_float2(fmaxf(-d1.x, 0.0f), fmaxf(-d1.y, 0.0f));
+            if (kEdge) {
+                const bool vy = t.y0 + r0 + j < t.h;
+                const bool v0 = vy && out_x < t.w, v1 = vy && out_x + 1 < t.w;
+                d = make_float2(v0 ? d.x : 0.0f, v1 ? d.y : 0.0f);
+                ring = make_float2(v0 ? ring.x : 0.0f, v1 ? ring.y : 0.0f);
+                blur = make_float2(v0 ? blur.x : 0.0f, v1 ? blur.y : 0.0f);
+            }
+            const float2 dd = __fmul2_rn(d, d);
+            const float2 rr = __fmul2_rn(ring, ring), bb = __fmul2_rn(blur, blur);
             sum[0] = __fadd2_rn(sum[0], d);
             sum[1] = __fadd2_rn(sum[1], __fmul2_rn(dd, dd));
             sum[2] = __fadd2_rn(sum[2], ring);
-            sum[3] = __fadd2_rn(sum[3], __fmul2_rn(r2, r2));
+            sum[3] = __fadd2_rn(sum[3], __fmul2_rn(rr, rr));
             sum[4] = __fadd2_rn(sum[4], blur);
-            sum[5] = __fadd2_rn(sum[5], __fmul2_rn(b2, b2));
+            sum[5] = __fadd2_rn(sum[5], __fmul2_rn(bb, bb));
         }
     }
+}
 
-    float s[6], comp[6];
+// The CTA's six sums as one compensated partial each (scale.comp:395-436,
+// with two-sum compensation in place of the plain ladder): every thread
+// folds its two lanes, 16 lanes per sum add the block's values, and a
+// 16-lane butterfly finishes. `red` (12 * NT floats) may alias the source
+// buffer once every thread is past its last read of it. Ends with a barrier.
+template <int NT>
+__device__ __forceinline__ void ReducePartials(const float2 (&sum)[6], float* red, double* out) {
+    const int tid = threadIdx.x;
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-        s[k] = sum[k].x;
-        comp[k] = 0.0f;
-        TwoSumAdd(s[k], comp[k], sum[k].y, 0.0f);
+        float s = sum[k].x, c = 0.0f;
+        TwoSumAdd(s, c, sum[k].y, 0.0f);
+        red[(2 * k) * NT + tid] = s;
+        red[(2 * k + 1) * NT + tid] = c;
     }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const float s2 = __shfl_xor_sync(0xffffffffu, s[k], off);
-            const float c2 = __shfl_xor_sync(0xffffffffu, comp[k], off);
-            TwoSumAdd(s[k], comp[k], s2, c2);
-        }
-    if (lane == 0)
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            red[warp][k] = s[k];
-            red[warp][6 + k] = comp[k];
-        }
     __syncthreads();
-    if (tid < 6) {
-        float a = red[0][tid], cc = red[0][6 + tid];
-        for (int wi = 1; wi < T::kWarps; ++wi) TwoSumAdd(a, cc, red[wi][tid], red[wi][6 + tid]);
-        partials[t.partial + tid] = static_cast<double>(a) + static_cast<double>(cc);
+    if (tid < 96) {  // warps 0-2, whole
+        const int k = tid >> 4, i = tid & 15;
+        float s = red[(2 * k) * NT + i], c = red[(2 * k + 1) * NT + i];
+#pragma unroll
+        for (int j = i + 16; j < NT; j += 16)
+            TwoSumAdd(s, c, red[(2 * k) * NT + j], red[(2 * k + 1) * NT + j]);
+#pragma unroll
+        for (int off = 8; off > 0; off >>= 1) {
+            const float s2 = __shfl_xor_sync(0xffffffffu, s, off);
+            const float c2 = __shfl_xor_sync(0xffffffffu, c, off);
+            TwoSumAdd(s, c, s2, c2);
+        }
+        if (i == 0) out[k] = static_cast<double>(s) + static_cast<double>(c);
     }
     __syncthreads();
 }
 
-// One output tile per CTA.
 template <int TW, int TH, int NT>
-__global__ void __launch_bounds__(NT) Ss2Blur2Kernel(DevBatch batch) {
-    using T = PackedTile<TW, TH, NT>;
+__device__ __forceinline__ void ComputeTile(float* src, float* hq, const TileRef& t,
+                                            double* partials) {
+    HorizontalPass<TW, TH, NT>(src, hq);
+    __syncthreads();
+    float2 sum[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) sum[k] = make_float2(0.0f, 0.0f);
+    if (t.x0 + TW <= t.w && t.y0 + TH <= t.h)
+        VerticalMaps<TW, TH, NT, false>(src, hq, t, sum);
+    else
+        VerticalMaps<TW, TH, NT, true>(src, hq, t, sum);
+    __syncthreads();  // the reduction overwrites the source window
+    ReducePartials<NT>(sum, src, partials + static_cast<size_t>(t.partial) * 6);
+}
+
+// One output tile per CTA; MB CTAs per SM is the occupancy the shared
+// memory allows, which bounds the registers per thread.
+template <int TW, int TH, int NT, int MB>
+__global__ void __launch_bounds__(NT, MB) Ss2BlurKernel(DevBatch batch) {
+    using T = Tile<TW, TH, NT>;
     extern __shared__ __align__(16) unsigned char smem[];
     float* src = reinterpret_cast<float*>(smem);
     float* hq = reinterpret_cast<float*>(smem + T::kSrcBytes);
-    __shared__ float red[T::kWarps][12];
     const TileRef t = LocateTile<TW, TH>(batch, blockIdx.x);
     IssueTileLoads<TW, TH, NT>(src, t);
     CpAsyncCommit();
     CpAsyncWait<0>();
     __syncthreads();
-    HorizontalPass<TW, TH, NT>(reinterpret_cast<const float2*>(src), hq);
-    __syncthreads();
-    VerticalMapsReduce<TW, TH, NT>(reinterpret_cast<const float2*>(src), hq, t, batch.partials, red);
+    ComputeTile<TW, TH, NT>(src, hq, t, batch.partials);
 }
 
 // Persistent: each CTA walks tiles blockIdx.x, + gridDim.x, ... and copies
-// tile i+1's sources into its second buffer while it computes tile i.
-template <int TW, int TH, int NT>
-__global__ void __launch_bounds__(NT) Ss2Blur3Kernel(DevBatch batch) {
-    using T = PackedTile<TW, TH, NT>;
+// tile i+1's window into its second buffer while it computes tile i.
+template <int TW, int TH, int NT, int MB>
+__global__ void __launch_bounds__(NT, MB) Ss2BlurPersistentKernel(DevBatch batch) {
+    using T = Tile<TW, TH, NT>;
     extern __shared__ __align__(16) unsigned char smem[];
     float* const buf0 = reinterpret_cast<float*>(smem);
     constexpr int kBufFloats = static_cast<int>(T::kSrcBytes / sizeof(float));
     float* hq = reinterpret_cast<float*>(smem + 2 * T::kSrcBytes);
-    __shared__ float red[T::kWarps][12];
     const uint32_t total = batch.blur_blocks;
     uint32_t tile = blockIdx.x;
     if (tile >= total) return;
@@ -358,27 +383,24 @@ __global__ void __launch_bounds__(NT) Ss2Blur3Kernel(DevBatch batch) {
             nxt = LocateTile<TW, TH>(batch, next);
             IssueTileLoads<TW, TH, NT>(buf0 + (b ^ 1) * kBufFloats, nxt);
         }
-        CpAsyncCommit();    // possibly empty, so the group count stays uniform
-        CpAsyncWait<1>();   // everything but the newest group: this tile's
+        CpAsyncCommit();   // possibly empty, so the group count stays uniform
+        CpAsyncWait<1>();  // everything but the newest group: this tile's
         __syncthreads();
-        HorizontalPass<TW, TH, NT>(reinterpret_cast<const float2*>(now), hq);
-        __syncthreads();
-        VerticalMapsReduce<TW, TH, NT>(reinterpret_cast<const float2*>(now), hq, cur,
-                                       batch.partials, red);
+        ComputeTile<TW, TH, NT>(now, hq, cur, batch.partials);
         cur = nxt;
         b ^= 1;
     }
     CpAsyncWait<0>();
 }
 
-// The variants compiled in: {tile width, tile height, threads, kind};
-// kind 0 scalar, 1 packed, 2 persistent packed.
+// The variants compiled in: {tile width, tile height, threads, persistent,
+// CTAs per SM}.
 struct BlurVariant {
-    int w, h, threads, kind;
+    int w, h, threads, persistent, per_sm;
 };
 constexpr BlurVariant kBlurVariants[] = {
-    {32, 32, 256, 0}, {32, 32, 128, 1}, {64, 32, 256, 1}, {32, 52, 128, 1},
-    {64, 20, 256, 1}, {32, 32, 128, 2}, {64, 32, 256, 2}, {32, 20, 128, 2},
+    {32, 32, 128, 0, 5}, {32, 28, 128, 0, 5}, {64, 32, 256, 0, 2}, {64, 20, 256, 0, 3},
+    {32, 32, 128, 1, 3}, {32, 20, 128, 1, 5}, {64, 32, 256, 1, 1},
 };
 constexpr int kBlurVariantCount = sizeof(kBlurVariants) / sizeof(kBlurVariants[0]);
 
@@ -400,6 +422,11 @@ cudaError_t Prepare(Kernel kernel, size_t smem, LaunchCache& cache, int threads,
         e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem));
         if (e != cudaSuccess) return e;
+        // All of the unified L1/shared storage as shared memory: the tiles
+        // are staged explicitly and nothing here relies on L1 hits.
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 static_cast<int>(cudaSharedmemCarveoutMaxShared));
+        if (e != cudaSuccess) return e;
         if (persistent) {
             int per_sm = 0, sms = 0;
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
@@ -414,28 +441,30 @@ cudaError_t Prepare(Kernel kernel, size_t smem, LaunchCache& cache, int threads,
     return cudaSuccess;
 }
 
-template <int TW, int TH, int NT>
-cudaError_t LaunchPacked(const DevBatch& b, cudaStream_t stream) {
-    using T = PackedTile<TW, TH, NT>;
+template <int TW, int TH, int NT, int MB>
+cudaError_t LaunchTiles(const DevBatch& b, cudaStream_t stream) {
+    using T = Tile<TW, TH, NT>;
     static LaunchCache cache;
     constexpr size_t smem = T::kSrcBytes + T::kHqBytes;
-    const cudaError_t e = Prepare(Ss2Blur2Kernel<TW, TH, NT>, smem, cache, NT, false, nullptr);
+    const cudaError_t e =
+        Prepare(Ss2BlurKernel<TW, TH, NT, MB>, smem, cache, NT, false, nullptr);
     if (e != cudaSuccess) return e;
-    Ss2Blur2Kernel<TW, TH, NT><<<b.blur_blocks, NT, smem, stream>>>(b);
+    Ss2BlurKernel<TW, TH, NT, MB><<<b.blur_blocks, NT, smem, stream>>>(b);
     return cudaGetLastError();
 }
 
-template <int TW, int TH, int NT>
+template <int TW, int TH, int NT, int MB>
 cudaError_t LaunchPersistent(const DevBatch& b, cudaStream_t stream) {
-    using T = PackedTile<TW, TH, NT>;
+    using T = Tile<TW, TH, NT>;
     static LaunchCache cache;
     constexpr size_t smem = 2 * T::kSrcBytes + T::kHqBytes;
     int grid = 0;
-    const cudaError_t e = Prepare(Ss2Blur3Kernel<TW, TH, NT>, smem, cache, NT, true, &grid);
+    const cudaError_t e =
+        Prepare(Ss2BlurPersistentKernel<TW, TH, NT, MB>, smem, cache, NT, true, &grid);
     if (e != cudaSuccess) return e;
     const uint32_t blocks = b.blur_blocks < static_cast<uint32_t>(grid) ? b.blur_blocks
                                                                         : static_cast<uint32_t>(grid);
-    Ss2Blur3Kernel<TW, TH, NT><<<blocks, NT, smem, stream>>>(b);
+    Ss2BlurPersistentKernel<TW, TH, NT, MB><<<blocks, NT, smem, stream>>>(b);
     return cudaGetLastError();
 }
 
@@ -450,16 +479,13 @@ cudaError_t SetConstants(const float* taps13, const double* weights108) {
 cudaError_t LaunchBlur(const DevBatch& b, int variant, cudaStream_t stream) {
     if (b.blur_blocks == 0) return cudaSuccess;
     switch (variant) {
-        case 0:
-            Ss2BlurKernel<32, 32><<<b.blur_blocks, 256, 0, stream>>>(b);
-            return cudaGetLastError();
-        case 1: return LaunchPacked<32, 32, 128>(b, stream);
-        case 2: return LaunchPacked<64, 32, 256>(b, stream);
-        case 3: return LaunchPacked<32, 52, 128>(b, stream);
-        case 4: return LaunchPacked<64, 20, 256>(b, stream);
-        case 5: return LaunchPersistent<32, 32, 128>(b, stream);
-        case 6: return LaunchPersistent<64, 32, 256>(b, stream);
-        case 7: return LaunchPersistent<32, 20, 128>(b, stream);
+        case 0: return LaunchTiles<32, 32, 128, 5>(b, stream);
+        case 1: return LaunchTiles<32, 28, 128, 5>(b, stream);
+        case 2: return LaunchTiles<64, 32, 256, 2>(b, stream);
+        case 3: return LaunchTiles<64, 20, 256, 3>(b, stream);
+        case 4: return LaunchPersistent<32, 32, 128, 3>(b, stream);
+        case 5: return LaunchPersistent<32, 20, 128, 5>(b, stream);
+        case 6: return LaunchPersistent<64, 32, 256, 1>(b, stream);
     }
     return cudaErrorInvalidValue;
 }

@@ -12,7 +12,8 @@
 // evaluate these same functions, so the pyramid planes agree bit for bit.
 //
 // Accuracy (checked by tests/test_detmath.py against double-precision libm):
-// every function evaluates in double with relative error below 1e-13 and
+// every function reaches a relative error below ~3e-13 (pow, exp and sin in
+// double; the cube root in single precision with an exact residual) and
 // rounds once to float, so the float result is the correctly rounded value
 // except in the rare cases where the exact value lies within that error of a
 // rounding boundary.
@@ -97,18 +98,32 @@ SS2_DM double pow2i(int n) {
     return from_bits64(static_cast<uint64_t>(n + 1023) << 52);
 }
 
-// Cube root of x >= 0, evaluated as x * r^2 with r = x^(-1/3): a bit-level
-// seed, three single-precision Newton steps on r (each roughly squares the
-// relative error: 0.04 -> 3e-3 -> 2e-5 -> ~1e-7) and one double-precision
-// step (-> ~1e-13). Returns 0 for x <= 0 and x for infinities and NaN.
+// Cube root of x >= 0, in single precision only:
+//   1. r = x^(-1/3) from a bit-level seed and three Newton steps (each
+//      roughly squares the relative error: 0.04 -> 3e-3 -> 2e-5 -> ~1e-7);
+//   2. y0 = x * r^2, within a few ulps of cbrt(x);
+//   3. one Newton step on the root, y = y0 + (x - y0^3) / (3 y0^2), whose
+//      residual x - y0^3 is formed without rounding error that matters:
+//      y0^3 = hi3 + lo3 by fused-multiply-add error-free products (the
+//      TwoProduct of Ogita, Rump and Oishi, "Accurate sum and dot product",
+//      SIAM J. Sci. Comput. 26(6), 2005), and x - hi3 is exact (Sterbenz).
+//      1 / (3 y0^2) is taken as r^2 / 3, and the step is applied with one
+//      rounding (a fused multiply-add).
+// The result is cbrt(x) with relative error below ~3e-13 before its single
+// rounding, so it is the correctly rounded float except when cbrt(x) lies
+// within that distance of a rounding boundary. Inputs outside [1e-20, 1e30]
+// are scaled by 2^-90 or 2^90 first (cbrt(x 2^3k) = cbrt(x) 2^k, exact), which
+// keeps every partial product above single precision's normal range. Returns
+// 0 for x <= 0 and x for infinities and NaN.
 SS2_DM float cbrt(float x) {
     if (!(x > 0.0f) || !(x < 3.402823466e38f)) return x > 0.0f ? x : 0.0f;
-    // Bring subnormal and tiny inputs into the normal range: cbrt(x * 2^90) =
-    // cbrt(x) * 2^30.
     float scale = 1.0f;
-    if (x < 1.0e-30f) {
+    if (x < 1.0e-20f) {
         x = x * 1.237940039285380274899e27f;  // 2^90
         scale = 9.313225746154785156e-10f;    // 2^-30
+    } else if (x > 1.0e30f) {
+        x = x * 8.077935669463160887e-28f;  // 2^-90
+        scale = 1073741824.0f;              // 2^30
     }
     // x^(-1/3) seed from the exponent and mantissa bits (log-linear).
     const uint32_t i = bits(x);
@@ -119,11 +134,14 @@ SS2_DM float cbrt(float x) {
         const float t = fmaf_(-x, r3, 1.0f);
         r = fmaf_(r * t, third, r);
     }
-    const double xd = static_cast<double>(x);
-    double rd = static_cast<double>(r);
-    const double t = fmad(-xd, rd * rd * rd, 1.0);
-    rd = fmad(rd * t, 0.33333333333333331483, rd);
-    return static_cast<float>(xd * rd * rd) * scale;
+    const float rr = r * r;
+    const float y0 = x * rr;
+    const float hi = y0 * y0;
+    const float lo = fmaf_(y0, y0, -hi);                  // y0^2 = hi + lo exactly
+    const float hi3 = hi * y0;
+    const float lo3 = fmaf_(lo, y0, fmaf_(hi, y0, -hi3));  // y0^3 = hi3 + lo3
+    const float e = (x - hi3) - lo3;
+    return fmaf_(e, rr * third, y0) * scale;
 }
 
 // log2 of a finite x > 0 in double: x = m 2^e with m in [sqrt(1/2), sqrt(2)),

@@ -5,8 +5,8 @@
 // one-pair call is a batch of one. Work is flattened into three launch
 // spaces so that every kernel covers every pair of the batch in one grid:
 //
-//   prepare  one CTA per (pair, image, 32x32 base tile): decode, linear RGB,
-//            XYB, and the whole 6-level 2x2 box pyramid of that tile
+//   prepare  one CTA per (pair, image, 64x64 base tile): decode, linear RGB,
+//            XYB, and the whole 2x2 box pyramid of that tile
 //            (reference: src/metrics/ssimulacra2/shaders/prepare.comp).
 //   blur     one CTA per (pair, level, kept channel, output tile): the five
 //            13-tap blurs, the SSIM' and edge maps and the six norm partials
@@ -17,8 +17,8 @@
 //            (reference: shaders/reduce.comp, vulkan.cc:545-583 ReadResult,
 //            score.cc:118-163 Score).
 //
-// Pyramid planes are FP32, row pitch a multiple of 32 floats (128 bytes), so
-// every row starts on a 128-byte boundary and float4 accesses are aligned.
+// Pyramid planes are FP32 in row pairs (ss2_layout.h): rows 2p and 2p + 1
+// interleaved column by column, each row pair on a 256-byte boundary.
 #pragma once
 
 #include <cstdint>
@@ -77,7 +77,7 @@ struct DevPair {
     uint64_t plane_off[kMaxLevels][kChannels];
     uint64_t image_stride;
     float* pyramid;
-    uint32_t prep_tiles_x, prep_tiles_y;  // 32x32 base tiles per image
+    uint32_t prep_tiles_x, prep_tiles_y;  // kPrepTile-square base tiles per image
     uint32_t seg_first, seg_count;        // this pair's blur segments
     double* result;                       // kResultDoubles per pair
 };

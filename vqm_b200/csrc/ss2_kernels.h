@@ -24,6 +24,6 @@ int BlurTileCount();
 void BlurTileShape(int index, int* w, int* h);
 int BlurTileThreads(int index);
 // The variant used when a caller does not choose one.
-constexpr int kDefaultBlurVariant = 1;
+constexpr int kDefaultBlurVariant = 0;
 
 }  // namespace vqm_b200

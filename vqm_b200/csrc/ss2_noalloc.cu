@@ -41,6 +41,7 @@
 #include "ss2_device.cuh"
 #include "ss2_host.h"
 #include "ss2_kernels.h"
+#include "ss2_layout.h"
 
 namespace vqm_b200 {
 namespace {
@@ -156,12 +157,12 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
     for (int l = 0; l < plan.count; ++l) {
         P.w[l] = plan.w[l];
         P.h[l] = plan.h[l];
-        P.pitch[l] = static_cast<uint32_t>(Align(plan.w[l], 32));
+        P.pitch[l] = RowPairPitch(plan.w[l]);
         P.mask[l] = plan.mask[l];
         for (int c = 0; c < 3; ++c) {
             if (!(plan.mask[l] & (1u << c))) continue;
             P.plane_off[l][c] = floats;
-            floats += static_cast<size_t>(P.pitch[l]) * plan.h[l];
+            floats += PlaneFloats(plan.w[l], plan.h[l]);
             DevSegment& s = t.seg[nseg];
             s.pair = 0;
             s.level = static_cast<uint32_t>(l);
@@ -175,8 +176,8 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
         }
     }
     P.image_stride = floats;
-    P.prep_tiles_x = (((o->width + 1) / 2) + 15) / 16;
-    P.prep_tiles_y = (((o->height + 1) / 2) + 15) / 16;
+    P.prep_tiles_x = PrepTiles(o->width);
+    P.prep_tiles_y = PrepTiles(o->height);
     P.seg_first = 0;
     P.seg_count = nseg;
 

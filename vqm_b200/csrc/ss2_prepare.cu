@@ -1,18 +1,23 @@
 // Prepare stage for sm_100a: decode -> linear Rec.709 -> XYB -> the whole
-// 2x2-box pyramid of one image's 32x32 base tile, per CTA
+// 2x2-box pyramid of one image's 64x64 base tile, per CTA
 // (reference: src/metrics/ssimulacra2/shaders/prepare.comp).
 //
-// A CTA is 256 threads; thread (tx, ty) owns the base 2x2 block
-// (gx*16 + tx, gy*16 + ty). Levels 0 and 1 come from the thread's own four
-// samples; levels 2.. pass the previous level's tile through a shared-memory
-// ladder, two buffers alternating so each level costs one barrier. Because
-// the 2x2 box nests exactly, no CTA ever needs a neighbour's samples.
+// A CTA is 256 threads over the tile's 32x32 base 2x2 blocks: thread
+// (tx, ty) = (t & 15, t >> 4) owns blocks (2tx + hx, ty + 16vy), hx, vy in
+// {0, 1}, i.e. four base pixels in a row of two rows, twice. Levels 0 and 1
+// come from the thread's own samples; level 1 goes through a shared-memory
+// ladder from which levels 2.. are averaged, each level with a barrier among
+// the threads it still needs. Because the 2x2 box nests exactly, no CTA ever
+// needs a neighbour's samples.
 //
 // Two specialisations: 8-bit grey/RGB without alpha decode through the
-// image's 256-entry table in shared memory; every other format runs the
-// generic decode of ss2_decode.cuh. The cube root of the XYB transform is the
-// shared deterministic one (ss2_detmath.h), so the planes this kernel writes
-// are bit-identical to the CPU checker's.
+// image's 256-entry table in shared memory, reading four samples of a row
+// with one 32-bit load where the planes allow it; every other format runs
+// the generic decode of ss2_decode.cuh. The XYB transform of two pixels runs
+// on Blackwell's two-lane FP32 instructions, and its cube root is the shared
+// deterministic one (ss2_detmath.h) evaluated lane by lane with the same
+// operations, so the planes this kernel writes are bit-identical to the CPU
+// checker's.
 
 #include <cuda_runtime.h>
 
@@ -23,11 +28,13 @@
 #include "ss2_detmath.h"
 #include "ss2_device.cuh"
 #include "ss2_kernels.h"
+#include "ss2_layout.h"
 
 namespace vqm_b200 {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr uint32_t kBlocks = kPrepTile / 2;  // base 2x2 blocks per tile side
 
 // The last prefix entry <= index (start[0] == 0 <= index < start[count]).
 __device__ __forceinline__ uint32_t FindSlot(const uint32_t* __restrict__ start, uint32_t count,
@@ -49,25 +56,67 @@ constexpr float kM22 = static_cast<float>(1.0 - 0.24342268924547819 - 0.20476744
 constexpr float kBias = 0.0037930732552754493f;
 constexpr float kCbrtBias = 0.15595419704914093f;
 
-// prepare.comp:81-98. Only the channels in `mask` are produced; B's cube
-// root is skipped when B is not stored.
-__device__ __forceinline__ void Xyb(float r, float g, float b, uint32_t mask, float out[3]) {
-    float m0 = __fmaf_rn(kM00, r, __fmaf_rn(kM01, g, __fmaf_rn(kM02, b, kBias)));
-    float m1 = __fmaf_rn(kM10, r, __fmaf_rn(kM11, g, __fmaf_rn(kM12, b, kBias)));
-    m0 = fmaxf(m0, 0.0f);
-    m1 = fmaxf(m1, 0.0f);
-    const float c0 = __fsub_rn(ss2dm::cbrt(m0), kCbrtBias);
-    const float c1 = __fsub_rn(ss2dm::cbrt(m1), kCbrtBias);
-    const float sum = __fadd_rn(c0, c1);
-    out[0] = __fmaf_rn(__fmul_rn(0.5f, __fsub_rn(c0, c1)), 14.0f, 0.42f);
-    out[1] = __fmaf_rn(0.5f, sum, 0.01f);
-    out[2] = 0.0f;
-    if (mask & 4u) {
-        float m2 = __fmaf_rn(kM20, r, __fmaf_rn(kM21, g, __fmaf_rn(kM22, b, kBias)));
-        m2 = fmaxf(m2, 0.0f);
-        const float c2 = __fsub_rn(ss2dm::cbrt(m2), kCbrtBias);
-        out[2] = __fadd_rn(__fmaf_rn(-0.5f, sum, c2), 0.55f);
+__device__ __forceinline__ float2 Pack(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 Neg(float2 v) { return make_float2(-v.x, -v.y); }
+
+// ss2dm::cbrt of both lanes. For lanes in [1e-20, 1e30] (all that an XYB
+// mix of in-gamut light produces: the mix includes a bias of 0.0038) the
+// function takes its unscaled path, executed here with the same operations in
+// the same order two lanes at a time; any other lane pair calls it per lane.
+__device__ __forceinline__ float2 Cbrt2(float2 x) {
+    if (!(x.x >= 1.0e-20f && x.x <= 1.0e30f && x.y >= 1.0e-20f && x.y <= 1.0e30f))
+        return make_float2(ss2dm::cbrt(x.x), ss2dm::cbrt(x.y));
+    float2 r = make_float2(__uint_as_float(0x54a21d2au - __float_as_uint(x.x) / 3u),
+                           __uint_as_float(0x54a21d2au - __float_as_uint(x.y) / 3u));
+    const float2 third = Pack(0.333333343267440796f);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float2 r3 = __fmul2_rn(__fmul2_rn(r, r), r);
+        const float2 t = __ffma2_rn(Neg(x), r3, Pack(1.0f));
+        r = __ffma2_rn(__fmul2_rn(r, t), third, r);
     }
+    const float2 rr = __fmul2_rn(r, r);
+    const float2 y0 = __fmul2_rn(x, rr);
+    const float2 hi = __fmul2_rn(y0, y0);
+    const float2 lo = __ffma2_rn(y0, y0, Neg(hi));
+    const float2 hi3 = __fmul2_rn(hi, y0);
+    const float2 lo3 = __ffma2_rn(lo, y0, __ffma2_rn(hi, y0, Neg(hi3)));
+    const float2 e = __fadd2_rn(__fadd2_rn(x, Neg(hi3)), Neg(lo3));
+    return __ffma2_rn(e, __fmul2_rn(rr, third), y0);
+}
+
+__device__ __forceinline__ float2 Max0(float2 v) {
+    return make_float2(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f));
+}
+
+// prepare.comp:81-98 for two pixels. Only the channels in `mask` are
+// meaningful; B's cube root is skipped when B is not stored.
+__device__ __forceinline__ void Xyb2(float2 r, float2 g, float2 b, uint32_t mask, float2 out[3]) {
+    const float2 m0 = Max0(__ffma2_rn(Pack(kM00), r,
+                                      __ffma2_rn(Pack(kM01), g, __ffma2_rn(Pack(kM02), b, Pack(kBias)))));
+    const float2 m1 = Max0(__ffma2_rn(Pack(kM10), r,
+                                      __ffma2_rn(Pack(kM11), g, __ffma2_rn(Pack(kM12), b, Pack(kBias)))));
+    const float2 c0 = __fadd2_rn(Cbrt2(m0), Pack(-kCbrtBias));
+    const float2 c1 = __fadd2_rn(Cbrt2(m1), Pack(-kCbrtBias));
+    const float2 sum = __fadd2_rn(c0, c1);
+    out[0] = __ffma2_rn(__fmul2_rn(Pack(0.5f), __fadd2_rn(c0, Neg(c1))), Pack(14.0f), Pack(0.42f));
+    out[1] = __ffma2_rn(Pack(0.5f), sum, Pack(0.01f));
+    out[2] = Pack(0.0f);
+    if (mask & 4u) {
+        const float2 m2 = Max0(__ffma2_rn(
+            Pack(kM20), r, __ffma2_rn(Pack(kM21), g, __ffma2_rn(Pack(kM22), b, Pack(kBias)))));
+        const float2 c2 = __fadd2_rn(Cbrt2(m2), Pack(-kCbrtBias));
+        out[2] = __fadd2_rn(__ffma2_rn(Pack(-0.5f), sum, c2), Pack(0.55f));
+    }
+}
+
+// One pixel: the pair form with a duplicated lane.
+__device__ __forceinline__ void Xyb(float r, float g, float b, uint32_t mask, float out[3]) {
+    float2 o[3];
+    Xyb2(Pack(r), Pack(g), Pack(b), mask, o);
+    out[0] = o[0].x;
+    out[1] = o[1].x;
+    out[2] = o[2].x;
 }
 
 // prepare.comp:103-111: ((((0 + a) + b) + c) + d) * 0.25.
@@ -82,27 +131,72 @@ struct LevelInfo {
     uint32_t levels;
 };
 
-// Two adjacent samples of one 8-bit row: one 16-bit load when the address
-// allows it, the clamped pair otherwise.
-__device__ __forceinline__ void LoadByte2(const uint8_t* row, uint32_t x0, uint32_t x1,
-                                         uint32_t& a, uint32_t& b) {
-    const uint8_t* p = row + x0;
-    if (x1 == x0 + 1 && (reinterpret_cast<uintptr_t>(p) & 1u) == 0) {
-        const uint32_t v = __ldg(reinterpret_cast<const uint16_t*>(p));
-        a = v & 0xffu;
-        b = v >> 8;
-    } else {
-        a = __ldg(p);
-        b = __ldg(row + x1);
+// Writes pixel (x, y) of `level` with XYB value `xyb` (kept channels): the
+// value inside the level, 0 in the padding column and row of an odd-sized
+// level (ss2_layout.h), nothing beyond. Every padding entry has a thread: a
+// level's tile grid spans an even number (64 >> level) of columns and rows
+// per tile, so at least one past an odd size.
+__device__ __forceinline__ void StorePixel(const LevelInfo& lv, uint32_t level, uint32_t x,
+                                           uint32_t y, float x_, float y_, float b_) {
+    const uint32_t mask = lv.mask[level];
+    const uint32_t w = lv.w[level], h = lv.h[level];
+    if (!mask || x >= ((w + 1) & ~1u) || y >= ((h + 1) & ~1u)) return;
+    const bool inside = x < w && y < h;
+    const size_t at = PlaneIndex(lv.pitch[level], x, y);
+    if (mask & 1u) lv.plane[level][0][at] = inside ? x_ : 0.0f;
+    if (mask & 2u) lv.plane[level][1][at] = inside ? y_ : 0.0f;
+    if (mask & 4u) lv.plane[level][2][at] = inside ? b_ : 0.0f;
+}
+
+// The four samples of base block (bx, by) of an 8-bit image, as table
+// entries, in (0,0), (1,0), (0,1), (1,1) order, edge-clamped like
+// prepare.comp's loads. `w4[c]` holds the 32-bit words of rows 2by and
+// 2by + 1 at column 4 * (bx / 2) when `fast`.
+__device__ __forceinline__ void TableBlock(const DevSource& s, const float* lut, bool fast,
+                                           const uint32_t (&w4)[3][2], uint32_t hx, uint32_t bx,
+                                           uint32_t by, float lin[4][3]) {
+    const bool grey = s.family == 0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        uint32_t code[4];
+        if (fast) {
+            const int pc = grey ? 0 : c;
+            code[0] = (w4[pc][0] >> (16 * hx)) & 0xffu;
+            code[1] = (w4[pc][0] >> (16 * hx + 8)) & 0xffu;
+            code[2] = (w4[pc][1] >> (16 * hx)) & 0xffu;
+            code[3] = (w4[pc][1] >> (16 * hx + 8)) & 0xffu;
+        } else {
+            const int pl = grey ? 0 : c;
+            const uint32_t x0 = 2 * bx, y0 = 2 * by;
+            const uint32_t x1 = min(x0 + 1, s.width - 1), y1 = min(y0 + 1, s.height - 1);
+            const uint8_t* r0 = s.plane[pl] + static_cast<size_t>(y0) * s.row_bytes[pl];
+            const uint8_t* r1 = s.plane[pl] + static_cast<size_t>(y1) * s.row_bytes[pl];
+            code[0] = __ldg(r0 + x0);
+            code[1] = __ldg(r0 + x1);
+            code[2] = __ldg(r1 + x0);
+            code[3] = __ldg(r1 + x1);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) lin[i][c] = lut[code[i]];
+    }
+    if (!s.identity2) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) ApplyMatrix(s.m2, lin[i]);
     }
 }
 
+// Five CTAs (40 warps) per SM for the table decode, two for the generic
+// one, whose decode needs more registers.
 template <bool kTable>
-__global__ void __launch_bounds__(kThreads) PrepareKernel(DevBatch batch) {
-    __shared__ float ladder[2][256 * 3];
+__global__ void __launch_bounds__(kThreads, kTable ? 5 : 2) PrepareKernel(DevBatch batch) {
+    // Level-1 tile (32x32) of each channel, then the levels after it in two
+    // alternating buffers: odd levels in `ladder_a`, even ones in `ladder_b`.
+    __shared__ float ladder_a[3][kBlocks * kBlocks];
+    __shared__ float ladder_b[3][kBlocks * kBlocks / 4];
     __shared__ float lut[256];
     __shared__ DevSource src_s;
     __shared__ LevelInfo lv;
+    __shared__ uint32_t aligned4;
 
     const uint32_t tid = threadIdx.x;
     const int group = kTable ? 0 : 1;
@@ -113,8 +207,8 @@ __global__ void __launch_bounds__(kThreads) PrepareKernel(DevBatch batch) {
     const DevPrepItem item = items[it];
     const DevPair& P = batch.pair[item.pair];
     const uint32_t t = blockIdx.x - __ldg(&start[it]);
-    const uint32_t gx = t % P.prep_tiles_x;
     const uint32_t gy = t / P.prep_tiles_x;
+    const uint32_t gx = t - gy * P.prep_tiles_x;
     const int image = static_cast<int>(item.image);
 
     {
@@ -136,108 +230,123 @@ __global__ void __launch_bounds__(kThreads) PrepareKernel(DevBatch batch) {
             lv.pitch[tid] = P.pitch[tid];
             lv.mask[tid] = tid < P.levels ? P.mask[tid] : 0u;
         }
-        if (tid == 0) lv.levels = P.levels;
+        if (tid == 0) {
+            lv.levels = P.levels;
+            // 32-bit sample loads need every plane and row on a 4-byte boundary.
+            const DevSource& ps = P.src[image];
+            uint32_t ok = 1;
+            for (int c = 0; c < (ps.family == 0 ? 1 : 3); ++c)
+                ok &= ((reinterpret_cast<uintptr_t>(ps.plane[c]) | ps.row_bytes[c]) & 3u) == 0;
+            aligned4 = ok;
+        }
     }
     __syncthreads();
     const DevSource& s = src_s;
     const uint32_t levels = lv.levels;
     const uint32_t width = s.width, height = s.height;
-    const uint32_t bx = gx * 16 + (tid & 15);
-    const uint32_t by = gy * 16 + (tid >> 4);
-    const bool in_block = bx < (width + 1) / 2 && by < (height + 1) / 2;
+    const uint32_t wb = (width + 1) / 2, hb = (height + 1) / 2;  // base blocks
+    const uint32_t tx = tid & 15, ty = tid >> 4;
+    const uint32_t mask0 = lv.mask[0];
 
-    // The block's four samples in (0,0), (1,0), (0,1), (1,1) order.
-    float lin[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    if (in_block) {
-        const uint32_t x0 = 2 * bx, y0 = 2 * by;
-        const uint32_t x1 = min(x0 + 1, width - 1), y1 = min(y0 + 1, height - 1);
-        if (kTable) {
-            const bool grey = s.family == 0;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const int pl = grey ? 0 : c;
-                const uint8_t* r0 = s.plane[pl] + static_cast<size_t>(y0) * s.row_bytes[pl];
-                const uint8_t* r1 = s.plane[pl] + static_cast<size_t>(y1) * s.row_bytes[pl];
-                uint32_t a, b, d, e;
-                LoadByte2(r0, x0, x1, a, b);
-                LoadByte2(r1, x0, x1, d, e);
-                lin[0][c] = lut[a];
-                lin[1][c] = lut[b];
-                lin[2][c] = lut[d];
-                lin[3][c] = lut[e];
-            }
-            if (!s.identity2) {
-#pragma unroll
-                for (int i = 0; i < 4; ++i) ApplyMatrix(s.m2, lin[i]);
-            }
-        } else {
-            BlockLinearGeneric(s, bx, by, lin);
-        }
-        // Level 0: rows y0 and (if inside) y0 + 1, each as one float2 when
-        // both columns are inside, else the single last column.
-        const uint32_t mask0 = lv.mask[0];
-        if (mask0) {
-            float v[4][3];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) Xyb(lin[i][0], lin[i][1], lin[i][2], mask0, v[i]);
-            const bool two = x0 + 1 < width;
-            const bool second_row = y0 + 1 < height;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                if (!(mask0 & (1u << c))) continue;
-                float* row0 = lv.plane[0][c] + static_cast<size_t>(y0) * lv.pitch[0] + x0;
-                float* row1 = row0 + lv.pitch[0];
-                if (two) {
-                    *reinterpret_cast<float2*>(row0) = make_float2(v[0][c], v[1][c]);
-                    if (second_row) *reinterpret_cast<float2*>(row1) = make_float2(v[2][c], v[3][c]);
-                } else {
-                    row0[0] = v[0][c];
-                    if (second_row) row1[0] = v[2][c];
-                }
-            }
-        }
-    }
-
-    // Levels past the deepest one that stores a channel are not computed:
-    // nothing reads them (at six scales level 5 keeps no channel).
-    uint32_t last = 0;
+    uint32_t last = 0;  // the deepest level that stores a channel
     for (uint32_t l = 1; l < levels; ++l)
         if (lv.mask[l]) last = l;
 
-    // Level 1: every thread, from its own four samples.
-    if (last >= 1) {
-        float v[3];
+#pragma unroll 1
+    for (uint32_t vy = 0; vy < 2; ++vy) {
+        const uint32_t by = gy * kBlocks + ty + 16 * vy;
+        const uint32_t bx0 = gx * kBlocks + 2 * tx;
+        // Both blocks' samples of each plane as two 32-bit words when the
+        // four columns and two rows are inside and aligned.
+        uint32_t w4[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+        bool fast = false;
+        if (kTable) {
+            fast = aligned4 && 2 * bx0 + 3 < width && 2 * by + 1 < height;
+            if (fast) {
+                const int np = s.family == 0 ? 1 : 3;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) v[c] = BoxAverage(lin[0][c], lin[1][c], lin[2][c], lin[3][c]);
-        const uint32_t x = gx * 16 + (tid & 15), y = gy * 16 + (tid >> 4);
-        const uint32_t mask = lv.mask[1];
-        if (mask && x < lv.w[1] && y < lv.h[1]) {
-            float xyb[3];
-            Xyb(v[0], v[1], v[2], mask, xyb);
-            const size_t at = static_cast<size_t>(y) * lv.pitch[1] + x;
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-                if (mask & (1u << c)) lv.plane[1][c][at] = xyb[c];
+                for (int c = 0; c < 3; ++c) {
+                    if (c >= np) break;
+                    const uint8_t* r0 =
+                        s.plane[c] + static_cast<size_t>(2 * by) * s.row_bytes[c] + 2 * bx0;
+                    w4[c][0] = __ldg(reinterpret_cast<const uint32_t*>(r0));
+                    w4[c][1] = __ldg(reinterpret_cast<const uint32_t*>(r0 + s.row_bytes[c]));
+                }
+            }
         }
-        if (last >= 2) {
+        float l1[2][3];
+#pragma unroll 1
+        for (uint32_t hx = 0; hx < 2; ++hx) {
+            const uint32_t bx = bx0 + hx;
+            float lin[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            const bool in_block = bx < wb && by < hb;
+            if (in_block) {
+                if (kTable) TableBlock(s, lut, fast, w4, hx, bx, by, lin);
+                else BlockLinearGeneric(s, bx, by, lin);
+                // Level 0: the block is one aligned float4 of the row-pair
+                // plane, (x0, y0), (x0, y0+1), (x0+1, y0), (x0+1, y0+1); a
+                // column or row past the image is the plane's zero padding.
+                if (mask0) {
+                    float2 top[3], bottom[3];
+                    Xyb2(make_float2(lin[0][0], lin[1][0]), make_float2(lin[0][1], lin[1][1]),
+                         make_float2(lin[0][2], lin[1][2]), mask0, top);
+                    Xyb2(make_float2(lin[2][0], lin[3][0]), make_float2(lin[2][1], lin[3][1]),
+                         make_float2(lin[2][2], lin[3][2]), mask0, bottom);
+                    const uint32_t x0 = 2 * bx, y0 = 2 * by;
+                    const bool two = x0 + 1 < width;
+                    const bool second_row = y0 + 1 < height;
 #pragma unroll
-            for (int c = 0; c < 3; ++c) ladder[1][tid * 3 + c] = v[c];
+                    for (int c = 0; c < 3; ++c) {
+                        if (!(mask0 & (1u << c))) continue;
+                        float* at = lv.plane[0][c] + PlaneIndex(lv.pitch[0], x0, y0);
+                        *reinterpret_cast<float4*>(at) = make_float4(
+                            top[c].x, second_row ? bottom[c].x : 0.0f, two ? top[c].y : 0.0f,
+                            two && second_row ? bottom[c].y : 0.0f);
+                    }
+                }
+            }
+            float avg[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) avg[c] = BoxAverage(lin[0][c], lin[1][c], lin[2][c], lin[3][c]);
+            // Register copies, not an index: the loop is not unrolled.
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                if (hx == 0) l1[0][c] = avg[c];
+                else l1[1][c] = avg[c];
+            }
+        }
+        // Level 1: pixels (bx0, by) and (bx0 + 1, by).
+        if (last >= 1) {
+            float2 xyb[3];
+            Xyb2(make_float2(l1[0][0], l1[1][0]), make_float2(l1[0][1], l1[1][1]),
+                 make_float2(l1[0][2], l1[1][2]), lv.mask[1], xyb);
+            StorePixel(lv, 1, bx0, by, xyb[0].x, xyb[1].x, xyb[2].x);
+            StorePixel(lv, 1, bx0 + 1, by, xyb[0].y, xyb[1].y, xyb[2].y);
+            if (last >= 2) {
+                const uint32_t at = (ty + 16 * vy) * kBlocks + 2 * tx;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    ladder_a[c][at] = l1[0][c];
+                    ladder_a[c][at + 1] = l1[1][c];
+                }
+            }
         }
     }
     if (last < 2) return;
     __syncthreads();
 
-    // Levels 2..last: the first side^2 threads (64, 16, 4, 1) average the
+    // Levels 2..last: the first side^2 threads (256, 64, 16, 4) average the
     // previous level's 2x2 blocks from the ladder (prepare.comp:149-168,
     // clamped to the previous level's last column and row); threads that no
     // longer take part leave, and the rest meet at a barrier of their own.
+#pragma unroll 1
     for (uint32_t level = 2; level <= last; ++level) {
-        const uint32_t side = 32u >> level;  // a power of two: shifts, not divisions
+        const uint32_t shift = 6 - level;             // side = 64 >> level
+        const uint32_t side = 1u << shift;
         const uint32_t active = side * side;
         if (tid >= active) return;
         const uint32_t jx = tid & (side - 1);
-        const uint32_t jy = tid >> (5 - level);
-        const uint32_t slot = (level - 1) & 1u;
+        const uint32_t jy = tid >> shift;
         const uint32_t prev_side = side * 2;
         const uint32_t pw = lv.w[level - 1], ph = lv.h[level - 1];
         const uint32_t ox = min(gx * prev_side, pw - 1);
@@ -245,29 +354,25 @@ __global__ void __launch_bounds__(kThreads) PrepareKernel(DevBatch batch) {
         const uint32_t lx = pw - 1 - ox, ly = ph - 1 - oy;
         const uint32_t cx0 = min(2 * jx, lx), cx1 = min(2 * jx + 1, lx);
         const uint32_t cy0 = min(2 * jy, ly), cy1 = min(2 * jy + 1, ly);
+        const float* prev0 = (level & 1u) ? &ladder_b[0][0] : &ladder_a[0][0];
+        const uint32_t prev_stride = (level & 1u) ? kBlocks * kBlocks / 4 : kBlocks * kBlocks;
         float v[3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-            v[c] = BoxAverage(ladder[slot][(cy0 * prev_side + cx0) * 3 + c],
-                              ladder[slot][(cy0 * prev_side + cx1) * 3 + c],
-                              ladder[slot][(cy1 * prev_side + cx0) * 3 + c],
-                              ladder[slot][(cy1 * prev_side + cx1) * 3 + c]);
-        const uint32_t x = gx * side + jx;
-        const uint32_t y = gy * side + jy;
-        const uint32_t mask = lv.mask[level];
-        if (mask && x < lv.w[level] && y < lv.h[level]) {
-            float xyb[3];
-            Xyb(v[0], v[1], v[2], mask, xyb);
-            const size_t at = static_cast<size_t>(y) * lv.pitch[level] + x;
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-                if (mask & (1u << c)) lv.plane[level][c][at] = xyb[c];
+        for (int c = 0; c < 3; ++c) {
+            const float* p = prev0 + c * prev_stride;
+            v[c] = BoxAverage(p[cy0 * prev_side + cx0], p[cy0 * prev_side + cx1],
+                              p[cy1 * prev_side + cx0], p[cy1 * prev_side + cx1]);
         }
+        float xyb[3];
+        Xyb(v[0], v[1], v[2], lv.mask[level], xyb);
+        StorePixel(lv, level, gx * side + jx, gy * side + jy, xyb[0], xyb[1], xyb[2]);
         if (level < last) {
+            float* next0 = (level & 1u) ? &ladder_a[0][0] : &ladder_b[0][0];
+            const uint32_t next_stride = (level & 1u) ? kBlocks * kBlocks : kBlocks * kBlocks / 4;
 #pragma unroll
-            for (int c = 0; c < 3; ++c) ladder[level & 1u][tid * 3 + c] = v[c];
+            for (int c = 0; c < 3; ++c) next0[c * next_stride + tid] = v[c];
             if (active > 32) {
-                // Level 2's 64 threads are warps 0 and 1, whole.
+                // 256 or 64 threads: whole warps from warp 0.
                 asm volatile("bar.sync 1, %0;" ::"r"(active) : "memory");
             } else {
                 __syncwarp((1u << active) - 1u);

@@ -29,6 +29,7 @@
 #include "ss2_device.cuh"
 #include "ss2_host.h"
 #include "ss2_kernels.h"
+#include "ss2_layout.h"
 
 namespace vqm_b200 {
 namespace {
@@ -211,19 +212,19 @@ Tables BuildTables(const std::vector<std::pair<uint32_t, uint32_t>>& sizes, Blur
         for (int l = 0; l < plan.count; ++l) {
             P.w[l] = plan.w[l];
             P.h[l] = plan.h[l];
-            P.pitch[l] = static_cast<uint32_t>(AlignUp(plan.w[l], 32));
+            P.pitch[l] = RowPairPitch(plan.w[l]);
             P.mask[l] = plan.mask[l];
             for (int c = 0; c < 3; ++c) {
                 if (!(plan.mask[l] & (1u << c))) continue;
                 P.plane_off[l][c] = floats;
-                floats += static_cast<size_t>(P.pitch[l]) * plan.h[l];
+                floats += PlaneFloats(plan.w[l], plan.h[l]);
             }
         }
         P.image_stride = floats;
         t.pyramid_first.push_back(t.pyramid_floats);
         t.pyramid_floats += AlignUp(2 * floats, 64);
-        P.prep_tiles_x = (((sizes[i].first + 1) / 2) + 15) / 16;
-        P.prep_tiles_y = (((sizes[i].second + 1) / 2) + 15) / 16;
+        P.prep_tiles_x = PrepTiles(sizes[i].first);
+        P.prep_tiles_y = PrepTiles(sizes[i].second);
         prep += 2ull * P.prep_tiles_x * P.prep_tiles_y;
         P.seg_first = static_cast<uint32_t>(t.segs.size());
         for (int l = 0; l < plan.count; ++l)
@@ -747,9 +748,12 @@ public:
         const DevPair& P = tables_.pairs[0];
         const float* src = mem_.pyramid.as<float>() + tables_.pyramid_first[0] +
                            image * P.image_stride + P.plane_off[level][channel];
+        const uint32_t w = P.w[level], h = P.h[level], pitch = P.pitch[level];
+        std::vector<float> pairs(PlaneFloats(w, h));
         VQM_CK(cudaSetDevice(device_));
-        VQM_CK(cudaMemcpy2D(out, P.w[level] * sizeof(float), src, P.pitch[level] * sizeof(float),
-                            P.w[level] * sizeof(float), P.h[level], cudaMemcpyDeviceToHost));
+        VQM_CK(cudaMemcpy(pairs.data(), src, pairs.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        for (uint32_t y = 0; y < h; ++y)
+            for (uint32_t x = 0; x < w; ++x) out[static_cast<size_t>(y) * w + x] = pairs[PlaneIndex(pitch, x, y)];
     }
 
     void Usage(vqm_cu_memory_usage* u) const {
