@@ -25,7 +25,9 @@ workload, and prints the same JSON line with "impl": "reference".
 from __future__ import annotations
 
 import argparse
+import glob
 import json
+import re
 import os
 import statistics
 import subprocess
@@ -157,16 +159,20 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_launch(stage):
-    """Per-launch DRAM bytes of `stage` from the committed ncu summary, if
-    one exists for this workload."""
-    path = os.path.join(ROOT, "profiles", "traffic.json")
-    if not os.path.exists(path):
+def traffic_per_launch(stage, pairs):
+    """Per-launch DRAM bytes (read + write) of `stage` at the default
+    workload (64 pairs of 1920x1080), from the ncu summaries under
+    profiles/ (their "traffic_bytes_per_launch <stage> <bytes>" lines); None
+    for any other workload."""
+    if (WIDTH, HEIGHT, pairs) != (1920, 1080, 64):
         return None
-    with open(path) as f:
-        t = json.load(f)
-    entry = t.get(f"{WIDTH}x{HEIGHT}x{PAIRS}", {}).get(stage)
-    return None if entry is None else entry.get("bytes_per_launch")
+    pattern = re.compile(r"traffic_bytes_per_launch\s+(\w+)\s+([0-9.eE+]+)")
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        with open(path) as f:
+            for m in pattern.finditer(f.read()):
+                if m.group(1) == stage:
+                    return float(m.group(2))
+    return None
 
 
 def cpu_baseline(pairs, threads):
@@ -336,7 +342,7 @@ def main(argv=None):
     per_launch = {0: prep_b, 1: blur_b, 2: 0}[dom] * args.pairs
     peak, peak_kind = peaks()
     achieved = per_launch / (avg[dom] / 1e3) / 1e9
-    traffic = traffic_per_launch(names[dom])
+    traffic = traffic_per_launch(names[dom], args.pairs)
 
     if args.batched_only:
         if rank == 0:
@@ -378,17 +384,19 @@ def main(argv=None):
             imgs.append(ss2.Image(WIDTH, HEIGHT, img.format, buf))
             h2d += img.data.nbytes
         host.append(tuple(imgs))
-    batch.set_timing(False)
+    # Two workers of 16-pair chunks: each chunk's host-to-device copies
+    # overlap the kernels of the chunk before it.
+    pool = ss2.Ssimulacra2Pool(workers=2, chunk=16, device=local)
     for _ in range(2):
-        batch.compute_many(host)
+        pool.compute_many(host)
     barrier()
-    es, ee = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    es.record(stream)
-    for _ in range(args.e2e_steps):
-        batch.compute_many(host)
-    ee.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(es.elapsed_time(ee))
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        pool.compute_many(host)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(1e3 * (time.perf_counter() - t0))
+    pool.close()
     e2e_value = world * args.pairs * args.e2e_steps / (e2e_ms / 1e3)
 
     line = None
@@ -414,7 +422,7 @@ def main(argv=None):
                        "tuning_blur_ms": {str(k): round(v, 4) for k, v in tuned.blur_ms.items()}},
             "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": 112 * 8 * args.pairs,
-                    "path": "Ssimulacra2Batch.compute_many on pinned host images"},
+                    "path": "Ssimulacra2Pool(workers=2, chunk=16).compute_many on pinned host images"},
             "plain": {"value": plain_value, "unit": "pairs/s",
                       "path": "Ssimulacra2Pipeline.compute, one pair per call, resident",
                       "latency_ms_p50": float(np.percentile(lat, 50)),

@@ -81,3 +81,15 @@ def test_sinpi():
     near_zero = np.abs(exact) < 1e-6
     assert d[~near_zero].max() <= 1
     assert np.abs(got[near_zero] - exact[near_zero]).max() < 1e-12
+
+
+def test_cbrt_every_float_of_three_binades():
+    # The seed and every step scale exactly by 2^k when x scales by 2^3k, so
+    # [1, 8) covers the unscaled path's behaviour for every float: each one
+    # must be the correctly rounded cube root.
+    u = np.arange(np.float32(1.0).view(np.uint32), np.float32(8.0).view(np.uint32),
+                  dtype=np.uint32)
+    x = u.view(np.float32)
+    got = det(0, x)
+    want = np.cbrt(x.astype(np.float64)).astype(np.float32)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))

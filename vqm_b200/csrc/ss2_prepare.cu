@@ -160,11 +160,14 @@ __device__ __forceinline__ void TableBlock(const DevSource& s, const float* lut,
     for (int c = 0; c < 3; ++c) {
         uint32_t code[4];
         if (fast) {
-            const int pc = grey ? 0 : c;
-            code[0] = (w4[pc][0] >> (16 * hx)) & 0xffu;
-            code[1] = (w4[pc][0] >> (16 * hx + 8)) & 0xffu;
-            code[2] = (w4[pc][1] >> (16 * hx)) & 0xffu;
-            code[3] = (w4[pc][1] >> (16 * hx + 8)) & 0xffu;
+            // Bytes 2hx and 2hx + 1 of each row word, zero-extended.
+            const uint32_t row0 = grey ? w4[0][0] : w4[c][0];
+            const uint32_t row1 = grey ? w4[0][1] : w4[c][1];
+            const uint32_t sel = 0x4440u | (2u * hx);
+            code[0] = __byte_perm(row0, 0u, sel);
+            code[1] = __byte_perm(row0, 0u, sel + 1u);
+            code[2] = __byte_perm(row1, 0u, sel);
+            code[3] = __byte_perm(row1, 0u, sel + 1u);
         } else {
             const int pl = grey ? 0 : c;
             const uint32_t x0 = 2 * bx, y0 = 2 * by;
@@ -275,7 +278,9 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : 2) PrepareKernel(DevBat
             }
         }
         float l1[2][3];
-#pragma unroll 1
+        // Unrolled for the table decode (the words and averages stay in
+        // registers); rolled for the generic decode, whose body is large.
+#pragma unroll(kTable ? 2 : 1)
         for (uint32_t hx = 0; hx < 2; ++hx) {
             const uint32_t bx = bx0 + hx;
             float lin[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
@@ -308,7 +313,7 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : 2) PrepareKernel(DevBat
             float avg[3];
 #pragma unroll
             for (int c = 0; c < 3; ++c) avg[c] = BoxAverage(lin[0][c], lin[1][c], lin[2][c], lin[3][c]);
-            // Register copies, not an index: the loop is not unrolled.
+            // Register copies, not an index, for the rolled form.
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 if (hx == 0) l1[0][c] = avg[c];

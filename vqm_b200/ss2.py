@@ -622,25 +622,56 @@ class Ssimulacra2Pool:
     """Ssimulacra2Pool (include/vqm_pool.h:51-87): results in input order.
 
     The reference round-robins pairs over ``workers`` one-in-flight
-    pipelines; here one batch scorer takes the pairs ``chunk`` at a time,
-    each chunk one launch per stage."""
+    pipelines of one geometry. Here each worker is a batch scorer on its own
+    stream that takes ``chunk`` pairs (of any sizes) per submission, one
+    launch per stage; chunks go to the workers in turn, each worker with at
+    most one chunk in flight, so one chunk's host-to-device copies overlap
+    the previous chunk's kernels. If a submission fails, the chunks already
+    submitted are drained before the error propagates (pool.cc:64-112)."""
 
     def __init__(self, workers: int = 1, chunk: int = 64, chroma_filter: int = 0,
                  device: int = -1):
         if workers == 0:
             raise InvalidArgument("pool needs at least one worker")
-        self._workers = workers
         self._chunk = max(1, chunk)
-        self._batch = Ssimulacra2Batch(chroma_filter=chroma_filter, device=device)
+        self._batches = [Ssimulacra2Batch(max_pairs=self._chunk, chroma_filter=chroma_filter,
+                                          device=device) for _ in range(workers)]
 
     def workers(self) -> int:
-        return self._workers
+        return len(self._batches)
+
+    def close(self):
+        for b in self._batches:
+            b.close()
 
     def compute_many(self, pairs: Iterable, background: float = 0.5):
         pairs = list(pairs)
-        out = []
-        for i in range(0, len(pairs), self._chunk):
-            out.extend(self._batch.compute_many(pairs[i:i + self._chunk], background))
+        out = [None] * len(pairs)
+        pending = [None] * len(self._batches)  # (token, first index) per worker
+
+        def drain(w):
+            if pending[w] is not None:
+                token, first = pending[w]
+                pending[w] = None
+                for k, r in enumerate(self._batches[w].finish(token)):
+                    out[first + k] = r
+
+        w = 0
+        try:
+            for first in range(0, len(pairs), self._chunk):
+                drain(w)
+                token = self._batches[w].submit(pairs[first:first + self._chunk], background)
+                pending[w] = (token, first)
+                w = (w + 1) % len(self._batches)
+            for k in range(len(self._batches)):
+                drain((w + k) % len(self._batches))
+        except BaseException:
+            for k in range(len(self._batches)):
+                try:
+                    drain(k)
+                except Exception:
+                    pass
+            raise
         return out
 
     def score_many(self, pairs: Iterable, background: float = 0.5):
