@@ -222,6 +222,269 @@ def run_reference(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Further workloads (each prints its own JSON line; not the default bench):
+#   --workload uneven  128 10-bit 4:2:0 pairs of random sizes + 8 odd-sized
+#                      RGB pairs, one batch (one launch per stage)
+#   --workload serve   Poisson request streams through the serving loop
+#   --workload video   240 frame pairs of 3840x2160 10-bit 4:2:0, per frame
+# ---------------------------------------------------------------------------
+
+
+def _gen_kind(job):
+    kind, w, h, seed = job
+    from vqm_b200 import synthetic
+    make = synthetic.yuv_pair if kind == "yuv" else synthetic.rgb_pair
+    o, d, _ = make(w, h, seed)
+    return kind, o.width, o.height, o.data, d.data
+
+
+def _gen_frames(job):
+    first, last, count, w, h, seed = job
+    from vqm_b200 import synthetic
+    base = synthetic.video_base(count, w, h, seed)
+    offsets = synthetic.video_offsets(count, seed)
+    return [(f, o.data, d.data) for f in range(first, last)
+            for o, d in [synthetic.video_frame(f, count, w, h, seed, base, offsets)]]
+
+
+def _pool_map(fn, jobs):
+    from concurrent.futures import ProcessPoolExecutor
+    import multiprocessing as mp
+    workers = min(len(jobs), os.cpu_count() or 1, 16)
+    with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(fn, jobs))
+
+
+def make_kind_pairs(jobs):
+    """(kind, w, h, seed) jobs -> image pairs, generated in spawned workers."""
+    from vqm_b200 import ss2
+    fmts = {"rgb": ss2.srgb8_format(), "yuv": ss2.yuv420_10bit_bt709_format()}
+    out = []
+    for kind, w, h, o, d in _pool_map(_gen_kind, jobs):
+        out.append((ss2.Image(w, h, fmts[kind], o), ss2.Image(w, h, fmts[kind], d)))
+    return out
+
+
+def pair_alg_bytes(o):
+    """Algorithmic bytes of one pair (both inputs read, kept pyramid written
+    and read) -> (prepare, blur, whole)."""
+    from oracle import binding as ob  # plan + pruning only
+    from vqm_b200 import ss2
+    plan = ss2.plan_scales(o.width, o.height)
+    kept = sum(lw * lh for s, (lw, lh) in enumerate(plan) for c in range(3)
+               if not ob.channel_pruned(c, s, len(plan)))
+    inp = 2 * ss2.required_bytes(o.format, o.width, o.height)
+    return inp + 8 * kept, 8 * kept, inp + 16 * kept
+
+
+def to_device(pairs):
+    import torch
+    from vqm_b200 import ss2
+    dev = []
+    for o, d in pairs:
+        to = torch.from_numpy(o.data).cuda()
+        td = torch.from_numpy(d.data).cuda()
+        dev.append((ss2.DeviceImage.packed(o.width, o.height, o.format, to.data_ptr(), to),
+                    ss2.DeviceImage.packed(d.width, d.height, d.format, td.data_ptr(), td)))
+    return dev
+
+
+def pinned(pairs):
+    import torch
+    from vqm_b200 import ss2
+    out = []
+    for o, d in pairs:
+        imgs = []
+        for img in (o, d):
+            buf = torch.empty(img.data.nbytes, dtype=torch.uint8, pin_memory=True).numpy()
+            buf[:] = img.data
+            imgs.append(ss2.Image(img.width, img.height, img.format, buf))
+        out.append(tuple(imgs))
+    return out
+
+
+def run_uneven(args):
+    import torch
+    from vqm_b200 import autotune, ss2
+    rng = np.random.default_rng(2000)
+    jobs = [("yuv", int(rng.integers(320, 3841)), int(rng.integers(180, 2161)), 2001 + i)
+            for i in range(128)]
+    jobs += [("rgb", int(rng.integers(320, 3841)) | 1, int(rng.integers(180, 2161)) | 1,
+              12000 + i) for i in range(8)]
+    pairs = make_kind_pairs(jobs)
+    torch.cuda.set_device(0)
+    dev = to_device(pairs)
+    stream = torch.cuda.Stream()
+    tuned = autotune.tune(dev, stream=stream.cuda_stream, use_cache=False)
+    batches = [ss2.Ssimulacra2Batch(max_pairs=len(dev), variant=tuned.variant) for _ in range(2)]
+    for b in batches:
+        b.set_stream(stream.cuda_stream)
+        b.set_timing(True)
+    stage = []
+
+    def steps(n, collect):
+        pending = [None, None]
+        for k in range(n):
+            b = batches[k % 2]
+            if pending[k % 2] is not None:
+                b.finish(pending[k % 2])
+                if collect:
+                    stage.append(b.stage_ms())
+            pending[k % 2] = b.submit(dev)
+        for i in (0, 1):
+            if pending[i] is not None:
+                batches[i].finish(pending[i])
+                if collect:
+                    stage.append(batches[i].stage_ms())
+
+    steps(args.warmup, False)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clocks:
+        start.record(stream)
+        steps(args.steps, True)
+        end.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    ab = [pair_alg_bytes(o) for o, _ in pairs]
+    prep_b, blur_b, whole_b = (sum(x[i] for x in ab) for i in range(3))
+    avg = np.sum(np.array(stage), axis=0) / args.steps
+    peak, kind = peaks()
+    px = sum(o.width * o.height for o, _ in pairs)
+    print(json.dumps({
+        "workload": "uneven", "metric": "pairs/s", "value": len(pairs) * args.steps / (ms / 1e3),
+        "pairs": len(pairs), "megapixels_per_step": px / 1e6, "steps": args.steps,
+        "ms_per_step": ms / args.steps, "blur_variant": tuned.variant,
+        "tuning_blur_ms": {str(k): round(v, 4) for k, v in tuned.blur_ms.items()},
+        "stage_ms_per_step": dict(zip(("prepare", "blur", "finalize"), avg.tolist())),
+        "roofline": {"prepare_gbs": prep_b / (avg[0] / 1e3) / 1e9,
+                     "blur_gbs": blur_b / (avg[1] / 1e3) / 1e9,
+                     "step_gbs": whole_b / (ms / args.steps / 1e3) / 1e9, "peak": peak,
+                     "peak_source": kind},
+        "clocks": clocks.summary(),
+        "config": "128 10-bit 4:2:0 BT.709 limited pairs, W 320-3840 x H 180-2160 (even), "
+                  "+ 8 odd-sized 8-bit RGB pairs; resident in HBM; one batch per step"}),
+        flush=True)
+    return 0
+
+
+SERVE_SIZES = [((640, 360), 0.2), ((1280, 720), 0.3), ((1920, 1080), 0.3), ((2560, 1440), 0.1),
+               ((3840, 2160), 0.1)]
+
+
+def run_serve(args):
+    import torch
+    from vqm_b200 import ss2
+    per = max(1, args.serve_distinct)
+    jobs = [(kind, w, h, 30000 + 97 * i + 7 * j)
+            for i, ((w, h), _) in enumerate(SERVE_SIZES) for kind in ("rgb", "yuv")
+            for j in range(per)]
+    pairs = make_kind_pairs(jobs)
+    torch.cuda.set_device(0)
+    host = pinned(pairs)
+    # host[(size index, kind index, j)]
+    by = {}
+    for (kind, w, h, _), p in zip(jobs, host):
+        size_idx = [s for s, _ in SERVE_SIZES].index((w, h))
+        by.setdefault((size_idx, kind), []).append(p)
+    probs = np.array([p for _, p in SERVE_SIZES])
+    lines = []
+    for rate in [float(r) for r in args.rates.split(",")]:
+        rng = np.random.default_rng(int(rate))
+        n = max(int(rate * args.duration), 200)
+        gaps = rng.exponential(1.0 / rate, n)
+        sizes = rng.choice(len(SERVE_SIZES), n, p=probs)
+        kinds = rng.integers(0, 2, n)
+        picks = rng.integers(0, per, n)
+        reqs = [by[(int(sizes[i]), ("rgb", "yuv")[int(kinds[i])])][int(picks[i])]
+                for i in range(n)]
+        with ss2.Ssimulacra2Server(memory_budget=40 << 30, workers=args.serve_workers,
+                                   max_batch_pairs=64) as server:
+            # Warm-up: every size and format once.
+            for key in by:
+                server.wait(server.submit(*by[key][0]))
+            tickets = [None] * n
+            late = np.zeros(n)
+            t0 = time.perf_counter()
+            arrival = t0 + np.cumsum(gaps)
+
+            def produce():
+                for i in range(n):
+                    wait = arrival[i] - time.perf_counter()
+                    if wait > 0:
+                        time.sleep(wait)
+                    late[i] = max(0.0, time.perf_counter() - arrival[i])
+                    tickets[i] = server.submit(*reqs[i])
+
+            th = threading.Thread(target=produce)
+            with ClockSampler(0) as clocks:
+                th.start()
+                lat = np.zeros(n)
+                for i in range(n):
+                    while tickets[i] is None:
+                        time.sleep(0.0002)
+                    _, lat[i] = server.wait(tickets[i])
+                th.join()
+                t1 = time.perf_counter()
+            stats = server.stats()
+        total = lat + 1e3 * late  # arrival -> result on the host
+        px = sum(reqs[i][0].width * reqs[i][0].height for i in range(n))
+        line = {"workload": "serve", "rate_req_s": rate, "requests": n,
+                "throughput_req_s": n / (t1 - t0), "megapixels_per_s": px / 1e6 / (t1 - t0),
+                "latency_ms_p50": float(np.percentile(total, 50)),
+                "latency_ms_p99": float(np.percentile(total, 99)),
+                "latency_ms_max": float(total.max()),
+                "batches": int(stats.batches), "largest_batch": int(stats.largest_batch),
+                "peak_device_bytes": int(stats.peak_bytes), "clocks": clocks.summary(),
+                "config": "Poisson arrivals; sizes 640x360/1280x720/1920x1080/2560x1440/"
+                          "3840x2160 at 0.2/0.3/0.3/0.1/0.1; 8-bit RGB or 10-bit 4:2:0 50/50; "
+                          f"pinned host inputs; 40 GB budget; {args.serve_workers} workers"}
+        print(json.dumps(line), flush=True)
+        lines.append(line)
+    return 0
+
+
+def run_video(args):
+    import torch
+    from vqm_b200 import ss2
+    count, w, h, seed = args.frames, 3840, 2160, 4000
+    chunk = max(1, (count + 15) // 16)
+    jobs = [(a, min(a + chunk, count), count, w, h, seed) for a in range(0, count, chunk)]
+    fmt = ss2.yuv420_10bit_bt709_format()
+    frames = [None] * count
+    for part in _pool_map(_gen_frames, jobs):
+        for f, o, d in part:
+            frames[f] = (ss2.Image(w, h, fmt, o), ss2.Image(w, h, fmt, d))
+    torch.cuda.set_device(0)
+    host = pinned(frames)
+    dev = to_device(frames)
+    pipe = ss2.Ssimulacra2Pipeline(w, h)
+    out = {}
+    for name, src in (("streaming", host), ("resident", dev)):
+        for o, d in src[:3]:
+            pipe.compute(o, d)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        scores = [pipe.compute(o, d).score() for o, d in src]
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out[name] = {"frames_per_s": count / dt, "clip_mean_score": float(np.mean(scores))}
+    # The same frames as batches of 8 (one launch per stage per 8 frames).
+    batch = ss2.Ssimulacra2Batch(max_pairs=8)
+    t0 = time.perf_counter()
+    for a in range(0, count, 8):
+        batch.compute_many(dev[a:a + 8])
+    torch.cuda.synchronize()
+    out["resident_batched8"] = {"frames_per_s": count / (time.perf_counter() - t0)}
+    print(json.dumps({"workload": "video", "frames": count, "size": [w, h], **out,
+                      "config": "3840x2160 10-bit 4:2:0 BT.709 limited; reference translating "
+                                "1-3 px per frame; distorted: 8x8 quantisation step 8->48 plus "
+                                "noise sigma 2; one pipeline, CUDA-graph replay per frame"}),
+          flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -238,11 +501,21 @@ def main(argv=None):
                     help="blur kernel variant; default: chosen by the autotuner")
     ap.add_argument("--streams", type=int, default=1, choices=[1, 2],
                     help="streams for the two alternating batch scorers")
+    ap.add_argument("--workload", default="plain1080",
+                    choices=["plain1080", "uneven", "serve", "video"])
+    ap.add_argument("--rates", default="200,500,1000,2000", help="serve: requests/s")
+    ap.add_argument("--duration", type=float, default=5.0, help="serve: seconds per rate")
+    ap.add_argument("--serve-workers", type=int, default=3)
+    ap.add_argument("--serve-distinct", type=int, default=3,
+                    help="serve: distinct pairs per (size, format)")
+    ap.add_argument("--frames", type=int, default=240, help="video: frame pairs")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "plain1080":
+        return {"uneven": run_uneven, "serve": run_serve, "video": run_video}[args.workload](args)
 
     rank, world, local = rank_env()
     pairs = make_pairs(args.pairs, WIDTH, HEIGHT, SEED0 + 100_000 * rank)

@@ -286,6 +286,64 @@ int vqm_cu_ss2_batch_compute(vqm_cu_ss2_batch* batch, uint32_t n,
                              const vqm_cu_image* distorteds, float background,
                              double* norms, uint32_t* scales, double* scores);
 
+/* ------------------------------------------------------------------------ */
+/*      Serving loop (no reference counterpart: VQM scores synchronously    */
+/*      per caller; this is continuous batching for request streams)       */
+/* ------------------------------------------------------------------------ */
+
+/* A wait that ran out; the request is still pending. */
+#define VQM_CU_TIMEOUT 5
+
+typedef struct vqm_cu_ss2_server vqm_cu_ss2_server;
+
+typedef struct vqm_cu_ss2_server_config {
+    uint64_t memory_budget;  /* device bytes for admitted work; 0 = 40 GiB */
+    uint32_t workers;        /* batch scorers in flight at once; 0 = 2 */
+    uint32_t max_batch_pairs;/* pairs per launch at most; 0 = 64 */
+    uint32_t chroma_filter;  /* 0 bilinear, 1 bicubic, 2 lanczos */
+    int32_t device;          /* CUDA ordinal; -1 = the current device */
+    uint32_t variant;        /* blur kernel, as vqm_cu_ss2_batch_config */
+    uint32_t reserved;
+} vqm_cu_ss2_server_config;
+
+typedef struct vqm_cu_ss2_server_stats {
+    uint64_t submitted, completed, failed;
+    uint64_t batches;          /* three-kernel launches */
+    uint64_t largest_batch;    /* pairs in the largest batch formed */
+    uint64_t bytes_in_flight;  /* admitted and not yet completed */
+    uint64_t peak_bytes;       /* largest bytes_in_flight seen */
+    uint64_t queued;           /* submitted, not yet in a batch */
+} vqm_cu_ss2_server_stats;
+
+/* Starts a dispatcher thread, which forms batches from the queued requests
+ * in arrival order whenever a worker is free, and a completion thread, which
+ * finishes batches in submission order. Each worker (a batch scorer with its
+ * own stream and device memory, reused from batch to batch) admits a batch
+ * only if its device footprint fits memory_budget / workers, so the server
+ * never holds more than memory_budget of device memory for requests. */
+int vqm_cu_ss2_server_create(const vqm_cu_ss2_server_config* config,
+                             vqm_cu_ss2_server** server);
+/* Finishes every queued and in-flight request, then stops the threads. */
+int vqm_cu_ss2_server_destroy(vqm_cu_ss2_server* server);
+/* Queues one pair (host or device images, validated here). The images'
+ * memory must stay valid and unchanged until the request's wait returns.
+ * VQM_CU_INVALID_ARGUMENT if the pair alone exceeds a worker's budget. */
+int vqm_cu_ss2_server_submit(vqm_cu_ss2_server* server,
+                             const vqm_cu_image* original,
+                             const vqm_cu_image* distorted, float background,
+                             uint64_t* ticket);
+/* Waits up to timeout_ms (negative: no limit) and writes the pair's norms
+ * (108, zero beyond its scales), scale count, score and latency from submit
+ * to completion in milliseconds (any output may be null); the ticket is
+ * then released. VQM_CU_TIMEOUT leaves the request pending. A request whose
+ * batch failed returns that failure's status and message. */
+int vqm_cu_ss2_server_wait(vqm_cu_ss2_server* server, uint64_t ticket,
+                           int32_t timeout_ms, double* norms108,
+                           uint32_t* scales, double* score,
+                           double* latency_ms);
+int vqm_cu_ss2_server_get_stats(vqm_cu_ss2_server* server,
+                            vqm_cu_ss2_server_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -159,6 +159,24 @@ class _BatchConfig(ctypes.Structure):
     ]
 
 
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("memory_budget", ctypes.c_uint64),
+        ("workers", ctypes.c_uint32),
+        ("max_batch_pairs", ctypes.c_uint32),
+        ("chroma_filter", ctypes.c_uint32),
+        ("device", ctypes.c_int32),
+        ("variant", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "submitted", "completed", "failed", "batches", "largest_batch", "bytes_in_flight",
+        "peak_bytes", "queued")]
+
+
 class MemoryUsage(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in (
         "pyramid_bytes", "resident_bytes", "input_bytes", "scratch_bytes",
@@ -204,6 +222,11 @@ _SIGS = {
     "vqm_cu_ss2_blur_variants": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_stage_ms": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_compute": ([_P, ctypes.c_uint32, _P, _P, ctypes.c_float, _P, _P, _P], ctypes.c_int),
+    "vqm_cu_ss2_server_create": ([_P, _P], ctypes.c_int),
+    "vqm_cu_ss2_server_destroy": ([_P], ctypes.c_int),
+    "vqm_cu_ss2_server_submit": ([_P, _P, _P, ctypes.c_float, _P], ctypes.c_int),
+    "vqm_cu_ss2_server_wait": ([_P, ctypes.c_uint64, ctypes.c_int32, _P, _P, _P, _P], ctypes.c_int),
+    "vqm_cu_ss2_server_get_stats": ([_P, _P], ctypes.c_int),
 }
 for _name, (_args, _res) in _SIGS.items():
     _fn = getattr(_lib, _name)
@@ -234,7 +257,11 @@ class CudaError(RuntimeError):
     """std::runtime_error: no device, allocation or CUDA failure."""
 
 
-_ERRORS = {1: InvalidArgument, 2: LogicError, 3: CudaError, 4: OverflowError}
+class Timeout(TimeoutError):
+    """A server wait ran out; the request is still pending."""
+
+
+_ERRORS = {1: InvalidArgument, 2: LogicError, 3: CudaError, 4: OverflowError, 5: Timeout}
 
 
 def _check(status: int) -> None:
@@ -676,3 +703,70 @@ class Ssimulacra2Pool:
 
     def score_many(self, pairs: Iterable, background: float = 0.5):
         return [r.score() for r in self.compute_many(pairs, background)]
+
+
+class Ssimulacra2Server:
+    """Continuous batching of single-pair requests (vqm_cu_ss2_server_*).
+
+    ``submit`` queues a pair and returns at once with a ticket; a dispatcher
+    thread forms batches from the queue in arrival order whenever one of
+    ``workers`` batch scorers is free, admitting a batch only while its device
+    footprint fits ``memory_budget / workers``; a completion thread finishes
+    batches in order. ``wait`` returns the pair's result and its latency from
+    submit to completion. The images of a request are kept referenced here
+    until its wait returns. A request's result is bit-identical to scoring
+    the pair alone."""
+
+    def __init__(self, memory_budget: int = 0, workers: int = 2, max_batch_pairs: int = 64,
+                 chroma_filter: int = 0, device: int = -1, variant: int = 0):
+        cfg = _ServerConfig(memory_budget, workers, max_batch_pairs, chroma_filter, device,
+                            variant, 0)
+        self._s = ctypes.c_void_p()
+        _check(_lib.vqm_cu_ss2_server_create(ctypes.byref(cfg), ctypes.byref(self._s)))
+        self._keep = {}
+
+    def close(self):
+        if self._s:
+            _check(_lib.vqm_cu_ss2_server_destroy(self._s))
+            self._s = ctypes.c_void_p()
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, original, distorted, background: float = 0.5) -> int:
+        o, d = original._c(), distorted._c()
+        ticket = ctypes.c_uint64()
+        _check(_lib.vqm_cu_ss2_server_submit(self._s, ctypes.byref(o), ctypes.byref(d),
+                                             background, ctypes.byref(ticket)))
+        self._keep[ticket.value] = (original, distorted)
+        return ticket.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """(Ssimulacra2Result, latency in ms) of a submitted pair."""
+        norms = np.zeros(108, dtype=np.float64)
+        scales = ctypes.c_uint32()
+        score = ctypes.c_double()
+        latency = ctypes.c_double()
+        status = _lib.vqm_cu_ss2_server_wait(self._s, ticket, timeout_ms, norms.ctypes.data,
+                                             ctypes.byref(scales), ctypes.byref(score),
+                                             ctypes.byref(latency))
+        if status != 5:
+            self._keep.pop(ticket, None)
+        _check(status)
+        n = scales.value
+        return Ssimulacra2Result(norms[: 18 * n].reshape(n, 18).copy(), score.value), latency.value
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        _check(_lib.vqm_cu_ss2_server_get_stats(self._s, ctypes.byref(st)))
+        return st

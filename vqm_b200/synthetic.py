@@ -200,20 +200,47 @@ def uneven_batch(count: int = 128, seed0: int = 2000, odd_rgb: int = 8):
     return pairs
 
 
-def video_frames(count: int = 240, width: int = 3840, height: int = 2160, seed: int = 4000):
-    """Frame pairs of a texture translating 1-3 px per frame; the distorted
-    stream is 8x8 quantised with a step drifting 8 -> 48 plus noise sigma 2
-    (8-bit units). Yields (original, distorted) 10-bit 4:2:0 images."""
+def video_offsets(count: int, seed: int):
+    """Per-frame (x, y) offsets of the translating reference: 1-3 px right
+    and 0-1 px down per frame."""
     rng = np.random.default_rng(seed)
     total_shift = 3 * count + 4
-    base_rng = np.random.default_rng(seed + 1)
-    big = add_rectangles(texture(width + total_shift, height + total_shift, base_rng), base_rng)
     x = y = 0
-    for f in range(count):
+    out = []
+    for _ in range(count):
         x += int(rng.integers(1, 4))
         y += int(rng.integers(0, 2))
-        x, y = min(x, total_shift - 1), min(y, total_shift - 1)
-        ref = big[:, y:y + height, x:x + width]
-        step = 8 + (48 - 8) * f / max(count - 1, 1)
-        dist = block_quantise(ref, step) + rng.normal(0, 2, size=ref.shape)
-        yield yuv420_10bit_image(ref), yuv420_10bit_image(np.clip(dist, 0, 255))
+        out.append((min(x, total_shift - 1), min(y, total_shift - 1)))
+    return out
+
+
+def video_base(count: int, width: int, height: int, seed: int) -> np.ndarray:
+    """The texture the reference stream is cut from (large enough for every
+    frame's offset)."""
+    total_shift = 3 * count + 4
+    base_rng = np.random.default_rng(seed + 1)
+    return add_rectangles(texture(width + total_shift, height + total_shift, base_rng), base_rng)
+
+
+def video_frame(f: int, count: int, width: int, height: int, seed: int, base=None,
+                offsets=None):
+    """Frame pair f of the clip: the reference is the base texture at the
+    frame's offset; the distorted frame is 8x8 quantised with a step drifting
+    8 -> 48 over the clip plus noise sigma 2 (8-bit units, seeded per frame).
+    Both as 10-bit 4:2:0 images. Frames are independent of each other, so a
+    clip can be generated in parallel."""
+    base = video_base(count, width, height, seed) if base is None else base
+    x, y = (offsets or video_offsets(count, seed))[f]
+    ref = base[:, y:y + height, x:x + width]
+    step = 8 + (48 - 8) * f / max(count - 1, 1)
+    rng = np.random.default_rng(seed + 10 + f)
+    dist = block_quantise(ref, step) + rng.normal(0, 2, size=ref.shape).astype(np.float32)
+    return yuv420_10bit_image(ref), yuv420_10bit_image(np.clip(dist, 0, 255))
+
+
+def video_frames(count: int = 240, width: int = 3840, height: int = 2160, seed: int = 4000):
+    """The clip's frame pairs in order (see video_frame)."""
+    base = video_base(count, width, height, seed)
+    offsets = video_offsets(count, seed)
+    for f in range(count):
+        yield video_frame(f, count, width, height, seed, base, offsets)
