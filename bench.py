@@ -312,6 +312,8 @@ def run_uneven(args):
             for i in range(128)]
     jobs += [("rgb", int(rng.integers(320, 3841)) | 1, int(rng.integers(180, 2161)) | 1,
               12000 + i) for i in range(8)]
+    if args.uneven_pairs < len(jobs):  # a smaller case of the same draw (profiling)
+        jobs = jobs[: args.uneven_pairs]
     pairs = make_kind_pairs(jobs)
     torch.cuda.set_device(0)
     dev = to_device(pairs)
@@ -401,9 +403,15 @@ def run_serve(args):
                 for i in range(n)]
         with ss2.Ssimulacra2Server(memory_budget=40 << 30, workers=args.serve_workers,
                                    max_batch_pairs=64) as server:
-            # Warm-up: every size and format once.
+            # Warm-up: every size and format once, then bursts of the
+            # largest pairs so every worker's device memory has grown to its
+            # largest batch before the timed stream.
             for key in by:
                 server.wait(server.submit(*by[key][0]))
+            big = [by[(len(SERVE_SIZES) - 1, kind)][0] for kind in ("rgb", "yuv")]
+            burst = [server.submit(*big[k % 2]) for k in range(64 * args.serve_workers)]
+            for t in burst:
+                server.wait(t)
             tickets = [None] * n
             late = np.zeros(n)
             t0 = time.perf_counter()
@@ -433,8 +441,12 @@ def run_serve(args):
         line = {"workload": "serve", "rate_req_s": rate, "requests": n,
                 "throughput_req_s": n / (t1 - t0), "megapixels_per_s": px / 1e6 / (t1 - t0),
                 "latency_ms_p50": float(np.percentile(total, 50)),
+                "latency_ms_p90": float(np.percentile(total, 90)),
                 "latency_ms_p99": float(np.percentile(total, 99)),
                 "latency_ms_max": float(total.max()),
+                "latency_ms_mean": float(total.mean()),
+                "server_ms_p50_p99": [float(np.percentile(lat, 50)), float(np.percentile(lat, 99))],
+                "submit_late_ms_p99": float(1e3 * np.percentile(late, 99)),
                 "batches": int(stats.batches), "largest_batch": int(stats.largest_batch),
                 "peak_device_bytes": int(stats.peak_bytes), "clocks": clocks.summary(),
                 "config": "Poisson arrivals; sizes 640x360/1280x720/1920x1080/2560x1440/"
@@ -509,6 +521,8 @@ def main(argv=None):
     ap.add_argument("--serve-distinct", type=int, default=3,
                     help="serve: distinct pairs per (size, format)")
     ap.add_argument("--frames", type=int, default=240, help="video: frame pairs")
+    ap.add_argument("--uneven-pairs", type=int, default=136,
+                    help="uneven: pairs of the draw to use (136 = all)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3

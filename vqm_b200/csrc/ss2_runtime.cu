@@ -113,9 +113,12 @@ public:
         ptr_ = nullptr;
         bytes_ = 0;
     }
-    // Returns true when the address changed.
+    // Returns true when the address changed. A buffer that has to grow
+    // grows by half again at least, so a scorer fed batches of varying sizes
+    // reallocates (and synchronises the device) a few times, not per batch.
     bool ensure(size_t bytes) {
         if (bytes <= bytes_) return false;
+        if (bytes_) bytes = std::max(bytes, bytes_ + bytes_ / 2);
         reset();
         if (cudaMalloc(&ptr_, bytes) != cudaSuccess) {
             ptr_ = nullptr;
@@ -148,6 +151,7 @@ public:
     }
     bool ensure(size_t bytes) {
         if (bytes <= bytes_) return false;
+        if (bytes_) bytes = std::max(bytes, bytes_ + bytes_ / 2);
         reset();
         if (cudaMallocHost(&ptr_, bytes) != cudaSuccess) {
             ptr_ = nullptr;
