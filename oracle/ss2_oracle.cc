@@ -867,14 +867,17 @@ struct Decoder {
         BilinearPhase(px[1], scx, shx, cx, xb0, xb1, xwb0, xwb1);
         BilinearPhase(py[0], scy, shy, cy, ya0, ya1, ywa0, ywa1);
         BilinearPhase(py[2], scy, shy, cy, yb0, yb1, ywb0, ywb1);
+        // Along an axis that is not subsampled the second tap of a phase can
+        // fall one slot past the 3x3 window (color.glsl indexes past its
+        // array there), always with weight exactly 0: such a slot reads 0.
+        auto at = [&](int y, int x) { return y <= 2 && x <= 2 ? win[y * 3 + x] : T(0); };
         auto window = [&](int xa, int xb, int ya, int yb, T xwa, T xwb, T ywa,
                           T ywb) {
             const T w00 = xwa * ywa, w10 = xwb * ywa, w01 = xwa * ywb,
                     w11 = xwb * ywb;
-            return std::fma(w11, win[yb * 3 + xb],
-                            std::fma(w01, win[yb * 3 + xa],
-                                     std::fma(w10, win[ya * 3 + xb],
-                                              w00 * win[ya * 3 + xa])));
+            return std::fma(w11, at(yb, xb),
+                            std::fma(w01, at(yb, xa),
+                                     std::fma(w10, at(ya, xb), w00 * at(ya, xa))));
         };
         out[0] = window(xa0, xa1, ya0, ya1, xwa0, xwa1, ywa0, ywa1);
         out[1] = window(xb0, xb1, ya0, ya1, xwb0, xwb1, ywa0, ywa1);

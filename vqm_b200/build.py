@@ -30,7 +30,7 @@ CUDA_SOURCES = ["ss2_prepare.cu", "ss2_blur.cu", "ss2_finalize.cu", "ss2_runtime
                 "ss2_noalloc.cu"]
 HOST_SOURCES = ["ss2_host.cc", "ss2_server.cc"]
 HEADERS = ["ss2_device.cuh", "ss2_decode.cuh", "ss2_detmath.h", "ss2_kernels.h", "ss2_host.h",
-           "ss2_layout.h"]
+           "ss2_layout.h", "ss2_detmath_tables.h"]
 
 
 def _stale(target: str, deps: list[str]) -> bool:

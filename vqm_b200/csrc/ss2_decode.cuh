@@ -100,6 +100,7 @@ __device__ __forceinline__ void TransferRgb(const DevSource& s, float c[3]) {
         for (int i = 0; i < 3; ++i) c[i] = __fmul_rn(c[i], f);
         return;
     }
+#pragma unroll
     for (int i = 0; i < 3; ++i) c[i] = TransferDecode(s, c[i]);
 }
 // color.glsl:209-218.
@@ -157,23 +158,51 @@ __device__ __forceinline__ float FilterKernel(int filter, float x) {
     return __fmul_rn(a, b);
 }
 
-// color.glsl:288-299.
-__device__ __forceinline__ void BilinearPhase(uint32_t out_pos, float scale, float shift,
-                                              int centre, int& s0, int& s1, float& w0,
-                                              float& w1) {
+// color.glsl:288-299. `scale` is 1, 2 or 4, so dividing by it is the exact
+// product with its reciprocal.
+__device__ __forceinline__ void BilinearPhase(uint32_t out_pos, float inv_scale, float shift,
+                                              int centre, int& s0, float& w0, float& w1) {
     const float pos =
-        __fadd_rn(__fdiv_rn(__fadd_rn(static_cast<float>(out_pos), 0.5f), scale), shift);
+        __fadd_rn(__fmul_rn(__fadd_rn(static_cast<float>(out_pos), 0.5f), inv_scale), shift);
     const float base = __fadd_rn(RoundHalfup(__fsub_rn(pos, 1.0f)), 0.5f);
     const float t = __fsub_rn(pos, base);
     s0 = static_cast<int>(floorf(base)) - centre + 1;
-    s1 = s0 + 1;
     w0 = __fsub_rn(1.0f, t);
     w1 = t;
 }
 
+// Rows s and s + 1 of a 3x3 window, by selection rather than an index, so
+// the window stays in registers. s is 0, 1 or 2: along an axis that is not
+// subsampled the second tap of a phase can fall one slot past the window,
+// always with weight exactly 0, and reads 0 here.
+struct WinRows {
+    float top[3], bottom[3];
+};
+__device__ __forceinline__ WinRows PickRows(const float (&win)[9], int s) {
+    WinRows r;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        r.top[k] = s == 0 ? win[k] : (s == 1 ? win[3 + k] : win[6 + k]);
+        r.bottom[k] = s == 0 ? win[3 + k] : (s == 1 ? win[6 + k] : 0.0f);
+    }
+    return r;
+}
+// The bilinear value from rows r at columns s, s + 1 (s in 0..2, a column
+// past the window reading 0), in the reference's accumulation order.
+__device__ __forceinline__ float BilinearTap(const WinRows& r, int s, float xw0, float xw1,
+                                             float yw0, float yw1) {
+    const float w00 = __fmul_rn(xw0, yw0), w10 = __fmul_rn(xw1, yw0);
+    const float w01 = __fmul_rn(xw0, yw1), w11 = __fmul_rn(xw1, yw1);
+    const float t0 = s == 0 ? r.top[0] : (s == 1 ? r.top[1] : r.top[2]);
+    const float t1 = s == 0 ? r.top[1] : (s == 1 ? r.top[2] : 0.0f);
+    const float b0 = s == 0 ? r.bottom[0] : (s == 1 ? r.bottom[1] : r.bottom[2]);
+    const float b1 = s == 0 ? r.bottom[1] : (s == 1 ? r.bottom[2] : 0.0f);
+    return __fmaf_rn(w11, b1, __fmaf_rn(w01, b0, __fmaf_rn(w10, t1, __fmul_rn(w00, t0))));
+}
+
 // color.glsl:324-367: bilinear chroma of the block's four samples.
-__device__ void ChromaBilinear(const DevSource& s, int plane, const uint32_t px[4],
-                               const uint32_t py[4], float out[4]) {
+__device__ __forceinline__ void ChromaBilinear(const DevSource& s, int plane, const uint32_t px[4],
+                                               const uint32_t py[4], float out[4]) {
     const uint32_t dx = s.plane_w[plane], dy = s.plane_h[plane];
     const int cx = static_cast<int>(px[0] >> s.sub_w);
     const int cy = static_cast<int>(py[0] >> s.sub_h);
@@ -196,27 +225,19 @@ __device__ void ChromaBilinear(const DevSource& s, int plane, const uint32_t px[
             }
             win[(j + 1) * 3 + (i + 1)] = RawSample(s, plane, sx, sy);
         }
-    const float scx = static_cast<float>(1u << s.sub_w);
-    const float scy = static_cast<float>(1u << s.sub_h);
-    int xa0, xa1, xb0, xb1, ya0, ya1, yb0, yb1;
+    const float iscx = 1.0f / static_cast<float>(1u << s.sub_w);
+    const float iscy = 1.0f / static_cast<float>(1u << s.sub_h);
+    int xa, xb, ya, yb;
     float xwa0, xwa1, xwb0, xwb1, ywa0, ywa1, ywb0, ywb1;
-    BilinearPhase(px[0], scx, s.shift_x, cx, xa0, xa1, xwa0, xwa1);
-    BilinearPhase(px[1], scx, s.shift_x, cx, xb0, xb1, xwb0, xwb1);
-    BilinearPhase(py[0], scy, s.shift_y, cy, ya0, ya1, ywa0, ywa1);
-    BilinearPhase(py[2], scy, s.shift_y, cy, yb0, yb1, ywb0, ywb1);
-    auto window = [&](int xa, int xb, int ya, int yb, float xwa, float xwb, float ywa,
-                      float ywb) {
-        const float w00 = __fmul_rn(xwa, ywa), w10 = __fmul_rn(xwb, ywa);
-        const float w01 = __fmul_rn(xwa, ywb), w11 = __fmul_rn(xwb, ywb);
-        return __fmaf_rn(w11, win[yb * 3 + xb],
-                         __fmaf_rn(w01, win[yb * 3 + xa],
-                                   __fmaf_rn(w10, win[ya * 3 + xb],
-                                             __fmul_rn(w00, win[ya * 3 + xa]))));
-    };
-    out[0] = window(xa0, xa1, ya0, ya1, xwa0, xwa1, ywa0, ywa1);
-    out[1] = window(xb0, xb1, ya0, ya1, xwb0, xwb1, ywa0, ywa1);
-    out[2] = window(xa0, xa1, yb0, yb1, xwa0, xwa1, ywb0, ywb1);
-    out[3] = window(xb0, xb1, yb0, yb1, xwb0, xwb1, ywb0, ywb1);
+    BilinearPhase(px[0], iscx, s.shift_x, cx, xa, xwa0, xwa1);
+    BilinearPhase(px[1], iscx, s.shift_x, cx, xb, xwb0, xwb1);
+    BilinearPhase(py[0], iscy, s.shift_y, cy, ya, ywa0, ywa1);
+    BilinearPhase(py[2], iscy, s.shift_y, cy, yb, ywb0, ywb1);
+    const WinRows ra = PickRows(win, ya), rb = PickRows(win, yb);
+    out[0] = BilinearTap(ra, xa, xwa0, xwa1, ywa0, ywa1);
+    out[1] = BilinearTap(ra, xb, xwb0, xwb1, ywa0, ywa1);
+    out[2] = BilinearTap(rb, xa, xwa0, xwa1, ywb0, ywb1);
+    out[3] = BilinearTap(rb, xb, xwb0, xwb1, ywb0, ywb1);
 }
 
 // color.glsl:371-432: bicubic (4 taps) or Lanczos-3 (6 taps) chroma.
@@ -289,6 +310,7 @@ __device__ __forceinline__ void BlockLinearGeneric(const DevSource& s, uint32_t 
     }
     const bool has_alpha = s.alpha != 0;
     const bool premul = s.alpha == 2;
+#pragma unroll
     for (int i = 0; i < 4; ++i) {
         const float alpha = has_alpha ? RawSample(s, 3, px[i], py[i]) : 1.0f;
         float e[3];

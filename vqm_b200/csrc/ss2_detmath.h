@@ -25,6 +25,8 @@
 #include <cstdint>
 #include <cstring>
 
+#include "ss2_detmath_tables.h"
+
 #if defined(__CUDACC__)
 #define SS2_DM __host__ __device__ __forceinline__
 #else
@@ -144,8 +146,47 @@ SS2_DM float cbrt(float x) {
     return fmaf_(e, rr * third, y0) * scale;
 }
 
-// log2 of a finite x > 0 in double: x = m 2^e with m in [sqrt(1/2), sqrt(2)),
-// ln m = 2 atanh(s), s = (m - 1) / (m + 1), |s| <= 0.1716, ten odd terms.
+// The tables of log2d and exp2d (ss2_detmath_tables.h, written by
+// gen_detmath_tables.py): one copy for host code and one in device global
+// memory, where lanes that index different entries are served by the L1
+// cache rather than serialised as they would be from the constant bank.
+static const double kInvCHost[128] = {SS2DM_KINVC_VALUES};
+static const double kLog2InvCHost[128] = {SS2DM_KLOG2INVC_VALUES};
+static const double kExp2JHost[64] = {SS2DM_KEXP2J_VALUES};
+#if defined(__CUDACC__)
+static __device__ const double kInvCDev[128] = {SS2DM_KINVC_VALUES};
+static __device__ const double kLog2InvCDev[128] = {SS2DM_KLOG2INVC_VALUES};
+static __device__ const double kExp2JDev[64] = {SS2DM_KEXP2J_VALUES};
+#endif
+SS2_DM double InvC(int i) {
+#if defined(__CUDA_ARCH__)
+    return __ldg(&kInvCDev[i]);
+#else
+    return kInvCHost[i];
+#endif
+}
+SS2_DM double Log2InvC(int i) {
+#if defined(__CUDA_ARCH__)
+    return __ldg(&kLog2InvCDev[i]);
+#else
+    return kLog2InvCHost[i];
+#endif
+}
+SS2_DM double Exp2J(int j) {
+#if defined(__CUDA_ARCH__)
+    return __ldg(&kExp2JDev[j]);
+#else
+    return kExp2JHost[j];
+#endif
+}
+
+// log2 of a finite x > 0 in double, table-driven (the reduction of P. T. P.
+// Tang, "Table-driven implementation of the logarithm function in IEEE
+// floating-point arithmetic", ACM TOMS 16(4), 1990): x = m 2^e, m in [1, 2);
+// the top 7 bits of m's fraction pick c near m, and
+//   log2 x = e - log2(RN(1/c)) + log2(1 + r),  r = m RN(1/c) - 1 (one fused
+// multiply-add, |r| < 2^-8), with ln(1 + r) by its Taylor series to r^7
+// (remainder below 2^-67).
 SS2_DM double log2d(double x) {
     uint64_t u = bits(x);
     int e = static_cast<int>((u >> 52) & 0x7ff);
@@ -155,54 +196,44 @@ SS2_DM double log2d(double x) {
         e = static_cast<int>((u >> 52) & 0x7ff) - 54;
     }
     e -= 1023;
-    double m = from_bits64((u & 0x000fffffffffffffull) | 0x3ff0000000000000ull);  // [1, 2)
-    if (m > 1.4142135623730951) {
-        m = m * 0.5;
-        e += 1;
-    }
-    const double s = (m - 1.0) / (m + 1.0);
-    const double s2 = s * s;
-    double p = 1.0 / 21.0;
-    p = fmad(p, s2, 1.0 / 19.0);
-    p = fmad(p, s2, 1.0 / 17.0);
-    p = fmad(p, s2, 1.0 / 15.0);
-    p = fmad(p, s2, 1.0 / 13.0);
-    p = fmad(p, s2, 1.0 / 11.0);
-    p = fmad(p, s2, 1.0 / 9.0);
-    p = fmad(p, s2, 1.0 / 7.0);
-    p = fmad(p, s2, 1.0 / 5.0);
-    p = fmad(p, s2, 1.0 / 3.0);
-    const double ln_m = 2.0 * fmad(s * s2, p, s);
-    return static_cast<double>(e) + ln_m * 1.4426950408889634074;  // 1/ln 2
+    const uint64_t frac = u & 0x000fffffffffffffull;
+    const int i = static_cast<int>(frac >> 45);
+    const double m = from_bits64(frac | 0x3ff0000000000000ull);  // [1, 2)
+    const double r = fmad(m, InvC(i), -1.0);
+    double p = 1.0 / 7.0;
+    p = fmad(p, r, -1.0 / 6.0);
+    p = fmad(p, r, 1.0 / 5.0);
+    p = fmad(p, r, -1.0 / 4.0);
+    p = fmad(p, r, 1.0 / 3.0);
+    p = fmad(p, r, -0.5);
+    const double ln1r = fmad(r * r, p, r);
+    return fmad(ln1r, 1.4426950408889634074, Log2InvC(i) + static_cast<double>(e));
 }
 
-// 2^t in double for |t| < 1000: t = n + f, f in [-1/2, 1/2], e^(f ln 2) by a
-// degree-13 Taylor polynomial.
+// 2^t in double for |t| < 1000, table-driven: t = (64 n + j) / 64 + f with
+// j in [0, 64) and |f| <= 1/128 (f exact), 2^t = 2^n 2^(j/64) e^(f ln 2),
+// e^z - 1 by its Taylor series to z^6 (|z| < 0.0055, remainder below 4e-20).
 SS2_DM double exp2d(double t) {
     if (t > 1000.0) t = 1000.0;
     if (t < -1000.0) return 0.0;
-    const double nf = floord(t + 0.5);
-    const double f = t - nf;
+    const double kd = floord(t * 64.0 + 0.5);
+    const double f = t - kd * 0.015625;
+    const int k = static_cast<int>(kd);
+    const int j = k & 63;
+    int n = (k - j) / 64;
     const double z = f * 0.69314718055994530942;
-    double p = 1.0 / 6227020800.0;  // 1/13!
-    p = fmad(p, z, 1.0 / 479001600.0);
-    p = fmad(p, z, 1.0 / 39916800.0);
-    p = fmad(p, z, 1.0 / 3628800.0);
-    p = fmad(p, z, 1.0 / 362880.0);
-    p = fmad(p, z, 1.0 / 40320.0);
-    p = fmad(p, z, 1.0 / 5040.0);
-    p = fmad(p, z, 1.0 / 720.0);
+    double p = 1.0 / 720.0;
     p = fmad(p, z, 1.0 / 120.0);
     p = fmad(p, z, 1.0 / 24.0);
     p = fmad(p, z, 1.0 / 6.0);
     p = fmad(p, z, 0.5);
     p = fmad(p, z, 1.0);
-    p = fmad(p, z, 1.0);
-    int n = static_cast<int>(nf);
+    const double tj = Exp2J(j);
+    const double v = fmad(tj, p * z, tj);  // 2^(j/64) (1 + (e^z - 1))
     // Split the scale so every factor stays a normal double.
     if (n > 1000) n = 1000;
     const int n1 = n / 2, n2 = n - n1;
-    return p * pow2i(n1) * pow2i(n2);
+    return v * pow2i(n1) * pow2i(n2);
 }
 
 // x^y for float x > 0 (0 for x == 0 and y > 0), both as float values.

@@ -188,10 +188,15 @@ __device__ __forceinline__ void TableBlock(const DevSource& s, const float* lut,
     }
 }
 
-// Five CTAs (40 warps) per SM for the table decode, two for the generic
-// one, whose decode needs more registers.
+// Five CTAs (40 warps) per SM for the table decode, four for the generic
+// one: its long FP64 transfer chains want the warps more than the registers
+// (measured: 4 CTAs with some spilling beat 2 without by a quarter).
+#ifndef VQM_GENERIC_PREPARE_CTAS
+#define VQM_GENERIC_PREPARE_CTAS 4
+#endif
 template <bool kTable>
-__global__ void __launch_bounds__(kThreads, kTable ? 5 : 2) PrepareKernel(DevBatch batch) {
+__global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTAS)
+    PrepareKernel(DevBatch batch) {
     // Level-1 tile (32x32) of each channel, then the levels after it in two
     // alternating buffers: odd levels in `ladder_a`, even ones in `ladder_b`.
     __shared__ float ladder_a[3][kBlocks * kBlocks];
