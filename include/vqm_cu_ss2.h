@@ -218,6 +218,12 @@ int vqm_cu_ss2_debug_plane(vqm_cu_ss2_pipeline* pipeline, uint32_t image,
 /* CUDA-graph replay of the pair's kernels (prepare, blur, finalize): on by
  * default; 0 launches them one by one. */
 int vqm_cu_ss2_set_graphs(vqm_cu_ss2_pipeline* pipeline, int enabled);
+/* The reference-pyramid reuse of VQM's pipeline (src/metrics/ssimulacra2/
+ * vulkan.cc:238-243, 714-736): a submission whose original is the same
+ * resident slot handle, with the same background, as the previous
+ * submission's skips the original's decode and pyramid. *count receives how
+ * many submissions have done so. */
+int vqm_cu_ss2_reference_reuses(vqm_cu_ss2_pipeline* pipeline, uint64_t* count);
 
 /* ---- scoring without allocation --------------------------------------- */
 

@@ -275,6 +275,36 @@ def test_resident_and_streaming_agree_bitwise():
         assert p.compute(c, b).score() == 100.0
 
 
+def test_reference_pyramid_reuse():
+    """vulkan.cc:238-243, 714-736: the same resident original with the same
+    background skips its prepare; results stay bit-identical."""
+    o, d1, _ = synthetic.rgb_pair(320, 180, 71)
+    _, d2, _ = synthetic.rgb_pair(320, 180, 72)
+    with ss2.Ssimulacra2Pipeline(320, 180, gpu_resident_images=3) as p:
+        ref = [p.compute(o, d).norms for d in (d1, d2)]
+        ref_bg = p.compute(o, d2, 0.2).norms
+        assert p.reference_reuses() == 0
+        a, b1, b2 = p.upload(o), p.upload(d1), p.upload(d2)
+        assert np.array_equal(p.compute(a, b1).norms, ref[0])
+        assert np.array_equal(p.compute(a, b2).norms, ref[1])
+        assert p.reference_reuses() == 1
+        assert np.array_equal(p.compute(a, d1).norms, ref[0])  # streamed distorted
+        assert p.reference_reuses() == 2
+        assert np.array_equal(p.compute(a, b2, 0.2).norms, ref_bg)  # new background
+        assert p.reference_reuses() == 2
+        p.compute(o, d1)  # a streamed original replaces the cached planes
+        assert np.array_equal(p.compute(a, b2).norms, ref[1])
+        assert p.reference_reuses() == 2
+        p.set_graphs(False)
+        assert np.array_equal(p.compute(a, b1).norms, ref[0])
+        assert p.reference_reuses() == 3
+        p.release(b1)
+        p.release(a)  # forgets the cached original
+        a2 = p.upload(d1)
+        assert np.array_equal(p.compute(a2, b2).norms, p.compute(d1, d2).norms)
+        assert p.reference_reuses() == 3
+
+
 def test_submit_finish_contracts():
     o, d = helpers.plain_256_pair()
     with ss2.Ssimulacra2Pipeline(256, 256) as p:

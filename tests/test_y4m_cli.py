@@ -1,0 +1,106 @@
+"""The sequence path: the Y4M reader (tools/image_io/io.cc:405-600 of the
+reference) and the CLI's per-frame scores, clip mean and raw norms."""
+
+import io
+import json
+
+import numpy as np
+import pytest
+
+from tests import helpers
+from vqm_b200 import ss2, synthetic, y4m
+
+
+def _clip(tmp_path, frames=3, w=64, h=48):
+    pairs = [synthetic.yuv_pair(w, h, 500 + f)[:2] for f in range(frames)]
+    po, pd = tmp_path / "o.y4m", tmp_path / "d.y4m"
+    y4m.write(str(po), [o for o, _ in pairs], "420p10")
+    y4m.write(str(pd), [d for _, d in pairs], "420p10")
+    return pairs, str(po), str(pd)
+
+
+def test_header_defaults_and_tags():
+    h = y4m.read_header(io.BytesIO(b"YUV4MPEG2 W64 H48 F30000:1001 Ip A1:1\n"))
+    f = h.format
+    assert (h.width, h.height, h.fps, h.progressive, h.tag) == (64, 48, (30000, 1001), True,
+                                                               "420jpeg")
+    assert f.chroma_location == ss2.ChromaLocation.Center
+    assert (f.range, f.matrix, f.transfer, f.primaries) == (
+        ss2.PixelRange.Limited, ss2.MatrixCoefficients.Bt470Bg,
+        ss2.TransferCharacteristics.Bt709, ss2.ColorPrimaries.Bt709)
+    assert (f.type, f.depth, f.subsample_w, f.subsample_h) == (ss2.PixelType.Byte, 0, 1, 1)
+    h = y4m.read_header(io.BytesIO(b"YUV4MPEG2 W16 H8 C422p12\n"))
+    assert (h.format.type, h.format.depth, h.format.subsample_w, h.format.subsample_h,
+            h.format.chroma_location) == (ss2.PixelType.Word, 12, 1, 0, ss2.ChromaLocation.Left)
+    assert y4m.read_header(io.BytesIO(b"YUV4MPEG2 W8 H8 C444alpha\n")).format.alpha == \
+        ss2.AlphaType.Straight
+    assert y4m.read_header(io.BytesIO(b"YUV4MPEG2 W8 H8 Cmono\n")).format.family == \
+        ss2.ColorFamily.Grey
+    assert y4m.read_header(io.BytesIO(b"YUV4MPEG2 W8 H8 C420paldv\n")).format.chroma_location \
+        == ss2.ChromaLocation.TopLeft
+
+
+@pytest.mark.parametrize("header,message", [
+    (b"YUV4MPEG3 W8 H8\n", "not a YUV4MPEG2"),
+    (b"YUV4MPEG2 W8\n", "no frame size"),
+    (b"YUV4MPEG2 W9 H8 C420\n", "not divisible"),
+    (b"YUV4MPEG2 W8 H8 C420p11\n", "unsupported y4m chroma tag"),
+    (b"YUV4MPEG2 W8 H8 C400\n", "unsupported y4m chroma tag"),
+])
+def test_header_errors(header, message):
+    with pytest.raises(y4m.Y4mError, match=message):
+        y4m.read_header(io.BytesIO(header))
+
+
+def test_frames_round_trip_and_truncation(tmp_path):
+    pairs, po, _ = _clip(tmp_path)
+    with y4m.Reader(po) as r:
+        got = list(r)
+    assert len(got) == len(pairs)
+    for img, (o, _) in zip(got, pairs):
+        assert np.array_equal(img.data, o.data)
+        assert img.format.depth == 10 and img.format.type == ss2.PixelType.Word
+    data = open(po, "rb").read()
+    (tmp_path / "t.y4m").write_bytes(data[:-5])
+    with y4m.Reader(str(tmp_path / "t.y4m")) as r, pytest.raises(y4m.Y4mError, match="truncated"):
+        list(r)
+
+
+def test_cli_rejects_mismatched_clips(tmp_path, capsys):
+    from vqm_b200 import cli
+    _, po, _ = _clip(tmp_path, frames=2)
+    short = tmp_path / "s.y4m"
+    o, _ = synthetic.yuv_pair(64, 48, 1)[:2]
+    y4m.write(str(short), [o], "420p10", fps=(30, 1))
+    assert cli.main([po, str(short)]) == 2
+    assert "frame rate" in capsys.readouterr().err
+
+
+@pytest.mark.gpu
+def test_cli_scores_frames_and_clip_mean(tmp_path):
+    from vqm_b200 import cli
+    pairs, po, pd = _clip(tmp_path)
+    # The reader gives the header's colours: limited BT.470BG, BT.709 transfer.
+    fmt = y4m.Reader(po).format
+    expected = []
+    for o, d in pairs:
+        oo, dd = ss2.Image(o.width, o.height, fmt, o.data), ss2.Image(d.width, d.height, fmt, d.data)
+        norms, score = helpers.oracle_compute(oo, dd)
+        expected.append((norms, score))
+    for batch in ("1", "2"):
+        out = io.StringIO()
+        assert cli.run([po, pd, "--json", "--raw", "--batch", batch], out=out) == 0
+        doc = json.loads(out.getvalue())
+        assert doc["frames"] == len(pairs)
+        for s, (_, score) in zip(doc["frame_scores"], expected):
+            assert abs(s - score) <= helpers.SCORE_TOL
+        assert abs(doc["score"] - np.mean([s for _, s in expected])) <= helpers.SCORE_TOL
+        assert len(doc["frame_norms"][0]) == 108
+        # Channel-major raw order: channel 0, scale 0, n 0 = ssim[0], ring[0], blur[2].
+        n0 = expected[0][0]
+        assert abs(doc["frame_norms"][0][0] - n0[0, 0]) <= 1e-4 * abs(n0[0, 0]) + 1e-9
+    out = io.StringIO()
+    assert cli.run([po, pd, "--raw"], out=out) == 0
+    lines = out.getvalue().strip().splitlines()
+    assert len(lines) == len(pairs) + 1
+    assert abs(float(lines[-1]) - doc["score"]) < 1e-7

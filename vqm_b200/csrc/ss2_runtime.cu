@@ -259,17 +259,20 @@ Tables BuildTables(const std::vector<std::pair<uint32_t, uint32_t>>& sizes, Blur
 // Splits the images into the table-decoded group and the generic group
 // (table[i][k]: image k of pair i decodes by table) and lays out each
 // group's prefix tile offsets. The list sizes do not depend on the split.
-void BuildPrepLists(Tables& t, const std::vector<std::array<bool, 2>>& table) {
+// `skip_original`, when set, leaves every pair's image 0 out (its pyramid is
+// already in place).
+void BuildPrepLists(Tables& t, const std::vector<std::array<bool, 2>>& table,
+                    bool skip_original = false) {
     uint32_t n[2] = {0, 0};
     for (size_t i = 0; i < t.pairs.size(); ++i)
-        for (int k = 0; k < 2; ++k) ++n[table[i][k] ? 0 : 1];
+        for (int k = skip_original ? 1 : 0; k < 2; ++k) ++n[table[i][k] ? 0 : 1];
     uint32_t at[2] = {0, n[0]};
     uint32_t* start[2] = {t.prep_start.data(), t.prep_start.data() + n[0] + 1};
     uint32_t blocks[2] = {0, 0};
     start[0][0] = 0;
     start[1][0] = 0;
     for (size_t i = 0; i < t.pairs.size(); ++i)
-        for (uint32_t k = 0; k < 2; ++k) {
+        for (uint32_t k = skip_original ? 1 : 0; k < 2; ++k) {
             const int g = table[i][k] ? 0 : 1;
             const uint32_t idx = at[g]++;
             t.prep_items[idx] = DevPrepItem{static_cast<uint32_t>(i), k};
@@ -504,6 +507,8 @@ public:
         stream_ = s ? static_cast<cudaStream_t>(s) : own_stream_;
     }
     void* GetStream() const { return stream_; }
+    // Submissions that reused the cached original's pyramid.
+    uint64_t ReferenceReuses() const { return reference_reuses_; }
     void SetGraphs(bool on) {
         RequireIdle();
         graphs_ = on;
@@ -571,7 +576,7 @@ public:
         VQM_CK(cudaSetDevice(device_));
         const Slot* s[2] = {&sa, &sb};
         for (int i = 0; i < 2; ++i) SourceFromDevice(i, s[i]->format, s[i]->memory.as<uint8_t>(), bg);
-        return Launch();
+        return LaunchWithOriginal(a, bg);
     }
 
     uint64_t SubmitResidentImage(uint64_t a, const vqm_cu_image* d, float bg) {
@@ -595,12 +600,12 @@ public:
                          strides);
             FillPlanes(src, d->format, d->width, d->height, planes, strides, "distorted");
             VQM_CK(cudaEventRecord(copied_, stream_));
-            const uint64_t token = Launch();
+            const uint64_t token = LaunchWithOriginal(a, bg);
             VQM_CK(cudaEventSynchronize(copied_));
             return token;
         }
         FillPlanes(src, d->format, d->width, d->height, d->planes, d->strides, "distorted");
-        return Launch();
+        return LaunchWithOriginal(a, bg);
     }
 
     uint64_t SubmitBuffers(uint64_t a, uint64_t b, float bg) {
@@ -619,6 +624,7 @@ public:
         VQM_CK(cudaSetDevice(device_));
         const cudaError_t e = cudaEventSynchronize(done_);
         in_flight_ = false;
+        if (e != cudaSuccess) reference_valid_ = false;
         Check(e, "pair execution");
         VQM_CK(cudaGetLastError());
         const double* r = mem_.results_host.as<double>();
@@ -669,6 +675,7 @@ public:
 
     void Release(uint64_t handle) {
         RequireIdle("Release");
+        if (reference_valid_ && handle == reference_handle_) reference_valid_ = false;
         const uint64_t idx = handle & kIndexMask;
         if (idx == 0 || idx > slots_.size()) return;
         Slot& s = slots_[idx - 1];
@@ -795,14 +802,35 @@ private:
         FillPlanes(src, f, cfg_.width, cfg_.height, planes, strides, i == 0 ? "original" : "distorted");
     }
 
+    // The reference-pyramid reuse of vulkan.cc:238-243, 714-736: when the
+    // original is the same resident slot (same handle, so the same image) as
+    // in the previous submission, with the same background, its pyramid
+    // planes are still in place and its prepare is skipped. Only resident
+    // slots are immutable; any other kind of submission, a Release of the
+    // slot or a failed run forgets the cached original.
+    uint64_t LaunchWithOriginal(uint64_t handle, float bg) {
+        const bool reuse =
+            reference_valid_ && handle == reference_handle_ && bg == reference_background_;
+        reference_valid_ = false;
+        const uint64_t token = Launch(reuse);
+        if (reuse) ++reference_reuses_;
+        reference_valid_ = true;
+        reference_handle_ = handle;
+        reference_background_ = bg;
+        return token;
+    }
+
     // [upload the pair record, prepare, blur, finalize, read back], as one
-    // graph replay when graphs are on.
-    uint64_t Launch() {
-        // Which images decode by table decides the two prepare launches; one
-        // graph per combination.
+    // graph replay when graphs are on. `skip_original` leaves the original's
+    // prepare out (its pyramid is cached).
+    uint64_t Launch(bool skip_original = false) {
+        if (!skip_original) reference_valid_ = false;
+        // Which images decode by table, and whether the original is
+        // prepared, decide the prepare launches; one graph per combination.
         const DevPair* hp = mem_.HostPair(0);
-        const int key = (hp->src[0].lut ? 1 : 0) | (hp->src[1].lut ? 2 : 0);
-        BuildPrepLists(tables_, {{hp->src[0].lut != 0, hp->src[1].lut != 0}});
+        const int key = (hp->src[0].lut ? 1 : 0) | (hp->src[1].lut ? 2 : 0) |
+                        (skip_original ? 4 : 0);
+        BuildPrepLists(tables_, {{hp->src[0].lut != 0, hp->src[1].lut != 0}}, skip_original);
         mem_.StagePrep(tables_);
         const size_t upload = mem_.head_bytes;
         // Stream capture needs a real stream; the legacy default stream runs
@@ -844,7 +872,11 @@ private:
     int device_ = 0;
     cudaStream_t own_stream_ = nullptr, stream_ = nullptr;
     cudaEvent_t done_ = nullptr, copied_ = nullptr;
-    cudaGraphExec_t graph_exec_[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaGraphExec_t graph_exec_[8] = {};
+    bool reference_valid_ = false;
+    uint64_t reference_handle_ = 0;
+    float reference_background_ = 0.0f;
+    uint64_t reference_reuses_ = 0;
     bool graphs_ = true;
     Tables tables_;
     BatchMemory mem_;
@@ -1173,6 +1205,14 @@ int vqm_cu_ss2_set_graphs(vqm_cu_ss2_pipeline* p, int enabled) {
     return Guard([&] {
         NotNull(p, "pipeline");
         p->impl.SetGraphs(enabled != 0);
+    });
+}
+
+int vqm_cu_ss2_reference_reuses(vqm_cu_ss2_pipeline* p, uint64_t* count) {
+    return Guard([&] {
+        NotNull(p, "pipeline");
+        NotNull(count, "count");
+        *count = p->impl.ReferenceReuses();
     });
 }
 

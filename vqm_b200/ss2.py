@@ -198,6 +198,7 @@ _SIGS = {
     "vqm_cu_ss2_set_stream": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_get_stream": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_set_graphs": ([_P, ctypes.c_int], ctypes.c_int),
+    "vqm_cu_ss2_reference_reuses": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_submit": ([_P, _P, _P, ctypes.c_float, _P], ctypes.c_int),
     "vqm_cu_ss2_submit_resident": ([_P, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float, _P], ctypes.c_int),
     "vqm_cu_ss2_submit_resident_image": ([_P, ctypes.c_uint64, _P, ctypes.c_float, _P], ctypes.c_int),
@@ -491,6 +492,13 @@ class Ssimulacra2Pipeline:
 
     def set_graphs(self, enabled: bool):
         _check(_lib.vqm_cu_ss2_set_graphs(self._p, int(enabled)))
+
+    def reference_reuses(self) -> int:
+        """Submissions that reused the cached pyramid of a resident original
+        (vulkan.cc:238-243, 714-736)."""
+        n = ctypes.c_uint64()
+        _check(_lib.vqm_cu_ss2_reference_reuses(self._p, ctypes.byref(n)))
+        return n.value
 
     def submit(self, original, distorted, background: float = 0.5) -> int:
         tok = ctypes.c_uint64()
