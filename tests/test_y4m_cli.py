@@ -104,3 +104,24 @@ def test_cli_scores_frames_and_clip_mean(tmp_path):
     lines = out.getvalue().strip().splitlines()
     assert len(lines) == len(pairs) + 1
     assert abs(float(lines[-1]) - doc["score"]) < 1e-7
+
+
+@pytest.mark.gpu
+def test_cli_alpha_keeps_the_worse_background(tmp_path):
+    from vqm_b200 import cli
+    fmt = y4m.read_header(io.BytesIO(b"YUV4MPEG2 W64 H48 C444alpha\n")).format
+    rng = np.random.default_rng(3)
+    base = synthetic.texture(64, 48, rng) / 255.0
+    alpha = 0.2 + 0.8 * base[2]
+    ov = [base[0], (base[1] - 0.5) * 0.6, (base[2] - 0.5) * 0.6, alpha]
+    dv = [np.clip(v + rng.normal(0, 0.03, v.shape), -0.5 if i in (1, 2) else 0, 1)
+          for i, v in enumerate(ov)]
+    o, d = helpers.pack_planes(fmt, 64, 48, ov), helpers.pack_planes(fmt, 64, 48, dv)
+    po, pd = str(tmp_path / "o.y4m"), str(tmp_path / "d.y4m")
+    y4m.write(po, [o], "444alpha")
+    y4m.write(pd, [d], "444alpha")
+    with ss2.Ssimulacra2Pipeline(64, 48) as p:
+        worse = min(p.compute(o, d, 0.1).score(), p.compute(o, d, 0.9).score())
+    out = io.StringIO()
+    assert cli.run([po, pd, "--json", "--batch", "1"], out=out) == 0
+    assert json.loads(out.getvalue())["frame_scores"] == [worse]

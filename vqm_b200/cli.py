@@ -67,7 +67,7 @@ def raw_norms(result) -> list[float]:
 
 
 def _format(header, args):
-    f = ss2.ImageFormat(*[getattr(header.format, n) for n, _ in header.format._fields_])
+    f = ss2.ImageFormat.from_buffer_copy(header.format)
     if args.input_range:
         f.range = ss2.PixelRange.Full if args.input_range == "full" else ss2.PixelRange.Limited
     if args.input_matrix:
