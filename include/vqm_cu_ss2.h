@@ -82,7 +82,9 @@ typedef struct vqm_cu_ss2_config {
     uint32_t width;
     uint32_t height;
     uint32_t gpu_resident_images; /* slots for upload(); default 2 */
-    uint32_t half_planes;         /* 1: FP16 pyramid planes */
+    uint32_t half_planes;         /* 1: binary16 pyramid planes: FP32 arithmetic,
+                                     the planes and the level averages rounded
+                                     to binary16 (ssimu2_common.glsl:45-91) */
     uint32_t chroma_filter;       /* 0 bilinear, 1 bicubic, 2 lanczos */
     uint32_t streaming_inputs;    /* 1: host-image submit overloads allowed */
     uint64_t input_bytes;         /* pool for allocate_image(); 0 = none */
@@ -259,6 +261,8 @@ typedef struct vqm_cu_ss2_batch_config {
     uint32_t tile_w, tile_h; /* blur tile; 0 = the tuned default */
     uint32_t variant;      /* blur kernel: 0 = by tile (or the tuned
                               default), k = compiled variant k - 1 */
+    uint32_t half_planes;  /* 1: binary16 pyramid planes, as
+                              vqm_cu_ss2_config.half_planes */
 } vqm_cu_ss2_batch_config;
 
 /* The blur kernels compiled into the library, for tuning: *count variants,

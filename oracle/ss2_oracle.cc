@@ -30,6 +30,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <limits>
 #include <stdexcept>
 #include <string>
@@ -1013,12 +1014,38 @@ struct Pyramid {
     std::vector<T> planes[kMaxScales][3];
 };
 
-// prepare.comp:103-111: ((((0+a)+b)+c)+d) * 0.25.
+// IEEE binary16 rounding (to nearest, ties to even) of a float, returned as
+// float: the plane_round / plane_store of the half-plane build
+// (ssimu2_common.glsl:45-56, 86-91). Normal halves keep 11 significant bits;
+// below 2^-14 the quantum is 2^-24; beyond 65504 the value becomes infinite.
+float RoundHalf(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    const uint32_t a = u & 0x7fffffffu;
+    if (a >= 0x7f800000u) return f;  // inf, NaN
+    float r;
+    if (a >= 0x38800000u) {  // |f| >= 2^-14: drop 13 mantissa bits, ties to even
+        const uint32_t lsb = (u >> 13) & 1u;
+        const uint32_t v = (u + 0xfffu + lsb) & ~0x1fffu;
+        std::memcpy(&r, &v, 4);
+        if (std::fabs(r) > 65504.0f) r = std::copysign(INFINITY, f);
+    } else {  // subnormal half: a multiple of 2^-24
+        r = std::nearbyint(f * 16777216.0f) * 5.9604644775390625e-8f;
+        if (r == 0.0f) r = std::copysign(0.0f, f);
+    }
+    return r;
+}
+
+// prepare.comp:103-111: ((((0+a)+b)+c)+d) * 0.25, rounded to half with
+// half planes (the average used to pass through the plane region).
 template <class T>
-T BoxAverage(T a, T b, T c, T d) {
+T BoxAverage(T a, T b, T c, T d, bool half = false) {
     T s = T(0);
     s += a; s += b; s += c; s += d;
-    return s * T(0.25);
+    s = s * T(0.25);
+    if constexpr (std::is_same_v<T, float>)
+        if (half) s = RoundHalf(s);
+    return s;
 }
 
 // prepare.comp:170-232: level 0 from the decoded blocks, level l >= 1 the
@@ -1026,7 +1053,7 @@ T BoxAverage(T a, T b, T c, T d) {
 // for the channels the pruning mask keeps.
 template <class T>
 void BuildPyramid(const ss2o_image& img, const Desc& desc, T bg, const Plan& plan,
-                  Pyramid<T>& pyr) {
+                  Pyramid<T>& pyr, bool half = false) {
     pyr.levels = plan.count;
     for (int l = 0; l < plan.count; ++l) {
         pyr.sizes[l] = plan.sizes[l];
@@ -1060,8 +1087,12 @@ void BuildPyramid(const ss2o_image& img, const Desc& desc, T bg, const Plan& pla
                 T xyb[3];
                 Xyb(&lin[(size_t(y) * w + x) * 3], xyb);
                 for (int c = 0; c < 3; ++c)
-                    if (!pyr.planes[l][c].empty())
-                        pyr.planes[l][c][size_t(y) * w + x] = xyb[c];
+                    if (!pyr.planes[l][c].empty()) {
+                        T v = xyb[c];
+                        if constexpr (std::is_same_v<T, float>)
+                            if (half) v = RoundHalf(v);
+                        pyr.planes[l][c][size_t(y) * w + x] = v;
+                    }
             }
         if (l + 1 < plan.count) {
             const uint32_t nw = plan.sizes[l + 1].w, nh = plan.sizes[l + 1].h;
@@ -1073,7 +1104,8 @@ void BuildPyramid(const ss2o_image& img, const Desc& desc, T bg, const Plan& pla
                     for (int c = 0; c < 3; ++c)
                         next[(size_t(y) * nw + x) * 3 + c] = BoxAverage(
                             lin[(size_t(y0) * w + x0) * 3 + c], lin[(size_t(y0) * w + x1) * 3 + c],
-                            lin[(size_t(y1) * w + x0) * 3 + c], lin[(size_t(y1) * w + x1) * 3 + c]);
+                            lin[(size_t(y1) * w + x0) * 3 + c], lin[(size_t(y1) * w + x1) * 3 + c],
+                            half);
                 }
             lin.swap(next);
         }
@@ -1229,7 +1261,7 @@ struct PairResult {
 // The whole pair: both pyramids, then every kept (level, channel).
 template <class T>
 PairResult<T> ComputePair(const ss2o_image& o, const ss2o_image& dsrc, float background,
-                          int chroma_filter) {
+                          int chroma_filter, bool half = false) {
     if (o.width != dsrc.width || o.height != dsrc.height)
         throw std::invalid_argument("image sizes differ");
     const Plan plan = PlanScales(o.width, o.height);
@@ -1239,8 +1271,8 @@ PairResult<T> ComputePair(const ss2o_image& o, const ss2o_image& dsrc, float bac
         dsrc.bytes < RequiredBytes(dsrc.format, dsrc.width, dsrc.height))
         throw std::invalid_argument("data size does not match the image format");
     Pyramid<T> p0, p1;
-    BuildPyramid<T>(o, d0, static_cast<T>(background), plan, p0);
-    BuildPyramid<T>(dsrc, d1, static_cast<T>(background), plan, p1);
+    BuildPyramid<T>(o, d0, static_cast<T>(background), plan, p0, half);
+    BuildPyramid<T>(dsrc, d1, static_cast<T>(background), plan, p1, half);
     const auto wt = Taps<T>();
     PairResult<T> r;
     r.scales = plan.count;
@@ -1293,7 +1325,7 @@ int ComputeOne(const ss2o_image* o, const ss2o_image* d, float bg, int filter,
         const auto r = ComputePair<double>(*o, *d, bg, filter);
         ReadResult(r, plan, norms);
     } else {
-        const auto r = ComputePair<float>(*o, *d, bg, filter);
+        const auto r = ComputePair<float>(*o, *d, bg, filter, precision == 16);
         ReadResult(r, plan, norms);
     }
     if (scales) *scales = static_cast<uint32_t>(plan.count);
@@ -1472,6 +1504,7 @@ int ss2o_detmath(int fn, const float* x, float y, float* out, size_t n) {
             case 1: out[i] = ss2dm::pow(x[i], y); break;
             case 2: out[i] = ss2dm::exp(x[i]); break;
             case 3: out[i] = ss2dm::sinpi(x[i]); break;
+            case 4: out[i] = RoundHalf(x[i]); break;
             default: g_error = "unknown function"; return SS2O_INVALID;
         }
     }

@@ -64,7 +64,8 @@ typedef struct ss2o_image {
 #define SS2O_INVALID 1
 
 /* Scores one pair. precision: 32 = the FP32 restatement (VQM proxy), 64 =
- * the same algorithm in FP64. Writes 18*scales doubles into norms[108], the
+ * the same algorithm in FP64, 16 = the FP32 restatement of VQM's half-plane
+ * build (pyramid planes and level averages rounded to binary16). Writes 18*scales doubles into norms[108], the
  * scale count into *scales and the score into *score. */
 int ss2o_compute(const ss2o_image* original, const ss2o_image* distorted,
                  float background, int chroma_filter, int precision,
@@ -97,7 +98,8 @@ int ss2o_level_sums(const ss2o_image* original, const ss2o_image* distorted,
                     float background, int chroma_filter, float* sums,
                     uint32_t* scales);
 /* The shared deterministic functions, for their accuracy tests: fn 0 cube
- * root, 1 pow(x, y), 2 exp, 3 sin(pi x). */
+ * root, 1 pow(x, y), 2 exp, 3 sin(pi x), 4 rounding to binary16 (the
+ * half-plane build's plane rounding). */
 int ss2o_detmath(int fn, const float* x, float y, float* out, size_t n);
 const char* ss2o_last_error(void);
 

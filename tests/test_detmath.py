@@ -93,3 +93,14 @@ def test_cbrt_every_float_of_three_binades():
     got = det(0, x)
     want = np.cbrt(x.astype(np.float64)).astype(np.float32)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_round_half_matches_ieee_binary16():
+    rng = np.random.default_rng(7)
+    x = np.concatenate([
+        rng.uniform(-2, 2, 1_000_000), np.exp(rng.uniform(np.log(1e-9), np.log(7e4), 500_000)),
+        np.float32([0.0, -0.0, 65504.0, 65519.0, 65520.0, 6.0e-8, 2.98e-8, 6.1035e-5,
+                    np.inf, -np.inf])]).astype(np.float32)
+    want = x.astype(np.float16).astype(np.float32)
+    got = det(4, x)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))

@@ -25,6 +25,7 @@
 // A persistent form keeps each CTA resident and copies its next tile's
 // window into a second buffer while it computes the current one.
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -93,15 +94,23 @@ struct TileRef {
     int w, h, x0, y0;
 };
 
-template <int TW, int TH>
+// With half planes pa and pb point at binary16 elements (typed float* only
+// to share the struct).
+template <int TW, int TH, bool kHalf = false>
 __device__ __forceinline__ TileRef LocateTile(const DevBatch& batch, uint32_t blk) {
     const uint32_t si = FindSlot(batch.blur_start, batch.segments, blk);
     const DevSegment seg = batch.seg[si];
     const uint32_t tile = blk - __ldg(&batch.blur_start[si]);
     const DevPair& P = batch.pair[seg.pair];
     TileRef t;
-    t.pa = P.pyramid + P.plane_off[seg.level][seg.channel];
-    t.pb = t.pa + P.image_stride;
+    if (kHalf) {
+        const __half* a = reinterpret_cast<const __half*>(P.pyramid) + P.plane_off[seg.level][seg.channel];
+        t.pa = reinterpret_cast<const float*>(a);
+        t.pb = reinterpret_cast<const float*>(a + P.image_stride);
+    } else {
+        t.pa = P.pyramid + P.plane_off[seg.level][seg.channel];
+        t.pb = t.pa + P.image_stride;
+    }
     t.pitch = P.pitch[seg.level];
     t.w = static_cast<int>(P.w[seg.level]);
     t.h = static_cast<int>(P.h[seg.level]);
@@ -145,6 +154,63 @@ __device__ __forceinline__ void IssueTileLoads(float* buf, const TileRef& t) {
         const uint32_t dst = base + 4u * static_cast<uint32_t>(rp * T::SRS + 4 * cp);
         CpAsync16(dst, t.pa + off, in);
         CpAsync16(dst + 4u * T::IMG, t.pb + off, in);
+    }
+}
+
+// Half planes: 16-byte chunks are 4 columns x 2 rows of binary16 elements,
+// so the copied window starts 8 columns left of the tile (4-column aligned,
+// as x0 is) and spans TW + 16 columns; it is staged in `staging` (the
+// horizontal planes' space, unused until the horizontal pass) and widened to
+// the float window by ConvertHalfTile.
+template <int TW, int TH, int NT>
+struct HalfWindow {
+    using T = Tile<TW, TH, NT>;
+    static constexpr int CQ = (TW + 16) / 4;              // chunks per row pair
+    static constexpr int CHUNKS = T::RP * CQ;             // per image
+    static constexpr size_t kBytes = 2 * CHUNKS * 16;
+    static_assert(kBytes <= T::kHqBytes, "the staging fits the horizontal planes");
+};
+
+template <int TW, int TH, int NT>
+__device__ __forceinline__ void IssueTileLoadsHalf(unsigned char* staging, const TileRef& t) {
+    using H = HalfWindow<TW, TH, NT>;
+    const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(staging));
+    const uint32_t wq = static_cast<uint32_t>(t.w + 3) >> 2;  // chunks per row pair
+    const uint32_t hp = static_cast<uint32_t>(t.h + 1) >> 1;  // row pairs
+    const int cq0 = (t.x0 >> 2) - 2, ry0 = (t.y0 >> 1) - kRadius / 2;
+    const __half* pa = reinterpret_cast<const __half*>(t.pa);
+    const __half* pb = reinterpret_cast<const __half*>(t.pb);
+    for (int k = threadIdx.x; k < H::CHUNKS; k += NT) {
+        const int rp = k / H::CQ, q = k - rp * H::CQ;
+        const int gy = ry0 + rp, gq = cq0 + q;
+        const bool in = static_cast<uint32_t>(gy) < hp && static_cast<uint32_t>(gq) < wq;
+        const uint32_t off = in ? static_cast<uint32_t>(gy) * t.pitch + 8u * static_cast<uint32_t>(gq)
+                                : 0u;
+        const uint32_t dst = base + 16u * static_cast<uint32_t>(k);
+        CpAsync16(dst, reinterpret_cast<const float*>(pa + off), in);
+        CpAsync16(dst + 16u * H::CHUNKS, reinterpret_cast<const float*>(pb + off), in);
+    }
+}
+
+// The staged binary16 window to the float row-pair window of `src`.
+template <int TW, int TH, int NT>
+__device__ __forceinline__ void ConvertHalfTile(const unsigned char* staging, float* src) {
+    using T = Tile<TW, TH, NT>;
+    using H = HalfWindow<TW, TH, NT>;
+    for (int k = threadIdx.x; k < 2 * H::CHUNKS; k += NT) {
+        const int img = k >= H::CHUNKS ? 1 : 0;
+        const int kk = k - img * H::CHUNKS;
+        const int rp = kk / H::CQ, q = kk - rp * H::CQ;
+        const uint4 v = *reinterpret_cast<const uint4*>(staging + 16 * k);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+        float* row = src + img * T::IMG + rp * T::SRS;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int col = 4 * q + i - 2;  // float window column (x0 - 6 based)
+            if (col < 0 || col >= T::SW) continue;
+            const __half2 h = *reinterpret_cast<const __half2*>(&w[i]);
+            *reinterpret_cast<float2*>(row + 2 * col) = __half22float2(h);
+        }
     }
 }
 
@@ -345,17 +411,22 @@ __device__ __forceinline__ void ComputeTile(float* src, float* hq, const TileRef
 
 // One output tile per CTA; MB CTAs per SM is the occupancy the shared
 // memory allows, which bounds the registers per thread.
-template <int TW, int TH, int NT, int MB>
+template <int TW, int TH, int NT, int MB, bool kHalf = false>
 __global__ void __launch_bounds__(NT, MB) Ss2BlurKernel(DevBatch batch) {
     using T = Tile<TW, TH, NT>;
     extern __shared__ __align__(16) unsigned char smem[];
     float* src = reinterpret_cast<float*>(smem);
     float* hq = reinterpret_cast<float*>(smem + T::kSrcBytes);
-    const TileRef t = LocateTile<TW, TH>(batch, blockIdx.x);
-    IssueTileLoads<TW, TH, NT>(src, t);
+    const TileRef t = LocateTile<TW, TH, kHalf>(batch, blockIdx.x);
+    if (kHalf) IssueTileLoadsHalf<TW, TH, NT>(smem + T::kSrcBytes, t);
+    else IssueTileLoads<TW, TH, NT>(src, t);
     CpAsyncCommit();
     CpAsyncWait<0>();
     __syncthreads();
+    if (kHalf) {
+        ConvertHalfTile<TW, TH, NT>(smem + T::kSrcBytes, src);
+        __syncthreads();
+    }
     ComputeTile<TW, TH, NT>(src, hq, t, batch.partials);
 }
 
@@ -441,16 +512,21 @@ cudaError_t Prepare(Kernel kernel, size_t smem, LaunchCache& cache, int threads,
     return cudaSuccess;
 }
 
-template <int TW, int TH, int NT, int MB>
-cudaError_t LaunchTiles(const DevBatch& b, cudaStream_t stream) {
+template <int TW, int TH, int NT, int MB, bool kHalf>
+cudaError_t LaunchTilesAs(const DevBatch& b, cudaStream_t stream) {
     using T = Tile<TW, TH, NT>;
     static LaunchCache cache;
     constexpr size_t smem = T::kSrcBytes + T::kHqBytes;
     const cudaError_t e =
-        Prepare(Ss2BlurKernel<TW, TH, NT, MB>, smem, cache, NT, false, nullptr);
+        Prepare(Ss2BlurKernel<TW, TH, NT, MB, kHalf>, smem, cache, NT, false, nullptr);
     if (e != cudaSuccess) return e;
-    Ss2BlurKernel<TW, TH, NT, MB><<<b.blur_blocks, NT, smem, stream>>>(b);
+    Ss2BlurKernel<TW, TH, NT, MB, kHalf><<<b.blur_blocks, NT, smem, stream>>>(b);
     return cudaGetLastError();
+}
+template <int TW, int TH, int NT, int MB>
+cudaError_t LaunchTiles(const DevBatch& b, cudaStream_t stream) {
+    return b.half ? LaunchTilesAs<TW, TH, NT, MB, true>(b, stream)
+                  : LaunchTilesAs<TW, TH, NT, MB, false>(b, stream);
 }
 
 template <int TW, int TH, int NT, int MB>
@@ -478,6 +554,9 @@ cudaError_t SetConstants(const float* taps13, const double* weights108) {
 
 cudaError_t LaunchBlur(const DevBatch& b, int variant, cudaStream_t stream) {
     if (b.blur_blocks == 0) return cudaSuccess;
+    // Half planes run the one-tile-per-CTA kernel of the same tile shape.
+    if (b.half) variant = HalfPlaneVariant(variant);
+    if (variant < 0) return cudaErrorInvalidValue;
     switch (variant) {
         case 0: return LaunchTiles<32, 32, 128, 5>(b, stream);
         case 1: return LaunchTiles<32, 28, 128, 5>(b, stream);
@@ -488,6 +567,16 @@ cudaError_t LaunchBlur(const DevBatch& b, int variant, cudaStream_t stream) {
         case 6: return LaunchPersistent<64, 32, 256, 1>(b, stream);
     }
     return cudaErrorInvalidValue;
+}
+
+int HalfPlaneVariant(int variant) {
+    if (variant < 0 || variant >= kBlurVariantCount) return -1;
+    if (!kBlurVariants[variant].persistent) return variant;
+    for (int i = 0; i < kBlurVariantCount; ++i)
+        if (!kBlurVariants[i].persistent && kBlurVariants[i].w == kBlurVariants[variant].w &&
+            kBlurVariants[i].h == kBlurVariants[variant].h)
+            return i;
+    return -1;
 }
 
 int BlurTileCount() { return kBlurVariantCount; }

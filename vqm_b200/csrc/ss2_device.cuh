@@ -118,6 +118,7 @@ struct DevBatch {
     double* seg_sums;            // 6 doubles per segment
     uint32_t* pair_done;         // per pair: segments finalized so far
     uint32_t* status;            // nonzero: a kernel found bad input
+    uint32_t half;               // 1: pyramid elements are binary16
 };
 
 }  // namespace vqm_b200

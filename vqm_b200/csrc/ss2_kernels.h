@@ -23,6 +23,9 @@ cudaError_t LaunchFinalize(const DevBatch& batch, cudaStream_t stream);
 int BlurTileCount();
 void BlurTileShape(int index, int* w, int* h);
 int BlurTileThreads(int index);
+// The one-tile-per-CTA variant with variant's tile shape (the variant
+// itself when it is one), which half planes run; -1 when there is none.
+int HalfPlaneVariant(int variant);
 // The variant used when a caller does not choose one.
 constexpr int kDefaultBlurVariant = 0;
 

@@ -7,10 +7,11 @@
 // 2x2 block as one float4; the blur kernel copies its tiles in 16-byte chunks
 // and its horizontal pass gets two rows of a column from one 64-bit load.
 //
-// pitch = 2 * round_up(w, 32) floats, so every row pair starts on a 256-byte
-// boundary. Column w (when w is odd) and row h (when h is odd) are padding
-// that prepare writes as 0: a 2x2 chunk at the right or bottom edge then
-// reads zeros there, which is the blur's zero padding (scale.comp:107-124).
+// pitch = 2 * round_up(w, 32) elements, so every row pair starts on a
+// 256-byte boundary (128 with half planes). The columns up to PaddedColumns(w)
+// and row h (when h is odd) are padding that prepare writes as 0: a copy chunk
+// at the right or bottom edge then reads zeros there, which is the blur's zero
+// padding (scale.comp:107-124). With half planes the elements are binary16.
 #pragma once
 
 #include <cstddef>
@@ -33,6 +34,13 @@ SS2_HD uint32_t RowPairPitch(uint32_t w) { return 2u * ((w + 31u) / 32u * 32u); 
 SS2_HD uint32_t RowPairs(uint32_t h) { return (h + 1u) / 2u; }
 SS2_HD size_t PlaneFloats(uint32_t w, uint32_t h) {
     return static_cast<size_t>(RowPairPitch(w)) * RowPairs(h);
+}
+// Columns of a level plane that prepare writes: the level's width rounded up
+// to the blur's copy unit, 2 columns (one 16-byte chunk of float row pairs)
+// or 4 with half planes (binary16 elements, same element layout); the
+// columns past the width are written as 0.
+SS2_HD uint32_t PaddedColumns(uint32_t w, bool half) {
+    return half ? (w + 3u) & ~3u : (w + 1u) & ~1u;
 }
 SS2_HD size_t PlaneIndex(uint32_t pitch, uint32_t x, uint32_t y) {
     return static_cast<size_t>(y >> 1) * pitch + 2u * x + (y & 1u);

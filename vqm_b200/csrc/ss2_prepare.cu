@@ -19,6 +19,7 @@
 // operations, so the planes this kernel writes are bit-identical to the CPU
 // checker's.
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -119,33 +120,66 @@ __device__ __forceinline__ void Xyb(float r, float g, float b, uint32_t mask, fl
     out[2] = o[2].x;
 }
 
-// prepare.comp:103-111: ((((0 + a) + b) + c) + d) * 0.25.
-__device__ __forceinline__ float BoxAverage(float a, float b, float c, float d) {
-    return __fmul_rn(__fadd_rn(__fadd_rn(__fadd_rn(a, b), c), d), 0.25f);
+// The half-plane build's rounding of a plane value (ssimu2_common.glsl:86-91).
+template <bool kHalf>
+__device__ __forceinline__ float PlaneRound(float v) {
+    return kHalf ? __half2float(__float2half_rn(v)) : v;
 }
 
-// Per-level addressing of this image's planes, staged in shared memory.
+// prepare.comp:103-111: ((((0 + a) + b) + c) + d) * 0.25, rounded like a
+// plane value (the average used to reach the next level through the planes).
+template <bool kHalf>
+__device__ __forceinline__ float BoxAverage(float a, float b, float c, float d) {
+    return PlaneRound<kHalf>(__fmul_rn(__fadd_rn(__fadd_rn(__fadd_rn(a, b), c), d), 0.25f));
+}
+
+// Per-level addressing of this image's planes, staged in shared memory:
+// float elements, or binary16 ones with half planes.
 struct LevelInfo {
-    float* plane[kMaxLevels][3];  // nullptr when pruned
+    void* plane[kMaxLevels][3];  // nullptr when pruned
     uint32_t w[kMaxLevels], h[kMaxLevels], pitch[kMaxLevels], mask[kMaxLevels];
     uint32_t levels;
 };
 
+template <bool kHalf>
+__device__ __forceinline__ void PutPlane(void* plane, size_t at, float v) {
+    if (kHalf) static_cast<__half*>(plane)[at] = __float2half_rn(v);
+    else static_cast<float*>(plane)[at] = v;
+}
+
 // Writes pixel (x, y) of `level` with XYB value `xyb` (kept channels): the
-// value inside the level, 0 in the padding column and row of an odd-sized
-// level (ss2_layout.h), nothing beyond. Every padding entry has a thread: a
-// level's tile grid spans an even number (64 >> level) of columns and rows
-// per tile, so at least one past an odd size.
+// value inside the level, 0 in the padding columns and row past an unaligned
+// size (ss2_layout.h: to a multiple of 2 columns, 4 with half planes), nothing
+// beyond. Every padding entry has a thread: a level's tile grid spans a
+// multiple of 64 >> level (at least 4) columns and rows.
+template <bool kHalf>
 __device__ __forceinline__ void StorePixel(const LevelInfo& lv, uint32_t level, uint32_t x,
                                            uint32_t y, float x_, float y_, float b_) {
     const uint32_t mask = lv.mask[level];
     const uint32_t w = lv.w[level], h = lv.h[level];
-    if (!mask || x >= ((w + 1) & ~1u) || y >= ((h + 1) & ~1u)) return;
+    if (!mask || x >= PaddedColumns(w, kHalf) || y >= ((h + 1) & ~1u)) return;
     const bool inside = x < w && y < h;
     const size_t at = PlaneIndex(lv.pitch[level], x, y);
-    if (mask & 1u) lv.plane[level][0][at] = inside ? x_ : 0.0f;
-    if (mask & 2u) lv.plane[level][1][at] = inside ? y_ : 0.0f;
-    if (mask & 4u) lv.plane[level][2][at] = inside ? b_ : 0.0f;
+    if (mask & 1u) PutPlane<kHalf>(lv.plane[level][0], at, inside ? x_ : 0.0f);
+    if (mask & 2u) PutPlane<kHalf>(lv.plane[level][1], at, inside ? y_ : 0.0f);
+    if (mask & 4u) PutPlane<kHalf>(lv.plane[level][2], at, inside ? b_ : 0.0f);
+}
+
+// Level 0's 2x2 block at (x0, y0) as one aligned store of the row-pair plane:
+// (x0, y0), (x0, y0+1), (x0+1, y0), (x0+1, y0+1).
+template <bool kHalf>
+__device__ __forceinline__ void PutBlock(void* plane, size_t at, float a, float b, float c,
+                                         float d) {
+    if (kHalf) {
+        __half2* p = reinterpret_cast<__half2*>(static_cast<__half*>(plane) + at);
+        uint2 v;
+        const __half2 lo = __floats2half2_rn(a, b), hi = __floats2half2_rn(c, d);
+        v.x = *reinterpret_cast<const uint32_t*>(&lo);
+        v.y = *reinterpret_cast<const uint32_t*>(&hi);
+        *reinterpret_cast<uint2*>(p) = v;
+    } else {
+        *reinterpret_cast<float4*>(static_cast<float*>(plane) + at) = make_float4(a, b, c, d);
+    }
 }
 
 // The four samples of base block (bx, by) of an 8-bit image, as table
@@ -194,7 +228,7 @@ __device__ __forceinline__ void TableBlock(const DevSource& s, const float* lut,
 #ifndef VQM_GENERIC_PREPARE_CTAS
 #define VQM_GENERIC_PREPARE_CTAS 4
 #endif
-template <bool kTable>
+template <bool kTable, bool kHalf>
 __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTAS)
     PrepareKernel(DevBatch batch) {
     // Level-1 tile (32x32) of each channel, then the levels after it in two
@@ -228,9 +262,10 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
         if (tid < kMaxLevels * 3) {
             const uint32_t l = tid / 3, c = tid % 3;
             const bool kept = l < P.levels && (P.mask[l] & (1u << c));
-            lv.plane[l][c] = kept ? P.pyramid + static_cast<size_t>(image) * P.image_stride +
-                                        P.plane_off[l][c]
-                                  : nullptr;
+            const size_t elem = static_cast<size_t>(image) * P.image_stride + P.plane_off[l][c];
+            lv.plane[l][c] = !kept ? nullptr
+                             : kHalf ? static_cast<void*>(reinterpret_cast<__half*>(P.pyramid) + elem)
+                                     : static_cast<void*>(P.pyramid + elem);
         }
         if (tid < kMaxLevels) {
             lv.w[tid] = P.w[tid];
@@ -253,6 +288,8 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
     const uint32_t levels = lv.levels;
     const uint32_t width = s.width, height = s.height;
     const uint32_t wb = (width + 1) / 2, hb = (height + 1) / 2;  // base blocks
+    // Blocks of level 0's plane, padding included (ss2_layout.h).
+    const uint32_t wb_pad = PaddedColumns(width, kHalf) / 2;
     const uint32_t tx = tid & 15, ty = tid >> 4;
     const uint32_t mask0 = lv.mask[0];
 
@@ -290,6 +327,14 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
             const uint32_t bx = bx0 + hx;
             float lin[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
             const bool in_block = bx < wb && by < hb;
+            if (kHalf && !in_block && bx < wb_pad && by < hb && mask0) {
+                // Padding blocks past the image's last column: zeros.
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    if (mask0 & (1u << c))
+                        PutBlock<kHalf>(lv.plane[0][c], PlaneIndex(lv.pitch[0], 2 * bx, 2 * by),
+                                        0.0f, 0.0f, 0.0f, 0.0f);
+            }
             if (in_block) {
                 if (kTable) TableBlock(s, lut, fast, w4, hx, bx, by, lin);
                 else BlockLinearGeneric(s, bx, by, lin);
@@ -308,16 +353,16 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         if (!(mask0 & (1u << c))) continue;
-                        float* at = lv.plane[0][c] + PlaneIndex(lv.pitch[0], x0, y0);
-                        *reinterpret_cast<float4*>(at) = make_float4(
-                            top[c].x, second_row ? bottom[c].x : 0.0f, two ? top[c].y : 0.0f,
-                            two && second_row ? bottom[c].y : 0.0f);
+                        PutBlock<kHalf>(lv.plane[0][c], PlaneIndex(lv.pitch[0], x0, y0), top[c].x,
+                                        second_row ? bottom[c].x : 0.0f, two ? top[c].y : 0.0f,
+                                        two && second_row ? bottom[c].y : 0.0f);
                     }
                 }
             }
             float avg[3];
 #pragma unroll
-            for (int c = 0; c < 3; ++c) avg[c] = BoxAverage(lin[0][c], lin[1][c], lin[2][c], lin[3][c]);
+            for (int c = 0; c < 3; ++c)
+                avg[c] = BoxAverage<kHalf>(lin[0][c], lin[1][c], lin[2][c], lin[3][c]);
             // Register copies, not an index, for the rolled form.
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
@@ -330,8 +375,8 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
             float2 xyb[3];
             Xyb2(make_float2(l1[0][0], l1[1][0]), make_float2(l1[0][1], l1[1][1]),
                  make_float2(l1[0][2], l1[1][2]), lv.mask[1], xyb);
-            StorePixel(lv, 1, bx0, by, xyb[0].x, xyb[1].x, xyb[2].x);
-            StorePixel(lv, 1, bx0 + 1, by, xyb[0].y, xyb[1].y, xyb[2].y);
+            StorePixel<kHalf>(lv, 1, bx0, by, xyb[0].x, xyb[1].x, xyb[2].x);
+            StorePixel<kHalf>(lv, 1, bx0 + 1, by, xyb[0].y, xyb[1].y, xyb[2].y);
             if (last >= 2) {
                 const uint32_t at = (ty + 16 * vy) * kBlocks + 2 * tx;
 #pragma unroll
@@ -370,12 +415,12 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const float* p = prev0 + c * prev_stride;
-            v[c] = BoxAverage(p[cy0 * prev_side + cx0], p[cy0 * prev_side + cx1],
-                              p[cy1 * prev_side + cx0], p[cy1 * prev_side + cx1]);
+            v[c] = BoxAverage<kHalf>(p[cy0 * prev_side + cx0], p[cy0 * prev_side + cx1],
+                                     p[cy1 * prev_side + cx0], p[cy1 * prev_side + cx1]);
         }
         float xyb[3];
         Xyb(v[0], v[1], v[2], lv.mask[level], xyb);
-        StorePixel(lv, level, gx * side + jx, gy * side + jy, xyb[0], xyb[1], xyb[2]);
+        StorePixel<kHalf>(lv, level, gx * side + jx, gy * side + jy, xyb[0], xyb[1], xyb[2]);
         if (level < last) {
             float* next0 = (level & 1u) ? &ladder_a[0][0] : &ladder_b[0][0];
             const uint32_t next_stride = (level & 1u) ? kBlocks * kBlocks : kBlocks * kBlocks / 4;
@@ -394,8 +439,13 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
 }  // namespace
 
 cudaError_t LaunchPrepare(const DevBatch& b, cudaStream_t stream) {
-    if (b.prep_blocks[0]) PrepareKernel<true><<<b.prep_blocks[0], kThreads, 0, stream>>>(b);
-    if (b.prep_blocks[1]) PrepareKernel<false><<<b.prep_blocks[1], kThreads, 0, stream>>>(b);
+    if (b.half) {
+        if (b.prep_blocks[0]) PrepareKernel<true, true><<<b.prep_blocks[0], kThreads, 0, stream>>>(b);
+        if (b.prep_blocks[1]) PrepareKernel<false, true><<<b.prep_blocks[1], kThreads, 0, stream>>>(b);
+    } else {
+        if (b.prep_blocks[0]) PrepareKernel<true, false><<<b.prep_blocks[0], kThreads, 0, stream>>>(b);
+        if (b.prep_blocks[1]) PrepareKernel<false, false><<<b.prep_blocks[1], kThreads, 0, stream>>>(b);
+    }
     return cudaGetLastError();
 }
 

@@ -171,6 +171,27 @@ private:
 
 size_t AlignUp(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// An IEEE binary16 value (its bits) as float; every binary16 is a float.
+float HalfBitsToFloat(uint16_t h) {
+    const uint32_t sign = static_cast<uint32_t>(h & 0x8000u) << 16;
+    const uint32_t exp = (h >> 10) & 0x1fu, man = h & 0x3ffu;
+    uint32_t bits;
+    if (exp == 0x1fu) {
+        bits = sign | 0x7f800000u | (man << 13);
+    } else if (exp != 0) {
+        bits = sign | ((exp + 112u) << 23) | (man << 13);
+    } else if (man == 0) {
+        bits = sign;
+    } else {  // subnormal: man * 2^-24
+        float f = static_cast<float>(man) * 5.9604644775390625e-8f;
+        std::memcpy(&bits, &f, 4);
+        bits |= sign;
+    }
+    float f;
+    std::memcpy(&f, &bits, 4);
+    return f;
+}
+
 // ---------------------------------------------------------------------------
 // Batch tables: pyramid plane offsets, work segments and prefix offsets.
 // ---------------------------------------------------------------------------
@@ -297,6 +318,7 @@ struct BatchMemory {
     size_t head_bytes = 0, table_bytes = 0;
     DevBatch dev{};
     uint32_t pair_count = 0;
+    size_t elem_bytes = 4;  // pyramid element: float, or binary16 with half planes
 
     // Sizes and uploads-to-be for `t`; returns true if any address moved.
     bool Layout(const Tables& t) {
@@ -310,7 +332,7 @@ struct BatchMemory {
         table_bytes = AlignUp(off_blur + sizeof(uint32_t) * t.blur_start.size(), 256);
         moved |= table.ensure(table_bytes);
         moved |= table_host.ensure(table_bytes);
-        moved |= pyramid.ensure(std::max<size_t>(t.pyramid_floats, 64) * sizeof(float));
+        moved |= pyramid.ensure(std::max<size_t>(t.pyramid_floats, 64) * elem_bytes);
         moved |= partials.ensure(std::max<size_t>(t.partials, 1) * 6 * sizeof(double));
         moved |= seg_sums.ensure(std::max<size_t>(t.segs.size(), 1) * 6 * sizeof(double));
         if (pair_done.ensure(std::max<size_t>(t.pairs.size(), 1) * sizeof(uint32_t))) {
@@ -333,13 +355,15 @@ struct BatchMemory {
         dev.seg_sums = seg_sums.as<double>();
         dev.pair_done = pair_done.as<uint32_t>();
         dev.status = nullptr;
+        dev.half = elem_bytes == 2 ? 1u : 0u;
         return moved;
     }
 
     // Writes the host mirror of the tables with device pointers filled in.
     void Stage(Tables& t) {
         for (size_t i = 0; i < t.pairs.size(); ++i) {
-            t.pairs[i].pyramid = pyramid.as<float>() + t.pyramid_first[i];
+            t.pairs[i].pyramid =
+                reinterpret_cast<float*>(pyramid.as<uint8_t>() + t.pyramid_first[i] * elem_bytes);
             t.pairs[i].result = results.as<double>() + i * kResultDoubles;
         }
         uint8_t* h = table_host.as<uint8_t>();
@@ -474,8 +498,9 @@ public:
             throw std::invalid_argument("gpu_resident_images is limited to " +
                                         std::to_string(kIndexMask) + " slots");
         if (cfg.chroma_filter > 2) throw std::invalid_argument("invalid chroma filter");
-        if (cfg.half_planes)
-            throw std::invalid_argument("cuda: half_planes is not supported by this build");
+        // Half planes (ssimulacra2.h:41-46): binary16 pyramid elements, FP32
+        // arithmetic, the level averages rounded like the planes.
+        mem_.elem_bytes = cfg.half_planes ? 2 : 4;
         device_ = ResolveDevice(cfg.device);
         EnsureDevice(device_);
         VQM_CK(cudaSetDevice(device_));
@@ -757,14 +782,27 @@ public:
         if (!(plan_.mask[level] & (1u << channel)))
             throw std::invalid_argument("cuda: the channel is pruned at this level");
         const DevPair& P = tables_.pairs[0];
-        const float* src = mem_.pyramid.as<float>() + tables_.pyramid_first[0] +
-                           image * P.image_stride + P.plane_off[level][channel];
+        const size_t eb = mem_.elem_bytes;
+        const uint8_t* src = mem_.pyramid.as<uint8_t>() +
+                             (tables_.pyramid_first[0] + image * P.image_stride +
+                              P.plane_off[level][channel]) * eb;
         const uint32_t w = P.w[level], h = P.h[level], pitch = P.pitch[level];
-        std::vector<float> pairs(PlaneFloats(w, h));
+        std::vector<uint8_t> pairs(PlaneFloats(w, h) * eb);
         VQM_CK(cudaSetDevice(device_));
-        VQM_CK(cudaMemcpy(pairs.data(), src, pairs.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        VQM_CK(cudaMemcpy(pairs.data(), src, pairs.size(), cudaMemcpyDeviceToHost));
         for (uint32_t y = 0; y < h; ++y)
-            for (uint32_t x = 0; x < w; ++x) out[static_cast<size_t>(y) * w + x] = pairs[PlaneIndex(pitch, x, y)];
+            for (uint32_t x = 0; x < w; ++x) {
+                const size_t i = PlaneIndex(pitch, x, y);
+                float v;
+                if (eb == 2) {
+                    uint16_t hbits;
+                    std::memcpy(&hbits, &pairs[i * 2], 2);
+                    v = HalfBitsToFloat(hbits);
+                } else {
+                    std::memcpy(&v, &pairs[i * 4], 4);
+                }
+                out[static_cast<size_t>(y) * w + x] = v;
+            }
     }
 
     void Usage(vqm_cu_memory_usage* u) const {
@@ -911,6 +949,12 @@ public:
             }
             if (found < 0) throw std::invalid_argument("cuda: blur tile shape is not compiled in");
             shape_ = BlurShape::Of(found);
+        }
+        if (cfg.half_planes) {
+            // Half planes run the one-tile-per-CTA blur; a persistent variant
+            // without such a twin falls back to the default tile.
+            mem_.elem_bytes = 2;
+            if (HalfPlaneVariant(shape_.variant) < 0) shape_ = BlurShape::Of(kDefaultBlurVariant);
         }
         device_ = ResolveDevice(cfg.device);
         EnsureDevice(device_);

@@ -156,6 +156,7 @@ class _BatchConfig(ctypes.Structure):
         ("tile_w", ctypes.c_uint32),
         ("tile_h", ctypes.c_uint32),
         ("variant", ctypes.c_uint32),
+        ("half_planes", ctypes.c_uint32),
     ]
 
 
@@ -584,12 +585,14 @@ class Ssimulacra2Batch:
 
     def __init__(self, max_pairs: int = 0, max_pixels: int = 0, chroma_filter: int = 0,
                  device: int = -1, tile: tuple[int, int] | None = None,
-                 variant: int | None = None):
+                 variant: int | None = None, half_planes: bool = False):
         """`variant` picks a compiled blur kernel (see blur_variants());
-        `tile` picks one by its output tile; neither: the tuned default."""
+        `tile` picks one by its output tile; neither: the tuned default.
+        `half_planes` stores the pyramid as binary16 (ssimulacra2.h:41-46)."""
         tw, th = tile if tile else (0, 0)
         v = 0 if variant is None else variant + 1
-        cfg = _BatchConfig(max_pixels, max_pairs, chroma_filter, device, tw, th, v)
+        cfg = _BatchConfig(max_pixels, max_pairs, chroma_filter, device, tw, th, v,
+                           int(half_planes))
         self._b = ctypes.c_void_p()
         _check(_lib.vqm_cu_ss2_batch_create(ctypes.byref(cfg), ctypes.byref(self._b)))
 
