@@ -280,6 +280,15 @@ int vqm_cu_ss2_batch_submit(vqm_cu_ss2_batch* batch, uint32_t n,
                             const vqm_cu_image* originals,
                             const vqm_cu_image* distorteds, float background,
                             uint64_t* token);
+/* As vqm_cu_ss2_batch_submit, but host planes are copied asynchronously and
+ * stay borrowed until vqm_cu_ss2_batch_finish returns (no reference
+ * counterpart: VQM copies host pixels before Submit returns). A caller that
+ * keeps its images alive anyway, such as a pool scoring a list, lets the
+ * next submission's copies queue behind these ones. */
+int vqm_cu_ss2_batch_submit_borrowed(vqm_cu_ss2_batch* batch, uint32_t n,
+                                     const vqm_cu_image* originals,
+                                     const vqm_cu_image* distorteds,
+                                     float background, uint64_t* token);
 /* Waits and writes norms (n x 108, zero beyond each pair's scales), scale
  * counts and scores (FP64, computed on the device). */
 int vqm_cu_ss2_batch_finish(vqm_cu_ss2_batch* batch, uint64_t token,

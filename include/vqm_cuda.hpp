@@ -533,7 +533,9 @@ private:
                 drain(w);
                 const std::size_t count = std::min(chunk_, n - at);
                 std::uint64_t token = 0;
-                detail::Check(vqm_cu_ss2_batch_submit(batches_[w].get(),
+                // The images outlive the call, so their uploads may run
+                // behind it and queue back to back across workers.
+                detail::Check(vqm_cu_ss2_batch_submit_borrowed(batches_[w].get(),
                                                       static_cast<std::uint32_t>(count),
                                                       o.data() + at, d.data() + at, background,
                                                       &token));

@@ -979,7 +979,10 @@ public:
         stream_ = s ? static_cast<cudaStream_t>(s) : own_stream_;
     }
 
-    uint64_t Submit(uint32_t n, const vqm_cu_image* o, const vqm_cu_image* d, float bg) {
+    // `wait_copies` false leaves the host-to-device copies of host images in
+    // flight: their planes are then borrowed until Finish.
+    uint64_t Submit(uint32_t n, const vqm_cu_image* o, const vqm_cu_image* d, float bg,
+                    bool wait_copies = true) {
         if (in_flight_) throw std::logic_error("cuda: a batch is in flight; Finish it first");
         if (n == 0) throw std::invalid_argument("cuda: empty batch");
         if (cfg_.max_pairs && n > cfg_.max_pairs)
@@ -1042,7 +1045,7 @@ public:
         count_ = n;
         token_ = NextIncarnation();
         in_flight_ = true;
-        if (host_bytes) VQM_CK(cudaEventSynchronize(copied_));
+        if (host_bytes && wait_copies) VQM_CK(cudaEventSynchronize(copied_));
         return token_;
     }
 
@@ -1422,6 +1425,19 @@ int vqm_cu_ss2_batch_submit(vqm_cu_ss2_batch* b, uint32_t n, const vqm_cu_image*
             NotNull(d, "distorteds");
         }
         *token = b->impl.Submit(n, o, d, background);
+    });
+}
+
+int vqm_cu_ss2_batch_submit_borrowed(vqm_cu_ss2_batch* b, uint32_t n, const vqm_cu_image* o,
+                                     const vqm_cu_image* d, float background, uint64_t* token) {
+    return Guard([&] {
+        NotNull(b, "batch");
+        NotNull(token, "token");
+        if (n) {
+            NotNull(o, "originals");
+            NotNull(d, "distorteds");
+        }
+        *token = b->impl.Submit(n, o, d, background, false);
     });
 }
 

@@ -219,6 +219,7 @@ _SIGS = {
     "vqm_cu_ss2_batch_destroy": ([_P], ctypes.c_int),
     "vqm_cu_ss2_batch_set_stream": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_submit": ([_P, ctypes.c_uint32, _P, _P, ctypes.c_float, _P], ctypes.c_int),
+    "vqm_cu_ss2_batch_submit_borrowed": ([_P, ctypes.c_uint32, _P, _P, ctypes.c_float, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_finish": ([_P, ctypes.c_uint64, _P, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_set_timing": ([_P, ctypes.c_int], ctypes.c_int),
     "vqm_cu_ss2_blur_variants": ([_P, _P], ctypes.c_int),
@@ -631,12 +632,15 @@ class Ssimulacra2Batch:
         dists = (_CImage * n)(*[p[1]._c() for p in pairs])
         return n, origs, dists
 
-    def submit(self, pairs, background: float = 0.5) -> int:
+    def submit(self, pairs, background: float = 0.5, borrow: bool = False) -> int:
+        """Queues the pairs. With `borrow`, host images are copied
+        asynchronously and must stay unchanged until finish returns."""
         n, origs, dists = self._arrays(pairs)
         self._pending = n
         tok = ctypes.c_uint64()
-        _check(_lib.vqm_cu_ss2_batch_submit(self._b, n, origs, dists, background,
-                                            ctypes.byref(tok)))
+        fn = _lib.vqm_cu_ss2_batch_submit_borrowed if borrow else _lib.vqm_cu_ss2_batch_submit
+        _check(fn(self._b, n, origs, dists, background, ctypes.byref(tok)))
+        self._borrowed = pairs if borrow else None
         return tok.value
 
     def finish(self, token: int):
@@ -644,8 +648,10 @@ class Ssimulacra2Batch:
         norms = np.zeros((n, 108), dtype=np.float64)
         scales = np.zeros(n, dtype=np.uint32)
         scores = np.zeros(n, dtype=np.float64)
-        _check(_lib.vqm_cu_ss2_batch_finish(self._b, token, norms.ctypes.data,
-                                            scales.ctypes.data, scores.ctypes.data))
+        status = _lib.vqm_cu_ss2_batch_finish(self._b, token, norms.ctypes.data,
+                                              scales.ctypes.data, scores.ctypes.data)
+        self._borrowed = None
+        _check(status)
         return [Ssimulacra2Result(norms[i, : 18 * scales[i]].reshape(scales[i], 18).copy(),
                                   float(scores[i])) for i in range(n)]
 
@@ -698,7 +704,10 @@ class Ssimulacra2Pool:
         try:
             for first in range(0, len(pairs), self._chunk):
                 drain(w)
-                token = self._batches[w].submit(pairs[first:first + self._chunk], background)
+                # The pairs stay referenced until drained, so the copies may
+                # run behind the call: chunks' uploads queue back to back.
+                token = self._batches[w].submit(pairs[first:first + self._chunk], background,
+                                                borrow=True)
                 pending[w] = (token, first)
                 w = (w + 1) % len(self._batches)
             for k in range(len(self._batches)):
