@@ -209,22 +209,39 @@ __device__ __forceinline__ void ChromaBilinear(const DevSource& s, int plane, co
     float win[9];
     const bool interior =
         cx > 0 && cx + 1 < static_cast<int>(dx) && cy > 0 && cy + 1 < static_cast<int>(dy);
+    if (interior && s.type <= 1) {
+        // Integer samples away from the edges: three row addresses, nine
+        // loads, then the class-1 scale and offset (RawSample's arithmetic).
+        const size_t rb = s.row_bytes[plane];
+        const uint8_t* row = s.plane[plane] + static_cast<size_t>(cy - 1) * rb;
 #pragma unroll
-    for (int j = -1; j <= 1; ++j)
+        for (int j = 0; j < 3; ++j, row += rb)
 #pragma unroll
-        for (int i = -1; i <= 1; ++i) {
-            uint32_t sx, sy;
-            if (interior) {
-                sx = static_cast<uint32_t>(cx + i);
-                sy = static_cast<uint32_t>(cy + j);
-            } else {
-                sx = static_cast<uint32_t>(
-                    MirrorIndex(__fadd_rn(static_cast<float>(cx + i), 0.5f), dx));
-                sy = static_cast<uint32_t>(
-                    MirrorIndex(__fadd_rn(static_cast<float>(cy + j), 0.5f), dy));
+            for (int i = 0; i < 3; ++i) {
+                const uint32_t x = static_cast<uint32_t>(cx - 1 + i);
+                const float v = s.type == 0
+                                    ? static_cast<float>(__ldg(row + x))
+                                    : static_cast<float>(__ldg(reinterpret_cast<const uint16_t*>(row) + x));
+                win[j * 3 + i] = __fmaf_rn(v, s.scale[1], s.offset[1]);
             }
-            win[(j + 1) * 3 + (i + 1)] = RawSample(s, plane, sx, sy);
-        }
+    } else {
+#pragma unroll
+        for (int j = -1; j <= 1; ++j)
+#pragma unroll
+            for (int i = -1; i <= 1; ++i) {
+                uint32_t sx, sy;
+                if (interior) {
+                    sx = static_cast<uint32_t>(cx + i);
+                    sy = static_cast<uint32_t>(cy + j);
+                } else {
+                    sx = static_cast<uint32_t>(
+                        MirrorIndex(__fadd_rn(static_cast<float>(cx + i), 0.5f), dx));
+                    sy = static_cast<uint32_t>(
+                        MirrorIndex(__fadd_rn(static_cast<float>(cy + j), 0.5f), dy));
+                }
+                win[(j + 1) * 3 + (i + 1)] = RawSample(s, plane, sx, sy);
+            }
+    }
     const float iscx = 1.0f / static_cast<float>(1u << s.sub_w);
     const float iscy = 1.0f / static_cast<float>(1u << s.sub_h);
     int xa, xb, ya, yb;

@@ -187,15 +187,10 @@ SS2_DM double Exp2J(int j) {
 //   log2 x = e - log2(RN(1/c)) + log2(1 + r),  r = m RN(1/c) - 1 (one fused
 // multiply-add, |r| < 2^-8), with ln(1 + r) by its Taylor series to r^7
 // (remainder below 2^-67).
-SS2_DM double log2d(double x) {
-    uint64_t u = bits(x);
-    int e = static_cast<int>((u >> 52) & 0x7ff);
-    if (e == 0) {  // subnormal: normalise
-        x = x * 18014398509481984.0;  // 2^54
-        u = bits(x);
-        e = static_cast<int>((u >> 52) & 0x7ff) - 54;
-    }
-    e -= 1023;
+// The table-driven step for a normal double x with bits u, minus `shift`
+// in the exponent (the body of log2d).
+SS2_DM double log2d_normal(uint64_t u, int shift = 0) {
+    const int e = static_cast<int>((u >> 52) & 0x7ff) - 1023 - shift;
     const uint64_t frac = u & 0x000fffffffffffffull;
     const int i = static_cast<int>(frac >> 45);
     const double m = from_bits64(frac | 0x3ff0000000000000ull);  // [1, 2)
@@ -210,6 +205,14 @@ SS2_DM double log2d(double x) {
     return fmad(ln1r, 1.4426950408889634074, Log2InvC(i) + static_cast<double>(e));
 }
 
+SS2_DM double log2d(double x) {
+    uint64_t u = bits(x);
+    if (((u >> 52) & 0x7ff) == 0) {  // subnormal: normalise, then correct the exponent
+        return log2d_normal(bits(x * 18014398509481984.0), 54);  // x 2^54
+    }
+    return log2d_normal(u);
+}
+
 // 2^t in double for |t| < 1000, table-driven: t = (64 n + j) / 64 + f with
 // j in [0, 64) and |f| <= 1/128 (f exact), 2^t = 2^n 2^(j/64) e^(f ln 2),
 // e^z - 1 by its Taylor series to z^6 (|z| < 0.0055, remainder below 4e-20).
@@ -220,7 +223,7 @@ SS2_DM double exp2d(double t) {
     const double f = t - kd * 0.015625;
     const int k = static_cast<int>(kd);
     const int j = k & 63;
-    int n = (k - j) / 64;
+    int n = (k - j) >> 6;  // k - j is a multiple of 64
     const double z = f * 0.69314718055994530942;
     double p = 1.0 / 720.0;
     p = fmad(p, z, 1.0 / 120.0);
@@ -230,8 +233,10 @@ SS2_DM double exp2d(double t) {
     p = fmad(p, z, 1.0);
     const double tj = Exp2J(j);
     const double v = fmad(tj, p * z, tj);  // 2^(j/64) (1 + (e^z - 1))
-    // Split the scale so every factor stays a normal double.
     if (n > 1000) n = 1000;
+    // v is in [0.5, 2]: one scaling when 2^n is a normal double; else split
+    // it so every factor is (the product is the same: v 2^n1 is exact).
+    if (n >= -1022) return v * pow2i(n);
     const int n1 = n / 2, n2 = n - n1;
     return v * pow2i(n1) * pow2i(n2);
 }
@@ -240,7 +245,10 @@ SS2_DM double exp2d(double t) {
 SS2_DM float pow(float x, float y) {
     if (x == 1.0f || y == 0.0f) return 1.0f;
     if (!(x > 0.0f)) return x == 0.0f ? (y > 0.0f ? 0.0f : 3.402823466e38f * 10.0f) : x - x;
-    return static_cast<float>(exp2d(static_cast<double>(y) * log2d(static_cast<double>(x))));
+    // A positive float is a normal double, so log2d's subnormal step is not
+    // needed.
+    return static_cast<float>(
+        exp2d(static_cast<double>(y) * log2d_normal(bits(static_cast<double>(x)))));
 }
 
 // e^x for float x.
