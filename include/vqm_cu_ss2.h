@@ -266,8 +266,10 @@ typedef struct vqm_cu_ss2_batch_config {
 } vqm_cu_ss2_batch_config;
 
 /* The blur kernels compiled into the library, for tuning: *count variants,
- * and for each (if `shapes` is not null) its tile width, tile height and
- * threads per CTA, 3 words per variant. */
+ * and for each (if `shapes` is not null) VQM_CU_SS2_VARIANT_WORDS words: its
+ * tile width, tile height, threads per CTA, tiles per CTA down a column (1:
+ * one tile per CTA) and 1 if its CTAs stay resident over many tiles. */
+#define VQM_CU_SS2_VARIANT_WORDS 5
 int vqm_cu_ss2_blur_variants(uint32_t* count, uint32_t* shapes);
 
 int vqm_cu_ss2_batch_create(const vqm_cu_ss2_batch_config* config,

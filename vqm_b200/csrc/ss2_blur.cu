@@ -23,7 +23,9 @@
 //   4. The CTA's six sums are combined with two-sum compensation into one
 //      partial per tile; the finalize kernel adds the partials in FP64.
 // A persistent form keeps each CTA resident and copies its next tile's
-// window into a second buffer while it computes the current one.
+// window into a second buffer while it computes the current one; a strip
+// form walks a few tiles down one column and reuses the horizontal results
+// of the rows the windows share.
 
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -94,13 +96,11 @@ struct TileRef {
     int w, h, x0, y0;
 };
 
-// With half planes pa and pb point at binary16 elements (typed float* only
-// to share the struct).
+// Output tile (tx, ty) of a segment. With half planes pa and pb point at
+// binary16 elements (typed float* only to share the struct).
 template <int TW, int TH, bool kHalf = false>
-__device__ __forceinline__ TileRef LocateTile(const DevBatch& batch, uint32_t blk) {
-    const uint32_t si = FindSlot(batch.blur_start, batch.segments, blk);
-    const DevSegment seg = batch.seg[si];
-    const uint32_t tile = blk - __ldg(&batch.blur_start[si]);
+__device__ __forceinline__ TileRef SegmentTile(const DevBatch& batch, const DevSegment& seg,
+                                               uint32_t tx, uint32_t ty) {
     const DevPair& P = batch.pair[seg.pair];
     TileRef t;
     if (kHalf) {
@@ -114,11 +114,20 @@ __device__ __forceinline__ TileRef LocateTile(const DevBatch& batch, uint32_t bl
     t.pitch = P.pitch[seg.level];
     t.w = static_cast<int>(P.w[seg.level]);
     t.h = static_cast<int>(P.h[seg.level]);
-    const uint32_t ty = tile / seg.tiles_x;
-    t.x0 = static_cast<int>((tile - ty * seg.tiles_x) * TW);
+    t.x0 = static_cast<int>(tx * TW);
     t.y0 = static_cast<int>(ty * TH);
-    t.partial = seg.partial_first + tile;
+    t.partial = seg.partial_first + ty * seg.tiles_x + tx;
     return t;
+}
+
+// Block `blk` of a one-tile-per-block launch (blur_start counts tiles).
+template <int TW, int TH, bool kHalf = false>
+__device__ __forceinline__ TileRef LocateTile(const DevBatch& batch, uint32_t blk) {
+    const uint32_t si = FindSlot(batch.blur_start, batch.segments, blk);
+    const DevSegment seg = batch.seg[si];
+    const uint32_t tile = blk - __ldg(&batch.blur_start[si]);
+    const uint32_t ty = tile / seg.tiles_x;
+    return SegmentTile<TW, TH, kHalf>(batch, seg, tile - ty * seg.tiles_x, ty);
 }
 
 // Asynchronous 16-byte global-to-shared copy; a source size of 0 writes
@@ -138,14 +147,15 @@ __device__ __forceinline__ void CpAsyncWait() {
 
 // Issues the copies of one tile's two source windows into `buf`: chunk
 // (rp, cp) of the window is the 2x2 block at window column 2cp, row 2rp.
+// Row pairs below `rp_begin` are left as they are.
 template <int TW, int TH, int NT>
-__device__ __forceinline__ void IssueTileLoads(float* buf, const TileRef& t) {
+__device__ __forceinline__ void IssueTileLoads(float* buf, const TileRef& t, int rp_begin = 0) {
     using T = Tile<TW, TH, NT>;
     const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(buf));
     const uint32_t wp = static_cast<uint32_t>(t.w + 1) >> 1;  // chunks per row pair
     const uint32_t hp = static_cast<uint32_t>(t.h + 1) >> 1;  // row pairs
     const int cx0 = (t.x0 >> 1) - kRadius / 2, ry0 = (t.y0 >> 1) - kRadius / 2;
-    for (int k = threadIdx.x; k < T::RP * T::CP; k += NT) {
+    for (int k = rp_begin * T::CP + threadIdx.x; k < T::RP * T::CP; k += NT) {
         const int rp = k / T::CP, cp = k - rp * T::CP;
         const int gy = ry0 + rp, gx = cx0 + cp;
         const bool in = static_cast<uint32_t>(gy) < hp && static_cast<uint32_t>(gx) < wp;
@@ -218,7 +228,8 @@ __device__ __forceinline__ float2 Pack(float v) { return make_float2(v, v); }
 __device__ __forceinline__ float2 Neg(float2 v) { return make_float2(-v.x, -v.y); }
 
 // Horizontal pass (scale.comp:149-207): row pair rp, output columns
-// c0..c0+3, all five quantities, both rows per instruction.
+// c0..c0+3, all five quantities, both rows per instruction, for the row
+// pairs from `rp_begin` (even) on.
 //
 // Task -> (rp, column group): within every 8 lanes, lanes 0-3 take four
 // column groups of row pair rp and lanes 4-7 the same groups of rp + 1. The
@@ -227,13 +238,14 @@ __device__ __forceinline__ float2 Neg(float2 v) { return make_float2(-v.x, -v.y)
 // 16-byte column block index XORed with 4 on rows whose (row >> 1) is odd,
 // so the quarter warp's stores (rows 2rp and 2rp + 2) do not collide either.
 template <int TW, int TH, int NT>
-__device__ __forceinline__ void HorizontalPass(const float* src, float* hq) {
+__device__ __forceinline__ void HorizontalPass(const float* src, float* hq, int rp_begin = 0) {
     using T = Tile<TW, TH, NT>;
     constexpr int KH = T::KH;
-    for (int task = threadIdx.x; task < T::HT; task += NT) {
+    const int tasks = T::HT - rp_begin * T::NG;
+    for (int task = threadIdx.x; task < tasks; task += NT) {
         const int cg_lo = task & 3, rp_lo = (task >> 2) & 1, rest = task >> 3;
         const int cg = (rest % (T::NG / 4)) * 4 + cg_lo;
-        const int rp = (rest / (T::NG / 4)) * 2 + rp_lo;
+        const int rp = rp_begin + (rest / (T::NG / 4)) * 2 + rp_lo;
         const float* ra = src + rp * T::SRS + 2 * KH * cg;
         const float* rb = ra + T::IMG;
         float2 A[KH + 12], B[KH + 12];
@@ -360,28 +372,37 @@ __device__ __forceinline__ void VerticalMaps(const float* src, const float* hq, 
     }
 }
 
+// Scratch of the reduction: 12 arrays of NT floats, here back to back
+// (the source window once every thread is past its last read of it).
+template <int NT>
+struct LinearScratch {
+    float* base;
+    __device__ __forceinline__ float* operator()(int a) const { return base + a * NT; }
+};
+
 // The CTA's six sums as one compensated partial each (scale.comp:395-436,
 // with two-sum compensation in place of the plain ladder): every thread
 // folds its two lanes, 16 lanes per sum add the block's values, and a
-// 16-lane butterfly finishes. `red` (12 * NT floats) may alias the source
-// buffer once every thread is past its last read of it. Ends with a barrier.
-template <int NT>
-__device__ __forceinline__ void ReducePartials(const float2 (&sum)[6], float* red, double* out) {
+// 16-lane butterfly finishes. `red(a)` is scratch array a (a < 12) of NT
+// floats. Ends with a barrier.
+template <int NT, class Scratch>
+__device__ __forceinline__ void ReducePartials(const float2 (&sum)[6], Scratch red, double* out) {
     const int tid = threadIdx.x;
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
         float s = sum[k].x, c = 0.0f;
         TwoSumAdd(s, c, sum[k].y, 0.0f);
-        red[(2 * k) * NT + tid] = s;
-        red[(2 * k + 1) * NT + tid] = c;
+        red(2 * k)[tid] = s;
+        red(2 * k + 1)[tid] = c;
     }
     __syncthreads();
     if (tid < 96) {  // warps 0-2, whole
         const int k = tid >> 4, i = tid & 15;
-        float s = red[(2 * k) * NT + i], c = red[(2 * k + 1) * NT + i];
+        const float* rs = red(2 * k);
+        const float* rc = red(2 * k + 1);
+        float s = rs[i], c = rc[i];
 #pragma unroll
-        for (int j = i + 16; j < NT; j += 16)
-            TwoSumAdd(s, c, red[(2 * k) * NT + j], red[(2 * k + 1) * NT + j]);
+        for (int j = i + 16; j < NT; j += 16) TwoSumAdd(s, c, rs[j], rc[j]);
 #pragma unroll
         for (int off = 8; off > 0; off >>= 1) {
             const float s2 = __shfl_xor_sync(0xffffffffu, s, off);
@@ -406,7 +427,7 @@ __device__ __forceinline__ void ComputeTile(float* src, float* hq, const TileRef
     else
         VerticalMaps<TW, TH, NT, true>(src, hq, t, sum);
     __syncthreads();  // the reduction overwrites the source window
-    ReducePartials<NT>(sum, src, partials + static_cast<size_t>(t.partial) * 6);
+    ReducePartials<NT>(sum, LinearScratch<NT>{src}, partials + static_cast<size_t>(t.partial) * 6);
 }
 
 // One output tile per CTA; MB CTAs per SM is the occupancy the shared
@@ -464,14 +485,95 @@ __global__ void __launch_bounds__(NT, MB) Ss2BlurPersistentKernel(DevBatch batch
     CpAsyncWait<0>();
 }
 
+// Strips: a CTA computes up to S vertically consecutive tiles of one column.
+// Tile k + 1's window starts TH rows below tile k's, so the horizontal
+// results of its first 12 rows are tile k's last 12, already in `hq`: they
+// are moved up instead of being computed again, and only the window's rows
+// 6.. are copied in (6..11 for the maps' raw values, 12.. for the horizontal
+// pass). Every value is computed by the same instructions as in the one-tile
+// kernel, so the maps are bit-identical to it; each tile keeps its own
+// partial.
+//
+// The reduction's scratch is rows 12..TH-1 of the horizontal planes, free
+// while the halo rows move.
+template <int TW, int TH, int NT>
+struct HqScratch {
+    using T = Tile<TW, TH, NT>;
+    static constexpr int kPerPlane = (TH - 2 * kRadius) * TW / NT;  // arrays per plane
+    static_assert(5 * kPerPlane >= 12, "the reduction fits the free horizontal rows");
+    float* hq;
+    __device__ __forceinline__ float* operator()(int a) const {
+        return hq + (a / kPerPlane) * T::SH * TW + 2 * kRadius * TW + (a % kPerPlane) * NT;
+    }
+};
+
+// Horizontal rows TH..TH+11 of every quantity to rows 0..11. TH is a
+// multiple of 4, so a row and its destination share the store swizzle.
+template <int TW, int TH, int NT>
+__device__ __forceinline__ void MoveHalo(float* hq) {
+    using T = Tile<TW, TH, NT>;
+    constexpr int kRowVec = TW / 4;                   // float4 per row
+    constexpr int kPlaneVec = 2 * kRadius * kRowVec;  // float4 per plane's halo
+    static_assert(TH % 4 == 0, "swizzle parity");
+    for (int i = threadIdx.x; i < 5 * kPlaneVec; i += NT) {
+        const int q = i / kPlaneVec, j = i - q * kPlaneVec;
+        float4* plane = reinterpret_cast<float4*>(hq + q * T::SH * TW);
+        plane[j] = plane[TH * kRowVec + j];
+    }
+}
+
+template <int TW, int TH, int NT, int MB, int S>
+__global__ void __launch_bounds__(NT, MB) Ss2BlurStripKernel(DevBatch batch) {
+    using T = Tile<TW, TH, NT>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* src = reinterpret_cast<float*>(smem);
+    float* hq = reinterpret_cast<float*>(smem + T::kSrcBytes);
+    const uint32_t si = FindSlot(batch.blur_start, batch.segments, blockIdx.x);
+    const DevSegment seg = batch.seg[si];
+    const uint32_t strip = blockIdx.x - __ldg(&batch.blur_start[si]);
+    const uint32_t sy = strip / seg.tiles_x;
+    const uint32_t tiles_y = seg.tiles / seg.tiles_x;
+    const uint32_t ty0 = sy * S;
+    const int count = static_cast<int>(min(static_cast<uint32_t>(S), tiles_y - ty0));
+    TileRef t = SegmentTile<TW, TH>(batch, seg, strip - sy * seg.tiles_x, ty0);
+    IssueTileLoads<TW, TH, NT>(src, t);
+    CpAsyncCommit();
+    for (int k = 0; k < count; ++k) {
+        CpAsyncWait<0>();
+        __syncthreads();
+        HorizontalPass<TW, TH, NT>(src, hq, k == 0 ? 0 : kRadius);
+        __syncthreads();
+        float2 sum[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) sum[i] = make_float2(0.0f, 0.0f);
+        if (t.x0 + TW <= t.w && t.y0 + TH <= t.h)
+            VerticalMaps<TW, TH, NT, false>(src, hq, t, sum);
+        else
+            VerticalMaps<TW, TH, NT, true>(src, hq, t, sum);
+        __syncthreads();  // every read of the window and of `hq` is done
+        const uint32_t partial = t.partial;
+        if (k + 1 < count) {
+            t.y0 += TH;
+            t.partial += seg.tiles_x;
+            IssueTileLoads<TW, TH, NT>(src, t, kRadius / 2);
+            CpAsyncCommit();
+            MoveHalo<TW, TH, NT>(hq);
+        }
+        ReducePartials<NT>(sum, HqScratch<TW, TH, NT>{hq},
+                           batch.partials + static_cast<size_t>(partial) * 6);
+    }
+}
+
 // The variants compiled in: {tile width, tile height, threads, persistent,
-// CTAs per SM}.
+// CTAs per SM, tiles per CTA (a strip of that many; 1 = one tile)}.
 struct BlurVariant {
-    int w, h, threads, persistent, per_sm;
+    int w, h, threads, persistent, per_sm, strip;
 };
 constexpr BlurVariant kBlurVariants[] = {
-    {32, 32, 128, 0, 5}, {32, 28, 128, 0, 5}, {64, 32, 256, 0, 2}, {64, 20, 256, 0, 3},
-    {32, 32, 128, 1, 3}, {32, 20, 128, 1, 5}, {64, 32, 256, 1, 1},
+    {32, 32, 128, 0, 5, 1}, {32, 28, 128, 0, 5, 1}, {64, 32, 256, 0, 2, 1},
+    {64, 20, 256, 0, 3, 1}, {32, 32, 128, 1, 3, 1}, {32, 20, 128, 1, 5, 1},
+    {64, 32, 256, 1, 1, 1}, {32, 32, 128, 0, 5, 2}, {32, 32, 128, 0, 5, 4},
+    {32, 32, 128, 0, 5, 8}, {32, 28, 128, 0, 5, 4},
 };
 constexpr int kBlurVariantCount = sizeof(kBlurVariants) / sizeof(kBlurVariants[0]);
 
@@ -544,6 +646,18 @@ cudaError_t LaunchPersistent(const DevBatch& b, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
+template <int TW, int TH, int NT, int MB, int S>
+cudaError_t LaunchStrips(const DevBatch& b, cudaStream_t stream) {
+    using T = Tile<TW, TH, NT>;
+    static LaunchCache cache;
+    constexpr size_t smem = T::kSrcBytes + T::kHqBytes;
+    const cudaError_t e =
+        Prepare(Ss2BlurStripKernel<TW, TH, NT, MB, S>, smem, cache, NT, false, nullptr);
+    if (e != cudaSuccess) return e;
+    Ss2BlurStripKernel<TW, TH, NT, MB, S><<<b.blur_blocks, NT, smem, stream>>>(b);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 cudaError_t SetConstants(const float* taps13, const double* weights108) {
@@ -565,15 +679,20 @@ cudaError_t LaunchBlur(const DevBatch& b, int variant, cudaStream_t stream) {
         case 4: return LaunchPersistent<32, 32, 128, 3>(b, stream);
         case 5: return LaunchPersistent<32, 20, 128, 5>(b, stream);
         case 6: return LaunchPersistent<64, 32, 256, 1>(b, stream);
+        case 7: return LaunchStrips<32, 32, 128, 5, 2>(b, stream);
+        case 8: return LaunchStrips<32, 32, 128, 5, 4>(b, stream);
+        case 9: return LaunchStrips<32, 32, 128, 5, 8>(b, stream);
+        case 10: return LaunchStrips<32, 28, 128, 5, 4>(b, stream);
     }
     return cudaErrorInvalidValue;
 }
 
 int HalfPlaneVariant(int variant) {
     if (variant < 0 || variant >= kBlurVariantCount) return -1;
-    if (!kBlurVariants[variant].persistent) return variant;
+    const auto one_tile = [](const BlurVariant& v) { return !v.persistent && v.strip == 1; };
+    if (one_tile(kBlurVariants[variant])) return variant;
     for (int i = 0; i < kBlurVariantCount; ++i)
-        if (!kBlurVariants[i].persistent && kBlurVariants[i].w == kBlurVariants[variant].w &&
+        if (one_tile(kBlurVariants[i]) && kBlurVariants[i].w == kBlurVariants[variant].w &&
             kBlurVariants[i].h == kBlurVariants[variant].h)
             return i;
     return -1;
@@ -581,6 +700,12 @@ int HalfPlaneVariant(int variant) {
 
 int BlurTileCount() { return kBlurVariantCount; }
 int BlurTileThreads(int index) { return kBlurVariants[index].threads; }
+int BlurTileStrip(int index) { return kBlurVariants[index].strip; }
+bool BlurTilePersistent(int index) { return kBlurVariants[index].persistent != 0; }
+uint32_t BlurBlocks(int index, uint32_t tiles_x, uint32_t tiles_y) {
+    const uint32_t s = static_cast<uint32_t>(kBlurVariants[index].strip);
+    return tiles_x * ((tiles_y + s - 1) / s);
+}
 void BlurTileShape(int index, int* w, int* h) {
     *w = kBlurVariants[index].w;
     *h = kBlurVariants[index].h;

@@ -23,6 +23,12 @@ cudaError_t LaunchFinalize(const DevBatch& batch, cudaStream_t stream);
 int BlurTileCount();
 void BlurTileShape(int index, int* w, int* h);
 int BlurTileThreads(int index);
+// Tiles one CTA computes down a column (1: one tile per CTA).
+int BlurTileStrip(int index);
+bool BlurTilePersistent(int index);
+// Blocks of variant `index` for a segment of tiles_x x tiles_y tiles: the
+// prefix sums of these are a batch's blur_start.
+uint32_t BlurBlocks(int index, uint32_t tiles_x, uint32_t tiles_y);
 // The one-tile-per-CTA variant with variant's tile shape (the variant
 // itself when it is one), which half planes run; -1 when there is none.
 int HalfPlaneVariant(int variant);

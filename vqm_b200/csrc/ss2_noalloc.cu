@@ -152,7 +152,7 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
     DevPair& P = t.pair;
     P.levels = static_cast<uint32_t>(plan.count);
     size_t floats = 0;
-    uint32_t nseg = 0, tiles = 0;
+    uint32_t nseg = 0, tiles = 0, blocks = 0;
     t.blur_start[0] = 0;
     for (int l = 0; l < plan.count; ++l) {
         P.w[l] = plan.w[l];
@@ -168,11 +168,13 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
             s.level = static_cast<uint32_t>(l);
             s.channel = static_cast<uint32_t>(c);
             s.tiles_x = (plan.w[l] + tw - 1) / tw;
-            s.tiles = s.tiles_x * ((plan.h[l] + th - 1) / th);
+            const uint32_t ty = (plan.h[l] + th - 1) / th;
+            s.tiles = s.tiles_x * ty;
             s.partial_first = tiles;
             tiles += s.tiles;
+            blocks += BlurBlocks(kDefaultBlurVariant, s.tiles_x, ty);
             ++nseg;
-            t.blur_start[nseg] = tiles;
+            t.blur_start[nseg] = blocks;
         }
     }
     P.image_stride = floats;
@@ -236,7 +238,7 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
     b.prep_items[1] = n[1];
     b.prep_blocks[0] = n[0] * per_image;
     b.prep_blocks[1] = n[1] * per_image;
-    b.blur_blocks = tiles;
+    b.blur_blocks = blocks;
     b.pair = &dev_tables->pair;
     b.seg = dev_tables->seg;
     b.prep_item = dev_tables->item;

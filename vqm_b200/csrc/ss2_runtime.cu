@@ -264,7 +264,7 @@ Tables BuildTables(const std::vector<std::pair<uint32_t, uint32_t>>& sizes, Blur
                 s.tiles = s.tiles_x * ty;
                 s.partial_first = static_cast<uint32_t>(t.partials);
                 t.partials += s.tiles;
-                blur += s.tiles;
+                blur += BlurBlocks(shape.variant, s.tiles_x, ty);
                 t.segs.push_back(s);
                 t.blur_start.push_back(static_cast<uint32_t>(blur));
             }
@@ -450,17 +450,45 @@ void FillPlanes(DevSource& src, const vqm_cu_format& f, uint32_t w, uint32_t h,
 }
 
 // Copies a host image into a packed device buffer (vqm::Image's layout).
+// Planes whose rows are packed go as linear copies, and planes that also
+// follow one another without a gap in both the host image and the packed
+// layout (a vqm::Image buffer, for one) go as one copy: a 2D copy of short
+// rows, or several copies of one image, leave the copy engine idle between
+// rows and between copies.
 void CopyHostImage(const vqm_cu_image& img, uint8_t* dst, cudaStream_t stream) {
     const auto layout = PlaneLayout(img.format, img.width, img.height);
+    const uint8_t* run_src = nullptr;  // the pending linear run
+    size_t run_offset = 0, run_bytes = 0;
+    const auto flush = [&] {
+        if (run_bytes)
+            VQM_CK(cudaMemcpyAsync(dst + run_offset, run_src, run_bytes, cudaMemcpyHostToDevice,
+                                   stream));
+        run_bytes = 0;
+    };
     for (int p = 0; p < 4; ++p) {
         if (!layout[p].present()) continue;
         const size_t row = layout[p].width * layout[p].sample_bytes;
         const size_t stride = img.strides[p] ? img.strides[p] : row;
         if (img.planes[p] == nullptr) throw std::invalid_argument("image: plane is null");
         if (stride < row) throw std::invalid_argument("image: plane stride is shorter than a row");
-        VQM_CK(cudaMemcpy2DAsync(dst + layout[p].offset, row, img.planes[p], stride, row,
-                                 layout[p].height, cudaMemcpyHostToDevice, stream));
+        const auto* src = static_cast<const uint8_t*>(img.planes[p]);
+        if (stride != row) {
+            flush();
+            VQM_CK(cudaMemcpy2DAsync(dst + layout[p].offset, row, src, stride, row,
+                                     layout[p].height, cudaMemcpyHostToDevice, stream));
+            continue;
+        }
+        const size_t bytes = row * layout[p].height;
+        if (run_bytes && run_src + run_bytes == src && run_offset + run_bytes == layout[p].offset) {
+            run_bytes += bytes;
+            continue;
+        }
+        flush();
+        run_src = src;
+        run_offset = layout[p].offset;
+        run_bytes = bytes;
     }
+    flush();
 }
 
 void PackedPlanes(const vqm_cu_format& f, uint32_t w, uint32_t h, const uint8_t* base,
@@ -939,22 +967,25 @@ public:
                 throw std::invalid_argument("cuda: no such blur variant");
             shape_ = BlurShape::Of(static_cast<int>(cfg.variant) - 1);
         } else if (cfg.tile_w || cfg.tile_h) {
-            // The last compiled variant with that tile (the packed ones come
-            // after the scalar one).
+            // The one-tile-per-CTA variant with that tile.
             int found = -1;
-            for (int i = 0; i < BlurTileCount(); ++i) {
+            for (int i = 0; i < BlurTileCount() && found < 0; ++i) {
                 int w, h;
                 BlurTileShape(i, &w, &h);
-                if (w == static_cast<int>(cfg.tile_w) && h == static_cast<int>(cfg.tile_h)) found = i;
+                if (w == static_cast<int>(cfg.tile_w) && h == static_cast<int>(cfg.tile_h) &&
+                    BlurTileStrip(i) == 1 && !BlurTilePersistent(i))
+                    found = i;
             }
             if (found < 0) throw std::invalid_argument("cuda: blur tile shape is not compiled in");
             shape_ = BlurShape::Of(found);
         }
         if (cfg.half_planes) {
-            // Half planes run the one-tile-per-CTA blur; a persistent variant
-            // without such a twin falls back to the default tile.
+            // Half planes run the one-tile-per-CTA blur of the same tile (the
+            // default tile when there is none), and the tables count its
+            // blocks.
             mem_.elem_bytes = 2;
-            if (HalfPlaneVariant(shape_.variant) < 0) shape_ = BlurShape::Of(kDefaultBlurVariant);
+            const int v = HalfPlaneVariant(shape_.variant);
+            shape_ = BlurShape::Of(v < 0 ? kDefaultBlurVariant : v);
         }
         device_ = ResolveDevice(cfg.device);
         EnsureDevice(device_);
@@ -1457,9 +1488,12 @@ int vqm_cu_ss2_blur_variants(uint32_t* count, uint32_t* shapes) {
             for (int i = 0; i < vqm_b200::BlurTileCount(); ++i) {
                 int w, h;
                 vqm_b200::BlurTileShape(i, &w, &h);
-                shapes[3 * i] = static_cast<uint32_t>(w);
-                shapes[3 * i + 1] = static_cast<uint32_t>(h);
-                shapes[3 * i + 2] = static_cast<uint32_t>(vqm_b200::BlurTileThreads(i));
+                uint32_t* v = shapes + VQM_CU_SS2_VARIANT_WORDS * i;
+                v[0] = static_cast<uint32_t>(w);
+                v[1] = static_cast<uint32_t>(h);
+                v[2] = static_cast<uint32_t>(vqm_b200::BlurTileThreads(i));
+                v[3] = static_cast<uint32_t>(vqm_b200::BlurTileStrip(i));
+                v[4] = vqm_b200::BlurTilePersistent(i) ? 1u : 0u;
             }
     });
 }

@@ -572,13 +572,18 @@ class Ssimulacra2Pipeline:
 # ---------------------------------------------------------------------------
 
 
+VARIANT_WORDS = 5
+
+
 def blur_variants():
-    """[(tile_w, tile_h, threads)] of the blur kernels compiled in."""
+    """[(tile_w, tile_h, threads, strip, persistent)] of the blur kernels
+    compiled in; strip = tiles one CTA computes down a column."""
     n = ctypes.c_uint32()
     _check(_lib.vqm_cu_ss2_blur_variants(ctypes.byref(n), None))
-    shapes = (ctypes.c_uint32 * (3 * n.value))()
+    k = VARIANT_WORDS
+    shapes = (ctypes.c_uint32 * (k * n.value))()
     _check(_lib.vqm_cu_ss2_blur_variants(ctypes.byref(n), shapes))
-    return [tuple(shapes[3 * i:3 * i + 3]) for i in range(n.value)]
+    return [tuple(shapes[k * i:k * i + k]) for i in range(n.value)]
 
 
 class Ssimulacra2Batch:
