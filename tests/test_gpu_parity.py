@@ -243,9 +243,16 @@ def test_every_blur_variant(variant):
              synthetic.rgb_pair(8, 8, 43)[:2], synthetic.rgb_pair(97, 2000, 44)[:2]]
     b = ss2.Ssimulacra2Batch(variant=variant)
     ref = ss2.Ssimulacra2Batch(variant=0).compute_many(pairs)
+    # Variants with variant 0's tile (strips, persistent CTAs) reduce every
+    # tile the same way, so they agree with it bit for bit: a batch's
+    # automatic choice among them never changes a pair's result.
+    same_tile = ss2.blur_variants()[variant][:2] == ss2.blur_variants()[0][:2]
     for (o, d), r, r0 in zip(pairs, b.compute_many(pairs), ref):
         check_parity(r, o, d, label=f"variant {variant} {o.width}x{o.height}")
-        assert not helpers.feature_mismatch(r.norms, r0.norms, rtol=1e-6, atol=1e-12)
+        if same_tile:
+            assert np.array_equal(r.norms, r0.norms) and r.device_score == r0.device_score
+        else:
+            assert not helpers.feature_mismatch(r.norms, r0.norms, rtol=1e-6, atol=1e-12)
 
 
 def test_pool_score_many_in_order():

@@ -702,6 +702,24 @@ int BlurTileCount() { return kBlurVariantCount; }
 int BlurTileThreads(int index) { return kBlurVariants[index].threads; }
 int BlurTileStrip(int index) { return kBlurVariants[index].strip; }
 bool BlurTilePersistent(int index) { return kBlurVariants[index].persistent != 0; }
+int AutoBlurVariant(uint64_t tiles, int sms) {
+    // The longest 32x32 strip that still gives every CTA slot of the device
+    // 8 CTAs (fewer, and the last wave's idle slots cost more than the
+    // shared rows save: measured on 1080p and 4K pairs, one or many).
+    const BlurVariant& base = kBlurVariants[kDefaultBlurVariant];
+    const uint64_t slots = static_cast<uint64_t>(sms > 0 ? sms : 1) * base.per_sm;
+    int best = kDefaultBlurVariant, strip = 1;
+    for (int i = 0; i < kBlurVariantCount; ++i) {
+        const BlurVariant& v = kBlurVariants[i];
+        if (v.persistent || v.w != base.w || v.h != base.h || v.threads != base.threads) continue;
+        if (v.strip > strip && tiles / static_cast<uint64_t>(v.strip) >= 8 * slots) {
+            best = i;
+            strip = v.strip;
+        }
+    }
+    return best;
+}
+
 uint32_t BlurBlocks(int index, uint32_t tiles_x, uint32_t tiles_y) {
     const uint32_t s = static_cast<uint32_t>(kBlurVariants[index].strip);
     return tiles_x * ((tiles_y + s - 1) / s);

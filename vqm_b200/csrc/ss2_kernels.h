@@ -29,6 +29,11 @@ bool BlurTilePersistent(int index);
 // Blocks of variant `index` for a segment of tiles_x x tiles_y tiles: the
 // prefix sums of these are a batch's blur_start.
 uint32_t BlurBlocks(int index, uint32_t tiles_x, uint32_t tiles_y);
+// The variant used when a caller does not choose one, for a launch of
+// `tiles` output tiles of the default variant on a device with `sms` SMs:
+// the default itself for small launches, a strip of its tile for large ones.
+// Both reduce each tile alike, so the choice never changes a result.
+int AutoBlurVariant(uint64_t tiles, int sms);
 // The one-tile-per-CTA variant with variant's tile shape (the variant
 // itself when it is one), which half planes run; -1 when there is none.
 int HalfPlaneVariant(int variant);

@@ -277,6 +277,28 @@ Tables BuildTables(const std::vector<std::pair<uint32_t, uint32_t>>& sizes, Blur
     return t;
 }
 
+// Output tiles of the default blur variant over pairs of the given sizes.
+uint64_t DefaultTileCount(const std::vector<std::pair<uint32_t, uint32_t>>& sizes) {
+    int tw = 0, th = 0;
+    BlurTileShape(kDefaultBlurVariant, &tw, &th);
+    uint64_t tiles = 0;
+    for (const auto& wh : sizes) {
+        const ScalePlan plan = PlanScales(wh.first, wh.second);
+        for (int l = 0; l < plan.count; ++l)
+            for (int c = 0; c < 3; ++c)
+                if (plan.mask[l] & (1u << c))
+                    tiles += static_cast<uint64_t>((plan.w[l] + tw - 1) / tw) *
+                             ((plan.h[l] + th - 1) / th);
+    }
+    return tiles;
+}
+
+int DeviceSms(int device) {
+    int sms = 0;
+    VQM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    return sms;
+}
+
 // Splits the images into the table-decoded group and the generic group
 // (table[i][k]: image k of pair i decodes by table) and lays out each
 // group's prefix tile offsets. The list sizes do not depend on the split.
@@ -536,6 +558,9 @@ public:
         stream_ = own_stream_;
         VQM_CK(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming));
         VQM_CK(cudaEventCreateWithFlags(&copied_, cudaEventDisableTiming));
+        if (!cfg.half_planes)
+            shape_ = BlurShape::Of(
+                AutoBlurVariant(DefaultTileCount({{cfg.width, cfg.height}}), DeviceSms(device_)));
         tables_ = BuildTables({{cfg.width, cfg.height}}, shape_);
         BuildPrepLists(tables_, {{true, true}});
         mem_.Layout(tables_);
@@ -987,9 +1012,12 @@ public:
             const int v = HalfPlaneVariant(shape_.variant);
             shape_ = BlurShape::Of(v < 0 ? kDefaultBlurVariant : v);
         }
+        // No variant chosen: each submit picks one for its tile count.
+        auto_shape_ = !cfg.variant && !cfg.tile_w && !cfg.tile_h && !cfg.half_planes;
         device_ = ResolveDevice(cfg.device);
         EnsureDevice(device_);
         VQM_CK(cudaSetDevice(device_));
+        sms_ = DeviceSms(device_);
         VQM_CK(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
         stream_ = own_stream_;
         VQM_CK(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming));
@@ -1034,7 +1062,9 @@ public:
                 host_bytes += AlignUp(RequiredBytes(d[i].format, d[i].width, d[i].height), 256);
         }
         VQM_CK(cudaSetDevice(device_));
-        Tables t = BuildTables(sizes, shape_);
+        const BlurShape shape =
+            auto_shape_ ? BlurShape::Of(AutoBlurVariant(DefaultTileCount(sizes), sms_)) : shape_;
+        Tables t = BuildTables(sizes, shape);
         mem_.Layout(t);
         inputs_.ensure(std::max<size_t>(host_bytes, 256));
         size_t cursor = 0;
@@ -1069,7 +1099,7 @@ public:
         if (host_bytes) VQM_CK(cudaEventRecord(copied_, stream_));
         mem_.EnqueueUpload(mem_.table_bytes, stream_);
         VQM_CK(cudaMemsetAsync(mem_.pair_done.as<void>(), 0, sizeof(uint32_t) * n, stream_));
-        mem_.EnqueueKernels(shape_, stream_, timing_ ? stage_ev_ : nullptr);
+        mem_.EnqueueKernels(shape, stream_, timing_ ? stage_ev_ : nullptr);
         timed_ = timing_;
         mem_.EnqueueReadback(stream_);
         VQM_CK(cudaEventRecord(done_, stream_));
@@ -1111,6 +1141,8 @@ public:
 private:
     vqm_cu_ss2_batch_config cfg_;
     BlurShape shape_;
+    bool auto_shape_ = false;
+    int sms_ = 0;
     int device_ = 0;
     cudaStream_t own_stream_ = nullptr, stream_ = nullptr;
     cudaEvent_t done_ = nullptr, copied_ = nullptr;
