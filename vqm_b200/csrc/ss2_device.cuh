@@ -57,6 +57,9 @@ struct DevSource {
     uint8_t identity1, identity2;
     uint8_t chroma_variant;    // subsampled chroma planes present
     uint8_t lut;               // 1: 8-bit RGB, no alpha: decode by table
+    uint8_t in_range;          // 1: table entries finite, >= 0, <= 1e20 and no
+                               // primaries matrix, so every XYB mix of the
+                               // image and its levels lies in [bias, 1e30]
     float scale[3], offset[3]; // luma, chroma, alpha
     float m1[9], m2[9];        // encoded->RGB (or ICtCp->LMS), primaries->709
     float kr, kg, kb, to_linear;

@@ -503,6 +503,7 @@ void BuildSourceConstants(const vqm_cu_format& f, uint32_t chroma_filter, float 
              tid != 11)
                 ? 1
                 : 0;
+    d.in_range = 0;
     if (!d.lut) {
         std::memset(d.srgb_lut, 0, sizeof(d.srgb_lut));
         return;
@@ -525,6 +526,12 @@ void BuildSourceConstants(const vqm_cu_format& f, uint32_t chroma_filter, float 
         it = cache.emplace(key, table).first;
     }
     std::memcpy(d.srgb_lut, it->second.data(), sizeof(d.srgb_lut));
+    // Non-negative linear samples (and averages of them) mixed by the
+    // all-positive opsin rows plus the bias stay in the cube root's direct
+    // range; a primaries matrix could make them negative.
+    bool in_range = d.identity2 != 0;
+    for (float v : d.srgb_lut) in_range = in_range && v >= 0.0f && v <= 1.0e20f;
+    d.in_range = in_range ? 1 : 0;
 }
 
 bool ChannelPruned(int channel, int scale, int scales) {

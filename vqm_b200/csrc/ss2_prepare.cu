@@ -24,6 +24,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <type_traits>
 
 #include "ss2_decode.cuh"
 #include "ss2_detmath.h"
@@ -64,8 +65,11 @@ __device__ __forceinline__ float2 Neg(float2 v) { return make_float2(-v.x, -v.y)
 // mix of in-gamut light produces: the mix includes a bias of 0.0038) the
 // function takes its unscaled path, executed here with the same operations in
 // the same order two lanes at a time; any other lane pair calls it per lane.
+// kInRange: the caller knows both lanes are in that range (no check).
+template <bool kInRange = false>
 __device__ __forceinline__ float2 Cbrt2(float2 x) {
-    if (!(x.x >= 1.0e-20f && x.x <= 1.0e30f && x.y >= 1.0e-20f && x.y <= 1.0e30f))
+    if (!kInRange &&
+        !(x.x >= 1.0e-20f && x.x <= 1.0e30f && x.y >= 1.0e-20f && x.y <= 1.0e30f))
         return make_float2(ss2dm::cbrt(x.x), ss2dm::cbrt(x.y));
     float2 r = make_float2(__uint_as_float(0x54a21d2au - __float_as_uint(x.x) / 3u),
                            __uint_as_float(0x54a21d2au - __float_as_uint(x.y) / 3u));
@@ -91,14 +95,16 @@ __device__ __forceinline__ float2 Max0(float2 v) {
 }
 
 // prepare.comp:81-98 for two pixels. Only the channels in `mask` are
-// meaningful; B's cube root is skipped when B is not stored.
+// meaningful; B's cube root is skipped when B is not stored. kInRange: the
+// inputs are non-negative and finite (so every mix is at least the bias).
+template <bool kInRange = false>
 __device__ __forceinline__ void Xyb2(float2 r, float2 g, float2 b, uint32_t mask, float2 out[3]) {
     const float2 m0 = Max0(__ffma2_rn(Pack(kM00), r,
                                       __ffma2_rn(Pack(kM01), g, __ffma2_rn(Pack(kM02), b, Pack(kBias)))));
     const float2 m1 = Max0(__ffma2_rn(Pack(kM10), r,
                                       __ffma2_rn(Pack(kM11), g, __ffma2_rn(Pack(kM12), b, Pack(kBias)))));
-    const float2 c0 = __fadd2_rn(Cbrt2(m0), Pack(-kCbrtBias));
-    const float2 c1 = __fadd2_rn(Cbrt2(m1), Pack(-kCbrtBias));
+    const float2 c0 = __fadd2_rn(Cbrt2<kInRange>(m0), Pack(-kCbrtBias));
+    const float2 c1 = __fadd2_rn(Cbrt2<kInRange>(m1), Pack(-kCbrtBias));
     const float2 sum = __fadd2_rn(c0, c1);
     out[0] = __ffma2_rn(__fmul2_rn(Pack(0.5f), __fadd2_rn(c0, Neg(c1))), Pack(14.0f), Pack(0.42f));
     out[1] = __ffma2_rn(Pack(0.5f), sum, Pack(0.01f));
@@ -106,15 +112,16 @@ __device__ __forceinline__ void Xyb2(float2 r, float2 g, float2 b, uint32_t mask
     if (mask & 4u) {
         const float2 m2 = Max0(__ffma2_rn(
             Pack(kM20), r, __ffma2_rn(Pack(kM21), g, __ffma2_rn(Pack(kM22), b, Pack(kBias)))));
-        const float2 c2 = __fadd2_rn(Cbrt2(m2), Pack(-kCbrtBias));
+        const float2 c2 = __fadd2_rn(Cbrt2<kInRange>(m2), Pack(-kCbrtBias));
         out[2] = __fadd2_rn(__ffma2_rn(Pack(-0.5f), sum, c2), Pack(0.55f));
     }
 }
 
 // One pixel: the pair form with a duplicated lane.
+template <bool kInRange = false>
 __device__ __forceinline__ void Xyb(float r, float g, float b, uint32_t mask, float out[3]) {
     float2 o[3];
-    Xyb2(Pack(r), Pack(g), Pack(b), mask, o);
+    Xyb2<kInRange>(Pack(r), Pack(g), Pack(b), mask, o);
     out[0] = o[0].x;
     out[1] = o[1].x;
     out[2] = o[2].x;
@@ -284,6 +291,10 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
         }
     }
     __syncthreads();
+    // The rest of the kernel, for inputs whose every mix is known to be in
+    // the cube root's direct range (kInRange) or not.
+    const auto body = [=](auto in_range) {
+    constexpr bool kInRange = decltype(in_range)::value;
     const DevSource& s = src_s;
     const uint32_t levels = lv.levels;
     const uint32_t width = s.width, height = s.height;
@@ -343,10 +354,12 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
                 // column or row past the image is the plane's zero padding.
                 if (mask0) {
                     float2 top[3], bottom[3];
-                    Xyb2(make_float2(lin[0][0], lin[1][0]), make_float2(lin[0][1], lin[1][1]),
-                         make_float2(lin[0][2], lin[1][2]), mask0, top);
-                    Xyb2(make_float2(lin[2][0], lin[3][0]), make_float2(lin[2][1], lin[3][1]),
-                         make_float2(lin[2][2], lin[3][2]), mask0, bottom);
+                    Xyb2<kInRange>(make_float2(lin[0][0], lin[1][0]),
+                                   make_float2(lin[0][1], lin[1][1]),
+                                   make_float2(lin[0][2], lin[1][2]), mask0, top);
+                    Xyb2<kInRange>(make_float2(lin[2][0], lin[3][0]),
+                                   make_float2(lin[2][1], lin[3][1]),
+                                   make_float2(lin[2][2], lin[3][2]), mask0, bottom);
                     const uint32_t x0 = 2 * bx, y0 = 2 * by;
                     const bool two = x0 + 1 < width;
                     const bool second_row = y0 + 1 < height;
@@ -373,8 +386,8 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
         // Level 1: pixels (bx0, by) and (bx0 + 1, by).
         if (last >= 1) {
             float2 xyb[3];
-            Xyb2(make_float2(l1[0][0], l1[1][0]), make_float2(l1[0][1], l1[1][1]),
-                 make_float2(l1[0][2], l1[1][2]), lv.mask[1], xyb);
+            Xyb2<kInRange>(make_float2(l1[0][0], l1[1][0]), make_float2(l1[0][1], l1[1][1]),
+                           make_float2(l1[0][2], l1[1][2]), lv.mask[1], xyb);
             StorePixel<kHalf>(lv, 1, bx0, by, xyb[0].x, xyb[1].x, xyb[2].x);
             StorePixel<kHalf>(lv, 1, bx0 + 1, by, xyb[0].y, xyb[1].y, xyb[2].y);
             if (last >= 2) {
@@ -419,7 +432,7 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
                                      p[cy1 * prev_side + cx0], p[cy1 * prev_side + cx1]);
         }
         float xyb[3];
-        Xyb(v[0], v[1], v[2], lv.mask[level], xyb);
+        Xyb<kInRange>(v[0], v[1], v[2], lv.mask[level], xyb);
         StorePixel<kHalf>(lv, level, gx * side + jx, gy * side + jy, xyb[0], xyb[1], xyb[2]);
         if (level < last) {
             float* next0 = (level & 1u) ? &ladder_a[0][0] : &ladder_b[0][0];
@@ -433,6 +446,13 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
                 __syncwarp((1u << active) - 1u);
             }
         }
+    }
+    };
+    if constexpr (kTable) {
+        if (src_s.in_range) body(std::true_type{});
+        else body(std::false_type{});
+    } else {
+        body(std::false_type{});
     }
 }
 
