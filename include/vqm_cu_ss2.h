@@ -272,6 +272,19 @@ typedef struct vqm_cu_ss2_batch_config {
 #define VQM_CU_SS2_VARIANT_WORDS 5
 int vqm_cu_ss2_blur_variants(uint32_t* count, uint32_t* shapes);
 
+/* Which device decode an image of format `format` takes (a diagnostic; no
+ * device is touched): VQM_CU_DECODE_GENERIC, _TABLE (8-bit grey/RGB through a
+ * per-image table), _TABLE_IN_RANGE (the same, with every linear sample
+ * non-negative so the cube roots need no range check) or _YUV (integer YUV
+ * with a power-law transfer and at most 2x chroma subsampling, phases fixed
+ * per pixel parity). The results are the same whichever path runs. */
+#define VQM_CU_DECODE_GENERIC 0
+#define VQM_CU_DECODE_TABLE 1
+#define VQM_CU_DECODE_TABLE_IN_RANGE 2
+#define VQM_CU_DECODE_YUV 3
+int vqm_cu_ss2_decode_path(const vqm_cu_format* format, uint32_t chroma_filter,
+                           uint32_t* path);
+
 int vqm_cu_ss2_batch_create(const vqm_cu_ss2_batch_config* config,
                             vqm_cu_ss2_batch** batch);
 int vqm_cu_ss2_batch_destroy(vqm_cu_ss2_batch* batch);

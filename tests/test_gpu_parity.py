@@ -108,6 +108,64 @@ def test_pyramid_planes_bit_exact(case):
                         (case, image, level, c, np.abs(got - want[level][c]).max())
 
 
+def _yuv_fast_formats():
+    F, T = ss2.ImageFormat, ss2.TransferCharacteristics
+
+    def yuv(**kw):
+        base = dict(type=ss2.PixelType.Word, depth=10, family=ss2.ColorFamily.Yuv,
+                    range=ss2.PixelRange.Limited, matrix=ss2.MatrixCoefficients.Bt709,
+                    transfer=T.Bt709, primaries=ss2.ColorPrimaries.Bt709, subsample_w=1,
+                    subsample_h=1)
+        base.update(kw)
+        return F(**base)
+
+    L = ss2.ChromaLocation
+    return {
+        "420p10_left": yuv(chroma_location=L.Left),
+        "420p10_center": yuv(chroma_location=L.Center),
+        "420p10_topleft": yuv(chroma_location=L.TopLeft),
+        "420p10_top": yuv(chroma_location=L.Top),
+        "420p10_bottomleft": yuv(chroma_location=L.BottomLeft),
+        "420p10_bottom": yuv(chroma_location=L.Bottom),
+        "422p8": yuv(type=ss2.PixelType.Byte, depth=0, subsample_h=0),
+        "444p10": yuv(subsample_w=0, subsample_h=0),
+        "440p10": yuv(subsample_w=0),
+        "420p12_bt2020": yuv(depth=12, matrix=ss2.MatrixCoefficients.Bt2020Ncl,
+                             transfer=T.Bt2020_12, primaries=ss2.ColorPrimaries.Bt2020),
+        "420p8_gamma22": yuv(type=ss2.PixelType.Byte, depth=0, transfer=T.Bt470M),
+        "420p16_gamma28_full": yuv(depth=16, range=ss2.PixelRange.Full, transfer=T.Bt470Bg),
+    }
+
+
+@pytest.mark.parametrize("name", list(_yuv_fast_formats()))
+def test_yuv_fast_path_planes_bit_exact(name):
+    """Integer YUV with a power-law transfer takes the fast decode (staged
+    chroma window, per-parity taps); its planes equal the oracle's generic
+    decode bit for bit, inside the image and along its edges."""
+    from oracle import binding as ob
+    fmt = _yuv_fast_formats()[name]
+    assert ss2.decode_path(fmt) == "yuv"
+    w, h = 200, 134
+    ov = _values(fmt, w, h, 21)
+    rng = np.random.default_rng(4)
+    dv = [None if v is None else np.clip(v + rng.normal(0, 0.03, v.shape),
+                                         -0.5 if i in (1, 2) else 0, 1)
+          for i, v in enumerate(ov)]
+    imgs = (helpers.pack_planes(fmt, w, h, ov), helpers.pack_planes(fmt, w, h, dv))
+    with ss2.Ssimulacra2Pipeline(w, h) as p:
+        p.compute(*imgs)
+        scales = len(ss2.plan_scales(w, h))
+        for image, img in enumerate(imgs):
+            want = ob.pyramid(helpers.to_oracle(img), 0.5)
+            for level in range(scales):
+                for c in range(3):
+                    if ob.channel_pruned(c, level, scales):
+                        continue
+                    got = p.debug_plane(image, level, c)
+                    assert np.array_equal(got.view(np.uint32), want[level][c].view(np.uint32)), \
+                        (name, image, level, c, np.abs(got - want[level][c]).max())
+
+
 def test_plain_256_pair():
     o, d = helpers.plain_256_pair()
     with ss2.Ssimulacra2Pipeline(256, 256) as p:
@@ -209,6 +267,30 @@ def test_input_formats(name, chroma_filter):
         for bg in ((0.1, 0.9) if fmt.alpha else (0.5,)):
             check_parity(p.compute(o, d, bg), o, d, bg, chroma_filter,
                          label=f"{name} filter {chroma_filter} bg {bg}")
+
+
+@pytest.mark.parametrize("name", ["rgb8_limited", "rgb8_bt2020", "grey8"])
+def test_table_decode_full_code_range(name):
+    """8-bit table decode over every code 0..255: limited range puts codes
+    below 16 at negative light (mixes that clamp to 0 and take the cube
+    root's checked path), BT.2020 primaries go through a matrix (checked
+    path), full-range grey stays non-negative (unchecked path)."""
+    F = ss2.ImageFormat
+    fmt = {"rgb8_limited": F(type=ss2.PixelType.Byte, range=ss2.PixelRange.Limited),
+           "rgb8_bt2020": F(type=ss2.PixelType.Byte, primaries=ss2.ColorPrimaries.Bt2020),
+           "grey8": F(type=ss2.PixelType.Byte, family=ss2.ColorFamily.Grey,
+                      matrix=ss2.MatrixCoefficients.Bt709)}[name]
+    w, h = 160, 96
+    rng = np.random.default_rng(77)
+    planes = 1 if fmt.family == ss2.ColorFamily.Grey else 3
+    ramp = np.tile(np.arange(w, dtype=np.int64) * 256 // w, (h, 1))
+    o = np.stack([(ramp + 37 * c + rng.integers(0, 9, (h, w))) % 256 for c in range(planes)])
+    o[:, :24, :40] = 0  # a block of code 0 in every plane
+    d = np.clip(o + rng.integers(-6, 7, o.shape), 0, 255)
+    oi = ss2.Image(w, h, fmt, o.astype(np.uint8).reshape(-1).copy())
+    di = ss2.Image(w, h, fmt, d.astype(np.uint8).reshape(-1).copy())
+    with ss2.Ssimulacra2Pipeline(w, h) as p:
+        check_parity(p.compute(oi, di), oi, di, label=name)
 
 
 def test_mixed_format_pair():

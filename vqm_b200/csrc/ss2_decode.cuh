@@ -16,6 +16,7 @@
 
 #include "ss2_detmath.h"
 #include "ss2_device.cuh"
+#include "ss2_layout.h"
 
 namespace vqm_b200 {
 
@@ -363,6 +364,110 @@ __device__ __forceinline__ void BlockLinearGeneric(const DevSource& s, uint32_t 
         rgb[i][0] = e[0];
         rgb[i][1] = e[1];
         rgb[i][2] = e[2];
+    }
+}
+
+// The YUV fast path (DevSource::yuv_fast): the CTA's chroma window of both
+// planes staged once in shared memory (kPrepTile >> sub samples per axis plus
+// one on each side, edge-clamped: for the one-past-the-edge positions a block
+// can touch that is the reference's mirror index), already scaled like
+// RawSample. kChromaStage floats per plane.
+constexpr int kChromaStage = ((kPrepTile >> 1) + 2) * (kPrepTile + 2);
+__device__ __forceinline__ void StageChroma(const DevSource& s, uint32_t gx, uint32_t gy,
+                                            float* stage) {
+    const uint32_t sw = (kPrepTile >> s.sub_w) + 2, sh = (kPrepTile >> s.sub_h) + 2;
+    const int c0x = static_cast<int>((gx * kPrepTile) >> s.sub_w) - 1;
+    const int c0y = static_cast<int>((gy * kPrepTile) >> s.sub_h) - 1;
+    const uint32_t n = sw * sh;
+    for (uint32_t k = threadIdx.x; k < 2 * n; k += blockDim.x) {
+        const int p = k >= n ? 2 : 1;
+        const uint32_t idx = k - static_cast<uint32_t>(p - 1) * n;
+        const uint32_t j = idx / sw, i = idx - j * sw;
+        const int dx = static_cast<int>(s.plane_w[p]), dy = static_cast<int>(s.plane_h[p]);
+        const uint32_t x = static_cast<uint32_t>(min(max(c0x + static_cast<int>(i), 0), dx - 1));
+        const uint32_t y = static_cast<uint32_t>(min(max(c0y + static_cast<int>(j), 0), dy - 1));
+        const uint8_t* row = s.plane[p] + static_cast<size_t>(y) * s.row_bytes[p];
+        const float v = s.type == 0
+                            ? static_cast<float>(__ldg(row + x))
+                            : static_cast<float>(__ldg(reinterpret_cast<const uint16_t*>(row) + x));
+        stage[(p - 1) * kChromaStage + idx] = __fmaf_rn(v, s.scale[1], s.offset[1]);
+    }
+}
+
+// BlockLinearGeneric for a yuv_fast image's block (bx, by) of the CTA's tile
+// (gx, gy) whose two columns and rows are inside the image: the same values,
+// with the format's branches resolved, the chroma taps read from the staged
+// window at the host's per-parity slots and weights, and the transfer's power
+// without range steps (its arguments are below 2^40).
+__device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* stage,
+                                               uint32_t gx, uint32_t gy, uint32_t bx,
+                                               uint32_t by, float rgb[4][3]) {
+    const uint32_t x0 = 2 * bx, y0 = 2 * by;
+    float e[4][3];
+    {
+        const uint8_t* r0 = s.plane[0] + static_cast<size_t>(y0) * s.row_bytes[0];
+        const uint8_t* r1 = r0 + s.row_bytes[0];
+        float v[4];
+        if (s.type == 0) {
+            v[0] = __ldg(r0 + x0);
+            v[1] = __ldg(r0 + x0 + 1);
+            v[2] = __ldg(r1 + x0);
+            v[3] = __ldg(r1 + x0 + 1);
+        } else {
+            const uint16_t* w0 = reinterpret_cast<const uint16_t*>(r0);
+            const uint16_t* w1 = reinterpret_cast<const uint16_t*>(r1);
+            v[0] = __ldg(w0 + x0);
+            v[1] = __ldg(w0 + x0 + 1);
+            v[2] = __ldg(w1 + x0);
+            v[3] = __ldg(w1 + x0 + 1);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) e[i][0] = __fmaf_rn(v[i], s.scale[0], s.offset[0]);
+    }
+    if (s.chroma_variant) {
+        const uint32_t sw = (kPrepTile >> s.sub_w) + 2;
+        // Window slot 0 of this block is chroma sample (cx - 1, cy - 1), the
+        // staged entry (cx - 1 - c0x, cy - 1 - c0y).
+        const int bxs = static_cast<int>((x0 >> s.sub_w) - ((gx * kPrepTile) >> s.sub_w));
+        const int bys = static_cast<int>((y0 >> s.sub_h) - ((gy * kPrepTile) >> s.sub_h));
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int xp = i & 1, yp = i >> 1;
+                const float* t =
+                    stage + p * kChromaStage + (bys + s.cslot[1][yp]) * static_cast<int>(sw) +
+                    bxs + s.cslot[0][xp];
+                const float* w = s.cweight[yp][xp];
+                // A first slot of 2 puts the second tap past the window: 0.
+                const bool xpast = s.cslot[0][xp] == 2, ypast = s.cslot[1][yp] == 2;
+                const float t0 = t[0], t1 = xpast ? 0.0f : t[1];
+                const float b0 = ypast ? 0.0f : t[sw];
+                const float b1 = xpast || ypast ? 0.0f : t[sw + 1];
+                e[i][1 + p] = __fmaf_rn(
+                    w[3], b1, __fmaf_rn(w[2], b0, __fmaf_rn(w[1], t1, __fmul_rn(w[0], t0))));
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            e[i][1] = RawSample(s, 1, x0 + (i & 1), y0 + (i >> 1));
+            e[i][2] = RawSample(s, 2, x0 + (i & 1), y0 + (i >> 1));
+        }
+    }
+    const float g = s.gamma;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        if (!s.identity1) ApplyMatrix(s.m1, e[i]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float v = e[i][c];
+            e[i][c] = v < 0.0f ? 0.0f : ss2dm::pow_bounded(v, g);
+        }
+        if (!s.identity2) ApplyMatrix(s.m2, e[i]);
+        rgb[i][0] = e[i][0];
+        rgb[i][1] = e[i][1];
+        rgb[i][2] = e[i][2];
     }
 }
 

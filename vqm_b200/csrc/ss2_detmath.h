@@ -146,6 +146,33 @@ SS2_DM float cbrt(float x) {
     return fmaf_(e, rr * third, y0) * scale;
 }
 
+// The polynomial coefficients and conversion constants of log2d, exp2d and
+// sinpi, indexed by the K* names below. Device code reads them from the
+// constant bank, where a double-precision instruction takes them as an
+// operand (a literal would first be assembled in registers); host code uses
+// the same values.
+#define SS2DM_CONSTANT_VALUES                                                  \
+    1.0 / 7.0, -1.0 / 6.0, 1.0 / 5.0, -1.0 / 4.0, 1.0 / 3.0, -0.5,             \
+        1.4426950408889634074, 0.69314718055994530942, 1.0 / 720.0,            \
+        1.0 / 120.0, 1.0 / 24.0, 1.0 / 6.0, 0.5, 1.0
+enum {
+    kLogC7, kLogC6, kLogC5, kLogC4, kLogC3, kLogC2,  // log(1 + r) - r: r^7..r^2
+    kLog2E, kLn2,
+    kExpC6, kExpC5, kExpC4, kExpC3, kExpC2, kExpC1,  // e^z - 1: z^6..z (over z)
+    kConstantCount
+};
+static const double kConstHost[kConstantCount] = {SS2DM_CONSTANT_VALUES};
+#if defined(__CUDACC__)
+static __constant__ double kConstDev[kConstantCount] = {SS2DM_CONSTANT_VALUES};
+#endif
+SS2_DM double K(int i) {
+#if defined(__CUDA_ARCH__)
+    return kConstDev[i];
+#else
+    return kConstHost[i];
+#endif
+}
+
 // The tables of log2d and exp2d (ss2_detmath_tables.h, written by
 // gen_detmath_tables.py): one copy for host code and one in device global
 // memory, where lanes that index different entries are served by the L1
@@ -195,14 +222,14 @@ SS2_DM double log2d_normal(uint64_t u, int shift = 0) {
     const int i = static_cast<int>(frac >> 45);
     const double m = from_bits64(frac | 0x3ff0000000000000ull);  // [1, 2)
     const double r = fmad(m, InvC(i), -1.0);
-    double p = 1.0 / 7.0;
-    p = fmad(p, r, -1.0 / 6.0);
-    p = fmad(p, r, 1.0 / 5.0);
-    p = fmad(p, r, -1.0 / 4.0);
-    p = fmad(p, r, 1.0 / 3.0);
-    p = fmad(p, r, -0.5);
+    double p = K(kLogC7);
+    p = fmad(p, r, K(kLogC6));
+    p = fmad(p, r, K(kLogC5));
+    p = fmad(p, r, K(kLogC4));
+    p = fmad(p, r, K(kLogC3));
+    p = fmad(p, r, K(kLogC2));
     const double ln1r = fmad(r * r, p, r);
-    return fmad(ln1r, 1.4426950408889634074, Log2InvC(i) + static_cast<double>(e));
+    return fmad(ln1r, K(kLog2E), Log2InvC(i) + static_cast<double>(e));
 }
 
 SS2_DM double log2d(double x) {
@@ -216,23 +243,30 @@ SS2_DM double log2d(double x) {
 // 2^t in double for |t| < 1000, table-driven: t = (64 n + j) / 64 + f with
 // j in [0, 64) and |f| <= 1/128 (f exact), 2^t = 2^n 2^(j/64) e^(f ln 2),
 // e^z - 1 by its Taylor series to z^6 (|z| < 0.0055, remainder below 4e-20).
-SS2_DM double exp2d(double t) {
-    if (t > 1000.0) t = 1000.0;
-    if (t < -1000.0) return 0.0;
+// The reduction and polynomial of exp2d for |t| <= 1000: 2^(j/64) e^(f ln 2)
+// in [0.5, 2], and n with 2^t = that 2^n.
+SS2_DM double exp2d_core(double t, int& n) {
     const double kd = floord(t * 64.0 + 0.5);
     const double f = t - kd * 0.015625;
     const int k = static_cast<int>(kd);
     const int j = k & 63;
-    int n = (k - j) >> 6;  // k - j is a multiple of 64
-    const double z = f * 0.69314718055994530942;
-    double p = 1.0 / 720.0;
-    p = fmad(p, z, 1.0 / 120.0);
-    p = fmad(p, z, 1.0 / 24.0);
-    p = fmad(p, z, 1.0 / 6.0);
-    p = fmad(p, z, 0.5);
-    p = fmad(p, z, 1.0);
+    n = (k - j) >> 6;  // k - j is a multiple of 64
+    const double z = f * K(kLn2);
+    double p = K(kExpC6);
+    p = fmad(p, z, K(kExpC5));
+    p = fmad(p, z, K(kExpC4));
+    p = fmad(p, z, K(kExpC3));
+    p = fmad(p, z, K(kExpC2));
+    p = fmad(p, z, K(kExpC1));
     const double tj = Exp2J(j);
-    const double v = fmad(tj, p * z, tj);  // 2^(j/64) (1 + (e^z - 1))
+    return fmad(tj, p * z, tj);  // 2^(j/64) (1 + (e^z - 1))
+}
+
+SS2_DM double exp2d(double t) {
+    if (t > 1000.0) t = 1000.0;
+    if (t < -1000.0) return 0.0;
+    int n;
+    const double v = exp2d_core(t, n);
     if (n > 1000) n = 1000;
     // v is in [0.5, 2]: one scaling when 2^n is a normal double; else split
     // it so every factor is (the product is the same: v 2^n1 is exact).
@@ -251,9 +285,23 @@ SS2_DM float pow(float x, float y) {
         exp2d(static_cast<double>(y) * log2d_normal(bits(static_cast<double>(x)))));
 }
 
+// pow(x, y) for float x in [0, 2^40] and y in [1, 4] with no branch: the
+// same value as pow, whose range steps such arguments never take (y log2 x
+// lies in [-596, 160], so exp2d neither clamps nor splits its scaling).
+// Negative x gives 0 (pow gives NaN).
+SS2_DM float pow_bounded(float x, float y) {
+    int n;
+    const double v = exp2d_core(
+        static_cast<double>(y) *
+            log2d_normal(bits(static_cast<double>(x > 0.0f ? x : 1.0f))),
+        n);
+    const float r = static_cast<float>(v * pow2i(n));
+    return x == 1.0f ? 1.0f : (x > 0.0f ? r : 0.0f);
+}
+
 // e^x for float x.
 SS2_DM float exp(float x) {
-    return static_cast<float>(exp2d(static_cast<double>(x) * 1.4426950408889634074));
+    return static_cast<float>(exp2d(static_cast<double>(x) * K(kLog2E)));
 }
 
 // sin(pi x) for float x in [0, 8): reduced to [-1/2, 1/2] around the

@@ -66,6 +66,16 @@ struct DevSource {
     float shift_x, shift_y;
     float cl[4];               // constant-luminance corner values
     float background;          // alpha blend target
+    // The YUV fast path (BlockLinearYuv, ss2_decode.cuh): integer YUV without
+    // alpha, matrix mode, a pure power-law transfer and chroma subsampled by
+    // at most 2 with bilinear upsampling. For a 2x2 luma block at even
+    // coordinates the bilinear phase of each output depends only on its
+    // parity, so the host fixes the first window slot and the four tap
+    // weights per parity.
+    uint8_t yuv_fast;
+    int8_t cslot[2][2];        // [0 = x, 1 = y][parity]: first window slot
+    float gamma;               // the transfer exponent
+    float cweight[2][2][4];    // [y parity][x parity]: w00, w10, w01, w11
     float srgb_lut[256];       // transfer(raw * scale + offset) per byte code
 };
 

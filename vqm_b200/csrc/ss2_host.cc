@@ -420,6 +420,82 @@ void ValidateFormat(const vqm_cu_format& f, uint32_t w, uint32_t h, const char* 
     if (const char* reason = ModeError(f)) fail(reason);
 }
 
+namespace {
+
+// The device's BilinearPhase (ss2_decode.cuh, color.glsl:288-299) in the
+// same single-precision steps.
+void HostBilinearPhase(uint32_t out_pos, float inv_scale, float shift, int centre, int& s0,
+                       float& w0, float& w1) {
+    const auto round_halfup = [](float x) {
+        return x < 0.0f ? std::floor(x + 0.5f) : std::floor(x + 0.49999997f);
+    };
+    const float pos = (static_cast<float>(out_pos) + 0.5f) * inv_scale + shift;
+    const float base = round_halfup(pos - 1.0f) + 0.5f;
+    const float t = pos - base;
+    s0 = static_cast<int>(std::floor(base)) - centre + 1;
+    w0 = 1.0f - t;
+    w1 = t;
+}
+
+// DevSource's YUV fast-path fields: set when the format qualifies and every
+// block's bilinear phases are those of its parity (checked over block
+// indices across the whole coordinate range).
+void FastYuvConstants(const vqm_cu_format& f, int mode, int tid, uint32_t chroma_filter,
+                      DevSource& d) {
+    d.yuv_fast = 0;
+    d.gamma = 0.0f;
+    std::memset(d.cslot, 0, sizeof(d.cslot));
+    std::memset(d.cweight, 0, sizeof(d.cweight));
+    if (!(f.family == 2 && f.type <= 1 && f.alpha == 0 && mode == 0 && tid >= 1 && tid <= 3 &&
+          f.subsample_w <= 1 && f.subsample_h <= 1 && (!d.chroma_variant || chroma_filter == 0)))
+        return;
+    const float gammas[4] = {0.0f, 2.4f, 2.2f, 2.8f};  // TransferDecode cases 1-3
+    d.gamma = gammas[tid];
+    float w[2][2][2];  // [axis][parity][tap]
+    static const uint32_t kBlocks[] = {0, 1, 2, 3, 5, 77, 1000, 4095, 16383, 32767};
+    for (int axis = 0; axis < 2; ++axis) {
+        const int sub = axis ? f.subsample_h : f.subsample_w;
+        const float inv = 1.0f / static_cast<float>(1u << sub);
+        const float shift = axis ? d.shift_y : d.shift_x;
+        for (int par = 0; par < 2; ++par) {
+            int s_ref = 0;
+            float w0_ref = 0.0f, w1_ref = 0.0f;
+            for (size_t k = 0; k < sizeof(kBlocks) / sizeof(kBlocks[0]); ++k) {
+                const uint32_t b = kBlocks[k];
+                int s0;
+                float w0, w1;
+                HostBilinearPhase(2 * b + par, inv, shift, static_cast<int>((2 * b) >> sub), s0,
+                                  w0, w1);
+                if (k == 0) {
+                    s_ref = s0;
+                    w0_ref = w0;
+                    w1_ref = w1;
+                } else if (s0 != s_ref || std::memcmp(&w0, &w0_ref, 4) ||
+                           std::memcmp(&w1, &w1_ref, 4)) {
+                    return;
+                }
+            }
+            // Slot 2 (an axis that is not subsampled) puts the second tap past
+            // the 3x3 window, where the generic decode reads 0.
+            if (s_ref < 0 || s_ref > 2) return;
+            d.cslot[axis][par] = static_cast<int8_t>(s_ref);
+            w[axis][par][0] = w0_ref;
+            w[axis][par][1] = w1_ref;
+        }
+    }
+    for (int yp = 0; yp < 2; ++yp)
+        for (int xp = 0; xp < 2; ++xp) {
+            // BilinearTap's products, in single precision.
+            d.cweight[yp][xp][0] = w[0][xp][0] * w[1][yp][0];
+            d.cweight[yp][xp][1] = w[0][xp][1] * w[1][yp][0];
+            d.cweight[yp][xp][2] = w[0][xp][0] * w[1][yp][1];
+            d.cweight[yp][xp][3] = w[0][xp][1] * w[1][yp][1];
+        }
+    d.yuv_fast = 1;
+}
+
+}  // namespace
+
 void BuildSourceConstants(const vqm_cu_format& f, uint32_t chroma_filter, float background,
                           DevSource& d) {
     d.type = f.type;
@@ -497,6 +573,7 @@ void BuildSourceConstants(const vqm_cu_format& f, uint32_t chroma_filter, float 
         d.cl[3] = static_cast<float>(1.0 - Rec709Oetf(kr));
     }
     d.background = background;
+    FastYuvConstants(f, mode, tid, chroma_filter, d);
     // 8-bit grey/RGB without alpha: every sample decodes independently of its
     // neighbours, so one table per image holds the whole transfer decode.
     d.lut = (f.type == 0 && (f.family == 0 || f.family == 1) && f.alpha == 0 && mode == 0 &&

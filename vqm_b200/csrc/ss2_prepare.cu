@@ -246,6 +246,8 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
     __shared__ DevSource src_s;
     __shared__ LevelInfo lv;
     __shared__ uint32_t aligned4;
+    // Both chroma planes' window of the tile, for yuv_fast images.
+    __shared__ float chroma_stage[kTable ? 1 : 2 * kChromaStage];
 
     const uint32_t tid = threadIdx.x;
     const int group = kTable ? 0 : 1;
@@ -296,6 +298,12 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
     const auto body = [=](auto in_range) {
     constexpr bool kInRange = decltype(in_range)::value;
     const DevSource& s = src_s;
+    if constexpr (!kTable) {
+        if (s.yuv_fast && s.chroma_variant) {
+            StageChroma(s, gx, gy, chroma_stage);
+            __syncthreads();
+        }
+    }
     const uint32_t levels = lv.levels;
     const uint32_t width = s.width, height = s.height;
     const uint32_t wb = (width + 1) / 2, hb = (height + 1) / 2;  // base blocks
@@ -347,8 +355,14 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
                                         0.0f, 0.0f, 0.0f, 0.0f);
             }
             if (in_block) {
-                if (kTable) TableBlock(s, lut, fast, w4, hx, bx, by, lin);
-                else BlockLinearGeneric(s, bx, by, lin);
+                if constexpr (kTable) {
+                    TableBlock(s, lut, fast, w4, hx, bx, by, lin);
+                } else {
+                    if (s.yuv_fast && 2 * bx + 1 < width && 2 * by + 1 < height)
+                        BlockLinearYuv(s, chroma_stage, gx, gy, bx, by, lin);
+                    else
+                        BlockLinearGeneric(s, bx, by, lin);
+                }
                 // Level 0: the block is one aligned float4 of the row-pair
                 // plane, (x0, y0), (x0, y0+1), (x0+1, y0), (x0+1, y0+1); a
                 // column or row past the image is the plane's zero padding.

@@ -1512,6 +1512,20 @@ int vqm_cu_ss2_batch_finish(vqm_cu_ss2_batch* b, uint64_t token, double* norms, 
     });
 }
 
+int vqm_cu_ss2_decode_path(const vqm_cu_format* format, uint32_t chroma_filter,
+                           uint32_t* path) {
+    return Guard([&] {
+        NotNull(format, "format");
+        NotNull(path, "path");
+        if (chroma_filter > 2) throw std::invalid_argument("invalid chroma filter");
+        vqm_b200::ValidateFormat(*format, 4, 4, "format");
+        vqm_b200::DevSource d{};
+        vqm_b200::BuildSourceConstants(*format, chroma_filter, 0.5f, d);
+        *path = d.lut ? (d.in_range ? VQM_CU_DECODE_TABLE_IN_RANGE : VQM_CU_DECODE_TABLE)
+                      : (d.yuv_fast ? VQM_CU_DECODE_YUV : VQM_CU_DECODE_GENERIC);
+    });
+}
+
 int vqm_cu_ss2_blur_variants(uint32_t* count, uint32_t* shapes) {
     return Guard([&] {
         NotNull(count, "count");

@@ -223,6 +223,7 @@ _SIGS = {
     "vqm_cu_ss2_batch_finish": ([_P, ctypes.c_uint64, _P, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_set_timing": ([_P, ctypes.c_int], ctypes.c_int),
     "vqm_cu_ss2_blur_variants": ([_P, _P], ctypes.c_int),
+    "vqm_cu_ss2_decode_path": ([_P, ctypes.c_uint32, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_stage_ms": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_compute": ([_P, ctypes.c_uint32, _P, _P, ctypes.c_float, _P, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_server_create": ([_P, _P], ctypes.c_int),
@@ -573,6 +574,18 @@ class Ssimulacra2Pipeline:
 
 
 VARIANT_WORDS = 5
+
+DECODE_PATHS = ("generic", "table", "table_in_range", "yuv")
+
+
+def decode_path(fmt: "ImageFormat", chroma_filter: int = 0) -> str:
+    """Which device decode images of `fmt` take (the results are the same
+    whichever runs): "generic", "table" (8-bit grey/RGB through a table),
+    "table_in_range" (the same, non-negative linear samples) or "yuv"
+    (integer YUV, power-law transfer, at most 2x chroma subsampling)."""
+    path = ctypes.c_uint32()
+    _check(_lib.vqm_cu_ss2_decode_path(ctypes.byref(fmt), chroma_filter, ctypes.byref(path)))
+    return DECODE_PATHS[path.value]
 
 
 def blur_variants():
