@@ -654,6 +654,11 @@ float HalfToFloat(uint16_t h) {
 template <class T> T Pow(T a, T b);
 template <> float Pow<float>(float a, float b) { return ss2dm::pow(a, b); }
 template <> double Pow<double>(double a, double b) { return std::pow(a, b); }
+// The pure power-law transfers (color.glsl:157-159): the shared
+// single-precision power in the FP32 path.
+template <class T> T Gamma(T a, T b);
+template <> float Gamma<float>(float a, float b) { return ss2dm::powf_gamma(a, b); }
+template <> double Gamma<double>(double a, double b) { return std::pow(a, b); }
 template <class T> T Exp(T a);
 template <> float Exp<float>(float a) { return ss2dm::exp(a); }
 template <> double Exp<double>(double a) { return std::exp(a); }
@@ -749,9 +754,9 @@ struct Decoder {
     T Transfer(int id, T v) const {
         switch (id) {
             case 0: return v;
-            case 1: return v < T(0) ? T(0) : Pow<T>(v, T(2.4));
-            case 2: return v < T(0) ? T(0) : Pow<T>(v, T(2.2));
-            case 3: return v < T(0) ? T(0) : Pow<T>(v, T(2.8));
+            case 1: return v < T(0) ? T(0) : Gamma<T>(v, T(2.4));
+            case 2: return v < T(0) ? T(0) : Gamma<T>(v, T(2.2));
+            case 3: return v < T(0) ? T(0) : Gamma<T>(v, T(2.8));
             case 4: return SrgbEotf(v);
             case 5: return v <= T(0) ? T(0.01) : Pow<T>(T(10), T(2) * (v - T(1)));
             case 6: return v <= T(0) ? T(0.00316227766)
@@ -1505,6 +1510,7 @@ int ss2o_detmath(int fn, const float* x, float y, float* out, size_t n) {
             case 2: out[i] = ss2dm::exp(x[i]); break;
             case 3: out[i] = ss2dm::sinpi(x[i]); break;
             case 4: out[i] = RoundHalf(x[i]); break;
+            case 5: out[i] = ss2dm::powf_gamma(x[i], y); break;
             default: g_error = "unknown function"; return SS2O_INVALID;
         }
     }

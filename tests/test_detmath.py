@@ -1,10 +1,12 @@
-"""Accuracy of the deterministic pow / cube root / exp / sin(pi x) that the
-kernels, the host decode tables and the oracle share
-(vqm_b200/csrc/ss2_detmath.h), against double-precision libm.
+"""Accuracy of the deterministic functions that the kernels, the host decode
+tables and the oracle share (vqm_b200/csrc/ss2_detmath.h), against
+double-precision libm.
 
-Each function evaluates in double and rounds once, so it must land on the
-correctly rounded float in all but a tiny fraction of cases, and never more
-than one ulp away."""
+pow, cbrt, exp and sin(pi x) evaluate to ~3e-13 and round once, so they must
+land on the correctly rounded float in all but a tiny fraction of cases, and
+never more than one ulp away. powf_gamma (the power-law transfers' power)
+works in float pairs to ~2^-30: never more than one ulp away, off the
+correctly rounded float for well under 1 % of its arguments."""
 
 import ctypes
 
@@ -55,6 +57,37 @@ def test_pow(y):
     x = samples(1e-6, 1.5)
     check(det(1, x, yf), np.power(x.astype(np.float64), np.float64(yf)))
     assert det(1, np.float32([0.0, 1.0]), yf).tolist() == [0.0, 1.0]
+
+
+def test_powf_gamma_exhaustive_for_gamma_2_4():
+    """The power-law transfers' single-precision power, on every float of
+    its fast range [2^-30, 256) for VQM's gamma 2.4: never more than one ulp
+    from the correctly rounded power, and on it for all but ~0.35 %."""
+    yf = np.float32(2.4)
+    lo = int(np.float32(2.0 ** -30).view(np.uint32))
+    hi = int(np.float32(256.0).view(np.uint32))
+    off = total = 0
+    for start in range(lo, hi, 1 << 23):
+        x = np.arange(start, min(start + (1 << 23), hi), dtype=np.uint32).view(np.float32)
+        want = np.power(x.astype(np.float64), np.float64(yf)).astype(np.float32)
+        d = ulps(det(5, x, yf), want)
+        assert d.max() <= 1, (start, d.max())
+        off += int((d > 0).sum())
+        total += x.size
+    assert off / total < 0.005
+
+
+@pytest.mark.parametrize("y", [2.2, 2.8, 1.0, 4.0, 1 / 0.45, 2.6])
+def test_powf_gamma(y):
+    yf = np.float32(y)
+    x = samples(2.0 ** -30, 255.9, n=1_000_000)
+    d = ulps(det(5, x, yf), np.power(x.astype(np.float64), np.float64(yf)).astype(np.float32))
+    assert d.max() <= 1 and (d > 0).mean() < 0.01
+    # Outside its fast range (and for y outside [1, 4]) it is pow itself.
+    edge = np.float32([0.0, 1e-12, 2.0 ** -31, 256.0, 1e6])
+    assert np.array_equal(det(5, edge, yf), det(1, edge, yf))
+    assert det(5, np.float32([1.0]), yf)[0] == 1.0
+    assert np.array_equal(det(5, x[:1000], np.float32(0.5)), det(1, x[:1000], np.float32(0.5)))
 
 
 def test_pow_base10():

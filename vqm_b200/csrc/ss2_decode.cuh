@@ -67,9 +67,9 @@ __device__ __forceinline__ float AribInvOetf(float x) {
 __device__ __forceinline__ float TransferDecode(const DevSource& s, float v) {
     switch (s.transfer) {
         case 0: return v;
-        case 1: return v < 0.0f ? 0.0f : ss2dm::pow(v, 2.4f);
-        case 2: return v < 0.0f ? 0.0f : ss2dm::pow(v, 2.2f);
-        case 3: return v < 0.0f ? 0.0f : ss2dm::pow(v, 2.8f);
+        case 1: return v < 0.0f ? 0.0f : ss2dm::powf_gamma(v, 2.4f);
+        case 2: return v < 0.0f ? 0.0f : ss2dm::powf_gamma(v, 2.2f);
+        case 3: return v < 0.0f ? 0.0f : ss2dm::powf_gamma(v, 2.8f);
         case 4: return SrgbEotf(v);
         case 5: return v <= 0.0f ? 0.01f : ss2dm::pow(10.0f, __fmul_rn(2.0f, __fsub_rn(v, 1.0f)));
         case 6:
@@ -367,6 +367,52 @@ __device__ __forceinline__ void BlockLinearGeneric(const DevSource& s, uint32_t 
     }
 }
 
+// ss2dm::powf_gamma of two lanes with the same y, the floating-point steps
+// two lanes per instruction (FFMA2 / FMUL2 / FADD2), each the operation the
+// scalar function performs on that lane: the same values. A lane outside the
+// function's fast range sends both through the scalar function.
+__device__ __forceinline__ float2 PowfGamma2(float2 x, float y) {
+    const float lo_x = 9.31322574615478515625e-10f;  // 2^-30
+    if (!(x.x >= lo_x && x.x < 256.0f && x.y >= lo_x && x.y < 256.0f && y >= 1.0f && y <= 4.0f))
+        return make_float2(ss2dm::powf_gamma(x.x, y), ss2dm::powf_gamma(x.y, y));
+    const auto P = [](float v) { return make_float2(v, v); };
+    const auto N = [](float2 v) { return make_float2(-v.x, -v.y); };
+    const uint32_t ix0 = __float_as_uint(x.x), ix1 = __float_as_uint(x.y);
+    const int i0 = static_cast<int>((ix0 >> 16) & 127u), i1 = static_cast<int>((ix1 >> 16) & 127u);
+    const float2 m = make_float2(__uint_as_float((ix0 & 0x007fffffu) | 0x3f800000u),
+                                 __uint_as_float((ix1 & 0x007fffffu) | 0x3f800000u));
+    const float2 inv = make_float2(__ldg(&ss2dm::kInvCFDev[i0]), __ldg(&ss2dm::kInvCFDev[i1]));
+    const float2 p = __fmul2_rn(m, inv);
+    const float2 pe = __ffma2_rn(m, inv, N(p));
+    const float2 rh = __fadd2_rn(p, P(-1.0f));
+    const float k1 = 1.44269502163f, k2 = -0.721347510815f;
+    const float k3 = 0.480898350477f, k4 = -0.360673755407f;
+    const float2 poly = __ffma2_rn(__ffma2_rn(rh, P(k4), P(k3)), rh, P(k2));
+    const float2 lr = __ffma2_rn(P(k1), rh, __ffma2_rn(__fmul2_rn(rh, rh), poly, __fmul2_rn(P(k1), pe)));
+    const float2 ef = make_float2(static_cast<float>(static_cast<int>(ix0 >> 23) - 127),
+                                  static_cast<float>(static_cast<int>(ix1 >> 23) - 127));
+    const float2 lh = make_float2(__ldg(&ss2dm::kLog2InvCFHiDev[i0]),
+                                  __ldg(&ss2dm::kLog2InvCFHiDev[i1]));
+    const float2 ll = make_float2(__ldg(&ss2dm::kLog2InvCFLoDev[i0]),
+                                  __ldg(&ss2dm::kLog2InvCFLoDev[i1]));
+    const float2 hi = __fadd2_rn(ef, lh);
+    const float2 lo = __fadd2_rn(__fadd2_rn(__fadd2_rn(ef, N(hi)), lh), __fadd2_rn(ll, lr));
+    const float2 th = __fmul2_rn(P(y), hi);
+    const float2 tl = __ffma2_rn(P(y), lo, __ffma2_rn(P(y), hi, N(th)));
+    const float2 kf = __fadd2_rn(__ffma2_rn(th, P(64.0f), P(12582912.0f)), P(-12582912.0f));
+    const float ln2 = 0.693147182465f;
+    const float2 z =
+        __ffma2_rn(__ffma2_rn(kf, P(-0.015625f), th), P(ln2), __fmul2_rn(tl, P(ln2)));
+    const float2 q = __ffma2_rn(__ffma2_rn(z, P(0.166666671634f), P(0.5f)), __fmul2_rn(z, z), z);
+    const int k0 = static_cast<int>(kf.x), k1i = static_cast<int>(kf.y);
+    const int j0 = k0 & 63, j1 = k1i & 63;
+    const float2 tj = make_float2(__ldg(&ss2dm::kExp2JFHiDev[j0]), __ldg(&ss2dm::kExp2JFHiDev[j1]));
+    const float2 tjl = make_float2(__ldg(&ss2dm::kExp2JFLoDev[j0]), __ldg(&ss2dm::kExp2JFLoDev[j1]));
+    const float2 r = __fadd2_rn(tj, __ffma2_rn(tj, q, tjl));
+    return __fmul2_rn(r, make_float2(__uint_as_float(static_cast<uint32_t>((k0 >> 6) + 127) << 23),
+                                     __uint_as_float(static_cast<uint32_t>((k1i >> 6) + 127) << 23)));
+}
+
 // The YUV fast path (DevSource::yuv_fast): the CTA's chroma window of both
 // planes staged once in shared memory (kPrepTile >> sub samples per axis plus
 // one on each side, edge-clamped: for the one-past-the-edge positions a block
@@ -396,9 +442,8 @@ __device__ __forceinline__ void StageChroma(const DevSource& s, uint32_t gx, uin
 
 // BlockLinearGeneric for a yuv_fast image's block (bx, by) of the CTA's tile
 // (gx, gy) whose two columns and rows are inside the image: the same values,
-// with the format's branches resolved, the chroma taps read from the staged
-// window at the host's per-parity slots and weights, and the transfer's power
-// without range steps (its arguments are below 2^40).
+// with the format's branches resolved and the chroma taps read from the
+// staged window at the host's per-parity slots and weights.
 __device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* stage,
                                                uint32_t gx, uint32_t gy, uint32_t bx,
                                                uint32_t by, float rgb[4][3]) {
@@ -455,15 +500,24 @@ __device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* 
             e[i][2] = RawSample(s, 2, x0 + (i & 1), y0 + (i >> 1));
         }
     }
+    if (!s.identity1) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) ApplyMatrix(s.m1, e[i]);
+    }
+    // The transfer, v < 0 (and v == 0) giving 0 and everything else
+    // powf_gamma, two pixels per call.
     const float g = s.gamma;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        if (!s.identity1) ApplyMatrix(s.m1, e[i]);
+    for (int h = 0; h < 4; h += 2)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const float v = e[i][c];
-            e[i][c] = v < 0.0f ? 0.0f : ss2dm::pow_bounded(v, g);
+            const float a = e[h][c], b = e[h + 1][c];
+            const float2 r = PowfGamma2(make_float2(a > 0.0f ? a : 1.0f, b > 0.0f ? b : 1.0f), g);
+            e[h][c] = a > 0.0f ? r.x : 0.0f;
+            e[h + 1][c] = b > 0.0f ? r.y : 0.0f;
         }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
         if (!s.identity2) ApplyMatrix(s.m2, e[i]);
         rgb[i][0] = e[i][0];
         rgb[i][1] = e[i][1];

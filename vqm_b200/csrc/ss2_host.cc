@@ -312,9 +312,9 @@ float St2084EotfF(float x) {
 float TransferF(int id, float tl, float v) {
     switch (id) {
         case 0: return v;
-        case 1: return v < 0.0f ? 0.0f : HostPow(v, 2.4f);
-        case 2: return v < 0.0f ? 0.0f : HostPow(v, 2.2f);
-        case 3: return v < 0.0f ? 0.0f : HostPow(v, 2.8f);
+        case 1: return v < 0.0f ? 0.0f : ss2dm::powf_gamma(v, 2.4f);
+        case 2: return v < 0.0f ? 0.0f : ss2dm::powf_gamma(v, 2.2f);
+        case 3: return v < 0.0f ? 0.0f : ss2dm::powf_gamma(v, 2.8f);
         case 4: return v <= 0.04045f ? v / 12.92f : HostPow((v + 0.055f) / 1.055f, 2.4f);
         case 5: return v <= 0.0f ? 0.01f : HostPow(10.0f, 2.0f * (v - 1.0f));
         case 6: return v <= 0.0f ? 0.00316227766f : HostPow(10.0f, 2.5f * (v - 1.0f));
@@ -580,7 +580,9 @@ void BuildSourceConstants(const vqm_cu_format& f, uint32_t chroma_filter, float 
              tid != 11)
                 ? 1
                 : 0;
-    d.in_range = 0;
+    // Power-law YUV without a primaries matrix: the transfer maps every
+    // value to >= 0, so every mix is in the cube root's direct range too.
+    d.in_range = d.yuv_fast && d.identity2 ? 1 : 0;
     if (!d.lut) {
         std::memset(d.srgb_lut, 0, sizeof(d.srgb_lut));
         return;

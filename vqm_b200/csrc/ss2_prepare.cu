@@ -462,12 +462,8 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
         }
     }
     };
-    if constexpr (kTable) {
-        if (src_s.in_range) body(std::true_type{});
-        else body(std::false_type{});
-    } else {
-        body(std::false_type{});
-    }
+    if (src_s.in_range) body(std::true_type{});
+    else body(std::false_type{});
 }
 
 }  // namespace
