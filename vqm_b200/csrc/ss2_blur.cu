@@ -614,32 +614,34 @@ cudaError_t Prepare(Kernel kernel, size_t smem, LaunchCache& cache, int threads,
     return cudaSuccess;
 }
 
+// Each launcher prepares its kernel (which also loads it) and, when
+// `launch`, launches it.
 template <int TW, int TH, int NT, int MB, bool kHalf>
-cudaError_t LaunchTilesAs(const DevBatch& b, cudaStream_t stream) {
+cudaError_t LaunchTilesAs(const DevBatch& b, cudaStream_t stream, bool launch) {
     using T = Tile<TW, TH, NT>;
     static LaunchCache cache;
     constexpr size_t smem = T::kSrcBytes + T::kHqBytes;
     const cudaError_t e =
         Prepare(Ss2BlurKernel<TW, TH, NT, MB, kHalf>, smem, cache, NT, false, nullptr);
-    if (e != cudaSuccess) return e;
+    if (e != cudaSuccess || !launch) return e;
     Ss2BlurKernel<TW, TH, NT, MB, kHalf><<<b.blur_blocks, NT, smem, stream>>>(b);
     return cudaGetLastError();
 }
 template <int TW, int TH, int NT, int MB>
-cudaError_t LaunchTiles(const DevBatch& b, cudaStream_t stream) {
-    return b.half ? LaunchTilesAs<TW, TH, NT, MB, true>(b, stream)
-                  : LaunchTilesAs<TW, TH, NT, MB, false>(b, stream);
+cudaError_t LaunchTiles(const DevBatch& b, cudaStream_t stream, bool launch) {
+    return b.half ? LaunchTilesAs<TW, TH, NT, MB, true>(b, stream, launch)
+                  : LaunchTilesAs<TW, TH, NT, MB, false>(b, stream, launch);
 }
 
 template <int TW, int TH, int NT, int MB>
-cudaError_t LaunchPersistent(const DevBatch& b, cudaStream_t stream) {
+cudaError_t LaunchPersistent(const DevBatch& b, cudaStream_t stream, bool launch) {
     using T = Tile<TW, TH, NT>;
     static LaunchCache cache;
     constexpr size_t smem = 2 * T::kSrcBytes + T::kHqBytes;
     int grid = 0;
     const cudaError_t e =
         Prepare(Ss2BlurPersistentKernel<TW, TH, NT, MB>, smem, cache, NT, true, &grid);
-    if (e != cudaSuccess) return e;
+    if (e != cudaSuccess || !launch) return e;
     const uint32_t blocks = b.blur_blocks < static_cast<uint32_t>(grid) ? b.blur_blocks
                                                                         : static_cast<uint32_t>(grid);
     Ss2BlurPersistentKernel<TW, TH, NT, MB><<<blocks, NT, smem, stream>>>(b);
@@ -647,15 +649,32 @@ cudaError_t LaunchPersistent(const DevBatch& b, cudaStream_t stream) {
 }
 
 template <int TW, int TH, int NT, int MB, int S>
-cudaError_t LaunchStrips(const DevBatch& b, cudaStream_t stream) {
+cudaError_t LaunchStrips(const DevBatch& b, cudaStream_t stream, bool launch) {
     using T = Tile<TW, TH, NT>;
     static LaunchCache cache;
     constexpr size_t smem = T::kSrcBytes + T::kHqBytes;
     const cudaError_t e =
         Prepare(Ss2BlurStripKernel<TW, TH, NT, MB, S>, smem, cache, NT, false, nullptr);
-    if (e != cudaSuccess) return e;
+    if (e != cudaSuccess || !launch) return e;
     Ss2BlurStripKernel<TW, TH, NT, MB, S><<<b.blur_blocks, NT, smem, stream>>>(b);
     return cudaGetLastError();
+}
+
+cudaError_t Dispatch(const DevBatch& b, int variant, cudaStream_t stream, bool launch) {
+    switch (variant) {
+        case 0: return LaunchTiles<32, 32, 128, 5>(b, stream, launch);
+        case 1: return LaunchTiles<32, 28, 128, 5>(b, stream, launch);
+        case 2: return LaunchTiles<64, 32, 256, 2>(b, stream, launch);
+        case 3: return LaunchTiles<64, 20, 256, 3>(b, stream, launch);
+        case 4: return LaunchPersistent<32, 32, 128, 3>(b, stream, launch);
+        case 5: return LaunchPersistent<32, 20, 128, 5>(b, stream, launch);
+        case 6: return LaunchPersistent<64, 32, 256, 1>(b, stream, launch);
+        case 7: return LaunchStrips<32, 32, 128, 5, 2>(b, stream, launch);
+        case 8: return LaunchStrips<32, 32, 128, 5, 4>(b, stream, launch);
+        case 9: return LaunchStrips<32, 32, 128, 5, 8>(b, stream, launch);
+        case 10: return LaunchStrips<32, 28, 128, 5, 4>(b, stream, launch);
+    }
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace
@@ -671,20 +690,20 @@ cudaError_t LaunchBlur(const DevBatch& b, int variant, cudaStream_t stream) {
     // Half planes run the one-tile-per-CTA kernel of the same tile shape.
     if (b.half) variant = HalfPlaneVariant(variant);
     if (variant < 0) return cudaErrorInvalidValue;
-    switch (variant) {
-        case 0: return LaunchTiles<32, 32, 128, 5>(b, stream);
-        case 1: return LaunchTiles<32, 28, 128, 5>(b, stream);
-        case 2: return LaunchTiles<64, 32, 256, 2>(b, stream);
-        case 3: return LaunchTiles<64, 20, 256, 3>(b, stream);
-        case 4: return LaunchPersistent<32, 32, 128, 3>(b, stream);
-        case 5: return LaunchPersistent<32, 20, 128, 5>(b, stream);
-        case 6: return LaunchPersistent<64, 32, 256, 1>(b, stream);
-        case 7: return LaunchStrips<32, 32, 128, 5, 2>(b, stream);
-        case 8: return LaunchStrips<32, 32, 128, 5, 4>(b, stream);
-        case 9: return LaunchStrips<32, 32, 128, 5, 8>(b, stream);
-        case 10: return LaunchStrips<32, 28, 128, 5, 4>(b, stream);
-    }
-    return cudaErrorInvalidValue;
+    return Dispatch(b, variant, stream, true);
+}
+
+cudaError_t PreloadBlur() {
+    for (int v = 0; v < kBlurVariantCount; ++v)
+        for (int half = 0; half < 2; ++half) {
+            DevBatch b{};
+            b.half = static_cast<uint32_t>(half);
+            const int run = half ? HalfPlaneVariant(v) : v;
+            if (run < 0) continue;
+            const cudaError_t e = Dispatch(b, run, nullptr, false);
+            if (e != cudaSuccess) return e;
+        }
+    return cudaSuccess;
 }
 
 int HalfPlaneVariant(int variant) {

@@ -110,6 +110,11 @@ cudaError_t SetScoreWeights(const double* weights108) {
     return cudaMemcpyToSymbol(c_weights, weights108, sizeof(double) * 108);
 }
 
+cudaError_t PreloadFinalize() {
+    cudaFuncAttributes a;
+    return cudaFuncGetAttributes(&a, Ss2FinalizeKernel);
+}
+
 cudaError_t LaunchFinalize(const DevBatch& b, cudaStream_t stream) {
     if (b.segments == 0) return cudaSuccess;
     Ss2FinalizeKernel<<<b.segments, kFinThreads, 0, stream>>>(b);

@@ -18,6 +18,11 @@ cudaError_t LaunchPrepare(const DevBatch& batch, cudaStream_t stream);
 // one's output tile); the batch's segments must have been tiled with it.
 cudaError_t LaunchBlur(const DevBatch& batch, int variant, cudaStream_t stream);
 cudaError_t LaunchFinalize(const DevBatch& batch, cudaStream_t stream);
+// Load every kernel of each stage on the current device (and set the blur
+// kernels' shared-memory limits), so that no first launch pays for it.
+cudaError_t PreloadPrepare();
+cudaError_t PreloadBlur();
+cudaError_t PreloadFinalize();
 
 // The blur variants compiled into the library and their output tiles.
 int BlurTileCount();

@@ -468,6 +468,15 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
 
 }  // namespace
 
+cudaError_t PreloadPrepare() {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, PrepareKernel<true, false>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, PrepareKernel<false, false>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, PrepareKernel<true, true>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, PrepareKernel<false, true>);
+    return e;
+}
+
 cudaError_t LaunchPrepare(const DevBatch& b, cudaStream_t stream) {
     if (b.half) {
         if (b.prep_blocks[0]) PrepareKernel<true, true><<<b.prep_blocks[0], kThreads, 0, stream>>>(b);

@@ -73,6 +73,11 @@ void EnsureDevice(int device) {
     VQM_CK(cudaSetDevice(device));
     const auto taps = GaussianTaps();
     VQM_CK(SetConstants(taps.data(), ScoreWeights()));
+    // Kernels load lazily on their first launch otherwise: a first batch,
+    // or the first that selects a new blur variant, would pay for it.
+    VQM_CK(PreloadPrepare());
+    VQM_CK(PreloadBlur());
+    VQM_CK(PreloadFinalize());
     ready[device] = true;
 }
 
