@@ -73,21 +73,48 @@ def make_pairs(count, w, h, seed0, workers=None):
     return [(ss2.Image(w, h, fmt, o), ss2.Image(w, h, fmt, d)) for o, d in raw]
 
 
+# FP32 lane operations the blur must perform per kept pyramid pixel (one
+# image pair), counting a fused multiply-add or a division as one: the five
+# 13-tap passes in VQM's order (65 horizontal + 65 vertical: no symmetric
+# folding), the three products and 31 map and norm-sum operations (SSIM' 11,
+# edge maps 8, the six sums and their squares 12).
+BLUR_OPS_PER_KEPT_PIXEL = 164
+FFMA_LANES_PER_SM = 128
+
+
+def kept_pixels(w, h):
+    """Pixels of the kept (level, channel) planes of one image."""
+    from oracle import binding as ob  # plan + pruning only
+    from vqm_b200 import ss2
+    plan = ss2.plan_scales(w, h)
+    return sum(lw * lh for s, (lw, lh) in enumerate(plan) for c in range(3)
+               if not ob.channel_pruned(c, s, len(plan)))
+
+
 def alg_bytes(w, h):
     """Algorithmic bytes of one pair: raw input read once, plus the FP32 XYB
     pyramid of the kept channels written once and read once, both images.
     Returns (prepare, blur, whole pair)."""
-    from oracle import binding as ob  # plan + pruning only
     from vqm_b200 import ss2
-    plan = ss2.plan_scales(w, h)
-    kept = 0
-    for s, (lw, lh) in enumerate(plan):
-        for c in range(3):
-            if not ob.channel_pruned(c, s, len(plan)):
-                kept += lw * lh
+    kept = kept_pixels(w, h)
     inp = 2 * ss2.required_bytes(ss2.srgb8_format(), w, h)
     pyramid = 2 * 4 * kept
     return inp + pyramid, pyramid, inp + 2 * pyramid
+
+
+def fp32_roofline(blur_ms, pairs, clocks):
+    """The blur against the FP32 issue roof that bounds it: algorithmic lane
+    operations per launch over its CUDA-event time, against 128 FFMA lanes
+    per SM at the sampled SM clock."""
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    ops = BLUR_OPS_PER_KEPT_PIXEL * kept_pixels(WIDTH, HEIGHT) * pairs
+    achieved = ops / (blur_ms / 1e3) / 1e12
+    peak = sms * FFMA_LANES_PER_SM * mhz * 1e6 / 1e12
+    return {"bound": "fp32 issue", "kernel": "blur", "ops_per_kept_pixel": BLUR_OPS_PER_KEPT_PIXEL,
+            "achieved": achieved, "peak": peak, "unit": "T lane-op/s", "frac": achieved / peak,
+            "peak_basis": f"{sms} SMs x {FFMA_LANES_PER_SM} lanes x {mhz:.0f} MHz"}
 
 
 class ClockSampler:
@@ -723,6 +750,7 @@ def main(argv=None):
                          "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "alg_bytes_per_launch": per_launch},
+            "fp32_roofline": fp32_roofline(avg[1], args.pairs, clocks.summary()),
             "step_roofline": {"alg_bytes_per_pair": pair_b,
                               "achieved_gbs": pair_b * value / world / 1e9,
                               "frac": pair_b * value / world / 1e9 / peak},
