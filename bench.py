@@ -545,7 +545,7 @@ def main(argv=None):
     ap.add_argument("--workload", default="plain1080",
                     choices=["plain1080", "uneven", "serve", "video"])
     ap.add_argument("--rates", default="200,500,1000,2000", help="serve: requests/s")
-    ap.add_argument("--duration", type=float, default=5.0, help="serve: seconds per rate")
+    ap.add_argument("--duration", type=float, default=10.0, help="serve: seconds per rate")
     ap.add_argument("--serve-workers", type=int, default=3)
     ap.add_argument("--serve-distinct", type=int, default=3,
                     help="serve: distinct pairs per (size, format)")
