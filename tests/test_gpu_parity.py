@@ -509,3 +509,55 @@ def test_identity_at_4k():
     with ss2.Ssimulacra2Pipeline(3840, 2160) as p:
         r = p.compute(o, o)
     assert r.score() == 100.0 and np.all(r.norms == 0.0)
+
+
+def _random_case(seed):
+    """A seeded format, size, chroma siting, filter and background."""
+    rng = np.random.default_rng(9000 + seed)
+    F, T, P = ss2.ImageFormat, ss2.TransferCharacteristics, ss2.PixelType
+    kinds = [
+        lambda: F(type=P.Byte),
+        lambda: F(type=P.Byte, range=ss2.PixelRange.Limited, transfer=T.Bt709),
+        lambda: F(type=P.Word, depth=int(rng.choice([10, 12, 16]))),
+        lambda: F(type=P.Float, transfer=T.Linear),
+        lambda: F(type=P.Half),
+        lambda: F(type=P.Byte, family=ss2.ColorFamily.Grey, matrix=ss2.MatrixCoefficients.Bt709),
+        lambda: F(type=P.Byte, alpha=ss2.AlphaType.Straight),
+    ]
+    for sw, sh in ((1, 1), (1, 0), (0, 0), (0, 1)):
+        kinds.append(lambda sw=sw, sh=sh: F(
+            type=P.Word if rng.random() < 0.6 else P.Byte,
+            depth=int(rng.choice([10, 12])) if rng.random() < 0.6 else 0,
+            family=ss2.ColorFamily.Yuv, range=ss2.PixelRange.Limited,
+            matrix=ss2.MatrixCoefficients.Bt709,
+            transfer=[T.Bt709, T.Bt470M, T.Bt470Bg, T.Srgb][int(rng.integers(0, 4))],
+            primaries=ss2.ColorPrimaries.Bt709 if rng.random() < 0.7 else ss2.ColorPrimaries.Bt2020,
+            chroma_location=int(rng.integers(0, 6)), subsample_w=sw, subsample_h=sh))
+    fmt = kinds[int(rng.integers(0, len(kinds)))]()
+    if fmt.type == P.Byte and fmt.depth:
+        fmt.depth = 0
+    w = int(rng.integers(8, 400)) << fmt.subsample_w
+    h = int(rng.integers(8, 260)) << fmt.subsample_h
+    sub = fmt.subsample_w or fmt.subsample_h
+    chroma_filter = int(rng.integers(0, 3)) if sub else 0
+    background = float(rng.choice([0.1, 0.5, 0.9]))
+    return fmt, w, h, chroma_filter, background
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_randomized_formats_and_sizes(seed):
+    """Seeded sweep over formats, sizes (odd included where the format
+    allows), chroma sitings and filters, transfers and backgrounds: the
+    device result matches the oracle, whichever decode path each image
+    takes."""
+    fmt, w, h, chroma_filter, background = _random_case(seed)
+    ov = _values(fmt, w, h, 100 + seed)
+    rng = np.random.default_rng(200 + seed)
+    dv = [None if v is None else np.clip(v + rng.normal(0, 0.02, v.shape),
+                                         -0.5 if i in (1, 2) and fmt.family == 2 else 0, 1)
+          for i, v in enumerate(ov)]
+    o, d = helpers.pack_planes(fmt, w, h, ov), helpers.pack_planes(fmt, w, h, dv)
+    path = ss2.decode_path(fmt, chroma_filter)
+    with ss2.Ssimulacra2Pipeline(w, h, chroma_filter=chroma_filter) as p:
+        check_parity(p.compute(o, d, background), o, d, background, chroma_filter,
+                     label=f"seed {seed} {w}x{h} path {path}")
