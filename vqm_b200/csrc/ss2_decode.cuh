@@ -381,7 +381,8 @@ __device__ __forceinline__ float2 PowfGamma2(float2 x, float y) {
     const int i0 = static_cast<int>((ix0 >> 16) & 127u), i1 = static_cast<int>((ix1 >> 16) & 127u);
     const float2 m = make_float2(__uint_as_float((ix0 & 0x007fffffu) | 0x3f800000u),
                                  __uint_as_float((ix1 & 0x007fffffu) | 0x3f800000u));
-    const float2 inv = make_float2(__ldg(&ss2dm::kInvCFDev[i0]), __ldg(&ss2dm::kInvCFDev[i1]));
+    const ss2dm::LogEntryF L0 = ss2dm::LogF(i0), L1 = ss2dm::LogF(i1);
+    const float2 inv = make_float2(L0.inv, L1.inv);
     const float2 p = __fmul2_rn(m, inv);
     const float2 pe = __ffma2_rn(m, inv, N(p));
     const float2 rh = __fadd2_rn(p, P(-1.0f));
@@ -391,10 +392,8 @@ __device__ __forceinline__ float2 PowfGamma2(float2 x, float y) {
     const float2 lr = __ffma2_rn(P(k1), rh, __ffma2_rn(__fmul2_rn(rh, rh), poly, __fmul2_rn(P(k1), pe)));
     const float2 ef = make_float2(static_cast<float>(static_cast<int>(ix0 >> 23) - 127),
                                   static_cast<float>(static_cast<int>(ix1 >> 23) - 127));
-    const float2 lh = make_float2(__ldg(&ss2dm::kLog2InvCFHiDev[i0]),
-                                  __ldg(&ss2dm::kLog2InvCFHiDev[i1]));
-    const float2 ll = make_float2(__ldg(&ss2dm::kLog2InvCFLoDev[i0]),
-                                  __ldg(&ss2dm::kLog2InvCFLoDev[i1]));
+    const float2 lh = make_float2(L0.hi, L1.hi);
+    const float2 ll = make_float2(L0.lo, L1.lo);
     const float2 hi = __fadd2_rn(ef, lh);
     const float2 lo = __fadd2_rn(__fadd2_rn(__fadd2_rn(ef, N(hi)), lh), __fadd2_rn(ll, lr));
     const float2 th = __fmul2_rn(P(y), hi);
@@ -406,8 +405,9 @@ __device__ __forceinline__ float2 PowfGamma2(float2 x, float y) {
     const float2 q = __ffma2_rn(__ffma2_rn(z, P(0.166666671634f), P(0.5f)), __fmul2_rn(z, z), z);
     const int k0 = static_cast<int>(kf.x), k1i = static_cast<int>(kf.y);
     const int j0 = k0 & 63, j1 = k1i & 63;
-    const float2 tj = make_float2(__ldg(&ss2dm::kExp2JFHiDev[j0]), __ldg(&ss2dm::kExp2JFHiDev[j1]));
-    const float2 tjl = make_float2(__ldg(&ss2dm::kExp2JFLoDev[j0]), __ldg(&ss2dm::kExp2JFLoDev[j1]));
+    const ss2dm::ExpEntryF T0 = ss2dm::ExpF(j0), T1 = ss2dm::ExpF(j1);
+    const float2 tj = make_float2(T0.hi, T1.hi);
+    const float2 tjl = make_float2(T0.lo, T1.lo);
     const float2 r = __fadd2_rn(tj, __ffma2_rn(tj, q, tjl));
     return __fmul2_rn(r, make_float2(__uint_as_float(static_cast<uint32_t>((k0 >> 6) + 127) << 23),
                                      __uint_as_float(static_cast<uint32_t>((k1i >> 6) + 127) << 23)));
@@ -440,6 +440,43 @@ __device__ __forceinline__ void StageChroma(const DevSource& s, uint32_t gx, uin
     }
 }
 
+// The two 4:2:0 axis phases the host recognises (DevSource::chroma_pattern):
+// type 0 (siting offset 0): slots 0, 1 with weights (1/4, 3/4), (3/4, 1/4);
+// type 1 (offset 1/4): slots 1, 1 with (1, 0), (1/2, 1/2). Per output the
+// four taps are BilinearTap's, in its order, with the weight products
+// folded at compile time (exact: the factors are multiples of 1/4), so the
+// values equal the runtime path's; the window reads become fixed offsets.
+template <int kType>
+struct AxisPhase {
+    static __device__ constexpr int Slot(int par) { return par ? 1 : (kType ? 1 : 0); }
+    static __device__ constexpr float W0(int par) {
+        return par ? (kType ? 0.5f : 0.75f) : (kType ? 1.0f : 0.25f);
+    }
+    static __device__ constexpr float W1(int par) {
+        return par ? (kType ? 0.5f : 0.25f) : (kType ? 0.0f : 0.75f);
+    }
+};
+template <int kX, int kY>
+__device__ __forceinline__ void ChromaFixed(const float* stage, int bxs, int bys, float e[4][3]) {
+    using X = AxisPhase<kX>;
+    using Y = AxisPhase<kY>;
+    constexpr int sw = (kPrepTile >> 1) + 2;
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+        const float* base = stage + p * kChromaStage + bys * sw + bxs;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int xp = i & 1, yp = i >> 1;
+            const float* t = base + Y::Slot(yp) * sw + X::Slot(xp);
+            e[i][1 + p] = __fmaf_rn(
+                X::W1(xp) * Y::W1(yp), t[sw + 1],
+                __fmaf_rn(X::W0(xp) * Y::W1(yp), t[sw],
+                          __fmaf_rn(X::W1(xp) * Y::W0(yp), t[1],
+                                    __fmul_rn(X::W0(xp) * Y::W0(yp), t[0]))));
+        }
+    }
+}
+
 // BlockLinearGeneric for a yuv_fast image's block (bx, by) of the CTA's tile
 // (gx, gy) whose two columns and rows are inside the image: the same values,
 // with the format's branches resolved and the chroma taps read from the
@@ -469,7 +506,16 @@ __device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* 
 #pragma unroll
         for (int i = 0; i < 4; ++i) e[i][0] = __fmaf_rn(v[i], s.scale[0], s.offset[0]);
     }
-    if (s.chroma_variant) {
+    if (s.chroma_variant && s.chroma_pattern) {
+        const int bxs = static_cast<int>((x0 >> 1) - ((gx * kPrepTile) >> 1));
+        const int bys = static_cast<int>((y0 >> 1) - ((gy * kPrepTile) >> 1));
+        switch (s.chroma_pattern) {
+            case 1: ChromaFixed<0, 0>(stage, bxs, bys, e); break;
+            case 2: ChromaFixed<1, 0>(stage, bxs, bys, e); break;
+            case 3: ChromaFixed<0, 1>(stage, bxs, bys, e); break;
+            default: ChromaFixed<1, 1>(stage, bxs, bys, e); break;
+        }
+    } else if (s.chroma_variant) {
         const uint32_t sw = (kPrepTile >> s.sub_w) + 2;
         // Window slot 0 of this block is chroma sample (cx - 1, cy - 1), the
         // staged entry (cx - 1 - c0x, cy - 1 - c0y).

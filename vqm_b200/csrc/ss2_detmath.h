@@ -210,24 +210,37 @@ SS2_DM double Exp2J(int j) {
 #endif
 }
 
-// The single-precision tables of powf_gamma (same generator).
-static const float kInvCFHost[128] = {SS2DM_KINVCF_VALUES};
-static const float kLog2InvCFHiHost[128] = {SS2DM_KLOG2INVCFHI_VALUES};
-static const float kLog2InvCFLoHost[128] = {SS2DM_KLOG2INVCFLO_VALUES};
-static const float kExp2JFHiHost[64] = {SS2DM_KEXP2JFHI_VALUES};
-static const float kExp2JFLoHost[64] = {SS2DM_KEXP2JFLO_VALUES};
+// The single-precision tables of powf_gamma (same generator), interleaved:
+// kLogF4[4 i ..] = 1/c_i in float, then -log2 of it as a hi + lo pair, then
+// 0; kExpF2[2 j ..] = 2^(j/64) as a hi + lo pair. One vector load each.
+struct alignas(16) LogEntryF {
+    float inv, hi, lo, pad;
+};
+struct alignas(8) ExpEntryF {
+    float hi, lo;
+};
+static const float kLogF4Host[512] = {SS2DM_KLOGF4_VALUES};
+static const float kExpF2Host[128] = {SS2DM_KEXPF2_VALUES};
 #if defined(__CUDACC__)
-static __device__ const float kInvCFDev[128] = {SS2DM_KINVCF_VALUES};
-static __device__ const float kLog2InvCFHiDev[128] = {SS2DM_KLOG2INVCFHI_VALUES};
-static __device__ const float kLog2InvCFLoDev[128] = {SS2DM_KLOG2INVCFLO_VALUES};
-static __device__ const float kExp2JFHiDev[64] = {SS2DM_KEXP2JFHI_VALUES};
-static __device__ const float kExp2JFLoDev[64] = {SS2DM_KEXP2JFLO_VALUES};
+static __device__ const float4 kLogF4Dev[128] = {SS2DM_KLOGF4_VALUES};
+static __device__ const float2 kExpF2Dev[64] = {SS2DM_KEXPF2_VALUES};
 #endif
+SS2_DM LogEntryF LogF(int i) {
 #if defined(__CUDA_ARCH__)
-#define SS2DM_FTABLE(name, i) __ldg(&name##Dev[i])
+    const float4 v = __ldg(&kLogF4Dev[i]);
+    return LogEntryF{v.x, v.y, v.z, v.w};
 #else
-#define SS2DM_FTABLE(name, i) name##Host[i]
+    return LogEntryF{kLogF4Host[4 * i], kLogF4Host[4 * i + 1], kLogF4Host[4 * i + 2], 0.0f};
 #endif
+}
+SS2_DM ExpEntryF ExpF(int j) {
+#if defined(__CUDA_ARCH__)
+    const float2 v = __ldg(&kExpF2Dev[j]);
+    return ExpEntryF{v.x, v.y};
+#else
+    return ExpEntryF{kExpF2Host[2 * j], kExpF2Host[2 * j + 1]};
+#endif
+}
 
 // log2 of a finite x > 0 in double, table-driven (the reduction of P. T. P.
 // Tang, "Table-driven implementation of the logarithm function in IEEE
@@ -333,7 +346,8 @@ SS2_DM float powf_gamma(float x, float y) {
     const int e = static_cast<int>(ix >> 23) - 127;
     const int i = static_cast<int>((ix >> 16) & 127u);
     const float m = from_bits((ix & 0x007fffffu) | 0x3f800000u);
-    const float inv = SS2DM_FTABLE(kInvCF, i);
+    const LogEntryF L = LogF(i);
+    const float inv = L.inv;
     const float p = m * inv;
     const float pe = fmaf_(m, inv, -p);  // m inv = p + pe exactly
     const float rh = p - 1.0f;           // exact: p is within 2^-8 of 1
@@ -344,9 +358,9 @@ SS2_DM float powf_gamma(float x, float y) {
     const float lr = fmaf_(k1, rh, fmaf_(rh * rh, poly, k1 * pe));
     // log2 x = hi + lo: e + L_i exactly as a pair (|L_i| < 1 <= |e| or e = 0)
     const float ef = static_cast<float>(e);
-    const float lh = SS2DM_FTABLE(kLog2InvCFHi, i);
+    const float lh = L.hi;
     const float hi = ef + lh;
-    const float lo = ((ef - hi) + lh) + (SS2DM_FTABLE(kLog2InvCFLo, i) + lr);
+    const float lo = ((ef - hi) + lh) + (L.lo + lr);
     // t = y log2 x = th + tl
     const float th = y * hi;
     const float tl = fmaf_(y, lo, fmaf_(y, hi, -th));
@@ -357,8 +371,9 @@ SS2_DM float powf_gamma(float x, float y) {
     const float q = fmaf_(fmaf_(z, 0.166666671634f, 0.5f), z * z, z);  // e^z - 1
     const int k = static_cast<int>(kf);
     const int j = k & 63;
-    const float tj = SS2DM_FTABLE(kExp2JFHi, j);
-    const float r = tj + fmaf_(tj, q, SS2DM_FTABLE(kExp2JFLo, j));
+    const ExpEntryF T = ExpF(j);
+    const float tj = T.hi;
+    const float r = tj + fmaf_(tj, q, T.lo);
     return r * from_bits(static_cast<uint32_t>((k >> 6) + 127) << 23);
 }
 

@@ -73,6 +73,9 @@ struct DevSource {
     // parity, so the host fixes the first window slot and the four tap
     // weights per parity.
     uint8_t yuv_fast;
+    uint8_t chroma_pattern;    // 4:2:0 phases known at compile time: 1 + x type
+                               // + 2 y type (type 0: siting offset 0, type 1:
+                               // offset 1/4); 0: use cslot and cweight
     int8_t cslot[2][2];        // [0 = x, 1 = y][parity]: first window slot
     float gamma;               // the transfer exponent
     float cweight[2][2][4];    // [y parity][x parity]: w00, w10, w01, w11

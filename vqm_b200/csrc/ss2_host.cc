@@ -443,6 +443,7 @@ void HostBilinearPhase(uint32_t out_pos, float inv_scale, float shift, int centr
 void FastYuvConstants(const vqm_cu_format& f, int mode, int tid, uint32_t chroma_filter,
                       DevSource& d) {
     d.yuv_fast = 0;
+    d.chroma_pattern = 0;
     d.gamma = 0.0f;
     std::memset(d.cslot, 0, sizeof(d.cslot));
     std::memset(d.cweight, 0, sizeof(d.cweight));
@@ -482,6 +483,24 @@ void FastYuvConstants(const vqm_cu_format& f, int mode, int tid, uint32_t chroma
             w[axis][par][0] = w0_ref;
             w[axis][par][1] = w1_ref;
         }
+    }
+    // 4:2:0 axes whose phases are one of the two compiled patterns (the
+    // device's ChromaFixed): offset 0 gives slots 0, 1 and weights
+    // (1/4, 3/4), (3/4, 1/4); offset 1/4 gives slots 1, 1 and (1, 0),
+    // (1/2, 1/2).
+    d.chroma_pattern = 0;
+    if (f.subsample_w == 1 && f.subsample_h == 1) {
+        int type[2] = {-1, -1};
+        for (int axis = 0; axis < 2; ++axis) {
+            const auto is = [&](int s0, float a0, float b0, int s1, float a1, float b1) {
+                return d.cslot[axis][0] == s0 && w[axis][0][0] == a0 && w[axis][0][1] == b0 &&
+                       d.cslot[axis][1] == s1 && w[axis][1][0] == a1 && w[axis][1][1] == b1;
+            };
+            if (is(0, 0.25f, 0.75f, 1, 0.75f, 0.25f)) type[axis] = 0;
+            else if (is(1, 1.0f, 0.0f, 1, 0.5f, 0.5f)) type[axis] = 1;
+        }
+        if (type[0] >= 0 && type[1] >= 0)
+            d.chroma_pattern = static_cast<uint8_t>(1 + type[0] + 2 * type[1]);
     }
     for (int yp = 0; yp < 2; ++yp)
         for (int xp = 0; xp < 2; ++xp) {
