@@ -424,19 +424,23 @@ __device__ __forceinline__ void StageChroma(const DevSource& s, uint32_t gx, uin
     const uint32_t sw = (kPrepTile >> s.sub_w) + 2, sh = (kPrepTile >> s.sub_h) + 2;
     const int c0x = static_cast<int>((gx * kPrepTile) >> s.sub_w) - 1;
     const int c0y = static_cast<int>((gy * kPrepTile) >> s.sub_h) - 1;
-    const uint32_t n = sw * sh;
-    for (uint32_t k = threadIdx.x; k < 2 * n; k += blockDim.x) {
-        const int p = k >= n ? 2 : 1;
-        const uint32_t idx = k - static_cast<uint32_t>(p - 1) * n;
-        const uint32_t j = idx / sw, i = idx - j * sw;
+    // 64 columns by 4 rows per pass of the CTA's 256 threads (sw <= 66).
+    const uint32_t lanes_x = 64, rows_per_pass = blockDim.x / lanes_x;
+    for (int p = 1; p <= 2; ++p) {
         const int dx = static_cast<int>(s.plane_w[p]), dy = static_cast<int>(s.plane_h[p]);
-        const uint32_t x = static_cast<uint32_t>(min(max(c0x + static_cast<int>(i), 0), dx - 1));
-        const uint32_t y = static_cast<uint32_t>(min(max(c0y + static_cast<int>(j), 0), dy - 1));
-        const uint8_t* row = s.plane[p] + static_cast<size_t>(y) * s.row_bytes[p];
-        const float v = s.type == 0
-                            ? static_cast<float>(__ldg(row + x))
-                            : static_cast<float>(__ldg(reinterpret_cast<const uint16_t*>(row) + x));
-        stage[(p - 1) * kChromaStage + idx] = __fmaf_rn(v, s.scale[1], s.offset[1]);
+        float* out = stage + (p - 1) * kChromaStage;
+        for (uint32_t j = threadIdx.x / lanes_x; j < sh; j += rows_per_pass) {
+            const uint32_t y = static_cast<uint32_t>(min(max(c0y + static_cast<int>(j), 0), dy - 1));
+            const uint8_t* row = s.plane[p] + static_cast<size_t>(y) * s.row_bytes[p];
+            for (uint32_t i = threadIdx.x % lanes_x; i < sw; i += lanes_x) {
+                const uint32_t x =
+                    static_cast<uint32_t>(min(max(c0x + static_cast<int>(i), 0), dx - 1));
+                const float v =
+                    s.type == 0 ? static_cast<float>(__ldg(row + x))
+                                : static_cast<float>(__ldg(reinterpret_cast<const uint16_t*>(row) + x));
+                out[j * sw + i] = __fmaf_rn(v, s.scale[1], s.offset[1]);
+            }
+        }
     }
 }
 
@@ -483,14 +487,33 @@ __device__ __forceinline__ void ChromaFixed(const float* stage, int bxs, int bys
 // staged window at the host's per-parity slots and weights.
 __device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* stage,
                                                uint32_t gx, uint32_t gy, uint32_t bx,
-                                               uint32_t by, float rgb[4][3]) {
+                                               uint32_t by, bool aligned4, float rgb[4][3]) {
     const uint32_t x0 = 2 * bx, y0 = 2 * by;
     float e[4][3];
     {
         const uint8_t* r0 = s.plane[0] + static_cast<size_t>(y0) * s.row_bytes[0];
         const uint8_t* r1 = r0 + s.row_bytes[0];
         float v[4];
-        if (s.type == 0) {
+        if (aligned4) {
+            // Both samples of a row in one load (x0 is even; planes and rows
+            // are 4-byte aligned).
+            uint32_t a, b;
+            if (s.type == 0) {
+                a = __ldg(reinterpret_cast<const uint16_t*>(r0 + x0));
+                b = __ldg(reinterpret_cast<const uint16_t*>(r1 + x0));
+                v[0] = static_cast<float>(a & 0xffu);
+                v[1] = static_cast<float>(a >> 8);
+                v[2] = static_cast<float>(b & 0xffu);
+                v[3] = static_cast<float>(b >> 8);
+            } else {
+                a = __ldg(reinterpret_cast<const uint32_t*>(r0 + 2 * x0));
+                b = __ldg(reinterpret_cast<const uint32_t*>(r1 + 2 * x0));
+                v[0] = static_cast<float>(a & 0xffffu);
+                v[1] = static_cast<float>(a >> 16);
+                v[2] = static_cast<float>(b & 0xffffu);
+                v[3] = static_cast<float>(b >> 16);
+            }
+        } else if (s.type == 0) {
             v[0] = __ldg(r0 + x0);
             v[1] = __ldg(r0 + x0 + 1);
             v[2] = __ldg(r1 + x0);

@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
                     TableBlock(s, lut, fast, w4, hx, bx, by, lin);
                 } else {
                     if (s.yuv_fast && 2 * bx + 1 < width && 2 * by + 1 < height)
-                        BlockLinearYuv(s, chroma_stage, gx, gy, bx, by, lin);
+                        BlockLinearYuv(s, chroma_stage, gx, gy, bx, by, aligned4 != 0, lin);
                     else
                         BlockLinearGeneric(s, bx, by, lin);
                 }
