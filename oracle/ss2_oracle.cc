@@ -1174,6 +1174,13 @@ void BlurV(const std::vector<T>& src, std::vector<T>& dst, uint32_t w, uint32_t 
     }
 }
 
+// The maps' two quotients: in the FP32 path the shared division of
+// ss2_detmath.h that the kernels use (its divisors, at least 0.0009 and 1,
+// are in its domain), in the FP64 path the IEEE one.
+template <class T> T MapDiv(T a, T b);
+template <> float MapDiv<float>(float a, float b) { return ss2dm::divf(a, b); }
+template <> double MapDiv<double>(double a, double b) { return a / b; }
+
 // scale.comp:305-333: the SSIM' map in difference form and the edge maps.
 template <class T>
 void Maps(T mu1, T mu2, T s11, T s22, T s12, T img1, T img2, T out[6]) {
@@ -1182,13 +1189,13 @@ void Maps(T mu1, T mu2, T s11, T s22, T s12, T img1, T img2, T out[6]) {
     const T num_m = std::fma(-dm, dm, T(1));
     const T num_s = std::fma(T(2), std::fma(-mu1, mu2, s12), C2);
     const T denom = (std::fma(-mu1, mu1, s11) + std::fma(-mu2, mu2, s22)) + C2;
-    const T d = std::max(std::fma(-num_m, num_s, denom) / denom, T(0));
+    const T d = std::max(MapDiv<T>(std::fma(-num_m, num_s, denom), denom), T(0));
     const T dd = d * d;
     out[0] = d;
     out[1] = dd * dd;
     const T dist = T(1) + std::abs(img2 - mu2);
     const T orig = T(1) + std::abs(img1 - mu1);
-    const T d1 = (dist - orig) / orig;
+    const T d1 = MapDiv<T>(dist - orig, orig);
     const T ring = std::max(d1, T(0));
     const T blur = std::max(-d1, T(0));
     out[2] = ring;
@@ -1511,6 +1518,7 @@ int ss2o_detmath(int fn, const float* x, float y, float* out, size_t n) {
             case 3: out[i] = ss2dm::sinpi(x[i]); break;
             case 4: out[i] = RoundHalf(x[i]); break;
             case 5: out[i] = ss2dm::powf_gamma(x[i], y); break;
+            case 6: out[i] = ss2dm::divf(x[i], y); break;
             default: g_error = "unknown function"; return SS2O_INVALID;
         }
     }

@@ -99,7 +99,8 @@ int ss2o_level_sums(const ss2o_image* original, const ss2o_image* distorted,
                     uint32_t* scales);
 /* The shared deterministic functions, for their accuracy tests: fn 0 cube
  * root, 1 pow(x, y), 2 exp, 3 sin(pi x), 4 rounding to binary16 (the
- * half-plane build's plane rounding), 5 the power-law transfers' power. */
+ * half-plane build's plane rounding), 5 the power-law transfers' power,
+ * 6 the maps' division x / y. */
 int ss2o_detmath(int fn, const float* x, float y, float* out, size_t n);
 const char* ss2o_last_error(void);
 

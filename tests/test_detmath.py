@@ -90,6 +90,23 @@ def test_powf_gamma(y):
     assert np.array_equal(det(5, x[:1000], np.float32(0.5)), det(1, x[:1000], np.float32(0.5)))
 
 
+def test_divf_matches_ieee_division():
+    """The maps' division (seeded reciprocal, three Newton steps, one
+    residual correction) over its domain, b in [2^-20, 2^20], |a| < 2^20:
+    equal to IEEE single-precision division on every sampled quotient (60
+    divisors x 50,000 dividends) and on every dividend of the binade [1, 2)
+    for a spread of divisors."""
+    rng = np.random.default_rng(7)
+    for b in np.exp(rng.uniform(np.log(2.0 ** -20), np.log(2.0 ** 20), 60)).astype(np.float32):
+        a = (rng.uniform(-1, 1, 50_000) *
+             np.exp(rng.uniform(np.log(1e-7), np.log(2.0 ** 20), 50_000))).astype(np.float32)
+        assert np.array_equal(det(6, a, b), a / b)
+    a = np.arange(0x3F800000, 0x40000000, dtype=np.uint32).view(np.float32)
+    for b in np.float32([1.0, 1.5, 0.0009, 0.3337, 7.25, 2.0 ** -19, 1234.5]):
+        assert np.array_equal(det(6, a, b), a / b)
+    assert det(6, np.float32([0.0]), np.float32(3.0))[0] == 0.0
+
+
 def test_pow_base10():
     # 10^(2 (v - 1)) and 10^(2.5 (v - 1)) of the log transfers.
     e = np.random.default_rng(1).uniform(-5, 0, 200_000).astype(np.float32)

@@ -227,6 +227,19 @@ __device__ __forceinline__ void ConvertHalfTile(const unsigned char* staging, fl
 __device__ __forceinline__ float2 Pack(float v) { return make_float2(v, v); }
 __device__ __forceinline__ float2 Neg(float2 v) { return make_float2(-v.x, -v.y); }
 
+// ss2dm::divf (the maps' division, shared with the CPU checker) of both
+// lanes, two lanes per instruction: the same operations on each lane.
+__device__ __forceinline__ float2 Div2(float2 a, float2 b) {
+    float2 r = make_float2(__uint_as_float(0x7ef311c7u - __float_as_uint(b.x)),
+                           __uint_as_float(0x7ef311c7u - __float_as_uint(b.y)));
+    const float2 nb = Neg(b), one = Pack(1.0f);
+    r = __ffma2_rn(r, __ffma2_rn(nb, r, one), r);
+    r = __ffma2_rn(r, __ffma2_rn(nb, r, one), r);
+    r = __ffma2_rn(r, __ffma2_rn(nb, r, one), r);
+    const float2 q0 = __fmul2_rn(a, r);
+    return __ffma2_rn(__ffma2_rn(nb, q0, a), r, q0);
+}
+
 // Horizontal pass (scale.comp:149-207): row pair rp, output columns
 // c0..c0+3, all five quantities, both rows per instruction, for the row
 // pairs from `rp_begin` (even) on.
@@ -338,8 +351,8 @@ __device__ __forceinline__ void VerticalMaps(const float* src, const float* hq, 
                 __fadd2_rn(__ffma2_rn(Neg(mu1), mu1, V[2][j]), __ffma2_rn(Neg(mu2), mu2, V[3][j])),
                 Pack(0.0009f));
             const float2 numer = __ffma2_rn(Neg(num_m), num_s, denom);
-            float2 d = make_float2(fmaxf(__fdiv_rn(numer.x, denom.x), 0.0f),
-                                   fmaxf(__fdiv_rn(numer.y, denom.y), 0.0f));
+            const float2 q = Div2(numer, denom);
+            float2 d = make_float2(fmaxf(q.x, 0.0f), fmaxf(q.y, 0.0f));
             const float4 r1 = raw1[j >> 1], r2v = raw2[j >> 1];
             const float2 img1 = (j & 1) ? make_float2(r1.y, r1.w) : make_float2(r1.x, r1.z);
             const float2 img2 = (j & 1) ? make_float2(r2v.y, r2v.w) : make_float2(r2v.x, r2v.z);
@@ -350,7 +363,7 @@ __device__ __forceinline__ void VerticalMaps(const float* src, const float* hq, 
             const float2 dist = __fadd2_rn(Pack(1.0f), e2);
             const float2 orig = __fadd2_rn(Pack(1.0f), e1);
             const float2 diff = __fadd2_rn(dist, Neg(orig));
-            const float2 d1 = make_float2(__fdiv_rn(diff.x, orig.x), __fdiv_rn(diff.y, orig.y));
+            const float2 d1 = Div2(diff, orig);
             float2 ring = make_float2(fmaxf(d1.x, 0.0f), fmaxf(d1.y, 0.0f));
             float2 blur = make_float2(fmaxf(-d1.x, 0.0f), fmaxf(-d1.y, 0.0f));
             if (kEdge) {
