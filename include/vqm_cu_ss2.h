@@ -258,9 +258,12 @@ typedef struct vqm_cu_ss2_batch_config {
     uint32_t max_pairs;    /* largest pair count of one batch */
     uint32_t chroma_filter;
     int32_t device;        /* CUDA ordinal; -1 = the current device */
-    uint32_t tile_w, tile_h; /* blur tile; 0 = the tuned default */
-    uint32_t variant;      /* blur kernel: 0 = by tile (or the tuned
-                              default), k = compiled variant k - 1 */
+    uint32_t tile_w, tile_h; /* blur tile (its one-tile-per-CTA kernel);
+                                0 = chosen per submit */
+    uint32_t variant;      /* blur kernel: 0 = by tile, or chosen per submit
+                              from the tile count (a strip length of the
+                              default tile; same results), k = compiled
+                              variant k - 1 */
     uint32_t half_planes;  /* 1: binary16 pyramid planes, as
                               vqm_cu_ss2_config.half_planes */
 } vqm_cu_ss2_batch_config;

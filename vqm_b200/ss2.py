@@ -606,8 +606,10 @@ class Ssimulacra2Batch:
                  device: int = -1, tile: tuple[int, int] | None = None,
                  variant: int | None = None, half_planes: bool = False):
         """`variant` picks a compiled blur kernel (see blur_variants());
-        `tile` picks one by its output tile; neither: the tuned default.
-        `half_planes` stores the pyramid as binary16 (ssimulacra2.h:41-46)."""
+        `tile` picks the one-tile-per-CTA kernel of that output tile;
+        neither: each submit picks a 32x32 strip length from its tile count
+        (the results are the same whichever runs). `half_planes` stores the
+        pyramid as binary16 (ssimulacra2.h:41-46)."""
         tw, th = tile if tile else (0, 0)
         v = 0 if variant is None else variant + 1
         cfg = _BatchConfig(max_pixels, max_pairs, chroma_filter, device, tw, th, v,
