@@ -372,24 +372,23 @@ __device__ __forceinline__ void BlockLinearGeneric(const DevSource& s, uint32_t 
 // scalar function performs on that lane: the same values. A lane outside the
 // function's fast range sends both through the scalar function.
 __device__ __forceinline__ float2 PowfGamma2(float2 x, float y) {
-    const float lo_x = 9.31322574615478515625e-10f;  // 2^-30
-    if (!(x.x >= lo_x && x.x < 256.0f && x.y >= lo_x && x.y < 256.0f && y >= 1.0f && y <= 4.0f))
-        return make_float2(ss2dm::powf_gamma(x.x, y), ss2dm::powf_gamma(x.y, y));
+    using namespace ss2dm;
+    if (!(powf_gamma_fast(x.x, y) && powf_gamma_fast(x.y, y)))
+        return make_float2(powf_gamma(x.x, y), powf_gamma(x.y, y));
     const auto P = [](float v) { return make_float2(v, v); };
     const auto N = [](float2 v) { return make_float2(-v.x, -v.y); };
     const uint32_t ix0 = __float_as_uint(x.x), ix1 = __float_as_uint(x.y);
     const int i0 = static_cast<int>((ix0 >> 16) & 127u), i1 = static_cast<int>((ix1 >> 16) & 127u);
     const float2 m = make_float2(__uint_as_float((ix0 & 0x007fffffu) | 0x3f800000u),
                                  __uint_as_float((ix1 & 0x007fffffu) | 0x3f800000u));
-    const ss2dm::LogEntryF L0 = ss2dm::LogF(i0), L1 = ss2dm::LogF(i1);
+    const LogEntryF L0 = LogF(i0), L1 = LogF(i1);
     const float2 inv = make_float2(L0.inv, L1.inv);
     const float2 p = __fmul2_rn(m, inv);
     const float2 pe = __ffma2_rn(m, inv, N(p));
     const float2 rh = __fadd2_rn(p, P(-1.0f));
-    const float k1 = 1.44269502163f, k2 = -0.721347510815f;
-    const float k3 = 0.480898350477f, k4 = -0.360673755407f;
-    const float2 poly = __ffma2_rn(__ffma2_rn(rh, P(k4), P(k3)), rh, P(k2));
-    const float2 lr = __ffma2_rn(P(k1), rh, __ffma2_rn(__fmul2_rn(rh, rh), poly, __fmul2_rn(P(k1), pe)));
+    const float2 poly = __ffma2_rn(__ffma2_rn(rh, P(kGammaK4), P(kGammaK3)), rh, P(kGammaK2));
+    const float2 lr = __ffma2_rn(P(kGammaK1), rh,
+                                 __ffma2_rn(__fmul2_rn(rh, rh), poly, __fmul2_rn(P(kGammaK1), pe)));
     const float2 ef = make_float2(static_cast<float>(static_cast<int>(ix0 >> 23) - 127),
                                   static_cast<float>(static_cast<int>(ix1 >> 23) - 127));
     const float2 lh = make_float2(L0.hi, L1.hi);
@@ -399,13 +398,12 @@ __device__ __forceinline__ float2 PowfGamma2(float2 x, float y) {
     const float2 th = __fmul2_rn(P(y), hi);
     const float2 tl = __ffma2_rn(P(y), lo, __ffma2_rn(P(y), hi, N(th)));
     const float2 kf = __fadd2_rn(__ffma2_rn(th, P(64.0f), P(12582912.0f)), P(-12582912.0f));
-    const float ln2 = 0.693147182465f;
-    const float2 z =
-        __ffma2_rn(__ffma2_rn(kf, P(-0.015625f), th), P(ln2), __fmul2_rn(tl, P(ln2)));
-    const float2 q = __ffma2_rn(__ffma2_rn(z, P(0.166666671634f), P(0.5f)), __fmul2_rn(z, z), z);
+    const float2 z = __ffma2_rn(__ffma2_rn(kf, P(-0.015625f), th), P(kGammaLn2),
+                                __fmul2_rn(tl, P(kGammaLn2)));
+    const float2 q = __ffma2_rn(__ffma2_rn(z, P(kGammaSixth), P(0.5f)), __fmul2_rn(z, z), z);
     const int k0 = static_cast<int>(kf.x), k1i = static_cast<int>(kf.y);
     const int j0 = k0 & 63, j1 = k1i & 63;
-    const ss2dm::ExpEntryF T0 = ss2dm::ExpF(j0), T1 = ss2dm::ExpF(j1);
+    const ExpEntryF T0 = ExpF(j0), T1 = ExpF(j1);
     const float2 tj = make_float2(T0.hi, T1.hi);
     const float2 tjl = make_float2(T0.lo, T1.lo);
     const float2 r = __fadd2_rn(tj, __ffma2_rn(tj, q, tjl));

@@ -339,9 +339,23 @@ SS2_DM float pow(float x, float y) {
 // log and exp above, carried in float pairs: Tang 1990, and the pair
 // arithmetic of Dekker 1971). Outside that range, and for y outside [1, 4],
 // it is pow(x, y).
+// powf_gamma's constants (shared with its two-lane form in the kernels):
+// its fast range [2^-30, 256) and [1, 4], the Taylor coefficients of
+// log2(1 + r), ln 2 and 1/6, each the float nearest the exact value.
+constexpr float kGammaMinX = 9.31322574615478515625e-10f;  // 2^-30
+constexpr float kGammaMaxX = 256.0f;
+constexpr float kGammaK1 = 1.44269502163f;     // 1 / ln 2
+constexpr float kGammaK2 = -0.721347510815f;   // -1 / (2 ln 2)
+constexpr float kGammaK3 = 0.480898350477f;    // 1 / (3 ln 2)
+constexpr float kGammaK4 = -0.360673755407f;   // -1 / (4 ln 2)
+constexpr float kGammaLn2 = 0.693147182465f;
+constexpr float kGammaSixth = 0.166666671634f;
+SS2_DM bool powf_gamma_fast(float x, float y) {
+    return x >= kGammaMinX && x < kGammaMaxX && y >= 1.0f && y <= 4.0f;
+}
+
 SS2_DM float powf_gamma(float x, float y) {
-    if (!(x >= 9.31322574615478515625e-10f && x < 256.0f && y >= 1.0f && y <= 4.0f))
-        return pow(x, y);
+    if (!powf_gamma_fast(x, y)) return pow(x, y);
     const uint32_t ix = bits(x);
     const int e = static_cast<int>(ix >> 23) - 127;
     const int i = static_cast<int>((ix >> 16) & 127u);
@@ -352,10 +366,8 @@ SS2_DM float powf_gamma(float x, float y) {
     const float pe = fmaf_(m, inv, -p);  // m inv = p + pe exactly
     const float rh = p - 1.0f;           // exact: p is within 2^-8 of 1
     // log2(1 + r) ~ k1 r + k2 r^2 + k3 r^3 + k4 r^4, k_n = (-1)^(n+1) / (n ln 2)
-    const float k1 = 1.44269502163f, k2 = -0.721347510815f;
-    const float k3 = 0.480898350477f, k4 = -0.360673755407f;
-    const float poly = fmaf_(fmaf_(rh, k4, k3), rh, k2);
-    const float lr = fmaf_(k1, rh, fmaf_(rh * rh, poly, k1 * pe));
+    const float poly = fmaf_(fmaf_(rh, kGammaK4, kGammaK3), rh, kGammaK2);
+    const float lr = fmaf_(kGammaK1, rh, fmaf_(rh * rh, poly, kGammaK1 * pe));
     // log2 x = hi + lo: e + L_i exactly as a pair (|L_i| < 1 <= |e| or e = 0)
     const float ef = static_cast<float>(e);
     const float lh = L.hi;
@@ -366,9 +378,8 @@ SS2_DM float powf_gamma(float x, float y) {
     const float tl = fmaf_(y, lo, fmaf_(y, hi, -th));
     // 64 th to the nearest integer k (|64 th| < 2^22), then z = (t - k/64) ln 2
     const float kf = (th * 64.0f + 12582912.0f) - 12582912.0f;
-    const float ln2 = 0.693147182465f;
-    const float z = fmaf_(fmaf_(kf, -0.015625f, th), ln2, tl * ln2);
-    const float q = fmaf_(fmaf_(z, 0.166666671634f, 0.5f), z * z, z);  // e^z - 1
+    const float z = fmaf_(fmaf_(kf, -0.015625f, th), kGammaLn2, tl * kGammaLn2);
+    const float q = fmaf_(fmaf_(z, kGammaSixth, 0.5f), z * z, z);  // e^z - 1
     const int k = static_cast<int>(kf);
     const int j = k & 63;
     const ExpEntryF T = ExpF(j);
