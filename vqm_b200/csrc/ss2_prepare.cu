@@ -99,10 +99,13 @@ __device__ __forceinline__ float2 Max0(float2 v) {
 // inputs are non-negative and finite (so every mix is at least the bias).
 template <bool kInRange = false>
 __device__ __forceinline__ void Xyb2(float2 r, float2 g, float2 b, uint32_t mask, float2 out[3]) {
-    const float2 m0 = Max0(__ffma2_rn(Pack(kM00), r,
-                                      __ffma2_rn(Pack(kM01), g, __ffma2_rn(Pack(kM02), b, Pack(kBias)))));
-    const float2 m1 = Max0(__ffma2_rn(Pack(kM10), r,
-                                      __ffma2_rn(Pack(kM11), g, __ffma2_rn(Pack(kM12), b, Pack(kBias)))));
+    // In range, every mix is at least the bias, so the clamp at 0 is the
+    // identity and is left out.
+    const auto clamp = [](float2 v) { return kInRange ? v : Max0(v); };
+    const float2 m0 = clamp(__ffma2_rn(Pack(kM00), r,
+                                       __ffma2_rn(Pack(kM01), g, __ffma2_rn(Pack(kM02), b, Pack(kBias)))));
+    const float2 m1 = clamp(__ffma2_rn(Pack(kM10), r,
+                                       __ffma2_rn(Pack(kM11), g, __ffma2_rn(Pack(kM12), b, Pack(kBias)))));
     const float2 c0 = __fadd2_rn(Cbrt2<kInRange>(m0), Pack(-kCbrtBias));
     const float2 c1 = __fadd2_rn(Cbrt2<kInRange>(m1), Pack(-kCbrtBias));
     const float2 sum = __fadd2_rn(c0, c1);
@@ -110,7 +113,7 @@ __device__ __forceinline__ void Xyb2(float2 r, float2 g, float2 b, uint32_t mask
     out[1] = __ffma2_rn(Pack(0.5f), sum, Pack(0.01f));
     out[2] = Pack(0.0f);
     if (mask & 4u) {
-        const float2 m2 = Max0(__ffma2_rn(
+        const float2 m2 = clamp(__ffma2_rn(
             Pack(kM20), r, __ffma2_rn(Pack(kM21), g, __ffma2_rn(Pack(kM22), b, Pack(kBias)))));
         const float2 c2 = __fadd2_rn(Cbrt2<kInRange>(m2), Pack(-kCbrtBias));
         out[2] = __fadd2_rn(__ffma2_rn(Pack(-0.5f), sum, c2), Pack(0.55f));
