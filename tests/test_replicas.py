@@ -75,3 +75,37 @@ def test_score_sharded_two_gloo_ranks(tmp_path):
         assert sum(calls) <= len(sizes)
     # Each pair was scored exactly once, across the two ranks.
     assert sum(sum(c) for _, c in results) == len(sizes)
+
+
+def test_contiguous_ranges_cover_the_clip_in_order():
+    for count in (0, 1, 5, 240, 241):
+        for world in (1, 2, 3, 8):
+            ranges = replicas.contiguous(count, world)
+            assert [i for r in ranges for i in r] == list(range(count))
+            sizes = [len(r) for r in ranges]
+            assert max(sizes) - min(sizes) <= 1
+    with pytest.raises(ValueError):
+        replicas.contiguous(5, 0)
+
+
+def _gather_worker(rank, world, port, out_dir):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        count = 7
+        mine = replicas.contiguous(count, world)[rank]
+        local = [(i, i * i) for i in mine]
+        out = replicas.gather_ordered(local, mine.start, count)
+        with open(os.path.join(out_dir, f"g{rank}.txt"), "w") as f:
+            f.write(repr(out))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gather_ordered_two_gloo_ranks(tmp_path):
+    import torch.multiprocessing as mp
+    mp.spawn(_gather_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True)
+    for r in range(2):
+        assert eval((tmp_path / f"g{r}.txt").read_text()) == [(i, i * i) for i in range(7)]

@@ -3,6 +3,7 @@ reference) and the CLI's per-frame scores, clip mean and raw norms."""
 
 import io
 import json
+import os
 
 import numpy as np
 import pytest
@@ -66,6 +67,22 @@ def test_frames_round_trip_and_truncation(tmp_path):
         list(r)
 
 
+def test_reader_skip_and_remaining(tmp_path):
+    pairs, po, _ = _clip(tmp_path, frames=5)
+    with y4m.Reader(po) as r:
+        assert r.remaining() == 5
+        assert r.skip(2) == 2
+        assert r.remaining() == 3
+        img = next(iter(r))
+        assert np.array_equal(img.data, pairs[2][0].data)
+        assert r.skip(10) == 2
+        assert r.remaining() == 0
+    data = open(po, "rb").read()
+    (tmp_path / "t.y4m").write_bytes(data[:-5])
+    with y4m.Reader(str(tmp_path / "t.y4m")) as r, pytest.raises(y4m.Y4mError, match="truncated"):
+        r.skip(5)
+
+
 def test_cli_rejects_mismatched_clips(tmp_path, capsys):
     from vqm_b200 import cli
     _, po, _ = _clip(tmp_path, frames=2)
@@ -104,6 +121,36 @@ def test_cli_scores_frames_and_clip_mean(tmp_path):
     lines = out.getvalue().strip().splitlines()
     assert len(lines) == len(pairs) + 1
     assert abs(float(lines[-1]) - doc["score"]) < 1e-7
+
+
+@pytest.mark.gpu
+def test_cli_two_ranks_score_contiguous_ranges(tmp_path):
+    """Under torchrun with two ranks the CLI splits the clip into two frame
+    ranges and rank 0 prints the same clip as a single process."""
+    import socket
+    import subprocess
+    import sys
+    pairs, po, pd = _clip(tmp_path, frames=5)
+    one = io.StringIO()
+    from vqm_b200 import cli
+    assert cli.run([po, pd, "--json", "--raw", "--batch", "2"], out=one) == 0
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    res = subprocess.run(
+        [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+         "--master-addr", "127.0.0.1", "--master-port", str(port), "-m", "vqm_b200.cli",
+         po, pd, "--json", "--raw", "--batch", "2"],
+        capture_output=True, text=True, timeout=600,
+        cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    assert res.returncode == 0, res.stderr[-2000:]
+    lines = [l for l in res.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    got, want = json.loads(lines[0]), json.loads(one.getvalue())
+    assert got["frames"] == want["frames"] == 5
+    assert got["frame_scores"] == want["frame_scores"]
+    assert got["frame_norms"] == want["frame_norms"]
+    assert got["score"] == want["score"]
 
 
 @pytest.mark.gpu

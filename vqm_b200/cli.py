@@ -15,18 +15,27 @@ before its score; --json prints one JSON object instead.
 Frames go to the scorer `--batch` pairs at a time (one launch per stage per
 batch); 1 scores each pair through a pipeline whose kernels replay as one
 CUDA graph.
+
+Under torchrun (WORLD_SIZE > 1) every rank scores a contiguous range of the
+frames on its own GPU (LOCAL_RANK), reading only that range, and rank 0
+prints the whole clip in frame order; the ranks exchange only per-frame
+results (gloo, for the plumbing):
+
+    python -m torch.distributed.run --nproc-per-node 8 -m vqm_b200.cli a.y4m b.y4m
 """
 
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import math
+import os
 import statistics
 import sys
 import time
 
-from . import ss2, y4m
+from . import replicas, ss2, y4m
 
 _MATRICES = {
     "rgb": ss2.MatrixCoefficients.Rgb, "bt709": ss2.MatrixCoefficients.Bt709,
@@ -116,6 +125,16 @@ def run(argv=None, out=sys.stdout) -> int:
     ap.add_argument("--device", type=int, default=-1)
     args = ap.parse_args(argv)
 
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    device = args.device
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        # One GPU per rank; ranks beyond the GPU count share them (their
+        # work is independent).
+        device = int(os.environ.get("LOCAL_RANK", str(rank))) % max(1, torch.cuda.device_count())
     ro, rd = y4m.Reader(args.original), y4m.Reader(args.distorted)
     try:
         ho, hd = ro.header, rd.header
@@ -125,14 +144,26 @@ def run(argv=None, out=sys.stdout) -> int:
             raise y4m.Y4mError("clips differ in frame rate")
         ro.format, rd.format = _format(ho, args), _format(hd, args)
         alpha = ro.format.alpha != ss2.AlphaType.None_ or rd.format.alpha != ss2.AlphaType.None_
+        total = None
+        todo = None  # frames this rank scores; None: to the end
+        if world > 1:
+            total = ro.remaining()
+            if rd.remaining() != total:
+                raise y4m.Y4mError("clips differ in frame count")
+            mine = replicas.contiguous(total, world)[rank]
+            ro.skip(mine.start)
+            rd.skip(mine.start)
+            todo = len(mine)
         scorer = _Scorer(ho.width, ho.height, max(1, args.batch), _FILTERS[args.chroma_filter],
-                         args.device)
-        frames = []  # (score, result)
+                         device)
+        frames = []  # (score, raw norms)
         t0 = time.perf_counter()
         io, idis = iter(ro), iter(rd)
-        while True:
+        while todo is None or len(frames) < todo:
             chunk = []
-            for _ in range(max(1, args.batch)):
+            want = max(1, args.batch) if todo is None else min(max(1, args.batch),
+                                                                todo - len(frames))
+            for _ in range(want):
                 a, b = next(io, None), next(idis, None)
                 if (a is None) != (b is None):
                     raise y4m.Y4mError("clips differ in frame count")
@@ -147,12 +178,21 @@ def run(argv=None, out=sys.stdout) -> int:
                 picked = [x if x.score() <= y.score() else y for x, y in zip(dark, bright)]
             else:
                 picked = scorer.score(chunk, 0.5)
-            frames += [(r.score(), r) for r in picked]
+            frames += [(r.score(), raw_norms(r) if args.raw else None) for r in picked]
         seconds = time.perf_counter() - t0
         scorer.close()
     finally:
         ro.close()
         rd.close()
+    if world > 1:
+        import torch.distributed as dist
+        frames = replicas.gather_ordered(frames, mine.start, total)
+        slowest = [None] * world
+        dist.all_gather_object(slowest, seconds)
+        seconds = max(slowest)
+        dist.destroy_process_group()
+        if rank != 0:
+            return 0
     if not frames:
         raise y4m.Y4mError("clips have no frames")
 
@@ -162,7 +202,7 @@ def run(argv=None, out=sys.stdout) -> int:
         doc = {"metric": "ssimulacra2", "score": clip, "frames": len(frames),
                "frame_scores": scores, "scoring_fps": len(frames) / seconds}
         if args.raw:
-            doc["frame_norms"] = [raw_norms(r) for _, r in frames]
+            doc["frame_norms"] = [raw for _, raw in frames]
         print(json.dumps(doc), file=out)
         return 0
     if args.verbose:
@@ -175,8 +215,8 @@ def run(argv=None, out=sys.stdout) -> int:
         print(f"{'SSIMULACRA2':<12} {clip:>15.8g} {min(scores):>15.8g} {max(scores):>15.8g} "
               f"{sd:>15.8g} {sum(1 for s in scores if s == 100.0):>8}", file=out)
     if args.raw:
-        for _, r in frames:
-            print(",".join(f"{v:.12f}" for v in raw_norms(r)) + ",", file=out)
+        for _, raw in frames:
+            print(",".join(f"{v:.12f}" for v in raw) + ",", file=out)
     print(f"{clip:.8f}", file=out)
     return 0
 

@@ -4,8 +4,10 @@ Pairs are independent, so the multi-GPU form of the scorer has no data-path
 collective: every rank (one process per GPU, torch.distributed for the
 plumbing) takes a shard of the list, scores it on its own GPU with its own
 batch scorer, and the ranks exchange only the results (108 norms and a score
-per pair) to give every rank the whole list in input order. Shards balance
-pixels, longest pair first, since a pair's cost grows with its pixel count.
+per pair) to give every rank the whole list in input order. Shards of a
+list of pairs balance pixels, longest pair first, since a pair's cost grows
+with its pixel count; the frames of a video take contiguous ranges instead
+(one size, and each rank reads and scores its range in order).
 """
 
 from __future__ import annotations
@@ -26,6 +28,28 @@ def shard(pixels: Sequence[int], world: int) -> list[list[int]]:
         out[r].append(i)
         load[r] += int(pixels[i])
     return [sorted(s) for s in out]
+
+
+def contiguous(count: int, world: int) -> list[range]:
+    """Rank r's frames [r * count // world, (r + 1) * count // world): in
+    order, sizes differing by at most one."""
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    return [range(r * count // world, (r + 1) * count // world) for r in range(world)]
+
+
+def gather_ordered(local: list, first: int, count: int, group=None) -> list:
+    """Every rank's results for its contiguous range (starting at `first`),
+    reassembled in order on every rank."""
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    gathered: list = [None] * world
+    dist.all_gather_object(gathered, (first, list(local)), group=group)
+    out: list = [None] * count
+    for start, part in gathered:
+        out[start:start + len(part)] = part
+    return out
 
 
 def score_sharded(pairs: Sequence, score: Callable[[list], list], group=None) -> list:

@@ -140,6 +140,12 @@ def read_frame(f: BinaryIO, header: Header, fmt: ss2.ImageFormat | None = None):
     return ss2.Image(header.width, header.height, fmt, data)
 
 
+def frame_bytes(header: Header) -> int:
+    """Sample bytes of one frame (the FRAME line excluded)."""
+    return sum(g[1] * g[2] * g[3] for g in ss2.plane_layout(header.format, header.width,
+                                                             header.height) if g is not None)
+
+
 class Reader:
     """Iterates a Y4M file's frames as ss2.Image."""
 
@@ -154,6 +160,34 @@ class Reader:
             self._f.close()
             raise Y4mError("interlaced y4m input is not supported")
         self.format = fmt or self.header.format
+
+    def remaining(self) -> int:
+        """Frames left from the current position (the position is kept)."""
+        here = self._f.tell()
+        try:
+            return self.skip(1 << 62)
+        finally:
+            self._f.seek(here)
+
+    def skip(self, n: int) -> int:
+        """Skips up to n frames without reading their samples (each FRAME
+        line is read, since it may carry parameters); returns the number
+        skipped, fewer at the end of the stream."""
+        size = frame_bytes(self.header)
+        for k in range(n):
+            first = self._f.read(1)
+            if not first:
+                return k
+            line = first + _read_line(self._f)
+            if line != b"FRAME" and not line.startswith(b"FRAME "):
+                raise Y4mError("y4m file has no frame")
+            here = self._f.tell()
+            self._f.seek(0, 2)
+            end = self._f.tell()
+            if end - here < size:
+                raise Y4mError("truncated y4m frame")
+            self._f.seek(here + size)
+        return n
 
     def __iter__(self) -> Iterator[ss2.Image]:
         while True:
