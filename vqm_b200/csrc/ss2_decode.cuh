@@ -10,6 +10,9 @@
 // The 8-bit RGB / grey formats without alpha decode through a 256-entry table
 // built on the host per image (transfer(code * scale + offset)): the table
 // holds exactly the per-sample values, so both paths round identically.
+// Integer YUV with a pure power-law transfer and at most 2x chroma
+// subsampling takes BlockLinearYuv (below), the same values with the
+// format's branches resolved; everything else BlockLinearGeneric.
 #pragma once
 
 #include <cuda_fp16.h>

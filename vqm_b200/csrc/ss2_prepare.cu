@@ -10,14 +10,17 @@
 // the threads it still needs. Because the 2x2 box nests exactly, no CTA ever
 // needs a neighbour's samples.
 //
-// Two specialisations: 8-bit grey/RGB without alpha decode through the
-// image's 256-entry table in shared memory, reading four samples of a row
-// with one 32-bit load where the planes allow it; every other format runs
-// the generic decode of ss2_decode.cuh. The XYB transform of two pixels runs
-// on Blackwell's two-lane FP32 instructions, and its cube root is the shared
-// deterministic one (ss2_detmath.h) evaluated lane by lane with the same
-// operations, so the planes this kernel writes are bit-identical to the CPU
-// checker's.
+// Two kernels: 8-bit grey/RGB without alpha decode through the image's
+// 256-entry table in shared memory, reading four samples of a row with one
+// 32-bit load where the planes allow it; every other format runs the decode
+// of ss2_decode.cuh, whose YUV fast path (integer YUV, power-law transfer)
+// stages the tile's chroma window in shared memory first. Images whose
+// linear samples the host has proved non-negative run a body whose cube
+// roots skip their range check (the same values). The XYB transform of two
+// pixels runs on Blackwell's two-lane FP32 instructions, and its cube root is
+// the shared deterministic one (ss2_detmath.h) evaluated lane by lane with
+// the same operations, so the planes this kernel writes are bit-identical to
+// the CPU checker's.
 
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
