@@ -102,16 +102,7 @@ public:
         o.ptr_ = nullptr;
         o.bytes_ = 0;
     }
-    DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
-        if (this != &o) {
-            reset();
-            ptr_ = o.ptr_;
-            bytes_ = o.bytes_;
-            o.ptr_ = nullptr;
-            o.bytes_ = 0;
-        }
-        return *this;
-    }
+    DeviceBuffer& operator=(DeviceBuffer&&) = delete;
     ~DeviceBuffer() { reset(); }
     void reset() {
         if (ptr_) cudaFree(ptr_);
