@@ -408,8 +408,27 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
             float2 xyb[3];
             Xyb2<kInRange>(make_float2(l1[0][0], l1[1][0]), make_float2(l1[0][1], l1[1][1]),
                            make_float2(l1[0][2], l1[1][2]), lv.mask[1], xyb);
-            StorePixel<kHalf>(lv, 1, bx0, by, xyb[0].x, xyb[1].x, xyb[2].x);
-            StorePixel<kHalf>(lv, 1, bx0 + 1, by, xyb[0].y, xyb[1].y, xyb[2].y);
+            // Rows by and by ^ 1 of the row pair belong to lanes l and l ^ 16
+            // of the same warp. Where the pair's 2x2 block is inside the
+            // level and X and Y are its kept channels, each channel's block
+            // is one float4 of the row-pair plane: the even row's thread
+            // stores X and the odd row's Y, each taking the other row's
+            // values of its channel from its partner lane.
+            const bool odd = (by & 1u) != 0;
+            const float2 send = odd ? xyb[0] : xyb[1];
+            const float2 recv = make_float2(__shfl_xor_sync(0xffffffffu, send.x, 16),
+                                            __shfl_xor_sync(0xffffffffu, send.y, 16));
+            const uint32_t y0 = by & ~1u;
+            if (!kHalf && lv.mask[1] == 3u && bx0 + 1 < lv.w[1] && y0 + 1 < lv.h[1]) {
+                const float2 own = odd ? xyb[1] : xyb[0];
+                const float4 v = odd ? make_float4(recv.x, own.x, recv.y, own.y)
+                                     : make_float4(own.x, recv.x, own.y, recv.y);
+                float* plane = static_cast<float*>(lv.plane[1][odd ? 1 : 0]);
+                *reinterpret_cast<float4*>(plane + PlaneIndex(lv.pitch[1], bx0, y0)) = v;
+            } else {
+                StorePixel<kHalf>(lv, 1, bx0, by, xyb[0].x, xyb[1].x, xyb[2].x);
+                StorePixel<kHalf>(lv, 1, bx0 + 1, by, xyb[0].y, xyb[1].y, xyb[2].y);
+            }
             if (last >= 2) {
                 const uint32_t at = (ty + 16 * vy) * kBlocks + 2 * tx;
 #pragma unroll
