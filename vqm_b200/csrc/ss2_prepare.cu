@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
     PrepareKernel(DevBatch batch) {
     // Level-1 tile (32x32) of each channel, then the levels after it in two
     // alternating buffers: odd levels in `ladder_a`, even ones in `ladder_b`.
-    __shared__ float ladder_a[3][kBlocks * kBlocks];
+    __shared__ __align__(16) float ladder_a[3][kBlocks * kBlocks];
     __shared__ float ladder_b[3][kBlocks * kBlocks / 4];
     __shared__ float lut[256];
     __shared__ DevSource src_s;
@@ -430,12 +430,10 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
                 StorePixel<kHalf>(lv, 1, bx0 + 1, by, xyb[0].y, xyb[1].y, xyb[2].y);
             }
             if (last >= 2) {
-                const uint32_t at = (ty + 16 * vy) * kBlocks + 2 * tx;
+                const uint32_t at = (ty + 16 * vy) * kBlocks + 2 * tx;  // even
 #pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    ladder_a[c][at] = l1[0][c];
-                    ladder_a[c][at + 1] = l1[1][c];
-                }
+                for (int c = 0; c < 3; ++c)
+                    *reinterpret_cast<float2*>(&ladder_a[c][at]) = make_float2(l1[0][c], l1[1][c]);
             }
         }
     }
