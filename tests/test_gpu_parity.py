@@ -346,6 +346,26 @@ def test_pool_score_many_in_order():
         assert abs(s - want) <= helpers.SCORE_TOL
 
 
+def test_pool_streams_lists_in_any_order():
+    """Lists submitted back to back (the second before the first's results
+    are taken) give the same results as one list at a time, in either order
+    of taking them."""
+    a = [synthetic.rgb_pair(200 + 10 * i, 120, 70 + i)[:2] for i in range(5)]
+    b = [synthetic.yuv_pair(160, 90 + 2 * i, 80 + i)[:2] for i in range(3)]
+    pool = ss2.Ssimulacra2Pool(workers=2, chunk=2)
+    want_a, want_b = pool.compute_many(a), pool.compute_many(b)
+    ta, tb = pool.submit_many(a), pool.submit_many(b)
+    got_b, got_a = pool.results(tb), pool.results(ta)
+    for got, want in ((got_a, want_a), (got_b, want_b)):
+        assert len(got) == len(want)
+        for g, w in zip(got, want):
+            assert np.array_equal(g.norms, w.norms) and g.device_score == w.device_score
+    assert pool.results(pool.submit_many([])) == []
+    with pytest.raises(ss2.InvalidArgument):
+        pool.results(ta)  # already taken
+    pool.close()
+
+
 def test_resident_and_streaming_agree_bitwise():
     o, d = helpers.plain_256_pair()
     with ss2.Ssimulacra2Pipeline(256, 256, gpu_resident_images=2) as p:

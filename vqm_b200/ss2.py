@@ -15,6 +15,7 @@ CPU fallback: without the compiled extension, importing this module fails.
 
 from __future__ import annotations
 
+import collections
 import ctypes
 import os
 from dataclasses import dataclass, field
@@ -691,7 +692,14 @@ class Ssimulacra2Pool:
     launch per stage; chunks go to the workers in turn, each worker with at
     most one chunk in flight, so one chunk's host-to-device copies overlap
     the previous chunk's kernels. If a submission fails, the chunks already
-    submitted are drained before the error propagates (pool.cc:64-112)."""
+    submitted are drained before the error propagates (pool.cc:64-112).
+
+    ``compute_many`` is ``results(submit_many(...))``. A caller streaming
+    lists through the pool can ``submit_many`` the next list before taking
+    the ``results`` of the previous one: its chunks then go to the workers as
+    the previous list's chunks finish, so the copies never wait for the end
+    of a list. The pairs of a list stay referenced until its results are
+    taken."""
 
     def __init__(self, workers: int = 1, chunk: int = 64, chroma_filter: int = 0,
                  device: int = -1):
@@ -700,6 +708,12 @@ class Ssimulacra2Pool:
         self._chunk = max(1, chunk)
         self._batches = [Ssimulacra2Batch(max_pairs=self._chunk, chroma_filter=chroma_filter,
                                           device=device) for _ in range(workers)]
+        self._queue = collections.deque()     # (ticket, first, pairs, background) not submitted
+        self._inflight = collections.deque()  # (worker, token, ticket, first, pairs) in order
+        self._busy = [False] * workers
+        self._next = 0                        # next worker in turn
+        self._lists = {}                      # ticket -> [results, chunks left]
+        self._tickets = 0
 
     def workers(self) -> int:
         return len(self._batches)
@@ -708,38 +722,74 @@ class Ssimulacra2Pool:
         for b in self._batches:
             b.close()
 
-    def compute_many(self, pairs: Iterable, background: float = 0.5):
+    def _pump(self):
+        """Submits queued chunks while the next worker in turn is free."""
+        while self._queue and not self._busy[self._next]:
+            ticket, first, pairs, background = self._queue[0]
+            w = self._next
+            # The pairs stay referenced until drained, so the copies may run
+            # behind the call: chunks' uploads queue back to back.
+            token = self._batches[w].submit(pairs, background, borrow=True)
+            self._queue.popleft()
+            self._busy[w] = True
+            self._inflight.append((w, token, ticket, first, pairs))
+            self._next = (w + 1) % len(self._batches)
+
+    def _finish_oldest(self):
+        w, token, ticket, first, _ = self._inflight.popleft()
+        self._busy[w] = False
+        results = self._batches[w].finish(token)
+        entry = self._lists[ticket]
+        entry[0][first:first + len(results)] = results
+        entry[1] -= 1
+
+    def _drain(self):
+        while self._inflight:
+            try:
+                self._finish_oldest()
+            except Exception:
+                pass
+
+    def submit_many(self, pairs: Iterable, background: float = 0.5) -> int:
+        """Queues a list of pairs; returns the ticket for ``results``."""
         pairs = list(pairs)
-        out = [None] * len(pairs)
-        pending = [None] * len(self._batches)  # (token, first index) per worker
-
-        def drain(w):
-            if pending[w] is not None:
-                token, first = pending[w]
-                pending[w] = None
-                for k, r in enumerate(self._batches[w].finish(token)):
-                    out[first + k] = r
-
-        w = 0
+        ticket = self._tickets
+        self._tickets += 1
+        chunks = range(0, len(pairs), self._chunk)
+        self._lists[ticket] = [[None] * len(pairs), len(chunks)]
+        for first in chunks:
+            self._queue.append((ticket, first, pairs[first:first + self._chunk], background))
         try:
-            for first in range(0, len(pairs), self._chunk):
-                drain(w)
-                # The pairs stay referenced until drained, so the copies may
-                # run behind the call: chunks' uploads queue back to back.
-                token = self._batches[w].submit(pairs[first:first + self._chunk], background,
-                                                borrow=True)
-                pending[w] = (token, first)
-                w = (w + 1) % len(self._batches)
-            for k in range(len(self._batches)):
-                drain((w + k) % len(self._batches))
+            self._pump()
         except BaseException:
-            for k in range(len(self._batches)):
-                try:
-                    drain(k)
-                except Exception:
-                    pass
+            self._abort()
             raise
-        return out
+        return ticket
+
+    def results(self, ticket: int) -> list:
+        """The list's results in input order (waits for its chunks)."""
+        if ticket not in self._lists:
+            raise InvalidArgument("pool: no list with that ticket")
+        try:
+            while self._lists[ticket][1] > 0:
+                if not self._inflight:
+                    self._pump()
+                self._finish_oldest()
+                self._pump()
+        except BaseException:
+            self._abort()
+            raise
+        return self._lists.pop(ticket)[0]
+
+    def _abort(self):
+        """After a failure: drains what is in flight and drops every list."""
+        self._drain()
+        self._queue.clear()
+        self._busy = [False] * len(self._batches)
+        self._lists.clear()
+
+    def compute_many(self, pairs: Iterable, background: float = 0.5):
+        return self.results(self.submit_many(pairs, background))
 
     def score_many(self, pairs: Iterable, background: float = 0.5):
         return [r.score() for r in self.compute_many(pairs, background)]
