@@ -255,6 +255,8 @@ def run_reference(args):
 #                      RGB pairs, one batch (one launch per stage)
 #   --workload serve   Poisson request streams through the serving loop
 #   --workload video   240 frame pairs of 3840x2160 10-bit 4:2:0, per frame
+#   --workload plain256  one 256x256 8-bit sRGB pair per call (launch-bound:
+#                      latency), device-resident and from host memory
 # ---------------------------------------------------------------------------
 
 
@@ -526,6 +528,45 @@ def run_video(args):
     return 0
 
 
+def run_plain256(args):
+    """The single small pair: latency of one call through the pipeline
+    (its kernels replay as one CUDA graph), resident and from host memory,
+    and the CPU port's time for the same pair."""
+    import torch
+    from vqm_b200 import ss2, synthetic
+    torch.cuda.set_device(0)
+    o, d = synthetic.pair_plain_256(0)
+    dev = to_device([(o, d)])[0]
+    host = pinned([(o, d)])[0]
+    pipe = ss2.Ssimulacra2Pipeline(256, 256)
+    out = {}
+    for name, pair in (("resident", dev), ("host", host)):
+        for _ in range(20):
+            pipe.compute(*pair)
+        torch.cuda.synchronize()
+        lat = []
+        for _ in range(max(200, args.steps * 20)):
+            t0 = time.perf_counter()
+            score = pipe.compute(*pair).score()
+            lat.append(1e3 * (time.perf_counter() - t0))
+        out[name] = {"latency_ms_p50": float(np.percentile(lat, 50)),
+                     "latency_ms_p99": float(np.percentile(lat, 99)),
+                     "pairs_per_s": 1e3 / float(np.mean(lat)), "score": score}
+    from oracle import binding as ob
+    from tests.helpers import to_oracle
+    t0 = time.perf_counter()
+    reps = 5
+    for _ in range(reps):
+        ob.compute(to_oracle(o), to_oracle(d))
+    cpu_ms = 1e3 * (time.perf_counter() - t0) / reps
+    print(json.dumps({"workload": "plain256", **out,
+                      "cpu_port_ms": cpu_ms, "cpu_port_threads": 1,
+                      "config": "one 256x256 8-bit sRGB pair (seeded texture, noise sigma 4, "
+                                "8x8 quantisation step 16), one pipeline call per pair"}),
+          flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -543,7 +584,7 @@ def main(argv=None):
     ap.add_argument("--streams", type=int, default=1, choices=[1, 2],
                     help="streams for the two alternating batch scorers")
     ap.add_argument("--workload", default="plain1080",
-                    choices=["plain1080", "uneven", "serve", "video"])
+                    choices=["plain1080", "uneven", "serve", "video", "plain256"])
     ap.add_argument("--rates", default="200,500,1000,2000", help="serve: requests/s")
     ap.add_argument("--duration", type=float, default=10.0, help="serve: seconds per rate")
     ap.add_argument("--serve-workers", type=int, default=3)
@@ -558,7 +599,8 @@ def main(argv=None):
     if args.impl == "reference":
         return run_reference(args)
     if args.workload != "plain1080":
-        return {"uneven": run_uneven, "serve": run_serve, "video": run_video}[args.workload](args)
+        return {"uneven": run_uneven, "serve": run_serve, "video": run_video,
+                "plain256": run_plain256}[args.workload](args)
 
     rank, world, local = rank_env()
     pairs = make_pairs(args.pairs, WIDTH, HEIGHT, SEED0 + 100_000 * rank)
