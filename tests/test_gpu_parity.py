@@ -175,7 +175,8 @@ def test_plain_256_pair():
         assert np.array_equal(r.norms, again.norms)
 
 
-@pytest.mark.parametrize("w,h", [(1920, 1080), (333, 187), (1001, 77), (640, 361)])
+@pytest.mark.parametrize("w,h", [(1920, 1080), (333, 187), (1001, 77), (640, 361),
+                                 (2000, 9), (8, 1500)])
 def test_rgb8_sizes(w, h):
     o, d, kind = synthetic.rgb_pair(w, h, seed=w * 7 + h)
     with ss2.Ssimulacra2Pipeline(w, h) as p:

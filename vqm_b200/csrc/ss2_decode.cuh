@@ -373,8 +373,12 @@ __device__ __forceinline__ void BlockLinearGeneric(const DevSource& s, uint32_t 
 // ss2dm::powf_gamma of two lanes with the same y, the floating-point steps
 // two lanes per instruction (FFMA2 / FMUL2 / FADD2), each the operation the
 // scalar function performs on that lane: the same values. A lane outside the
-// function's fast range sends both through the scalar function.
-__device__ __forceinline__ float2 PowfGamma2(float2 x, float y) {
+// function's fast range sends both through the scalar function. `logt` and
+// `expt` are copies of the function's two tables (kLogF4, kExpF2) in shared
+// memory: each lane's entry depends on its value, and divergent entries of a
+// shared-memory table cost fewer cycles than the same loads through L1.
+__device__ __forceinline__ float2 PowfGamma2(float2 x, float y, const float4* logt,
+                                             const float2* expt) {
     using namespace ss2dm;
     if (!(powf_gamma_fast(x.x, y) && powf_gamma_fast(x.y, y)))
         return make_float2(powf_gamma(x.x, y), powf_gamma(x.y, y));
@@ -384,8 +388,8 @@ __device__ __forceinline__ float2 PowfGamma2(float2 x, float y) {
     const int i0 = static_cast<int>((ix0 >> 16) & 127u), i1 = static_cast<int>((ix1 >> 16) & 127u);
     const float2 m = make_float2(__uint_as_float((ix0 & 0x007fffffu) | 0x3f800000u),
                                  __uint_as_float((ix1 & 0x007fffffu) | 0x3f800000u));
-    const LogEntryF L0 = LogF(i0), L1 = LogF(i1);
-    const float2 inv = make_float2(L0.inv, L1.inv);
+    const float4 L0 = logt[i0], L1 = logt[i1];  // inv, hi, lo, 0
+    const float2 inv = make_float2(L0.x, L1.x);
     const float2 p = __fmul2_rn(m, inv);
     const float2 pe = __ffma2_rn(m, inv, N(p));
     const float2 rh = __fadd2_rn(p, P(-1.0f));
@@ -394,8 +398,8 @@ __device__ __forceinline__ float2 PowfGamma2(float2 x, float y) {
                                  __ffma2_rn(__fmul2_rn(rh, rh), poly, __fmul2_rn(P(kGammaK1), pe)));
     const float2 ef = make_float2(static_cast<float>(static_cast<int>(ix0 >> 23) - 127),
                                   static_cast<float>(static_cast<int>(ix1 >> 23) - 127));
-    const float2 lh = make_float2(L0.hi, L1.hi);
-    const float2 ll = make_float2(L0.lo, L1.lo);
+    const float2 lh = make_float2(L0.y, L1.y);
+    const float2 ll = make_float2(L0.z, L1.z);
     const float2 hi = __fadd2_rn(ef, lh);
     const float2 lo = __fadd2_rn(__fadd2_rn(__fadd2_rn(ef, N(hi)), lh), __fadd2_rn(ll, lr));
     const float2 th = __fmul2_rn(P(y), hi);
@@ -406,9 +410,9 @@ __device__ __forceinline__ float2 PowfGamma2(float2 x, float y) {
     const float2 q = __ffma2_rn(__ffma2_rn(z, P(kGammaSixth), P(0.5f)), __fmul2_rn(z, z), z);
     const int k0 = static_cast<int>(kf.x), k1i = static_cast<int>(kf.y);
     const int j0 = k0 & 63, j1 = k1i & 63;
-    const ExpEntryF T0 = ExpF(j0), T1 = ExpF(j1);
-    const float2 tj = make_float2(T0.hi, T1.hi);
-    const float2 tjl = make_float2(T0.lo, T1.lo);
+    const float2 T0 = expt[j0], T1 = expt[j1];  // hi, lo
+    const float2 tj = make_float2(T0.x, T1.x);
+    const float2 tjl = make_float2(T0.y, T1.y);
     const float2 r = __fadd2_rn(tj, __ffma2_rn(tj, q, tjl));
     return __fmul2_rn(r, make_float2(__uint_as_float(static_cast<uint32_t>((k0 >> 6) + 127) << 23),
                                      __uint_as_float(static_cast<uint32_t>((k1i >> 6) + 127) << 23)));
@@ -487,6 +491,7 @@ __device__ __forceinline__ void ChromaFixed(const float* stage, int bxs, int bys
 // with the format's branches resolved and the chroma taps read from the
 // staged window at the host's per-parity slots and weights.
 __device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* stage,
+                                               const float4* logt, const float2* expt,
                                                uint32_t gx, uint32_t gy, uint32_t bx,
                                                uint32_t by, bool aligned4, float rgb[4][3]) {
     const uint32_t x0 = 2 * bx, y0 = 2 * by;
@@ -582,7 +587,8 @@ __device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* 
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const float a = e[h][c], b = e[h + 1][c];
-            const float2 r = PowfGamma2(make_float2(a > 0.0f ? a : 1.0f, b > 0.0f ? b : 1.0f), g);
+            const float2 r =
+                PowfGamma2(make_float2(a > 0.0f ? a : 1.0f, b > 0.0f ? b : 1.0f), g, logt, expt);
             e[h][c] = a > 0.0f ? r.x : 0.0f;
             e[h + 1][c] = b > 0.0f ? r.y : 0.0f;
         }

@@ -252,8 +252,11 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
     __shared__ DevSource src_s;
     __shared__ LevelInfo lv;
     __shared__ uint32_t aligned4;
-    // Both chroma planes' window of the tile, for yuv_fast images.
+    // Both chroma planes' window of the tile, for yuv_fast images, and the
+    // power's tables.
     __shared__ float chroma_stage[kTable ? 1 : 2 * kChromaStage];
+    __shared__ float4 pow_log[kTable ? 1 : 128];
+    __shared__ float2 pow_exp[kTable ? 1 : 64];
 
     const uint32_t tid = threadIdx.x;
     const int group = kTable ? 0 : 1;
@@ -274,6 +277,8 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
         constexpr uint32_t words = offsetof(DevSource, srgb_lut) / 4;
         for (uint32_t i = tid; i < words; i += kThreads) to[i] = from[i];
         if (kTable) lut[tid] = P.src[image].srgb_lut[tid];
+        if (!kTable && tid < 128) pow_log[tid] = __ldg(&ss2dm::kLogF4Dev[tid]);
+        if (!kTable && tid < 64) pow_exp[tid] = __ldg(&ss2dm::kExpF2Dev[tid]);
         if (tid < kMaxLevels * 3) {
             const uint32_t l = tid / 3, c = tid % 3;
             const bool kept = l < P.levels && (P.mask[l] & (1u << c));
@@ -365,7 +370,8 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
                     TableBlock(s, lut, fast, w4, hx, bx, by, lin);
                 } else {
                     if (s.yuv_fast && 2 * bx + 1 < width && 2 * by + 1 < height)
-                        BlockLinearYuv(s, chroma_stage, gx, gy, bx, by, aligned4 != 0, lin);
+                        BlockLinearYuv(s, chroma_stage, pow_log, pow_exp, gx, gy, bx, by,
+                                       aligned4 != 0, lin);
                     else
                         BlockLinearGeneric(s, bx, by, lin);
                 }
