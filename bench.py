@@ -511,6 +511,25 @@ def run_video(args):
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         out[name] = {"frames_per_s": count / dt, "clip_mean_score": float(np.mean(scores))}
+    # Streaming through two pipelines in turn: frame i + 1's upload (on one
+    # pipeline's stream) runs while frame i's kernels run on the other's.
+    pipes = [pipe, ss2.Ssimulacra2Pipeline(w, h)]
+    for o, d in host[:3]:
+        pipes[1].compute(o, d)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pending, scores = [], []
+    for i, (o, d) in enumerate(host):
+        if len(pending) == 2:
+            p, tok = pending.pop(0)
+            scores.append(p.finish(tok).score())
+        p = pipes[i % 2]
+        pending.append((p, p.submit(o, d)))
+    for p, tok in pending:
+        scores.append(p.finish(tok).score())
+    dt = time.perf_counter() - t0
+    out["streaming_two_pipelines"] = {"frames_per_s": count / dt,
+                                      "clip_mean_score": float(np.mean(scores))}
     # The same frames as batches of 8 (one launch per stage per 8 frames).
     batch = ss2.Ssimulacra2Batch(max_pairs=8)
     batch.compute_many(dev[:8])  # warm-up: allocation and first kernel loads
