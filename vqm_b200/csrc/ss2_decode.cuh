@@ -396,26 +396,34 @@ __device__ __forceinline__ float2 PowfGamma2(float2 x, float y, const float4* lo
     const float2 poly = __ffma2_rn(__ffma2_rn(rh, P(kGammaK4), P(kGammaK3)), rh, P(kGammaK2));
     const float2 lr = __ffma2_rn(P(kGammaK1), rh,
                                  __ffma2_rn(__fmul2_rn(rh, rh), poly, __fmul2_rn(P(kGammaK1), pe)));
-    const float2 ef = make_float2(static_cast<float>(static_cast<int>(ix0 >> 23) - 127),
-                                  static_cast<float>(static_cast<int>(ix1 >> 23) - 127));
+    // e = (ix >> 23) - 127 as a float without a conversion: 2^23 + (ix >> 23)
+    // is a float's bit pattern, and subtracting 2^23 + 127 is exact.
+    const float2 ef = __fadd2_rn(make_float2(__uint_as_float(0x4b000000u | (ix0 >> 23)),
+                                             __uint_as_float(0x4b000000u | (ix1 >> 23))),
+                                 P(-8388735.0f));
     const float2 lh = make_float2(L0.y, L1.y);
     const float2 ll = make_float2(L0.z, L1.z);
     const float2 hi = __fadd2_rn(ef, lh);
     const float2 lo = __fadd2_rn(__fadd2_rn(__fadd2_rn(ef, N(hi)), lh), __fadd2_rn(ll, lr));
     const float2 th = __fmul2_rn(P(y), hi);
     const float2 tl = __ffma2_rn(P(y), lo, __ffma2_rn(P(y), hi, N(th)));
-    const float2 kf = __fadd2_rn(__ffma2_rn(th, P(64.0f), P(12582912.0f)), P(-12582912.0f));
+    // big = 1.5 2^23 + k, k = round(64 th), |k| < 2^13: its bit pattern is
+    // 0x4b400000 + k, so k's table index and exponent come from the bits (no
+    // conversion), and the table load issues before z and q are formed.
+    const float2 big = __ffma2_rn(th, P(64.0f), P(12582912.0f));
+    const uint32_t u0 = __float_as_uint(big.x), u1 = __float_as_uint(big.y);
+    const float2 T0 = expt[u0 & 63u], T1 = expt[u1 & 63u];  // hi, lo of 2^(j/64)
+    const float2 kf = __fadd2_rn(big, P(-12582912.0f));
     const float2 z = __ffma2_rn(__ffma2_rn(kf, P(-0.015625f), th), P(kGammaLn2),
                                 __fmul2_rn(tl, P(kGammaLn2)));
     const float2 q = __ffma2_rn(__ffma2_rn(z, P(kGammaSixth), P(0.5f)), __fmul2_rn(z, z), z);
-    const int k0 = static_cast<int>(kf.x), k1i = static_cast<int>(kf.y);
-    const int j0 = k0 & 63, j1 = k1i & 63;
-    const float2 T0 = expt[j0], T1 = expt[j1];  // hi, lo
     const float2 tj = make_float2(T0.x, T1.x);
     const float2 tjl = make_float2(T0.y, T1.y);
     const float2 r = __fadd2_rn(tj, __ffma2_rn(tj, q, tjl));
-    return __fmul2_rn(r, make_float2(__uint_as_float(static_cast<uint32_t>((k0 >> 6) + 127) << 23),
-                                     __uint_as_float(static_cast<uint32_t>((k1i >> 6) + 127) << 23)));
+    // 2^(k >> 6) = bits ((k >> 6) + 127) << 23, with k + 127 * 64 = u -
+    // 0x4b3fe040 in [448, 10176] over the fast range (t in [-120, 32]).
+    return __fmul2_rn(r, make_float2(__uint_as_float(((u0 - 0x4b3fe040u) << 17) & 0xff800000u),
+                                     __uint_as_float(((u1 - 0x4b3fe040u) << 17) & 0xff800000u)));
 }
 
 // The YUV fast path (DevSource::yuv_fast): the CTA's chroma window of both
