@@ -117,17 +117,22 @@ struct DevPrepItem {
     uint32_t image;
 };
 
+// The prepare kernels, one per decode: 8-bit images by table (group 0),
+// yuv_fast images (group 1), every other format (group 2).
+constexpr int kPrepGroups = 3;
+inline int PrepGroup(const DevSource& s) { return s.lut ? 0 : (s.yuv_fast ? 1 : 2); }
+
 struct DevBatch {
     uint32_t pairs;
     uint32_t segments;
-    uint32_t prep_items[2];   // table-decoded images, generic images
-    uint32_t prep_blocks[2];  // 32x32 base tiles in each group
+    uint32_t prep_items[kPrepGroups];   // images in each prepare group
+    uint32_t prep_blocks[kPrepGroups];  // 64x64 base tiles in each group
     uint32_t blur_blocks;     // sum over segments of tiles
     const DevPair* pair;
     const DevSegment* seg;
-    const DevPrepItem* prep_item;  // group 0 then group 1
-    // Prefix tile offsets: group 0 (prep_items[0] + 1 entries) then group 1
-    // (prep_items[1] + 1 entries).
+    const DevPrepItem* prep_item;  // group 0, then group 1, then group 2
+    // Prefix tile offsets, each group's prep_items[g] + 1 entries in group
+    // order.
     const uint32_t* prep_start;
     const uint32_t* blur_start;  // segments + 1 prefix offsets
     double* partials;            // 6 doubles per blur tile

@@ -60,7 +60,7 @@ struct PairTables {
     DevPair pair;
     DevSegment seg[kMaxSegments];
     DevPrepItem item[2];
-    uint32_t prep_start[4];
+    uint32_t prep_start[2 + kPrepGroups];
     uint32_t blur_start[kMaxSegments + 1];
 };
 static_assert(sizeof(PairTables) < 30000, "kernel parameter space");
@@ -212,21 +212,22 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
     P.pyramid = reinterpret_cast<float*>(base + off_pyramid);
     P.result = result;
 
-    // Prepare lists: images decoded by table first, then the generic ones.
+    // Prepare lists: the two images by prepare group (table, YUV, generic),
+    // each group's prefix offsets after the previous group's.
     const uint32_t per_image = P.prep_tiles_x * P.prep_tiles_y;
-    uint32_t n[2] = {0, 0};
-    const bool lut[2] = {P.src[0].lut != 0, P.src[1].lut != 0};
-    for (uint32_t k = 0; k < 2; ++k) ++n[lut[k] ? 0 : 1];
-    uint32_t at[2] = {0, n[0]};
-    t.prep_start[0] = 0;
-    t.prep_start[n[0] + 1] = 0;
-    for (uint32_t k = 0; k < 2; ++k) {
-        const int g = lut[k] ? 0 : 1;
-        const uint32_t idx = at[g]++;
-        t.item[idx] = DevPrepItem{0, k};
-        const uint32_t first = g ? n[0] + 1 : 0;
-        const uint32_t pos = idx - (g ? n[0] : 0);
-        t.prep_start[first + pos + 1] = t.prep_start[first + pos] + per_image;
+    const int group[2] = {PrepGroup(P.src[0]), PrepGroup(P.src[1])};
+    uint32_t n[kPrepGroups] = {};
+    for (uint32_t k = 0; k < 2; ++k) ++n[group[k]];
+    uint32_t item = 0, entry = 0;
+    for (int g = 0; g < kPrepGroups; ++g) {
+        t.prep_start[entry] = 0;
+        for (uint32_t k = 0; k < 2; ++k) {
+            if (group[k] != g) continue;
+            t.item[item++] = DevPrepItem{0, k};
+            t.prep_start[entry + 1] = t.prep_start[entry] + per_image;
+            ++entry;
+        }
+        ++entry;
     }
 
     PairTables* dev_tables = reinterpret_cast<PairTables*>(base + off_tables);
@@ -234,10 +235,10 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
     DevBatch b{};
     b.pairs = 1;
     b.segments = nseg;
-    b.prep_items[0] = n[0];
-    b.prep_items[1] = n[1];
-    b.prep_blocks[0] = n[0] * per_image;
-    b.prep_blocks[1] = n[1] * per_image;
+    for (int g = 0; g < kPrepGroups; ++g) {
+        b.prep_items[g] = n[g];
+        b.prep_blocks[g] = n[g] * per_image;
+    }
     b.blur_blocks = blocks;
     b.pair = &dev_tables->pair;
     b.seg = dev_tables->seg;

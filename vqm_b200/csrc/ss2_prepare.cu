@@ -235,34 +235,47 @@ __device__ __forceinline__ void TableBlock(const DevSource& s, const float* lut,
     }
 }
 
-// Five CTAs (40 warps) per SM for the table decode, four for the generic
-// one: its long FP64 transfer chains want the warps more than the registers
-// (measured: 4 CTAs with some spilling beat 2 without by a quarter).
+// CTAs per SM: five (40 warps) for the table and YUV decodes, four for the
+// generic one. The decodes' long dependency chains (the YUV power's table
+// loads, the generic FP64 transfers) want the warps more than the registers
+// (measured on 136 uneven pairs: the YUV kernel at 5 CTAs with some spilling
+// takes 8.48 ms, at 4 9.33 ms, and 8.93 ms with its generic blocks (past an
+// odd last column or row) as an out-of-line call; the generic decode at 4
+// beats 2 by a quarter).
 #ifndef VQM_GENERIC_PREPARE_CTAS
 #define VQM_GENERIC_PREPARE_CTAS 4
 #endif
-template <bool kTable, bool kHalf>
-__global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTAS)
+#ifndef VQM_YUV_PREPARE_CTAS
+#define VQM_YUV_PREPARE_CTAS 5
+#endif
+template <int kGroup, bool kHalf>
+__global__ void __launch_bounds__(kThreads, kGroup == 0   ? 5
+                                            : kGroup == 1 ? VQM_YUV_PREPARE_CTAS
+                                                          : VQM_GENERIC_PREPARE_CTAS)
     PrepareKernel(DevBatch batch) {
+    constexpr bool kTable = kGroup == 0;  // 8-bit RGB/grey by table
+    constexpr bool kYuv = kGroup == 1;    // yuv_fast images
     // Level-1 tile (32x32) of each channel, then the levels after it in two
     // alternating buffers: odd levels in `ladder_a`, even ones in `ladder_b`.
     __shared__ __align__(16) float ladder_a[3][kBlocks * kBlocks];
     __shared__ float ladder_b[3][kBlocks * kBlocks / 4];
-    __shared__ float lut[256];
+    __shared__ float lut[kTable ? 256 : 1];
     __shared__ DevSource src_s;
     __shared__ LevelInfo lv;
     __shared__ uint32_t aligned4;
     // Both chroma planes' window of the tile, for yuv_fast images, and the
     // power's tables.
-    __shared__ float chroma_stage[kTable ? 1 : 2 * kChromaStage];
-    __shared__ float4 pow_log[kTable ? 1 : 128];
-    __shared__ float2 pow_exp[kTable ? 1 : 64];
+    __shared__ float chroma_stage[kYuv ? 2 * kChromaStage : 1];
+    __shared__ float4 pow_log[kYuv ? 128 : 1];
+    __shared__ float2 pow_exp[kYuv ? 64 : 1];
 
     const uint32_t tid = threadIdx.x;
-    const int group = kTable ? 0 : 1;
-    const uint32_t n_items = batch.prep_items[group];
-    const DevPrepItem* items = batch.prep_item + (kTable ? 0 : batch.prep_items[0]);
-    const uint32_t* start = batch.prep_start + (kTable ? 0 : batch.prep_items[0] + 1);
+    const uint32_t n_items = batch.prep_items[kGroup];
+    uint32_t before = 0;  // images in the groups ahead of this one
+#pragma unroll
+    for (int g = 0; g < kGroup; ++g) before += batch.prep_items[g];
+    const DevPrepItem* items = batch.prep_item + before;
+    const uint32_t* start = batch.prep_start + before + kGroup;
     const uint32_t it = FindSlot(start, n_items, blockIdx.x);
     const DevPrepItem item = items[it];
     const DevPair& P = batch.pair[item.pair];
@@ -277,8 +290,8 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
         constexpr uint32_t words = offsetof(DevSource, srgb_lut) / 4;
         for (uint32_t i = tid; i < words; i += kThreads) to[i] = from[i];
         if (kTable) lut[tid] = P.src[image].srgb_lut[tid];
-        if (!kTable && tid < 128) pow_log[tid] = __ldg(&ss2dm::kLogF4Dev[tid]);
-        if (!kTable && tid < 64) pow_exp[tid] = __ldg(&ss2dm::kExpF2Dev[tid]);
+        if (kYuv && tid < 128) pow_log[tid] = __ldg(&ss2dm::kLogF4Dev[tid]);
+        if (kYuv && tid < 64) pow_exp[tid] = __ldg(&ss2dm::kExpF2Dev[tid]);
         if (tid < kMaxLevels * 3) {
             const uint32_t l = tid / 3, c = tid % 3;
             const bool kept = l < P.levels && (P.mask[l] & (1u << c));
@@ -309,8 +322,8 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
     const auto body = [=](auto in_range) {
     constexpr bool kInRange = decltype(in_range)::value;
     const DevSource& s = src_s;
-    if constexpr (!kTable) {
-        if (s.yuv_fast && s.chroma_variant) {
+    if constexpr (kYuv) {
+        if (s.chroma_variant) {
             StageChroma(s, gx, gy, chroma_stage);
             __syncthreads();
         }
@@ -368,12 +381,14 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
             if (in_block) {
                 if constexpr (kTable) {
                     TableBlock(s, lut, fast, w4, hx, bx, by, lin);
-                } else {
-                    if (s.yuv_fast && 2 * bx + 1 < width && 2 * by + 1 < height)
+                } else if constexpr (kYuv) {
+                    if (2 * bx + 1 < width && 2 * by + 1 < height)
                         BlockLinearYuv(s, chroma_stage, pow_log, pow_exp, gx, gy, bx, by,
                                        aligned4 != 0, lin);
                     else
                         BlockLinearGeneric(s, bx, by, lin);
+                } else {
+                    BlockLinearGeneric(s, bx, by, lin);
                 }
                 // Level 0: the block is one aligned float4 of the row-pair
                 // plane, (x0, y0), (x0, y0+1), (x0+1, y0), (x0+1, y0+1); a
@@ -497,23 +512,30 @@ __global__ void __launch_bounds__(kThreads, kTable ? 5 : VQM_GENERIC_PREPARE_CTA
 
 }  // namespace
 
-cudaError_t PreloadPrepare() {
+template <bool kHalf>
+cudaError_t PreloadPrepareOf() {
     cudaFuncAttributes a;
-    cudaError_t e = cudaFuncGetAttributes(&a, PrepareKernel<true, false>);
-    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, PrepareKernel<false, false>);
-    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, PrepareKernel<true, true>);
-    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, PrepareKernel<false, true>);
+    cudaError_t e = cudaFuncGetAttributes(&a, PrepareKernel<0, kHalf>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, PrepareKernel<1, kHalf>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, PrepareKernel<2, kHalf>);
     return e;
 }
+cudaError_t PreloadPrepare() {
+    const cudaError_t e = PreloadPrepareOf<false>();
+    return e == cudaSuccess ? PreloadPrepareOf<true>() : e;
+}
 
+template <bool kHalf>
+void LaunchPrepareOf(const DevBatch& b, cudaStream_t stream) {
+    if (b.prep_blocks[0]) PrepareKernel<0, kHalf><<<b.prep_blocks[0], kThreads, 0, stream>>>(b);
+    if (b.prep_blocks[1]) PrepareKernel<1, kHalf><<<b.prep_blocks[1], kThreads, 0, stream>>>(b);
+    if (b.prep_blocks[2]) PrepareKernel<2, kHalf><<<b.prep_blocks[2], kThreads, 0, stream>>>(b);
+}
 cudaError_t LaunchPrepare(const DevBatch& b, cudaStream_t stream) {
-    if (b.half) {
-        if (b.prep_blocks[0]) PrepareKernel<true, true><<<b.prep_blocks[0], kThreads, 0, stream>>>(b);
-        if (b.prep_blocks[1]) PrepareKernel<false, true><<<b.prep_blocks[1], kThreads, 0, stream>>>(b);
-    } else {
-        if (b.prep_blocks[0]) PrepareKernel<true, false><<<b.prep_blocks[0], kThreads, 0, stream>>>(b);
-        if (b.prep_blocks[1]) PrepareKernel<false, false><<<b.prep_blocks[1], kThreads, 0, stream>>>(b);
-    }
+    if (b.half)
+        LaunchPrepareOf<true>(b, stream);
+    else
+        LaunchPrepareOf<false>(b, stream);
     return cudaGetLastError();
 }
 

@@ -208,9 +208,9 @@ struct BlurShape {
 struct Tables {
     std::vector<DevPair> pairs;
     std::vector<DevSegment> segs;
-    std::vector<DevPrepItem> prep_items;  // table-decoded images, then generic
-    std::vector<uint32_t> prep_start;     // both groups' prefix offsets
-    uint32_t prep_count[2] = {0, 0}, prep_blocks[2] = {0, 0};
+    std::vector<DevPrepItem> prep_items;  // the images, by prepare group
+    std::vector<uint32_t> prep_start;     // every group's prefix offsets
+    uint32_t prep_count[kPrepGroups] = {}, prep_blocks[kPrepGroups] = {};
     std::vector<uint32_t> blur_start;
     std::vector<size_t> pyramid_first;  // float offset of each pair's planes
     size_t pyramid_floats = 0;
@@ -269,7 +269,7 @@ Tables BuildTables(const std::vector<std::pair<uint32_t, uint32_t>>& sizes, Blur
     if (prep > 0x7fffffffull || blur > 0x7fffffffull)
         throw std::invalid_argument("cuda: batch too large for one launch");
     t.prep_items.resize(2 * sizes.size());
-    t.prep_start.resize(2 * sizes.size() + 2);
+    t.prep_start.resize(2 * sizes.size() + kPrepGroups);
     return t;
 }
 
@@ -295,33 +295,36 @@ int DeviceSms(int device) {
     return sms;
 }
 
-// Splits the images into the table-decoded group and the generic group
-// (table[i][k]: image k of pair i decodes by table) and lays out each
-// group's prefix tile offsets. The list sizes do not depend on the split.
-// `skip_original`, when set, leaves every pair's image 0 out (its pyramid is
-// already in place).
-void BuildPrepLists(Tables& t, const std::vector<std::array<bool, 2>>& table,
-                    bool skip_original = false) {
-    uint32_t n[2] = {0, 0};
+// Splits the images into the prepare groups (group[i][k]: PrepGroup of
+// image k of pair i) and lays out each group's prefix tile offsets. The list
+// sizes do not depend on the split. `skip_original`, when set, leaves every
+// pair's image 0 out (its pyramid is already in place).
+using PrepGroups = std::vector<std::array<uint8_t, 2>>;
+void BuildPrepLists(Tables& t, const PrepGroups& group, bool skip_original = false) {
+    uint32_t n[kPrepGroups] = {};
     for (size_t i = 0; i < t.pairs.size(); ++i)
-        for (int k = skip_original ? 1 : 0; k < 2; ++k) ++n[table[i][k] ? 0 : 1];
-    uint32_t at[2] = {0, n[0]};
-    uint32_t* start[2] = {t.prep_start.data(), t.prep_start.data() + n[0] + 1};
-    uint32_t blocks[2] = {0, 0};
-    start[0][0] = 0;
-    start[1][0] = 0;
+        for (int k = skip_original ? 1 : 0; k < 2; ++k) ++n[group[i][k]];
+    uint32_t first[kPrepGroups];   // the group's first item
+    uint32_t* start[kPrepGroups];  // the group's prefix offsets
+    uint32_t blocks[kPrepGroups] = {};
+    for (uint32_t g = 0, items = 0; g < kPrepGroups; items += n[g], ++g) {
+        first[g] = items;
+        start[g] = t.prep_start.data() + items + g;
+        start[g][0] = 0;
+    }
+    uint32_t at[kPrepGroups] = {};
     for (size_t i = 0; i < t.pairs.size(); ++i)
         for (uint32_t k = skip_original ? 1 : 0; k < 2; ++k) {
-            const int g = table[i][k] ? 0 : 1;
-            const uint32_t idx = at[g]++;
-            t.prep_items[idx] = DevPrepItem{static_cast<uint32_t>(i), k};
+            const int g = group[i][k];
+            const uint32_t pos = at[g]++;
+            t.prep_items[first[g] + pos] = DevPrepItem{static_cast<uint32_t>(i), k};
             blocks[g] += t.pairs[i].prep_tiles_x * t.pairs[i].prep_tiles_y;
-            start[g][idx - (g ? n[0] : 0) + 1] = blocks[g];
+            start[g][pos + 1] = blocks[g];
         }
-    t.prep_count[0] = n[0];
-    t.prep_count[1] = n[1];
-    t.prep_blocks[0] = blocks[0];
-    t.prep_blocks[1] = blocks[1];
+    for (int g = 0; g < kPrepGroups; ++g) {
+        t.prep_count[g] = n[g];
+        t.prep_blocks[g] = blocks[g];
+    }
 }
 
 // The device tables of one batch: one table allocation, its pinned mirror,
@@ -396,7 +399,7 @@ struct BatchMemory {
         uint8_t* h = table_host.as<uint8_t>();
         std::memcpy(h + off_items, t.prep_items.data(), sizeof(DevPrepItem) * t.prep_items.size());
         std::memcpy(h + off_prep, t.prep_start.data(), sizeof(uint32_t) * t.prep_start.size());
-        for (int g = 0; g < 2; ++g) {
+        for (int g = 0; g < kPrepGroups; ++g) {
             dev.prep_items[g] = t.prep_count[g];
             dev.prep_blocks[g] = t.prep_blocks[g];
         }
@@ -558,7 +561,7 @@ public:
             shape_ = BlurShape::Of(
                 AutoBlurVariant(DefaultTileCount({{cfg.width, cfg.height}}), DeviceSms(device_)));
         tables_ = BuildTables({{cfg.width, cfg.height}}, shape_);
-        BuildPrepLists(tables_, {{true, true}});
+        BuildPrepLists(tables_, {{0, 0}});
         mem_.Layout(tables_);
         mem_.Stage(tables_);
         VQM_CK(cudaMemcpy(mem_.table.as<void>(), mem_.table_host.as<void>(), mem_.table_bytes,
@@ -912,12 +915,13 @@ private:
     // prepare out (its pyramid is cached).
     uint64_t Launch(bool skip_original = false) {
         if (!skip_original) reference_valid_ = false;
-        // Which images decode by table, and whether the original is
-        // prepared, decide the prepare launches; one graph per combination.
+        // Each image's prepare group, and whether the original is prepared,
+        // decide the prepare launches; one graph per combination.
         const DevPair* hp = mem_.HostPair(0);
-        const int key = (hp->src[0].lut ? 1 : 0) | (hp->src[1].lut ? 2 : 0) |
-                        (skip_original ? 4 : 0);
-        BuildPrepLists(tables_, {{hp->src[0].lut != 0, hp->src[1].lut != 0}}, skip_original);
+        const uint8_t g0 = static_cast<uint8_t>(PrepGroup(hp->src[0]));
+        const uint8_t g1 = static_cast<uint8_t>(PrepGroup(hp->src[1]));
+        const int key = g0 + kPrepGroups * (g1 + kPrepGroups * (skip_original ? 1 : 0));
+        BuildPrepLists(tables_, {{g0, g1}}, skip_original);
         mem_.StagePrep(tables_);
         const size_t upload = mem_.head_bytes;
         // Stream capture needs a real stream; the legacy default stream runs
@@ -959,7 +963,7 @@ private:
     int device_ = 0;
     cudaStream_t own_stream_ = nullptr, stream_ = nullptr;
     cudaEvent_t done_ = nullptr, copied_ = nullptr;
-    cudaGraphExec_t graph_exec_[8] = {};
+    cudaGraphExec_t graph_exec_[2 * kPrepGroups * kPrepGroups] = {};
     bool reference_valid_ = false;
     uint64_t reference_handle_ = 0;
     float reference_background_ = 0.0f;
@@ -1087,10 +1091,11 @@ public:
                 }
             }
         }
-        std::vector<std::array<bool, 2>> table(n);
+        PrepGroups group(n);
         for (uint32_t i = 0; i < n; ++i)
-            table[i] = {t.pairs[i].src[0].lut != 0, t.pairs[i].src[1].lut != 0};
-        BuildPrepLists(t, table);
+            group[i] = {static_cast<uint8_t>(PrepGroup(t.pairs[i].src[0])),
+                        static_cast<uint8_t>(PrepGroup(t.pairs[i].src[1]))};
+        BuildPrepLists(t, group);
         mem_.Stage(t);
         if (host_bytes) VQM_CK(cudaEventRecord(copied_, stream_));
         mem_.EnqueueUpload(mem_.table_bytes, stream_);
