@@ -61,11 +61,11 @@ def test_pow(y):
 
 def test_powf_gamma_exhaustive_for_gamma_2_4():
     """The power-law transfers' single-precision power, on every float of
-    its fast range [2^-30, 256) for VQM's gamma 2.4: never more than one ulp
+    its fast range [2^-30, 2^16) for VQM's gamma 2.4: never more than one ulp
     from the correctly rounded power, and on it for all but ~0.35 %."""
     yf = np.float32(2.4)
     lo = int(np.float32(2.0 ** -30).view(np.uint32))
-    hi = int(np.float32(256.0).view(np.uint32))
+    hi = int(np.float32(65536.0).view(np.uint32))
     off = total = 0
     for start in range(lo, hi, 1 << 23):
         x = np.arange(start, min(start + (1 << 23), hi), dtype=np.uint32).view(np.float32)
@@ -80,12 +80,19 @@ def test_powf_gamma_exhaustive_for_gamma_2_4():
 @pytest.mark.parametrize("y", [2.2, 2.8, 1.0, 4.0, 1 / 0.45, 2.6])
 def test_powf_gamma(y):
     yf = np.float32(y)
-    x = samples(2.0 ** -30, 255.9, n=1_000_000)
+    x = samples(2.0 ** -30, 65535.9, n=1_000_000)
     d = ulps(det(5, x, yf), np.power(x.astype(np.float64), np.float64(yf)).astype(np.float32))
     assert d.max() <= 1 and (d > 0).mean() < 0.01
-    # Outside its fast range (and for y outside [1, 4]) it is pow itself.
-    edge = np.float32([0.0, 1e-12, 2.0 ** -31, 256.0, 1e6])
-    assert np.array_equal(det(5, edge, yf), det(1, edge, yf))
+    # Below 2^-30 it is 0 for y in [2, 4] (the exact power is below 2^-60);
+    # from 2^16 up, and for y outside [2, 4], it is pow itself.
+    tiny = np.float32([0.0, 1e-12, 2.0 ** -31, np.nextafter(np.float32(2.0 ** -30), 0)])
+    big = np.float32([65536.0, 1e6])
+    if 2.0 <= yf <= 4.0:
+        assert np.all(det(5, tiny, yf) == 0.0)
+        assert det(5, np.float32([2.0 ** -30]), yf)[0] > 0.0
+    else:
+        assert np.array_equal(det(5, tiny, yf), det(1, tiny, yf))
+    assert np.array_equal(det(5, big, yf), det(1, big, yf))
     assert det(5, np.float32([1.0]), yf)[0] == 1.0
     assert np.array_equal(det(5, x[:1000], np.float32(0.5)), det(1, x[:1000], np.float32(0.5)))
 

@@ -370,18 +370,17 @@ __device__ __forceinline__ void BlockLinearGeneric(const DevSource& s, uint32_t 
     }
 }
 
-// ss2dm::powf_gamma of two lanes with the same y, the floating-point steps
-// two lanes per instruction (FFMA2 / FMUL2 / FADD2), each the operation the
-// scalar function performs on that lane: the same values. A lane outside the
-// function's fast range sends both through the scalar function. `logt` and
-// `expt` are copies of the function's two tables (kLogF4, kExpF2) in shared
-// memory: each lane's entry depends on its value, and divergent entries of a
-// shared-memory table cost fewer cycles than the same loads through L1.
+// ss2dm::powf_gamma of two lanes with the same y, both inside the function's
+// fast range (x in [2^-30, 2^16), y in [2, 4]; the caller selects the rest),
+// the floating-point steps two lanes per instruction (FFMA2 / FMUL2 / FADD2),
+// each the operation the scalar function performs on that lane: the same
+// values. `logt` and `expt` are copies of the function's two tables (kLogF4,
+// kExpF2) in shared memory: each lane's entry depends on its value, and
+// divergent entries of a shared-memory table cost fewer cycles than the same
+// loads through L1.
 __device__ __forceinline__ float2 PowfGamma2(float2 x, float y, const float4* logt,
                                              const float2* expt) {
     using namespace ss2dm;
-    if (!(powf_gamma_fast(x.x, y) && powf_gamma_fast(x.y, y)))
-        return make_float2(powf_gamma(x.x, y), powf_gamma(x.y, y));
     const auto P = [](float v) { return make_float2(v, v); };
     const auto N = [](float2 v) { return make_float2(-v.x, -v.y); };
     const uint32_t ix0 = __float_as_uint(x.x), ix1 = __float_as_uint(x.y);
@@ -421,7 +420,7 @@ __device__ __forceinline__ float2 PowfGamma2(float2 x, float y, const float4* lo
     const float2 tjl = make_float2(T0.y, T1.y);
     const float2 r = __fadd2_rn(tj, __ffma2_rn(tj, q, tjl));
     // 2^(k >> 6) = bits ((k >> 6) + 127) << 23, with k + 127 * 64 = u -
-    // 0x4b3fe040 in [448, 10176] over the fast range (t in [-120, 32]).
+    // 0x4b3fe040 in [448, 12224] over the fast range (t in [-120, 64)).
     return __fmul2_rn(r, make_float2(__uint_as_float(((u0 - 0x4b3fe040u) << 17) & 0xff800000u),
                                      __uint_as_float(((u1 - 0x4b3fe040u) << 17) & 0xff800000u)));
 }
@@ -587,18 +586,20 @@ __device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* 
 #pragma unroll
         for (int i = 0; i < 4; ++i) ApplyMatrix(s.m1, e[i]);
     }
-    // The transfer, v < 0 (and v == 0) giving 0 and everything else
-    // powf_gamma, two pixels per call.
+    // The transfer, powf_gamma two pixels per call: v below 2^-30 (negative
+    // included) gives 0; every other v is inside the fast range, the host
+    // having bounded the matrix's output below 2^16 for every sample code
+    // (DevSource::yuv_fast).
     const float g = s.gamma;
 #pragma unroll
     for (int h = 0; h < 4; h += 2)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const float a = e[h][c], b = e[h + 1][c];
-            const float2 r =
-                PowfGamma2(make_float2(a > 0.0f ? a : 1.0f, b > 0.0f ? b : 1.0f), g, logt, expt);
-            e[h][c] = a > 0.0f ? r.x : 0.0f;
-            e[h + 1][c] = b > 0.0f ? r.y : 0.0f;
+            const bool ia = a >= ss2dm::kGammaMinX, ib = b >= ss2dm::kGammaMinX;
+            const float2 r = PowfGamma2(make_float2(ia ? a : 1.0f, ib ? b : 1.0f), g, logt, expt);
+            e[h][c] = ia ? r.x : 0.0f;
+            e[h + 1][c] = ib ? r.y : 0.0f;
         }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {

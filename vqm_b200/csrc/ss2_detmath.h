@@ -19,7 +19,8 @@
 // that error of a rounding boundary. powf_gamma, the power of the pure
 // power-law transfers, works in float pairs to ~2^-30 and is faithfully
 // rounded: within one ulp, and on the correctly rounded float for all but
-// 0.3-0.4 % of the floats in [2^-30, 256) (exhaustive for y = 2.2, 2.4, 2.8).
+// 0.3-0.4 % of the floats in [2^-30, 2^16) (exhaustive for y = 2.4); below
+// 2^-30 it gives 0.
 //
 // Compiled as host C++ (g++, -ffp-contract=off) or as CUDA (nvcc,
 // -fmad=false): no expression below may be contracted differently.
@@ -320,11 +321,11 @@ SS2_DM float pow(float x, float y) {
         exp2d(static_cast<double>(y) * log2d_normal(bits(static_cast<double>(x)))));
 }
 
-// x^y for float x >= 0 and y in [1, 4] (the power-law transfer functions),
-// in single precision: faithfully rounded (never more than one ulp from the
-// exact power; the correctly rounded float in all but about one case in a
-// hundred) and built from float operations only, so it costs a fraction of
-// pow. For x in [2^-30, 2^8):
+// x^y for float x >= 0 and y in [2, 4] (the power-law transfer functions,
+// whose exponents are 2.2, 2.4 and 2.8), in single precision: faithfully
+// rounded (never more than one ulp from the exact power; the correctly
+// rounded float in all but about one case in a hundred) and built from float
+// operations only, so it costs a fraction of pow. For x in [2^-30, 2^16):
 //   x = 2^e m, m in [1, 2); the top 7 bits of m pick c_i = 1 + (i + 1/2)/128
 //   and its float reciprocal inv_i, so r = m inv_i - 1 is exact as the pair
 //   (m inv_i rounded - 1, the product's rounding error) with |r| < 2^-8;
@@ -337,24 +338,29 @@ SS2_DM float pow(float x, float y) {
 // The absolute error of t stays below ~2^-30, so the value before the last
 // rounding is within ~2^-30 relative of x^y (the method of the table-driven
 // log and exp above, carried in float pairs: Tang 1990, and the pair
-// arithmetic of Dekker 1971). Outside that range, and for y outside [1, 4],
-// it is pow(x, y).
+// arithmetic of Dekker 1971). For x in [0, 2^-30) the result is 0: the
+// exact power is below 2^-60 there, far under any value the metric resolves,
+// so the transfer's inputs need no branch below the fast range (the kernels'
+// two-lane form selects 0 for them). For x of 2^16 and above (and negative
+// or NaN x), and for y outside [2, 4], it is pow(x, y).
 // powf_gamma's constants (shared with its two-lane form in the kernels):
-// its fast range [2^-30, 256) and [1, 4], the Taylor coefficients of
+// its fast range [2^-30, 2^16) and [2, 4], the Taylor coefficients of
 // log2(1 + r), ln 2 and 1/6, each the float nearest the exact value.
 constexpr float kGammaMinX = 9.31322574615478515625e-10f;  // 2^-30
-constexpr float kGammaMaxX = 256.0f;
+constexpr float kGammaMaxX = 65536.0f;
 constexpr float kGammaK1 = 1.44269502163f;     // 1 / ln 2
 constexpr float kGammaK2 = -0.721347510815f;   // -1 / (2 ln 2)
 constexpr float kGammaK3 = 0.480898350477f;    // 1 / (3 ln 2)
 constexpr float kGammaK4 = -0.360673755407f;   // -1 / (4 ln 2)
 constexpr float kGammaLn2 = 0.693147182465f;
 constexpr float kGammaSixth = 0.166666671634f;
+SS2_DM bool powf_gamma_exponent(float y) { return y >= 2.0f && y <= 4.0f; }
 SS2_DM bool powf_gamma_fast(float x, float y) {
-    return x >= kGammaMinX && x < kGammaMaxX && y >= 1.0f && y <= 4.0f;
+    return x >= kGammaMinX && x < kGammaMaxX && powf_gamma_exponent(y);
 }
 
 SS2_DM float powf_gamma(float x, float y) {
+    if (powf_gamma_exponent(y) && x >= 0.0f && x < kGammaMinX) return 0.0f;
     if (!powf_gamma_fast(x, y)) return pow(x, y);
     const uint32_t ix = bits(x);
     const int e = static_cast<int>(ix >> 23) - 127;

@@ -71,7 +71,8 @@ struct DevSource {
     // at most 2 with bilinear upsampling. For a 2x2 luma block at even
     // coordinates the bilinear phase of each output depends only on its
     // parity, so the host fixes the first window slot and the four tap
-    // weights per parity.
+    // weights per parity. Also requires the YUV matrix to map every sample
+    // code below the transfer power's fast-range limit.
     uint8_t yuv_fast;
     uint8_t chroma_pattern;    // 4:2:0 phases known at compile time: 1 + x type
                                // + 2 y type (type 0: siting offset 0, type 1:

@@ -510,6 +510,26 @@ void FastYuvConstants(const vqm_cu_format& f, int mode, int tid, uint32_t chroma
             d.cweight[yp][xp][2] = w[0][xp][0] * w[1][yp][1];
             d.cweight[yp][xp][3] = w[0][xp][1] * w[1][yp][1];
         }
+    // The device's two-lane power takes every input from 2^-30 up without a
+    // range check: every sample code the container can hold (whatever the
+    // declared depth) must keep the YUV matrix's outputs below the power's
+    // fast-range limit (with a margin for their float rounding). Valid
+    // formats stay far below it (|R'G'B'| < 5; 9-bit codes filling 16 bits
+    // reach a few hundred).
+    const double code_max = f.type == 0 ? 255.0 : 65535.0;
+    double lim[3];
+    for (int p = 0; p < 3; ++p) {
+        const int q = p == 0 ? 0 : 1;
+        lim[p] = std::max(std::fabs(static_cast<double>(d.offset[q])),
+                          std::fabs(code_max * d.scale[q] + d.offset[q]));
+    }
+    for (int row = 0; row < 3; ++row) {
+        double bound = d.identity1 ? lim[row] : 0.0;
+        if (!d.identity1)
+            for (int j = 0; j < 3; ++j)
+                bound += std::fabs(static_cast<double>(d.m1[3 * row + j])) * lim[j];
+        if (!(bound < 0.5 * ss2dm::kGammaMaxX)) return;
+    }
     d.yuv_fast = 1;
 }
 
