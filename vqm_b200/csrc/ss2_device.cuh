@@ -119,9 +119,14 @@ struct DevPrepItem {
 };
 
 // The prepare kernels, one per decode: 8-bit images by table (group 0),
-// yuv_fast images (group 1), every other format (group 2).
+// yuv_fast images of even width and height (group 1: every 2x2 block is
+// whole, so its kernel carries no generic decode), every other image
+// (group 2).
 constexpr int kPrepGroups = 3;
-inline int PrepGroup(const DevSource& s) { return s.lut ? 0 : (s.yuv_fast ? 1 : 2); }
+inline int PrepGroup(const DevSource& s) {
+    if (s.lut) return 0;
+    return s.yuv_fast && s.width % 2 == 0 && s.height % 2 == 0 ? 1 : 2;
+}
 
 struct DevBatch {
     uint32_t pairs;

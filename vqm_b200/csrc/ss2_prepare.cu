@@ -239,9 +239,8 @@ __device__ __forceinline__ void TableBlock(const DevSource& s, const float* lut,
 // generic one. The decodes' long dependency chains (the YUV power's table
 // loads, the generic FP64 transfers) want the warps more than the registers
 // (measured on 136 uneven pairs: the YUV kernel at 5 CTAs with some spilling
-// takes 8.48 ms, at 4 9.33 ms, and 8.93 ms with its generic blocks (past an
-// odd last column or row) as an out-of-line call; the generic decode at 4
-// beats 2 by a quarter).
+// took 8.48 ms, at 4 9.33 ms; the generic decode at 4 beats 2 by a
+// quarter).
 #ifndef VQM_GENERIC_PREPARE_CTAS
 #define VQM_GENERIC_PREPARE_CTAS 4
 #endif
@@ -382,11 +381,9 @@ __global__ void __launch_bounds__(kThreads, kGroup == 0   ? 5
                 if constexpr (kTable) {
                     TableBlock(s, lut, fast, w4, hx, bx, by, lin);
                 } else if constexpr (kYuv) {
-                    if (2 * bx + 1 < width && 2 * by + 1 < height)
-                        BlockLinearYuv(s, chroma_stage, pow_log, pow_exp, gx, gy, bx, by,
-                                       aligned4 != 0, lin);
-                    else
-                        BlockLinearGeneric(s, bx, by, lin);
+                    // Even width and height (PrepGroup): the block is whole.
+                    BlockLinearYuv(s, chroma_stage, pow_log, pow_exp, gx, gy, bx, by,
+                                   aligned4 != 0, lin);
                 } else {
                     BlockLinearGeneric(s, bx, by, lin);
                 }
