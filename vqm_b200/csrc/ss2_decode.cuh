@@ -117,6 +117,20 @@ __device__ __forceinline__ void ApplyMatrix(const float* m, float v[3]) {
     v[1] = r[1];
     v[2] = r[2];
 }
+// ApplyMatrix on two pixels, two lanes per instruction: the same values.
+__device__ __forceinline__ void ApplyMatrix2(const float* m, float2 v[3]) {
+    float2 r[3];
+#pragma unroll
+    for (int row = 0; row < 3; ++row) {
+        const float2 a = make_float2(m[row * 3], m[row * 3]);
+        const float2 b = make_float2(m[row * 3 + 1], m[row * 3 + 1]);
+        const float2 c = make_float2(m[row * 3 + 2], m[row * 3 + 2]);
+        r[row] = __ffma2_rn(c, v[2], __ffma2_rn(b, v[1], __fmul2_rn(a, v[0])));
+    }
+    v[0] = r[0];
+    v[1] = r[1];
+    v[2] = r[2];
+}
 // color.glsl:223-236.
 __device__ __forceinline__ void ClToRgb(const DevSource& s, float e[3]) {
     const float u = e[1], v = e[2];
@@ -582,9 +596,16 @@ __device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* 
             e[i][2] = RawSample(s, 2, x0 + (i & 1), y0 + (i >> 1));
         }
     }
+    // From here on the block's two rows run as pixel pairs (pixels 0, 1 and
+    // 2, 3), two lanes per instruction, each lane the scalar operation.
+    float2 q[2][3];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) q[h][c] = make_float2(e[2 * h][c], e[2 * h + 1][c]);
     if (!s.identity1) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) ApplyMatrix(s.m1, e[i]);
+        for (int h = 0; h < 2; ++h) ApplyMatrix2(s.m1, q[h]);
     }
     // The transfer, powf_gamma two pixels per call: v below 2^-30 (negative
     // included) gives 0; every other v is inside the fast range, the host
@@ -592,21 +613,23 @@ __device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* 
     // (DevSource::yuv_fast).
     const float g = s.gamma;
 #pragma unroll
-    for (int h = 0; h < 4; h += 2)
+    for (int h = 0; h < 2; ++h)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const float a = e[h][c], b = e[h + 1][c];
-            const bool ia = a >= ss2dm::kGammaMinX, ib = b >= ss2dm::kGammaMinX;
-            const float2 r = PowfGamma2(make_float2(ia ? a : 1.0f, ib ? b : 1.0f), g, logt, expt);
-            e[h][c] = ia ? r.x : 0.0f;
-            e[h + 1][c] = ib ? r.y : 0.0f;
+            const float2 v = q[h][c];
+            const bool ia = v.x >= ss2dm::kGammaMinX, ib = v.y >= ss2dm::kGammaMinX;
+            const float2 r =
+                PowfGamma2(make_float2(ia ? v.x : 1.0f, ib ? v.y : 1.0f), g, logt, expt);
+            q[h][c] = make_float2(ia ? r.x : 0.0f, ib ? r.y : 0.0f);
         }
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        if (!s.identity2) ApplyMatrix(s.m2, e[i]);
-        rgb[i][0] = e[i][0];
-        rgb[i][1] = e[i][1];
-        rgb[i][2] = e[i][2];
+    for (int h = 0; h < 2; ++h) {
+        if (!s.identity2) ApplyMatrix2(s.m2, q[h]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            rgb[2 * h][c] = q[h][c].x;
+            rgb[2 * h + 1][c] = q[h][c].y;
+        }
     }
 }
 
