@@ -137,15 +137,17 @@ def _yuv_fast_formats():
     }
 
 
-@pytest.mark.parametrize("name", list(_yuv_fast_formats()))
-def test_yuv_fast_path_planes_bit_exact(name):
+@pytest.mark.parametrize("name,w,h", [(n, 200, 134) for n in _yuv_fast_formats()] +
+                         [("444p10", 201, 133), ("422p8", 200, 133), ("440p10", 201, 134)])
+def test_yuv_fast_path_planes_bit_exact(name, w, h):
     """Integer YUV with a power-law transfer takes the fast decode (staged
     chroma window, per-parity taps); its planes equal the oracle's generic
-    decode bit for bit, inside the image and along its edges."""
+    decode bit for bit, inside the image and along its edges. An image of
+    odd width or height runs the generic prepare kernel instead (the YUV
+    kernel takes whole 2x2 blocks only), with the same planes."""
     from oracle import binding as ob
     fmt = _yuv_fast_formats()[name]
     assert ss2.decode_path(fmt) == "yuv"
-    w, h = 200, 134
     ov = _values(fmt, w, h, 21)
     rng = np.random.default_rng(4)
     dv = [None if v is None else np.clip(v + rng.normal(0, 0.03, v.shape),

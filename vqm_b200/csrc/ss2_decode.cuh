@@ -491,18 +491,26 @@ __device__ __forceinline__ void ChromaFixed(const float* stage, int bxs, int bys
     using X = AxisPhase<kX>;
     using Y = AxisPhase<kY>;
     constexpr int sw = (kPrepTile >> 1) + 2;
+    // Both pixels of a row at once (xp = 0, 1 in the two lanes), each lane
+    // the scalar chain.
 #pragma unroll
     for (int p = 0; p < 2; ++p) {
         const float* base = stage + p * kChromaStage + bys * sw + bxs;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int xp = i & 1, yp = i >> 1;
-            const float* t = base + Y::Slot(yp) * sw + X::Slot(xp);
-            e[i][1 + p] = __fmaf_rn(
-                X::W1(xp) * Y::W1(yp), t[sw + 1],
-                __fmaf_rn(X::W0(xp) * Y::W1(yp), t[sw],
-                          __fmaf_rn(X::W1(xp) * Y::W0(yp), t[1],
-                                    __fmul_rn(X::W0(xp) * Y::W0(yp), t[0]))));
+        for (int yp = 0; yp < 2; ++yp) {
+            const float* t0 = base + Y::Slot(yp) * sw + X::Slot(0);
+            const float* t1 = base + Y::Slot(yp) * sw + X::Slot(1);
+            const auto w = [](float a, float b) { return make_float2(a, b); };
+            const float2 v = __ffma2_rn(
+                w(X::W1(0) * Y::W1(yp), X::W1(1) * Y::W1(yp)), make_float2(t0[sw + 1], t1[sw + 1]),
+                __ffma2_rn(w(X::W0(0) * Y::W1(yp), X::W0(1) * Y::W1(yp)),
+                           make_float2(t0[sw], t1[sw]),
+                           __ffma2_rn(w(X::W1(0) * Y::W0(yp), X::W1(1) * Y::W0(yp)),
+                                      make_float2(t0[1], t1[1]),
+                                      __fmul2_rn(w(X::W0(0) * Y::W0(yp), X::W0(1) * Y::W0(yp)),
+                                                 make_float2(t0[0], t1[0])))));
+            e[2 * yp][1 + p] = v.x;
+            e[2 * yp + 1][1 + p] = v.y;
         }
     }
 }
