@@ -450,22 +450,22 @@ __device__ __forceinline__ void StageChroma(const DevSource& s, uint32_t gx, uin
     const uint32_t sw = (kPrepTile >> s.sub_w) + 2, sh = (kPrepTile >> s.sub_h) + 2;
     const int c0x = static_cast<int>((gx * kPrepTile) >> s.sub_w) - 1;
     const int c0y = static_cast<int>((gy * kPrepTile) >> s.sub_h) - 1;
-    // 64 columns by 4 rows per pass of the CTA's 256 threads (sw <= 66).
-    const uint32_t lanes_x = 64, rows_per_pass = blockDim.x / lanes_x;
+    // A row of the window per sw threads, blockDim.x / sw rows per pass
+    // (sw <= 66, so at least 3 rows of the CTA's 256 threads).
+    const uint32_t rows_per_pass = blockDim.x / sw;
+    const uint32_t i = threadIdx.x % sw, j0 = threadIdx.x / sw;
+    if (j0 >= rows_per_pass) return;
     for (int p = 1; p <= 2; ++p) {
         const int dx = static_cast<int>(s.plane_w[p]), dy = static_cast<int>(s.plane_h[p]);
         float* out = stage + (p - 1) * kChromaStage;
-        for (uint32_t j = threadIdx.x / lanes_x; j < sh; j += rows_per_pass) {
+        const uint32_t x = static_cast<uint32_t>(min(max(c0x + static_cast<int>(i), 0), dx - 1));
+        for (uint32_t j = j0; j < sh; j += rows_per_pass) {
             const uint32_t y = static_cast<uint32_t>(min(max(c0y + static_cast<int>(j), 0), dy - 1));
             const uint8_t* row = s.plane[p] + static_cast<size_t>(y) * s.row_bytes[p];
-            for (uint32_t i = threadIdx.x % lanes_x; i < sw; i += lanes_x) {
-                const uint32_t x =
-                    static_cast<uint32_t>(min(max(c0x + static_cast<int>(i), 0), dx - 1));
-                const float v =
-                    s.type == 0 ? static_cast<float>(__ldg(row + x))
-                                : static_cast<float>(__ldg(reinterpret_cast<const uint16_t*>(row) + x));
-                out[j * sw + i] = __fmaf_rn(v, s.scale[1], s.offset[1]);
-            }
+            const float v =
+                s.type == 0 ? static_cast<float>(__ldg(row + x))
+                            : static_cast<float>(__ldg(reinterpret_cast<const uint16_t*>(row) + x));
+            out[j * sw + i] = __fmaf_rn(v, s.scale[1], s.offset[1]);
         }
     }
 }
