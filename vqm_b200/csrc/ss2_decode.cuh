@@ -455,18 +455,21 @@ __device__ __forceinline__ void StageChroma(const DevSource& s, uint32_t gx, uin
     const uint32_t rows_per_pass = blockDim.x / sw;
     const uint32_t i = threadIdx.x % sw, j0 = threadIdx.x / sw;
     if (j0 >= rows_per_pass) return;
-    for (int p = 1; p <= 2; ++p) {
-        const int dx = static_cast<int>(s.plane_w[p]), dy = static_cast<int>(s.plane_h[p]);
-        float* out = stage + (p - 1) * kChromaStage;
-        const uint32_t x = static_cast<uint32_t>(min(max(c0x + static_cast<int>(i), 0), dx - 1));
-        for (uint32_t j = j0; j < sh; j += rows_per_pass) {
-            const uint32_t y = static_cast<uint32_t>(min(max(c0y + static_cast<int>(j), 0), dy - 1));
-            const uint8_t* row = s.plane[p] + static_cast<size_t>(y) * s.row_bytes[p];
-            const float v =
-                s.type == 0 ? static_cast<float>(__ldg(row + x))
-                            : static_cast<float>(__ldg(reinterpret_cast<const uint16_t*>(row) + x));
-            out[j * sw + i] = __fmaf_rn(v, s.scale[1], s.offset[1]);
-        }
+    // Both chroma planes have the same size; each pass loads a sample of
+    // each (unrolled, so several passes' loads are in flight at once).
+    const int dx = static_cast<int>(s.plane_w[1]), dy = static_cast<int>(s.plane_h[1]);
+    const uint32_t x = static_cast<uint32_t>(min(max(c0x + static_cast<int>(i), 0), dx - 1));
+    const auto sample = [&](int p, uint32_t y) {
+        const uint8_t* row = s.plane[p] + static_cast<size_t>(y) * s.row_bytes[p];
+        return s.type == 0 ? static_cast<float>(__ldg(row + x))
+                           : static_cast<float>(__ldg(reinterpret_cast<const uint16_t*>(row) + x));
+    };
+#pragma unroll 3
+    for (uint32_t j = j0; j < sh; j += rows_per_pass) {
+        const uint32_t y = static_cast<uint32_t>(min(max(c0y + static_cast<int>(j), 0), dy - 1));
+        const float u = sample(1, y), v = sample(2, y);
+        stage[j * sw + i] = __fmaf_rn(u, s.scale[1], s.offset[1]);
+        stage[kChromaStage + j * sw + i] = __fmaf_rn(v, s.scale[1], s.offset[1]);
     }
 }
 
