@@ -280,7 +280,8 @@ int vqm_cu_ss2_blur_variants(uint32_t* count, uint32_t* shapes);
  * per-image table), _TABLE_IN_RANGE (the same, with every linear sample
  * non-negative so the cube roots need no range check) or _YUV (integer YUV
  * with a power-law transfer and at most 2x chroma subsampling, phases fixed
- * per pixel parity). The results are the same whichever path runs. */
+ * per pixel parity; an image of such a format with an odd width or height
+ * runs the generic decode). The results are the same whichever path runs. */
 #define VQM_CU_DECODE_GENERIC 0
 #define VQM_CU_DECODE_TABLE 1
 #define VQM_CU_DECODE_TABLE_IN_RANGE 2

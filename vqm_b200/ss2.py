@@ -583,7 +583,9 @@ def decode_path(fmt: "ImageFormat", chroma_filter: int = 0) -> str:
     """Which device decode images of `fmt` take (the results are the same
     whichever runs): "generic", "table" (8-bit grey/RGB through a table),
     "table_in_range" (the same, non-negative linear samples) or "yuv"
-    (integer YUV, power-law transfer, at most 2x chroma subsampling)."""
+    (integer YUV, power-law transfer, at most 2x chroma subsampling; an
+    image of such a format with an odd width or height runs the generic
+    decode)."""
     path = ctypes.c_uint32()
     _check(_lib.vqm_cu_ss2_decode_path(ctypes.byref(fmt), chroma_filter, ctypes.byref(path)))
     return DECODE_PATHS[path.value]
