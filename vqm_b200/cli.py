@@ -89,24 +89,34 @@ def _format(header, args):
 
 
 class _Scorer:
-    """Frame pairs -> results, batched or one pair per call."""
+    """Frame pairs -> results, batched, or one pair per call on two pipelines
+    in turn (frame i + 1's upload overlaps frame i's kernels)."""
 
     def __init__(self, width, height, batch, chroma_filter, device):
         self.batch = batch
         if batch > 1:
-            self.s = ss2.Ssimulacra2Batch(max_pairs=batch, chroma_filter=chroma_filter,
-                                          device=device)
+            self.s = [ss2.Ssimulacra2Batch(max_pairs=batch, chroma_filter=chroma_filter,
+                                           device=device)]
         else:
-            self.s = ss2.Ssimulacra2Pipeline(width, height, chroma_filter=chroma_filter,
-                                             device=device)
+            self.s = [ss2.Ssimulacra2Pipeline(width, height, chroma_filter=chroma_filter,
+                                              device=device) for _ in range(2)]
 
     def score(self, pairs, background):
         if self.batch > 1:
-            return self.s.compute_many(pairs, background)
-        return [self.s.compute(o, d, background) for o, d in pairs]
+            return self.s[0].compute_many(pairs, background)
+        results, pending = [], []
+        for i, (o, d) in enumerate(pairs):
+            if len(pending) == 2:
+                p, tok = pending.pop(0)
+                results.append(p.finish(tok))
+            p = self.s[i % 2]
+            pending.append((p, p.submit(o, d, background)))
+        results.extend(p.finish(tok) for p, tok in pending)
+        return results
 
     def close(self):
-        self.s.close()
+        for s in self.s:
+            s.close()
 
 
 def run(argv=None, out=sys.stdout) -> int:
