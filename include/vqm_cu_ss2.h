@@ -124,6 +124,12 @@ int vqm_cu_validate_format(const vqm_cu_format* format, uint32_t width,
  * up to 6 (width, height) pairs into sizes12, the count into *scales. */
 int vqm_cu_ss2_plan_scales(uint32_t width, uint32_t height, uint32_t* sizes12,
                            uint32_t* scales);
+/* Ssimulacra2ChannelPruned (src/metrics/ssimulacra2/score.cc:103-114): *pruned
+ * = 1 when all six weights of (channel, scale) in a `scales`-level plan are
+ * at most 0.01, so its norms are never computed and publish as 0. Channels
+ * 0-2 are X, Y, B; scale < scales <= 6, else VQM_CU_INVALID_ARGUMENT. */
+int vqm_cu_ss2_channel_pruned(uint32_t channel, uint32_t scale, uint32_t scales,
+                              int* pruned);
 /* Ssimulacra2Result::Score (src/metrics/ssimulacra2/score.cc:118-163), FP64,
  * norms in the layout above. VQM_CU_INVALID_ARGUMENT for more than six
  * scales or nonfinite norms, as the reference throws. */

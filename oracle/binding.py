@@ -20,7 +20,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle_ss2.so")
 REF_PATH = os.path.join(HERE, "_ref", "libvqm_ref.so")
-REFERENCE_CHECKOUT = "/root/reference"
+# The reference checkout whose host sources `make ref` compiles into
+# _ref/libvqm_ref.so; None when the environment does not name one (the GPU
+# box only uses the prebuilt library).
+REFERENCE_CHECKOUT = os.environ.get("VQM_REFERENCE") or None
 
 
 class Format(ctypes.Structure):
@@ -55,11 +58,13 @@ class _Image(ctypes.Structure):
     ]
 
 
-def build(reference: bool = True) -> None:
-    """Compile the oracle (and, when the checkout exists, the reference pins)."""
+def build(reference: bool = True, checkout: str | None = None) -> None:
+    """Compile the oracle and, when a reference checkout is given (argument
+    or VQM_REFERENCE), the reference pins."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if reference and os.path.isdir(REFERENCE_CHECKOUT):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    checkout = checkout or REFERENCE_CHECKOUT
+    if reference and checkout and os.path.isdir(checkout):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"VQM_REFERENCE={checkout}"], check=True)
 
 
 _lib = None
@@ -80,7 +85,7 @@ def ref() -> ctypes.CDLL | None:
     """The reference's own score.cc/input.cc, or None when it was not built."""
     global _ref
     if _ref is None:
-        if not os.path.exists(REF_PATH) and os.path.isdir(REFERENCE_CHECKOUT):
+        if not os.path.exists(REF_PATH) and REFERENCE_CHECKOUT:
             build(reference=True)
         if not os.path.exists(REF_PATH):
             return None

@@ -17,7 +17,7 @@ def pytest_configure(config):
         subprocess.run([sys.executable, "-m", "vqm_b200.build"], cwd=ROOT, check=True)
     from oracle import binding
     if not os.path.exists(binding.LIB_PATH):
-        binding.build(reference=os.path.isdir(binding.REFERENCE_CHECKOUT))
+        binding.build(reference=bool(binding.REFERENCE_CHECKOUT))
 
 
 def cuda_available() -> bool:

@@ -13,7 +13,8 @@ import math
 import numpy as np
 
 from oracle import binding as ob
-from vqm_b200 import ss2, synthetic
+from tests import synthetic
+from vqm_b200 import ss2
 
 SIDE = 32
 

@@ -8,7 +8,8 @@ import numpy as np
 import pytest
 
 from tests import helpers
-from vqm_b200 import ss2, synthetic
+from tests import synthetic
+from vqm_b200 import ss2
 
 pytestmark = pytest.mark.gpu
 

@@ -116,6 +116,23 @@ def test_plan_scales_matches_oracle():
         ss2.plan_scales(4, 8)
 
 
+@needs_ref
+def test_channel_pruning_matches_reference():
+    """Ssimulacra2ChannelPruned through the C ABI against score.cc compiled
+    from the reference's sources, for every plan length."""
+    for scales in range(1, 7):
+        for s in range(scales):
+            for c in range(3):
+                assert ss2.channel_pruned(c, s, scales) == bool(
+                    ref.vqmref_channel_pruned(c, s, scales)), (c, s, scales)
+    for bad in ((3, 0, 6), (0, 6, 6), (0, 0, 7), (0, 0, 0)):
+        with pytest.raises(ss2.InvalidArgument):
+            ss2.channel_pruned(*bad)
+    # 1080p keeps 11 of 18 planes: Y at L0, X and Y at L1-L2, X, Y and B at
+    # L3-L4, nothing at L5.
+    assert ss2.kept_pixels(1920, 1080) == 3_491_280
+
+
 def test_host_score_bit_exact():
     rng = np.random.default_rng(3)
     for scales in range(1, 7):

@@ -9,7 +9,8 @@ import numpy as np
 import pytest
 
 from tests import helpers
-from vqm_b200 import ss2, synthetic, y4m
+from tests import synthetic
+from vqm_b200 import ss2, y4m
 
 
 def _clip(tmp_path, frames=3, w=64, h=48):

@@ -1243,6 +1243,18 @@ int vqm_cu_ss2_plan_scales(uint32_t width, uint32_t height, uint32_t* sizes12, u
     });
 }
 
+int vqm_cu_ss2_channel_pruned(uint32_t channel, uint32_t scale, uint32_t scales, int* pruned) {
+    return Guard([&] {
+        NotNull(pruned, "pruned");
+        if (channel >= 3 || scales == 0 || scales > 6 || scale >= scales)
+            throw std::invalid_argument("channel, scale or scale count out of range");
+        *pruned = vqm_b200::ChannelPruned(static_cast<int>(channel), static_cast<int>(scale),
+                                          static_cast<int>(scales))
+                      ? 1
+                      : 0;
+    });
+}
+
 int vqm_cu_ss2_score(const double* norms, uint32_t scales, double* score) {
     return Guard([&] {
         NotNull(score, "score");

@@ -193,6 +193,7 @@ _SIGS = {
     "vqm_cu_required_bytes": ([_P, ctypes.c_uint32, ctypes.c_uint32, _P], ctypes.c_int),
     "vqm_cu_validate_format": ([_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p], ctypes.c_int),
     "vqm_cu_ss2_plan_scales": ([ctypes.c_uint32, ctypes.c_uint32, _P, _P], ctypes.c_int),
+    "vqm_cu_ss2_channel_pruned": ([ctypes.c_uint32] * 3 + [_P], ctypes.c_int),
     "vqm_cu_ss2_score": ([_P, ctypes.c_uint32, _P], ctypes.c_int),
     "vqm_cu_ss2_source_constants": ([_P, ctypes.c_uint32, _P], ctypes.c_int),
     "vqm_cu_ss2_create": ([_P, _P], ctypes.c_int),
@@ -433,6 +434,22 @@ def plan_scales(width: int, height: int):
     n = ctypes.c_uint32()
     _check(_lib.vqm_cu_ss2_plan_scales(width, height, sizes, ctypes.byref(n)))
     return [(sizes[2 * i], sizes[2 * i + 1]) for i in range(n.value)]
+
+
+def channel_pruned(channel: int, scale: int, scales: int) -> bool:
+    """Ssimulacra2ChannelPruned (src/metrics/ssimulacra2/score.cc:103-114):
+    whether (channel, scale) of a `scales`-level plan is never computed."""
+    out = ctypes.c_int()
+    _check(_lib.vqm_cu_ss2_channel_pruned(channel, scale, scales, ctypes.byref(out)))
+    return bool(out.value)
+
+
+def kept_pixels(width: int, height: int) -> int:
+    """Pixels of one image's kept (level, channel) pyramid planes: what the
+    prepare stage stores and the blur stage reads, per image."""
+    plan = plan_scales(width, height)
+    return sum(w * h for s, (w, h) in enumerate(plan) for c in range(3)
+               if not channel_pruned(c, s, len(plan)))
 
 
 # ---------------------------------------------------------------------------
@@ -693,8 +710,11 @@ class Ssimulacra2Pool:
     stream that takes ``chunk`` pairs (of any sizes) per submission, one
     launch per stage; chunks go to the workers in turn, each worker with at
     most one chunk in flight, so one chunk's host-to-device copies overlap
-    the previous chunk's kernels. If a submission fails, the chunks already
-    submitted are drained before the error propagates (pool.cc:64-112).
+    the previous chunk's kernels. If a submission or a finish fails, the
+    chunks already submitted are drained before that first error propagates
+    (pool.cc:64-72); if a drain itself fails, the workers are released and
+    every later call raises LogicError (pool.cc:94-109, "pool cannot be
+    reused after a failed drain").
 
     ``compute_many`` is ``results(submit_many(...))``. A caller streaming
     lists through the pool can ``submit_many`` the next list before taking
@@ -716,6 +736,7 @@ class Ssimulacra2Pool:
         self._next = 0                        # next worker in turn
         self._lists = {}                      # ticket -> [results, chunks left]
         self._tickets = 0
+        self._poisoned = False
 
     def workers(self) -> int:
         return len(self._batches)
@@ -745,15 +766,25 @@ class Ssimulacra2Pool:
         entry[0][first:first + len(results)] = results
         entry[1] -= 1
 
-    def _drain(self):
+    def _drain(self) -> bool:
+        """Finishes every chunk in flight; False if any finish failed."""
+        ok = True
         while self._inflight:
+            w, token, _, _, _ = self._inflight.popleft()
+            self._busy[w] = False
             try:
-                self._finish_oldest()
+                self._batches[w].finish(token)
             except Exception:
-                pass
+                ok = False
+        return ok
+
+    def _usable(self):
+        if self._poisoned:
+            raise LogicError("pool cannot be reused after a failed drain")
 
     def submit_many(self, pairs: Iterable, background: float = 0.5) -> int:
         """Queues a list of pairs; returns the ticket for ``results``."""
+        self._usable()
         pairs = list(pairs)
         ticket = self._tickets
         self._tickets += 1
@@ -770,6 +801,7 @@ class Ssimulacra2Pool:
 
     def results(self, ticket: int) -> list:
         """The list's results in input order (waits for its chunks)."""
+        self._usable()
         if ticket not in self._lists:
             raise InvalidArgument("pool: no list with that ticket")
         try:
@@ -784,11 +816,16 @@ class Ssimulacra2Pool:
         return self._lists.pop(ticket)[0]
 
     def _abort(self):
-        """After a failure: drains what is in flight and drops every list."""
-        self._drain()
+        """After a failure: drains what is in flight and drops every list;
+        a failed drain releases the workers and poisons the pool."""
+        drained = self._drain()
         self._queue.clear()
         self._busy = [False] * len(self._batches)
         self._lists.clear()
+        if not drained:
+            self.close()
+            self._batches = []
+            self._poisoned = True
 
     def compute_many(self, pairs: Iterable, background: float = 0.5):
         return self.results(self.submit_many(pairs, background))

@@ -16,11 +16,18 @@ matrix, chroma is the mean of each 2x2 block. 4:2:0 needs even sizes (the
 reference rejects odd ones, src/input.cc:176-179), so odd sizes drawn for
 those pairs are rounded up to even; odd geometries are exercised with 8-bit
 RGB pairs instead.
+
+This module is numpy only: it loads no native code, so the CPU reference
+arm of the benchmark and the CUDA arm draw the same pixels without the CPU
+arm touching the CUDA library. Images come back as `Planar` records (size,
+format kind, packed bytes in the reference's plane layout); the tests and
+the benchmark wrap them in the image type of whichever scorer they call.
 """
 
 from __future__ import annotations
 
 import math
+from typing import NamedTuple
 
 import numpy as np
 
@@ -29,7 +36,39 @@ try:  # scipy is in the image; only the blur distortion needs it
 except Exception:  # pragma: no cover
     gaussian_filter = None
 
-from . import ss2
+
+# vqm::ImageFormat (include/vqm_image.h:325-337) as its 12 byte fields: type,
+# family, alpha, range, matrix, transfer, primaries, chroma_location,
+# subsample_w, subsample_h, depth, reserved.
+FORMAT_FIELDS = {
+    # 8-bit sRGB planar RGB, full range, BT.709 primaries.
+    "srgb8": (0, 1, 0, 1, 0, 13, 1, 0, 0, 0, 0, 0),
+    # 10-bit 4:2:0 Y'CbCr, BT.709 matrix, transfer and primaries, limited
+    # range, Word samples, left chroma siting.
+    "yuv420p10": (1, 2, 0, 0, 1, 1, 1, 0, 1, 1, 10, 0),
+}
+
+
+class Planar(NamedTuple):
+    """One packed image: planes back to back, each starting on a 4-byte
+    boundary (src/input.cc:114-145)."""
+
+    width: int
+    height: int
+    kind: str          # a key of FORMAT_FIELDS
+    data: np.ndarray   # uint8
+
+
+def plane_offsets(kind: str, w: int, h: int):
+    """[(offset, width, height, sample bytes)] of the Y/R, U/G, V/B planes and
+    the total byte count (the reference's RequiredBytes)."""
+    sb, (cw, ch) = (1, (w, h)) if kind == "srgb8" else (2, (w >> 1, h >> 1))
+    planes, cursor = [], 0
+    for p in range(3):
+        pw, ph = (w, h) if p == 0 else (cw, ch)
+        planes.append((cursor, pw, ph, sb))
+        cursor = (cursor + pw * ph * sb + 3) // 4 * 4
+    return planes, cursor
 
 
 def _waves(w: int, h: int, rng: np.random.Generator) -> np.ndarray:
@@ -99,18 +138,17 @@ def to_u8(img: np.ndarray) -> np.ndarray:
     return np.clip(np.rint(img), 0, 255).astype(np.uint8)
 
 
-def rgb8_image(planes_u8: np.ndarray) -> ss2.Image:
+def rgb8_image(planes_u8: np.ndarray) -> Planar:
     _, h, w = planes_u8.shape
-    fmt = ss2.srgb8_format()
-    data = np.zeros(ss2.required_bytes(fmt, w, h), dtype=np.uint8)
-    layout = ss2.plane_layout(fmt, w, h)
+    layout, total = plane_offsets("srgb8", w, h)
+    data = np.zeros(total, dtype=np.uint8)
     for p in range(3):
         off = layout[p][0]
         data[off:off + w * h] = planes_u8[p].reshape(-1)
-    return ss2.Image(w, h, fmt, data)
+    return Planar(w, h, "srgb8", data)
 
 
-def yuv420_10bit_image(rgb: np.ndarray) -> ss2.Image:
+def yuv420_10bit_image(rgb: np.ndarray) -> Planar:
     """RGB code values (0..255 floats) -> BT.709 limited 10-bit 4:2:0."""
     _, h, w = rgb.shape
     if w % 2 or h % 2:
@@ -128,13 +166,12 @@ def yuv420_10bit_image(rgb: np.ndarray) -> ss2.Image:
     yc = np.clip(np.rint(64 + 876 * y), 64, 940)
     cbc = np.clip(np.rint(512 + 896 * sub(cb)), 64, 960)
     crc = np.clip(np.rint(512 + 896 * sub(cr)), 64, 960)
-    fmt = ss2.yuv420_10bit_bt709_format()
-    data = np.zeros(ss2.required_bytes(fmt, w, h), dtype=np.uint8)
-    layout = ss2.plane_layout(fmt, w, h)
+    layout, total = plane_offsets("yuv420p10", w, h)
+    data = np.zeros(total, dtype=np.uint8)
     for p, arr in enumerate((yc, cbc, crc)):
         off, pw, ph, _ = layout[p]
         data[off:off + pw * ph * 2] = arr.astype("<u2").reshape(-1).view(np.uint8)
-    return ss2.Image(w, h, fmt, data)
+    return Planar(w, h, "yuv420p10", data)
 
 
 # --- workloads --------------------------------------------------------------
@@ -184,20 +221,30 @@ def plain_1080p(count: int = 64, seed0: int = 1000, width: int = 1920, height: i
     return [rgb_pair(width, height, seed0 + i)[:2] for i in range(count)]
 
 
-def uneven_batch(count: int = 128, seed0: int = 2000, odd_rgb: int = 8):
-    """`count` 10-bit 4:2:0 pairs of sizes W in [320, 3840], H in [180, 2160]
-    (rounded to even), plus `odd_rgb` 8-bit RGB pairs keeping odd sizes."""
+def uneven_jobs(count: int = 128, seed0: int = 2000, odd_rgb: int = 8):
+    """The uneven batch's draw as (kind, width, height, seed) jobs: `count`
+    10-bit 4:2:0 pairs of sizes W in [320, 3840], H in [180, 2160] (rounded
+    up to even when generated), then `odd_rgb` 8-bit RGB pairs keeping odd
+    sizes. `make_pair` turns a job into its pair, so the jobs can be
+    generated in parallel."""
     rng = np.random.default_rng(seed0)
-    pairs = []
-    for i in range(count):
-        w = int(rng.integers(320, 3841))
-        h = int(rng.integers(180, 2161))
-        pairs.append(yuv_pair(w, h, seed0 + 1 + i)[:2])
-    for i in range(odd_rgb):
-        w = int(rng.integers(320, 3841)) | 1
-        h = int(rng.integers(180, 2161)) | 1
-        pairs.append(rgb_pair(w, h, seed0 + 10_000 + i)[:2])
-    return pairs
+    jobs = [("yuv", int(rng.integers(320, 3841)), int(rng.integers(180, 2161)), seed0 + 1 + i)
+            for i in range(count)]
+    jobs += [("rgb", int(rng.integers(320, 3841)) | 1, int(rng.integers(180, 2161)) | 1,
+              seed0 + 10_000 + i) for i in range(odd_rgb)]
+    return jobs
+
+
+def make_pair(job):
+    """(kind, width, height, seed) -> (original, distorted) Planar pair."""
+    kind, w, h, seed = job
+    make = yuv_pair if kind == "yuv" else rgb_pair
+    return make(w, h, seed)[:2]
+
+
+def uneven_batch(count: int = 128, seed0: int = 2000, odd_rgb: int = 8):
+    """The uneven batch's pairs in draw order (see `uneven_jobs`)."""
+    return [make_pair(j) for j in uneven_jobs(count, seed0, odd_rgb)]
 
 
 def video_offsets(count: int, seed: int):
