@@ -512,6 +512,7 @@ private:
     };
     std::vector<Ssimulacra2Result> Run(const std::vector<vqm_cu_image>& o,
                                        const std::vector<vqm_cu_image>& d, float background) {
+        if (poisoned_) throw std::logic_error("pool cannot be reused after a failed drain");
         const std::size_t n = o.size();
         std::vector<Ssimulacra2Result> out(n);
         std::vector<std::pair<std::uint64_t, std::size_t>> pending(batches_.size(), {0, 0});
@@ -519,13 +520,14 @@ private:
         std::vector<double> norms(chunk_ * VQM_CU_SS2_MAX_NORMS);
         std::vector<std::uint32_t> scales(chunk_);
         auto drain = [&](std::size_t w) {
-            if (!pending[w].second) return;
+            const std::size_t count = pending[w].second;
+            if (!count) return;
+            pending[w].second = 0;  // a finish consumes the submission, failed or not
             detail::Check(vqm_cu_ss2_batch_finish(batches_[w].get(), pending[w].first,
                                                   norms.data(), scales.data(), nullptr));
-            for (std::size_t i = 0; i < pending[w].second; ++i)
+            for (std::size_t i = 0; i < count; ++i)
                 out[first[w] + i] = Ssimulacra2Result::FromNorms(
                     norms.data() + i * VQM_CU_SS2_MAX_NORMS, scales[i]);
-            pending[w].second = 0;
         };
         std::size_t w = 0;
         try {
@@ -544,12 +546,21 @@ private:
             }
             for (std::size_t k = 0; k < batches_.size(); ++k) drain(k);
         } catch (...) {
-            // Drain what was submitted before rethrowing (pool.cc:64-112).
+            // Drain what was submitted before rethrowing the error that
+            // interrupted the list (pool.cc:64-72). If a drain itself fails,
+            // the workers are released and the pool refuses further use
+            // (pool.cc:94-109): no submission of this list outlives the call.
+            bool drain_failed = false;
             for (std::size_t k = 0; k < batches_.size(); ++k) {
                 if (!pending[k].second) continue;
-                vqm_cu_ss2_batch_finish(batches_[k].get(), pending[k].first, nullptr, nullptr,
-                                        nullptr);
+                if (vqm_cu_ss2_batch_finish(batches_[k].get(), pending[k].first, nullptr,
+                                            nullptr, nullptr) != VQM_CU_OK)
+                    drain_failed = true;
                 pending[k].second = 0;
+            }
+            if (drain_failed) {
+                batches_.clear();
+                poisoned_ = true;
             }
             throw;
         }
@@ -558,6 +569,7 @@ private:
     ChromaFilter chroma_filter_;
     std::size_t chunk_;
     std::vector<std::unique_ptr<vqm_cu_ss2_batch, Deleter>> batches_;
+    bool poisoned_ = false;
 };
 
 // ---- vqm_metrics.h (SSIMULACRA 2 only) ---------------------------------------
