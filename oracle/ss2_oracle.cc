@@ -1204,6 +1204,38 @@ void Maps(T mu1, T mu2, T s11, T s22, T s12, T img1, T img2, T out[6]) {
     out[5] = (blur * blur) * (blur * blur);
 }
 
+// The four-quantity form of the maps: sigma11 and sigma22 enter the SSIM'
+// denominator only as their sum, so s11 + s22 can be blurred as one quantity
+// `ssum` (the blur of a*a + b*b, formed as fma(a, a, b*b)). The denominator
+// is 2 * (0.5 * ssum - mu1^2 + 0.5 * (mu1 - mu2) * (mu1 + mu2)) + C2, whose
+// correction term is exactly 0 when mu1 == mu2. For identical inputs ssum is
+// exactly 2 * s11 (fma(a, a, a*a) == 2 * (a*a) and the taps commute with the
+// factor 2) and s12 == s11, so the denominator is bit-identical to num_s and
+// the map is exactly 0: identity still scores exactly 100. Not VQM's
+// rounding: a mode of the CUDA blur, measured against the five-quantity form.
+template <class T>
+void Maps4(T mu1, T mu2, T ssum, T s12, T img1, T img2, T out[6]) {
+    const T C2 = T(0.0009);
+    const T dm = mu1 - mu2;
+    const T num_m = std::fma(-dm, dm, T(1));
+    const T num_s = std::fma(T(2), std::fma(-mu1, mu2, s12), C2);
+    const T h = std::fma(-mu1, mu1, T(0.5) * ssum);
+    const T denom = std::fma(T(2), std::fma(T(0.5) * dm, mu1 + mu2, h), C2);
+    const T d = std::max(MapDiv<T>(std::fma(-num_m, num_s, denom), denom), T(0));
+    const T dd = d * d;
+    out[0] = d;
+    out[1] = dd * dd;
+    const T dist = T(1) + std::abs(img2 - mu2);
+    const T orig = T(1) + std::abs(img1 - mu1);
+    const T d1 = MapDiv<T>(dist - orig, orig);
+    const T ring = std::max(d1, T(0));
+    const T blur = std::max(-d1, T(0));
+    out[2] = ring;
+    out[3] = (ring * ring) * (ring * ring);
+    out[4] = blur;
+    out[5] = (blur * blur) * (blur * blur);
+}
+
 // One (level, channel): the six norm sums in VQM's reduction order
 // (scale.comp:370-436, reduce.comp:21-63): per 32x32 tile, each of 256
 // invocations sums its column's four rows, a halving ladder adds the 256
@@ -1211,18 +1243,19 @@ void Maps(T mu1, T mu2, T s11, T s22, T s12, T img1, T img2, T out[6]) {
 // 256-way strided and halves again.
 template <class T>
 void ChannelSums(const std::vector<T>& a, const std::vector<T>& b, uint32_t w,
-                 uint32_t h, const std::array<T, kTaps>& wt, T sums[6]) {
+                 uint32_t h, const std::array<T, kTaps>& wt, T sums[6], bool four = false) {
     std::vector<T> q[5], hq, bq[5];
     const size_t n = size_t(w) * h;
     for (int i = 0; i < 5; ++i) q[i].resize(n);
     for (size_t i = 0; i < n; ++i) {
         q[0][i] = a[i];
         q[1][i] = b[i];
-        q[2][i] = a[i] * a[i];
-        q[3][i] = b[i] * b[i];
+        q[2][i] = four ? std::fma(a[i], a[i], b[i] * b[i]) : a[i] * a[i];
+        q[3][i] = four ? T(0) : b[i] * b[i];
         q[4][i] = a[i] * b[i];
     }
     for (int i = 0; i < 5; ++i) {
+        if (four && i == 3) continue;
         BlurH(q[i], hq, w, h, wt);
         BlurV(hq, bq[i], w, h, wt);
     }
@@ -1240,7 +1273,10 @@ void ChannelSums(const std::vector<T>& a, const std::vector<T>& b, uint32_t w,
                     if (x >= w || y >= h) continue;
                     const size_t i = size_t(y) * w + x;
                     T m[6];
-                    Maps(bq[0][i], bq[1][i], bq[2][i], bq[3][i], bq[4][i], a[i], b[i], m);
+                    if (four)
+                        Maps4(bq[0][i], bq[1][i], bq[2][i], bq[4][i], a[i], b[i], m);
+                    else
+                        Maps(bq[0][i], bq[1][i], bq[2][i], bq[3][i], bq[4][i], a[i], b[i], m);
                     for (int k = 0; k < 6; ++k) s[k] += m[k];
                 }
                 for (int k = 0; k < 6; ++k) pool[k * 256 + tid] = s[k];
@@ -1273,7 +1309,7 @@ struct PairResult {
 // The whole pair: both pyramids, then every kept (level, channel).
 template <class T>
 PairResult<T> ComputePair(const ss2o_image& o, const ss2o_image& dsrc, float background,
-                          int chroma_filter, bool half = false) {
+                          int chroma_filter, bool half = false, bool four = false) {
     if (o.width != dsrc.width || o.height != dsrc.height)
         throw std::invalid_argument("image sizes differ");
     const Plan plan = PlanScales(o.width, o.height);
@@ -1294,7 +1330,7 @@ PairResult<T> ComputePair(const ss2o_image& o, const ss2o_image& dsrc, float bac
             if (ChannelPruned(c, l, plan.count)) continue;
             T s[6];
             ChannelSums<T>(p0.planes[l][c], p1.planes[l][c], plan.sizes[l].w,
-                           plan.sizes[l].h, wt, s);
+                           plan.sizes[l].h, wt, s, four);
             r.sums[l][c * 2 + 0] = s[0];
             r.sums[l][c * 2 + 1] = s[1];
             r.sums[l][6 + c * 4 + 0] = s[2];
@@ -1337,7 +1373,8 @@ int ComputeOne(const ss2o_image* o, const ss2o_image* d, float bg, int filter,
         const auto r = ComputePair<double>(*o, *d, bg, filter);
         ReadResult(r, plan, norms);
     } else {
-        const auto r = ComputePair<float>(*o, *d, bg, filter, precision == 16);
+        const auto r = ComputePair<float>(*o, *d, bg, filter, precision == 16,
+                                          precision == 33);
         ReadResult(r, plan, norms);
     }
     if (scales) *scales = static_cast<uint32_t>(plan.count);

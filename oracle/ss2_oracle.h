@@ -65,8 +65,10 @@ typedef struct ss2o_image {
 
 /* Scores one pair. precision: 32 = the FP32 restatement (VQM proxy), 64 =
  * the same algorithm in FP64, 16 = the FP32 restatement of VQM's half-plane
- * build (pyramid planes and level averages rounded to binary16). Writes 18*scales doubles into norms[108], the
- * scale count into *scales and the score into *score. */
+ * build (pyramid planes and level averages rounded to binary16), 33 = the
+ * FP32 restatement with s11 + s22 blurred as one quantity (the CUDA blur's
+ * four-quantity mode; not VQM's rounding). Writes 18*scales doubles into
+ * norms[108], the scale count into *scales and the score into *score. */
 int ss2o_compute(const ss2o_image* original, const ss2o_image* distorted,
                  float background, int chroma_filter, int precision,
                  double* norms, uint32_t* scales, double* score);

@@ -216,3 +216,25 @@ def test_required_bytes_matches_reference():
                                                ctypes.byref(out))
             assert status == 0
             assert ob.required_bytes(f, w, h) == out.value
+
+
+def test_four_quantity_blur_keeps_identity_but_leaves_the_bound():
+    """Blurring s11 + s22 as one quantity (oracle precision 33) would cut a
+    fifth of the blur's taps. Identity still scores exactly 100, but small,
+    rounding-dominated SSIM' features move far beyond 1e-4 relative against
+    the five-quantity FP32 oracle (measured over the seeded format sweep: up
+    to 1.0 relative, scores up to 0.015 apart), so the CUDA blur keeps VQM's
+    five quantities."""
+    import workloads
+    rng = np.random.default_rng(5)
+    base = workloads.texture(160, 120, rng) / 255.0
+    fmt = helpers.pinned_format()
+    o = helpers.pack_planes(fmt, 160, 120, [base[0], base[1], base[2], None])
+    noisy = [np.clip(v + rng.normal(0, 0.02, v.shape), 0, 1) for v in base] + [None]
+    d = helpers.pack_planes(fmt, 160, 120, noisy)
+    five, _ = helpers.oracle_compute(o, d, precision=32)
+    four, _ = helpers.oracle_compute(o, d, precision=33)
+    nz = five != 0
+    assert np.array_equal(five == 0, four == 0)
+    assert np.max(np.abs(four[nz] - five[nz]) / np.abs(five[nz])) > 1e-3
+    assert helpers.oracle_compute(o, o, precision=33)[1] == 100.0
