@@ -493,7 +493,10 @@ def serve(rates, duration, workers, distinct):
             "server_ms_p50_p99": [float(np.percentile(lat, 50)), float(np.percentile(lat, 99))],
             "submit_late_ms_p99": float(1e3 * np.percentile(late, 99)),
             "batches": int(stats.batches), "largest_batch": int(stats.largest_batch),
-            "peak_device_bytes": int(stats.peak_bytes), "clocks": clocks.summary(),
+            "budget_bytes": int(stats.budget_bytes),
+            "peak_device_bytes": int(stats.peak_device_bytes),
+            "peak_requested_bytes": int(stats.peak_bytes), "trims": int(stats.trims),
+            "clocks": clocks.summary(),
             "config": "Poisson arrivals; sizes 640x360/1280x720/1920x1080/2560x1440/"
                       "3840x2160 at 0.2/0.3/0.3/0.1/0.1; 8-bit RGB or 10-bit 4:2:0 50/50; "
                       f"pinned host inputs; 40 GB budget; {workers} workers"})

@@ -241,8 +241,11 @@ int vqm_cu_ss2_reference_reuses(vqm_cu_ss2_pipeline* pipeline, uint64_t* count);
  * of device images (memory == VQM_CU_MEMORY_DEVICE) on `stream` without any
  * allocation, with all scratch in one fixed 32 MiB device array that the
  * library reserves on every GPU that loads it, held until exit. Pairs whose
- * scratch exceeds it (above about 2.4 megapixels: 1920x1080 and 2048x1200
- * fit, 2560x1440 does not) return INVALID_ARGUMENT.
+ * scratch exceeds it return INVALID_ARGUMENT with the bytes they need; the
+ * need grows with the padded row width, not the area alone (1920x1080,
+ * 1080x1920 and 2048x1200 fit; 1200x2048 and 2560x1440 do not). Planes and
+ * the result must be device or managed memory of the current device, else
+ * INVALID_ARGUMENT before any kernel runs.
  * Returns once the work is queued; result_device (caller-owned device
  * memory, VQM_CU_SS2_RESULT_DOUBLES doubles) then receives 108 norms (18 per
  * scale, zero past the pair's scales), the FP64 score, the scale count and
@@ -268,8 +271,9 @@ typedef struct vqm_cu_ss2_batch_config {
                                 0 = chosen per submit */
     uint32_t variant;      /* blur kernel: 0 = by tile, or chosen per submit
                               from the tile count (a strip length of the
-                              default tile; same results), k = compiled
-                              variant k - 1 */
+                              default tile; strips regroup the compensated
+                              partial sums, so results agree to rounding,
+                              ~1e-7 relative), k = compiled variant k - 1 */
     uint32_t half_planes;  /* 1: binary16 pyramid planes, as
                               vqm_cu_ss2_config.half_planes */
 } vqm_cu_ss2_batch_config;
@@ -324,6 +328,21 @@ int vqm_cu_ss2_batch_finish(vqm_cu_ss2_batch* batch, uint64_t token,
  * holds the last batch's device milliseconds of each stage. */
 int vqm_cu_ss2_batch_set_timing(vqm_cu_ss2_batch* batch, int enabled);
 int vqm_cu_ss2_batch_stage_ms(vqm_cu_ss2_batch* batch, float* stage_ms3);
+/* The batch's device memory, after PipelineMemoryUsage::total
+ * (include/vqm_memory_types.h:24-33): *held = the bytes it holds now
+ * (pyramid, tables, partials, results, its copy of host inputs), reused from
+ * submit to submit and never shrunk by a submit. batch_device_bytes_after
+ * validates a submission as batch_submit would and gives what the batch
+ * will hold once it is submitted (its buffers grown as the submit grows
+ * them), allocating nothing. batch_trim frees the memory of an idle batch
+ * (VQM_CU_LOGIC_ERROR while one is in flight); its next submit allocates
+ * again. */
+int vqm_cu_ss2_batch_device_bytes(vqm_cu_ss2_batch* batch, uint64_t* held);
+int vqm_cu_ss2_batch_device_bytes_after(vqm_cu_ss2_batch* batch, uint32_t n,
+                                        const vqm_cu_image* originals,
+                                        const vqm_cu_image* distorteds,
+                                        uint64_t* bytes);
+int vqm_cu_ss2_batch_trim(vqm_cu_ss2_batch* batch);
 /* ComputeMany / ScoreMany = submit + finish. */
 int vqm_cu_ss2_batch_compute(vqm_cu_ss2_batch* batch, uint32_t n,
                              const vqm_cu_image* originals,
@@ -354,24 +373,35 @@ typedef struct vqm_cu_ss2_server_stats {
     uint64_t submitted, completed, failed;
     uint64_t batches;          /* three-kernel launches */
     uint64_t largest_batch;    /* pairs in the largest batch formed */
-    uint64_t bytes_in_flight;  /* admitted and not yet completed */
+    uint64_t bytes_in_flight;  /* device bytes the admitted, not yet
+                                  completed requests need */
     uint64_t peak_bytes;       /* largest bytes_in_flight seen */
     uint64_t queued;           /* submitted, not yet in a batch */
+    uint64_t budget_bytes;     /* the cap in force (see server_create) */
+    uint64_t device_bytes;     /* device memory the workers hold now */
+    uint64_t peak_device_bytes;/* largest device_bytes seen */
+    uint64_t trims;            /* idle workers' memory freed to admit work */
 } vqm_cu_ss2_server_stats;
 
 /* Starts a dispatcher thread, which forms batches from the queued requests
  * in arrival order whenever a worker is free, and a completion thread, which
- * finishes batches in submission order. Each worker (a batch scorer with its
- * own stream and device memory, reused from batch to batch) admits a batch
- * only if its device footprint fits memory_budget / workers, so the server
- * never holds more than memory_budget of device memory for requests. */
+ * finishes batches in submission order. Each worker is a batch scorer with
+ * its own stream and device memory, reused from batch to batch. The budget
+ * caps the device memory all workers hold together, counted as allocated
+ * (with the buffers' growth): a batch is formed only while the bytes its
+ * worker will hold, plus what the other workers hold, stay within it; when
+ * the head request does not fit, idle workers' memory is freed first, and
+ * otherwise the request waits for running batches to finish. So a request
+ * up to the whole budget is admitted once the rest of the server is idle.
+ * The cap in force is memory_budget, lowered at creation to the device's
+ * free memory less 256 MiB when that is smaller. */
 int vqm_cu_ss2_server_create(const vqm_cu_ss2_server_config* config,
                              vqm_cu_ss2_server** server);
 /* Finishes every queued and in-flight request, then stops the threads. */
 int vqm_cu_ss2_server_destroy(vqm_cu_ss2_server* server);
 /* Queues one pair (host or device images, validated here). The images'
  * memory must stay valid and unchanged until the request's wait returns.
- * VQM_CU_INVALID_ARGUMENT if the pair alone exceeds a worker's budget. */
+ * VQM_CU_INVALID_ARGUMENT if the pair alone needs more than the budget. */
 int vqm_cu_ss2_server_submit(vqm_cu_ss2_server* server,
                              const vqm_cu_image* original,
                              const vqm_cu_image* distorted, float background,

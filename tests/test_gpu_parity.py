@@ -304,7 +304,7 @@ def test_mixed_format_pair():
         check_parity(p.compute(o, d), o, d, label="rgb8 vs yuv420p10")
 
 
-def test_batch_matches_pipeline_bitwise():
+def test_batch_matches_pipeline():
     pairs = [synthetic.rgb_pair(333, 187, 1)[:2], synthetic.yuv_pair(640, 360, 2)[:2],
              synthetic.rgb_pair(8, 8, 3)[:2], synthetic.rgb_pair(1920, 1080, 4)[:2],
              synthetic.yuv_pair(1000, 563, 5)[:2], helpers.plain_256_pair()]
@@ -313,7 +313,9 @@ def test_batch_matches_pipeline_bitwise():
     for (o, d), r in zip(pairs, results):
         with ss2.Ssimulacra2Pipeline(o.width, o.height) as p:
             single = p.compute(o, d)
-        assert np.array_equal(single.norms, r.norms)
+        # The two may pick different strip lengths (they regroup the
+        # compensated partial sums), so they agree to rounding.
+        assert not helpers.feature_mismatch(single.norms, r.norms, rtol=1e-6, atol=1e-12)
         assert abs(r.device_score - r.score()) <= 1e-9
         check_parity(r, o, d, label=f"batch {o.width}x{o.height}")
     # A second, smaller batch on the same scorer reuses its memory.
@@ -324,18 +326,21 @@ def test_batch_matches_pipeline_bitwise():
 @pytest.mark.parametrize("variant", range(len(ss2.blur_variants())))
 def test_every_blur_variant(variant):
     """Every compiled blur kernel gives the oracle's features; they differ
-    from each other only in how tile partials group the sums."""
+    from each other only in how their partials group the sums (per tile, or
+    per strip of tiles), so they agree to rounding."""
     pairs = [synthetic.rgb_pair(333, 187, 41)[:2], synthetic.yuv_pair(1280, 720, 42)[:2],
              synthetic.rgb_pair(8, 8, 43)[:2], synthetic.rgb_pair(97, 2000, 44)[:2]]
     b = ss2.Ssimulacra2Batch(variant=variant)
     ref = ss2.Ssimulacra2Batch(variant=0).compute_many(pairs)
-    # Variants with variant 0's tile (strips, persistent CTAs) reduce every
-    # tile the same way, so they agree with it bit for bit: a batch's
-    # automatic choice among them never changes a pair's result.
-    same_tile = ss2.blur_variants()[variant][:2] == ss2.blur_variants()[0][:2]
-    for (o, d), r, r0 in zip(pairs, b.compute_many(pairs), ref):
+    # Variants with variant 0's tile and one tile per partial (persistent
+    # CTAs) reduce every tile as it does, so they agree with it bit for bit.
+    shape, shape0 = ss2.blur_variants()[variant], ss2.blur_variants()[0]
+    same_grouping = shape[:2] == shape0[:2] and shape[3] == 1
+    again = b.compute_many(pairs)
+    for (o, d), r, r0, r1 in zip(pairs, b.compute_many(pairs), ref, again):
         check_parity(r, o, d, label=f"variant {variant} {o.width}x{o.height}")
-        if same_tile:
+        assert np.array_equal(r.norms, r1.norms)  # each kernel repeats itself exactly
+        if same_grouping:
             assert np.array_equal(r.norms, r0.norms) and r.device_score == r0.device_score
         else:
             assert not helpers.feature_mismatch(r.norms, r0.norms, rtol=1e-6, atol=1e-12)

@@ -3,8 +3,10 @@ benchmark's uneven draw (sizes up to 3840x2160) and its 8 odd-sized 8-bit RGB
 pairs, scored in one Ssimulacra2Batch with the autotuned blur variant.
 
 Every pair must match the FP32 oracle (each of the 108 features within 1e-4
-relative, pruned features exactly 0, score within 1e-2), and equal, bit for
-bit, what the one-pair pipeline returns for it alone. The batch semantics
+relative, pruned features exactly 0, score within 1e-2), and what the
+one-pair pipeline returns for it alone within 1e-6 relative per feature (the
+two may group the compensated partial sums differently: a batch this size
+runs 8-tile blur strips, one pair alone one tile per CTA). The batch semantics
 follow Ssimulacra2Pool::ComputeMany (src/pool.cc:44-72): one result per pair,
 in input order.
 """
@@ -97,4 +99,5 @@ def test_uneven_batch_matches_oracle_and_pipeline(uneven_pairs):
     for i, ((o, d), r) in enumerate(zip(dev, results)):
         with ss2.Ssimulacra2Pipeline(o.width, o.height) as pipe:
             alone = pipe.compute(o, d)
-        assert np.array_equal(alone.norms, r.norms), f"pair {i} alone != in the batch"
+        assert not helpers.feature_mismatch(alone.norms, r.norms, rtol=1e-6, atol=1e-12), \
+            f"pair {i} alone != in the batch"

@@ -105,13 +105,24 @@ class _Scorer:
         if self.batch > 1:
             return self.s[0].compute_many(pairs, background)
         results, pending = [], []
-        for i, (o, d) in enumerate(pairs):
-            if len(pending) == 2:
+        try:
+            for i, (o, d) in enumerate(pairs):
+                if len(pending) == 2:
+                    p, tok = pending.pop(0)
+                    results.append(p.finish(tok))
+                p = self.s[i % 2]
+                pending.append((p, p.submit(o, d, background)))
+            while pending:
                 p, tok = pending.pop(0)
                 results.append(p.finish(tok))
-            p = self.s[i % 2]
-            pending.append((p, p.submit(o, d, background)))
-        results.extend(p.finish(tok) for p, tok in pending)
+        finally:
+            # After an error, finish what is still in flight before it
+            # propagates, so no submission outlives the call (pool.cc:64-72).
+            for p, tok in pending:
+                try:
+                    p.finish(tok)
+                except Exception:
+                    pass
         return results
 
     def close(self):

@@ -21,7 +21,8 @@
 //      again two lanes per instruction, then evaluates the maps of its eight
 //      pixels and keeps six running sums.
 //   4. The CTA's six sums are combined with two-sum compensation into one
-//      partial per tile; the finalize kernel adds the partials in FP64.
+//      partial per CTA (its tile, or its strip of tiles below); the finalize
+//      kernel adds the partials in FP64.
 // A persistent form keeps each CTA resident and copies its next tile's
 // window into a second buffer while it computes the current one; a strip
 // form walks a few tiles down one column and reuses the horizontal results
@@ -503,12 +504,17 @@ __global__ void __launch_bounds__(NT, MB) Ss2BlurPersistentKernel(DevBatch batch
 // results of its first 12 rows are tile k's last 12, already in `hq`: they
 // are moved up instead of being computed again, and only the window's rows
 // 6.. are copied in (6..11 for the maps' raw values, 12.. for the horizontal
-// pass). Every value is computed by the same instructions as in the one-tile
-// kernel, so the maps are bit-identical to it; each tile keeps its own
-// partial.
+// pass). Every blurred value and map value is computed by the same
+// instructions as in the one-tile kernel, so they are bit-identical to it.
+// Each thread keeps its six FP32 sums across the strip's tiles (at most
+// 4 S map values per lane) and the CTA reduces them once, with two-sum
+// compensation, into one partial for the strip: the compensated reduction,
+// its barriers and its scalar adds run once per strip instead of once per
+// tile. The partial's grouping differs from one tile per CTA, so results
+// agree with that kernel to rounding (~1e-7 relative), not bit for bit.
 //
 // The reduction's scratch is rows 12..TH-1 of the horizontal planes, free
-// while the halo rows move.
+// once the last tile's vertical pass is done.
 template <int TW, int TH, int NT>
 struct HqScratch {
     using T = Tile<TW, TH, NT>;
@@ -551,30 +557,28 @@ __global__ void __launch_bounds__(NT, MB) Ss2BlurStripKernel(DevBatch batch) {
     TileRef t = SegmentTile<TW, TH>(batch, seg, strip - sy * seg.tiles_x, ty0);
     IssueTileLoads<TW, TH, NT>(src, t);
     CpAsyncCommit();
+    float2 sum[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) sum[i] = make_float2(0.0f, 0.0f);
     for (int k = 0; k < count; ++k) {
         CpAsyncWait<0>();
         __syncthreads();
         HorizontalPass<TW, TH, NT>(src, hq, k == 0 ? 0 : kRadius);
         __syncthreads();
-        float2 sum[6];
-#pragma unroll
-        for (int i = 0; i < 6; ++i) sum[i] = make_float2(0.0f, 0.0f);
         if (t.x0 + TW <= t.w && t.y0 + TH <= t.h)
             VerticalMaps<TW, TH, NT, false>(src, hq, t, sum);
         else
             VerticalMaps<TW, TH, NT, true>(src, hq, t, sum);
         __syncthreads();  // every read of the window and of `hq` is done
-        const uint32_t partial = t.partial;
         if (k + 1 < count) {
             t.y0 += TH;
-            t.partial += seg.tiles_x;
             IssueTileLoads<TW, TH, NT>(src, t, kRadius / 2);
             CpAsyncCommit();
             MoveHalo<TW, TH, NT>(hq);
         }
-        ReducePartials<NT>(sum, HqScratch<TW, TH, NT>{hq},
-                           batch.partials + static_cast<size_t>(partial) * 6);
     }
+    ReducePartials<NT>(sum, HqScratch<TW, TH, NT>{hq},
+                       batch.partials + (static_cast<size_t>(seg.partial_first) + strip) * 6);
 }
 
 // The variants compiled in: {tile width, tile height, threads, persistent,

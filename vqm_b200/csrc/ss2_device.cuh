@@ -106,7 +106,8 @@ struct DevSegment {
     uint32_t channel;
     uint32_t tiles_x;
     uint32_t tiles;
-    uint32_t partial_first;  // index of this segment's first tile partial
+    uint32_t partial_first;  // index of this segment's first partial
+    uint32_t partials;       // partials the blur writes: one per CTA (a tile, or a strip)
 };
 
 // One image of one pair for the prepare stage. Images decoded through the

@@ -1,5 +1,6 @@
 // Finalize stage for sm_100a: one CTA per (pair, level, kept channel)
-// segment sums the segment's tile partials in FP64, in a fixed order so
+// segment sums the segment's blur partials (one per blur CTA: a tile or a
+// strip of tiles) in FP64, in a fixed order so
 // results repeat bit for bit; the last segment of a pair to finish turns the
 // pair's sums into its 108 norms (reference: vulkan.cc:545-583 ReadResult)
 // and FP64 score (score.cc:118-163).
@@ -50,7 +51,7 @@ __global__ void __launch_bounds__(kFinThreads) Ss2FinalizeKernel(DevBatch batch)
     const DevSegment seg = batch.seg[si];
     const uint32_t tid = threadIdx.x;
     double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (uint32_t t = tid; t < seg.tiles; t += kFinThreads) {
+    for (uint32_t t = tid; t < seg.partials; t += kFinThreads) {
         const double* p = batch.partials + (static_cast<size_t>(seg.partial_first) + t) * 6;
 #pragma unroll
         for (int k = 0; k < 6; ++k) acc[k] += __ldcg(p + k);

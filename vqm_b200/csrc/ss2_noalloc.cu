@@ -14,9 +14,14 @@
 // the device images to score and a device buffer for the result.
 //
 // Limits and rules:
-//   * kScratchBytes (32 MiB) bounds the pair: up to about 2.4 megapixels
-//     (1920x1080 and 2048x1200 fit, 2560x1440 does not); larger pairs are
-//     rejected with VQM_CU_INVALID_ARGUMENT.
+//   * kScratchBytes (32 MiB) bounds the scratch one pair needs: its FP32
+//     pyramid (rows padded to a multiple of 32 columns, so the need depends
+//     on the width, not on the pixel count alone), tile partials and tables.
+//     1920x1080, 1080x1920 and 2048x1200 fit; 1200x2048 (same area, narrow
+//     rows padded more) and 2560x1440 do not. Pairs that need more are
+//     rejected with VQM_CU_INVALID_ARGUMENT, naming the bytes they need.
+//   * Image planes and the result must be device (or managed) memory of the
+//     current device; anything else is rejected before a kernel runs.
 //   * Every GPU that loads the library holds the 32 MiB until the process
 //     exits.
 //   * All calls share the one array and it keeps the last call's contents:
@@ -106,6 +111,21 @@ unsigned char* ScratchAddress(int device) {
 
 size_t Align(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// A pointer the kernels may read or write: device or managed memory that
+// belongs to `device`. Host memory, even pinned and mapped, is refused, so a
+// caller's mistake is an error status and not a fault on the device.
+void RequireDeviceMemory(const void* p, int device, const std::string& what) {
+    cudaPointerAttributes a{};
+    const cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw std::invalid_argument(what + ": not a CUDA pointer");
+    }
+    const bool device_memory = a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (!device_memory || (a.type == cudaMemoryTypeDevice && a.device != device))
+        throw std::invalid_argument(what + ": must be device memory of the current device");
+}
+
 void SourcePlanes(DevSource& src, const vqm_cu_image& img, const char* name) {
     if (img.memory != VQM_CU_MEMORY_DEVICE)
         throw std::invalid_argument(std::string(name) +
@@ -171,8 +191,9 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
             const uint32_t ty = (plan.h[l] + th - 1) / th;
             s.tiles = s.tiles_x * ty;
             s.partial_first = tiles;
-            tiles += s.tiles;
-            blocks += BlurBlocks(kDefaultBlurVariant, s.tiles_x, ty);
+            s.partials = BlurBlocks(kDefaultBlurVariant, s.tiles_x, ty);
+            tiles += s.partials;
+            blocks += s.partials;
             ++nseg;
             t.blur_start[nseg] = blocks;
         }
@@ -196,19 +217,26 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
             "cuda: a " + std::to_string(o->width) + "x" + std::to_string(o->height) +
             " pair needs " + std::to_string(need) +
             " bytes of scratch; the no-allocation entry point has " +
-            std::to_string(kScratchBytes) + " (32 MiB: pairs up to about 2.4 megapixels, e.g. 1920x1080 or 2048x1200)");
+            std::to_string(kScratchBytes) +
+            " (32 MiB: e.g. 1920x1080 or 2048x1200 fit; the need grows with the row width)");
 
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) {
         cudaGetLastError();
         throw std::runtime_error("cuda: no usable compute device");
     }
-    unsigned char* base = ScratchAddress(device);
-
     BuildSourceConstants(o->format, chroma_filter, background, P.src[0]);
     BuildSourceConstants(d->format, chroma_filter, background, P.src[1]);
     SourcePlanes(P.src[0], *o, "original");
     SourcePlanes(P.src[1], *d, "distorted");
+    for (int k = 0; k < 2; ++k)
+        for (int p = 0; p < 4; ++p)
+            if (P.src[k].plane[p])
+                RequireDeviceMemory(P.src[k].plane[p], device,
+                                    std::string(k ? "distorted" : "original") + " plane " +
+                                        std::to_string(p));
+    RequireDeviceMemory(result, device, "result");
+    unsigned char* base = ScratchAddress(device);
     P.pyramid = reinterpret_cast<float*>(base + off_pyramid);
     P.result = result;
 

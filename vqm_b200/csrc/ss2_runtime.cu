@@ -109,12 +109,18 @@ public:
         ptr_ = nullptr;
         bytes_ = 0;
     }
+    // The size ensure(bytes) leaves: unchanged if it suffices, else bytes,
+    // and at least half again the old size when one was held.
+    size_t grown(size_t bytes) const {
+        if (bytes <= bytes_) return bytes_;
+        return bytes_ ? std::max(bytes, bytes_ + bytes_ / 2) : bytes;
+    }
     // Returns true when the address changed. A buffer that has to grow
     // grows by half again at least, so a scorer fed batches of varying sizes
     // reallocates (and synchronises the device) a few times, not per batch.
     bool ensure(size_t bytes) {
         if (bytes <= bytes_) return false;
-        if (bytes_) bytes = std::max(bytes, bytes_ + bytes_ / 2);
+        bytes = grown(bytes);
         reset();
         if (cudaMalloc(&ptr_, bytes) != cudaSuccess) {
             ptr_ = nullptr;
@@ -259,8 +265,9 @@ Tables BuildTables(const std::vector<std::pair<uint32_t, uint32_t>>& sizes, Blur
                 const uint32_t ty = (plan.h[l] + shape.h - 1) / shape.h;
                 s.tiles = s.tiles_x * ty;
                 s.partial_first = static_cast<uint32_t>(t.partials);
-                t.partials += s.tiles;
-                blur += BlurBlocks(shape.variant, s.tiles_x, ty);
+                s.partials = BlurBlocks(shape.variant, s.tiles_x, ty);
+                t.partials += s.partials;
+                blur += s.partials;
                 t.segs.push_back(s);
                 t.blur_start.push_back(static_cast<uint32_t>(blur));
             }
@@ -341,9 +348,9 @@ struct BatchMemory {
     uint32_t pair_count = 0;
     size_t elem_bytes = 4;  // pyramid element: float, or binary16 with half planes
 
-    // Sizes and uploads-to-be for `t`; returns true if any address moved.
-    bool Layout(const Tables& t) {
-        bool moved = false;
+    // Device bytes each buffer needs for `t`, in the order table, pyramid,
+    // partials, segment sums, pair counters, results (and the table offsets).
+    std::array<size_t, 6> Needs(const Tables& t) {
         off_pairs = 0;
         off_items = AlignUp(off_pairs + sizeof(DevPair) * t.pairs.size(), 16);
         off_prep = AlignUp(off_items + sizeof(DevPrepItem) * t.prep_items.size(), 16);
@@ -351,16 +358,39 @@ struct BatchMemory {
         off_segs = head_bytes;
         off_blur = AlignUp(off_segs + sizeof(DevSegment) * t.segs.size(), 256);
         table_bytes = AlignUp(off_blur + sizeof(uint32_t) * t.blur_start.size(), 256);
-        moved |= table.ensure(table_bytes);
+        return {table_bytes, std::max<size_t>(t.pyramid_floats, 64) * elem_bytes,
+                std::max<size_t>(t.partials, 1) * 6 * sizeof(double),
+                std::max<size_t>(t.segs.size(), 1) * 6 * sizeof(double),
+                std::max<size_t>(t.pairs.size(), 1) * sizeof(uint32_t),
+                std::max<size_t>(t.pairs.size(), 1) * kResultDoubles * sizeof(double)};
+    }
+    std::array<DeviceBuffer*, 6> Buffers() {
+        return {&table, &pyramid, &partials, &seg_sums, &pair_done, &results};
+    }
+    // Device bytes held now.
+    size_t DeviceBytes() {
+        size_t n = 0;
+        for (DeviceBuffer* b : Buffers()) n += b->bytes();
+        return n;
+    }
+    void ReleaseDevice() {
+        for (DeviceBuffer* b : Buffers()) b->reset();
+    }
+
+    // Sizes and uploads-to-be for `t`; returns true if any address moved.
+    bool Layout(const Tables& t) {
+        bool moved = false;
+        const std::array<size_t, 6> need = Needs(t);
+        moved |= table.ensure(need[0]);
         moved |= table_host.ensure(table_bytes);
-        moved |= pyramid.ensure(std::max<size_t>(t.pyramid_floats, 64) * elem_bytes);
-        moved |= partials.ensure(std::max<size_t>(t.partials, 1) * 6 * sizeof(double));
-        moved |= seg_sums.ensure(std::max<size_t>(t.segs.size(), 1) * 6 * sizeof(double));
-        if (pair_done.ensure(std::max<size_t>(t.pairs.size(), 1) * sizeof(uint32_t))) {
+        moved |= pyramid.ensure(need[1]);
+        moved |= partials.ensure(need[2]);
+        moved |= seg_sums.ensure(need[3]);
+        if (pair_done.ensure(need[4])) {
             moved = true;
             VQM_CK(cudaMemset(pair_done.as<void>(), 0, pair_done.bytes()));
         }
-        moved |= results.ensure(std::max<size_t>(t.pairs.size(), 1) * kResultDoubles * sizeof(double));
+        moved |= results.ensure(need[5]);
         moved |= results_host.ensure(std::max<size_t>(t.pairs.size(), 1) * kResultDoubles * sizeof(double));
         pair_count = static_cast<uint32_t>(t.pairs.size());
         uint8_t* base = table.as<uint8_t>();
@@ -1038,32 +1068,45 @@ public:
         stream_ = s ? static_cast<cudaStream_t>(s) : own_stream_;
     }
 
+    // Device bytes the batch holds now (pyramid, tables, partials, results
+    // and its copy of host inputs), reused from submit to submit.
+    size_t DeviceBytes() { return mem_.DeviceBytes() + inputs_.bytes(); }
+
+    // Device bytes the batch will hold once these pairs are submitted: its
+    // buffers grown as Submit grows them (never shrunk). Validates the pairs
+    // as Submit does; allocates nothing.
+    size_t DeviceBytesAfter(uint32_t n, const vqm_cu_image* o, const vqm_cu_image* d) {
+        std::vector<std::pair<uint32_t, uint32_t>> sizes;
+        const size_t host_bytes = ValidatePairs(n, o, d, sizes);
+        Tables t = BuildTables(sizes, ShapeFor(sizes));
+        BatchMemory probe;  // offsets only; the sizes come from mem_
+        probe.elem_bytes = mem_.elem_bytes;
+        const std::array<size_t, 6> need = probe.Needs(t);
+        const std::array<DeviceBuffer*, 6> buf = mem_.Buffers();
+        size_t bytes = inputs_.grown(std::max<size_t>(host_bytes, 256));
+        for (int i = 0; i < 6; ++i) bytes += buf[i]->grown(need[i]);
+        return bytes;
+    }
+
+    // Frees the device memory an idle batch holds; the next submit
+    // allocates what it needs again.
+    void Trim() {
+        if (in_flight_) throw std::logic_error("cuda: a batch is in flight; Finish it first");
+        VQM_CK(cudaSetDevice(device_));
+        VQM_CK(cudaStreamSynchronize(stream_));
+        mem_.ReleaseDevice();
+        inputs_.reset();
+    }
+
     // `wait_copies` false leaves the host-to-device copies of host images in
     // flight: their planes are then borrowed until Finish.
     uint64_t Submit(uint32_t n, const vqm_cu_image* o, const vqm_cu_image* d, float bg,
                     bool wait_copies = true) {
         if (in_flight_) throw std::logic_error("cuda: a batch is in flight; Finish it first");
-        if (n == 0) throw std::invalid_argument("cuda: empty batch");
-        if (cfg_.max_pairs && n > cfg_.max_pairs)
-            throw std::invalid_argument("cuda: batch exceeds max_pairs");
-        std::vector<std::pair<uint32_t, uint32_t>> sizes(n);
-        size_t host_bytes = 0;
-        for (uint32_t i = 0; i < n; ++i) {
-            const std::string no = "original[" + std::to_string(i) + "]";
-            const std::string nd = "distorted[" + std::to_string(i) + "]";
-            if (o[i].width != d[i].width || o[i].height != d[i].height)
-                throw std::invalid_argument(nd + ": image size does not match the original");
-            ValidateFormat(o[i].format, o[i].width, o[i].height, no.c_str());
-            ValidateFormat(d[i].format, d[i].width, d[i].height, nd.c_str());
-            sizes[i] = {o[i].width, o[i].height};
-            if (o[i].memory == VQM_CU_MEMORY_HOST)
-                host_bytes += AlignUp(RequiredBytes(o[i].format, o[i].width, o[i].height), 256);
-            if (d[i].memory == VQM_CU_MEMORY_HOST)
-                host_bytes += AlignUp(RequiredBytes(d[i].format, d[i].width, d[i].height), 256);
-        }
+        std::vector<std::pair<uint32_t, uint32_t>> sizes;
+        const size_t host_bytes = ValidatePairs(n, o, d, sizes);
         VQM_CK(cudaSetDevice(device_));
-        const BlurShape shape =
-            auto_shape_ ? BlurShape::Of(AutoBlurVariant(DefaultTileCount(sizes), sms_)) : shape_;
+        const BlurShape shape = ShapeFor(sizes);
         Tables t = BuildTables(sizes, shape);
         mem_.Layout(t);
         inputs_.ensure(std::max<size_t>(host_bytes, 256));
@@ -1115,6 +1158,39 @@ public:
         if (in_flight_) throw std::logic_error("cuda: a batch is in flight; Finish it first");
         timing_ = on;
     }
+
+private:
+    // Validates a submission; fills `sizes` and returns the device bytes its
+    // host images take once copied.
+    size_t ValidatePairs(uint32_t n, const vqm_cu_image* o, const vqm_cu_image* d,
+                         std::vector<std::pair<uint32_t, uint32_t>>& sizes) const {
+        if (n == 0) throw std::invalid_argument("cuda: empty batch");
+        if (!o || !d) throw std::invalid_argument("cuda: image arrays must not be null");
+        if (cfg_.max_pairs && n > cfg_.max_pairs)
+            throw std::invalid_argument("cuda: batch exceeds max_pairs");
+        sizes.resize(n);
+        size_t host_bytes = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            const std::string no = "original[" + std::to_string(i) + "]";
+            const std::string nd = "distorted[" + std::to_string(i) + "]";
+            if (o[i].width != d[i].width || o[i].height != d[i].height)
+                throw std::invalid_argument(nd + ": image size does not match the original");
+            ValidateFormat(o[i].format, o[i].width, o[i].height, no.c_str());
+            ValidateFormat(d[i].format, d[i].width, d[i].height, nd.c_str());
+            sizes[i] = {o[i].width, o[i].height};
+            if (o[i].memory == VQM_CU_MEMORY_HOST)
+                host_bytes += AlignUp(RequiredBytes(o[i].format, o[i].width, o[i].height), 256);
+            if (d[i].memory == VQM_CU_MEMORY_HOST)
+                host_bytes += AlignUp(RequiredBytes(d[i].format, d[i].width, d[i].height), 256);
+        }
+        return host_bytes;
+    }
+    BlurShape ShapeFor(const std::vector<std::pair<uint32_t, uint32_t>>& sizes) const {
+        return auto_shape_ ? BlurShape::Of(AutoBlurVariant(DefaultTileCount(sizes), sms_))
+                           : shape_;
+    }
+
+public:
     void StageMs(float* ms) const {
         if (in_flight_) throw std::logic_error("cuda: a batch is in flight; Finish it first");
         if (!timed_) throw std::logic_error("cuda: the last batch was not timed");
@@ -1569,6 +1645,30 @@ int vqm_cu_ss2_batch_stage_ms(vqm_cu_ss2_batch* b, float* ms3) {
         NotNull(b, "batch");
         NotNull(ms3, "stage_ms3");
         b->impl.StageMs(ms3);
+    });
+}
+
+int vqm_cu_ss2_batch_device_bytes(vqm_cu_ss2_batch* b, uint64_t* held) {
+    return Guard([&] {
+        NotNull(b, "batch");
+        NotNull(held, "held");
+        *held = b->impl.DeviceBytes();
+    });
+}
+
+int vqm_cu_ss2_batch_device_bytes_after(vqm_cu_ss2_batch* b, uint32_t n, const vqm_cu_image* o,
+                                        const vqm_cu_image* d, uint64_t* bytes) {
+    return Guard([&] {
+        NotNull(b, "batch");
+        NotNull(bytes, "bytes");
+        *bytes = b->impl.DeviceBytesAfter(n, o, d);
+    });
+}
+
+int vqm_cu_ss2_batch_trim(vqm_cu_ss2_batch* b) {
+    return Guard([&] {
+        NotNull(b, "batch");
+        b->impl.Trim();
     });
 }
 

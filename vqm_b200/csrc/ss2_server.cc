@@ -2,11 +2,15 @@
 // scorers (vqm_cu_ss2_batch_*), each with its own stream and device memory.
 //
 // Requests queue in arrival order. The dispatcher thread takes a free worker
-// whenever one exists and fills a batch from the head of the queue while the
-// batch's device footprint stays within memory_budget / workers and its pair
-// count within max_batch_pairs; the batch scorer copies host inputs (waiting
-// for the copies, so the dispatcher is the only thread feeding PCIe) and
-// launches its three kernels. The completion thread finishes batches in the
+// whenever one exists and fills a batch from the head of the queue while its
+// pair count stays within max_batch_pairs and the device memory the worker
+// will hold for it, plus what every other worker holds, stays within the
+// budget (memory counted as allocated, growth included: the workers' own
+// report, vqm_cu_ss2_batch_device_bytes[_after]). When the head request does
+// not fit, idle workers' memory is freed (vqm_cu_ss2_batch_trim); if it still
+// does not fit, it waits for running batches to finish. The batch scorer
+// copies host inputs (waiting for the copies, so the dispatcher is the only
+// thread feeding PCIe) and launches its three kernels. The completion thread finishes batches in the
 // order they were submitted (blocking on each batch's completion event),
 // publishes the results and returns the worker. So requests that arrive while
 // batches run are admitted as soon as a worker frees, and up to `workers`
@@ -28,6 +32,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include <cuda_runtime_api.h>
+
 #include "../../include/vqm_cu_ss2.h"
 #include "ss2_host.h"
 #include "ss2_kernels.h"
@@ -42,7 +48,8 @@ size_t Align(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // Device bytes one pair adds to a batch: its pyramid, tile partials, segment
 // sums, result block, table records and (for host images) the staged copy
-// of its inputs, as the batch scorer lays them out.
+// of its inputs, as the batch scorer lays them out, with room to spare for
+// alignment: an upper bound of what a batch of this pair alone allocates.
 size_t PairDeviceBytes(const vqm_cu_image& o, const vqm_cu_image& d, int variant) {
     int tw = 0, th = 0;
     BlurTileShape(variant, &tw, &th);
@@ -88,7 +95,8 @@ public:
         if (cfg.variant > static_cast<uint32_t>(BlurTileCount()))
             throw std::invalid_argument("cuda: no such blur variant");
         variant_ = cfg.variant ? static_cast<int>(cfg.variant) - 1 : kDefaultBlurVariant;
-        per_worker_ = budget_ / workers;
+        ClampToFreeMemory(cfg.device);
+        stats_.budget_bytes = budget_;
         for (uint32_t i = 0; i < workers; ++i) {
             vqm_cu_ss2_batch_config bc{};
             bc.max_pairs = max_pairs_;
@@ -133,11 +141,11 @@ public:
         r->d = d;
         r->background = background;
         r->bytes = PairDeviceBytes(o, d, variant_);
-        if (r->bytes > per_worker_)
+        if (r->bytes > budget_)
             throw std::invalid_argument(
                 "server: a " + std::to_string(o.width) + "x" + std::to_string(o.height) +
-                " pair needs " + std::to_string(r->bytes) + " device bytes; a worker's budget is " +
-                std::to_string(per_worker_));
+                " pair needs " + std::to_string(r->bytes) + " device bytes; the budget is " +
+                std::to_string(budget_));
         uint64_t ticket;
         {
             std::lock_guard<std::mutex> lock(mu_);
@@ -188,8 +196,62 @@ private:
         vqm_cu_ss2_batch* batch = nullptr;
         std::vector<uint64_t> tickets;
         uint64_t token = 0;
-        size_t bytes = 0;
+        size_t bytes = 0;  // what the batch's requests need
+        size_t held = 0;   // device memory the batch scorer holds
     };
+
+    // The budget in force: memory_budget, or the device's free memory less
+    // 256 MiB when that is smaller.
+    void ClampToFreeMemory(int32_t device) {
+        int current = 0;
+        if (cudaGetDevice(&current) != cudaSuccess) {
+            cudaGetLastError();
+            throw std::runtime_error("cuda: no device");
+        }
+        const int want = device < 0 ? current : device;
+        size_t free_bytes = 0, total = 0;
+        const bool ok = cudaSetDevice(want) == cudaSuccess &&
+                        cudaMemGetInfo(&free_bytes, &total) == cudaSuccess;
+        cudaSetDevice(current);
+        if (!ok) {
+            cudaGetLastError();
+            throw std::runtime_error("cuda: cannot read the device's free memory");
+        }
+        const size_t margin = size_t(256) << 20;
+        if (free_bytes > margin) budget_ = std::min(budget_, free_bytes - margin);
+    }
+
+    // With the lock held: whether worker `w`, holding what it will hold once
+    // `os`/`ds` are submitted to it (its own count; nothing is allocated),
+    // fits the budget beside `others`. A submission the worker cannot count
+    // is let through: its submit fails and reports why.
+    bool Fits(Worker& w, const std::vector<vqm_cu_image>& os,
+              const std::vector<vqm_cu_image>& ds, size_t others) {
+        uint64_t after = 0;
+        if (vqm_cu_ss2_batch_device_bytes_after(w.batch, static_cast<uint32_t>(os.size()),
+                                                os.data(), ds.data(), &after) != VQM_CU_OK)
+            return true;
+        return others <= budget_ && after <= budget_ - others;
+    }
+
+    void SetHeld(Worker& w, size_t held) {
+        stats_.device_bytes = stats_.device_bytes - w.held + held;
+        stats_.peak_device_bytes = std::max(stats_.peak_device_bytes, stats_.device_bytes);
+        w.held = held;
+    }
+
+    // With the lock held: frees the memory of the idle workers (`wi`, the
+    // one being filled, included) that hold any. Returns whether it freed any.
+    bool TrimIdle() {
+        bool freed = false;
+        for (int i : free_)
+            if (workers_[i].held && vqm_cu_ss2_batch_trim(workers_[i].batch) == VQM_CU_OK) {
+                SetHeld(workers_[i], 0);
+                ++stats_.trims;
+                freed = true;
+            }
+        return freed;
+    }
 
     void Dispatch() {
         std::unique_lock<std::mutex> lock(mu_);
@@ -201,18 +263,22 @@ private:
             }
             if (free_.empty()) continue;
             const int wi = free_.front();
-            free_.pop_front();
             Worker& w = workers_[wi];
             w.tickets.clear();
             w.bytes = 0;
             std::vector<vqm_cu_image> os, ds;
             float background = 0.5f;
+            const size_t others = stats_.device_bytes - w.held;
+            // Take requests while their estimate fits, then shrink the batch
+            // until the worker's own count of the memory it will hold fits.
             while (!queue_.empty() && w.tickets.size() < max_pairs_) {
                 Request* r = requests_.at(queue_.front()).get();
                 // One background per batch: a request with another one starts
                 // the next batch.
                 if (!w.tickets.empty() && r->background != background) break;
-                if (w.bytes + r->bytes > per_worker_) break;
+                if (!w.tickets.empty() && (others > budget_ ||
+                                           w.bytes + r->bytes > budget_ - others))
+                    break;
                 background = r->background;
                 w.bytes += r->bytes;
                 w.tickets.push_back(queue_.front());
@@ -220,6 +286,39 @@ private:
                 ds.push_back(r->d);
                 queue_.pop_front();
             }
+            while (!w.tickets.empty() && !Fits(w, os, ds, others)) {
+                queue_.push_front(w.tickets.back());
+                w.bytes -= requests_.at(w.tickets.back())->bytes;
+                w.tickets.pop_back();
+                os.pop_back();
+                ds.pop_back();
+            }
+            if (w.tickets.empty()) {
+                // The head request does not fit beside what the workers hold:
+                // free the idle workers' memory and try again, or wait for a
+                // running batch to finish (and become idle) first.
+                if (TrimIdle()) continue;
+                if (!inflight_.empty()) {
+                    // The completer finishes in-flight batches whether or
+                    // not the server is stopping, so this wait ends.
+                    const uint64_t seen = completions_;
+                    work_cv_.wait(lock, [&] { return completions_ != seen; });
+                    continue;
+                }
+                // Everything is idle and freed, and still no fit: the pair is
+                // larger than the budget by the workers' exact count.
+                Request* r = requests_.at(queue_.front()).get();
+                r->status = VQM_CU_INVALID_ARGUMENT;
+                r->error = "server: the pair needs more device memory than the budget";
+                r->completed = Clock::now();
+                r->done = true;
+                ++stats_.failed;
+                queue_.pop_front();
+                stats_.queued = queue_.size();
+                done_cv_.notify_all();
+                continue;
+            }
+            free_.pop_front();
             stats_.queued = queue_.size();
             stats_.bytes_in_flight += w.bytes;
             stats_.peak_bytes = std::max(stats_.peak_bytes, stats_.bytes_in_flight);
@@ -229,7 +328,10 @@ private:
             const int rc = vqm_cu_ss2_batch_submit(w.batch, static_cast<uint32_t>(os.size()),
                                                    os.data(), ds.data(), background, &token);
             const std::string msg = rc == VQM_CU_OK ? std::string() : vqm_cu_last_error();
+            uint64_t held = 0;
+            if (vqm_cu_ss2_batch_device_bytes(w.batch, &held) != VQM_CU_OK) held = w.held;
             lock.lock();
+            SetHeld(w, static_cast<size_t>(held));
             if (rc != VQM_CU_OK) {
                 Fail(w, rc, msg);
                 free_.push_back(wi);
@@ -283,6 +385,7 @@ private:
                 stats_.bytes_in_flight -= w.bytes;
             }
             free_.push_back(wi);
+            ++completions_;
             done_cv_.notify_all();
             work_cv_.notify_one();
         }
@@ -306,7 +409,8 @@ private:
         done_cv_.notify_all();
     }
 
-    size_t budget_ = 0, per_worker_ = 0;
+    size_t budget_ = 0;
+    uint64_t completions_ = 0;  // batches finished, for a dispatcher waiting on one
     uint32_t max_pairs_ = 64;
     int variant_ = 0;
     std::vector<Worker> workers_;

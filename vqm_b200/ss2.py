@@ -176,7 +176,7 @@ class _ServerConfig(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in (
         "submitted", "completed", "failed", "batches", "largest_batch", "bytes_in_flight",
-        "peak_bytes", "queued")]
+        "peak_bytes", "queued", "budget_bytes", "device_bytes", "peak_device_bytes", "trims")]
 
 
 class MemoryUsage(ctypes.Structure):
@@ -227,6 +227,9 @@ _SIGS = {
     "vqm_cu_ss2_blur_variants": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_decode_path": ([_P, ctypes.c_uint32, _P], ctypes.c_int),
     "vqm_cu_ss2_batch_stage_ms": ([_P, _P], ctypes.c_int),
+    "vqm_cu_ss2_batch_device_bytes": ([_P, _P], ctypes.c_int),
+    "vqm_cu_ss2_batch_device_bytes_after": ([_P, ctypes.c_uint32, _P, _P, _P], ctypes.c_int),
+    "vqm_cu_ss2_batch_trim": ([_P], ctypes.c_int),
     "vqm_cu_ss2_batch_compute": ([_P, ctypes.c_uint32, _P, _P, ctypes.c_float, _P, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_server_create": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_server_destroy": ([_P], ctypes.c_int),
@@ -628,7 +631,8 @@ class Ssimulacra2Batch:
         """`variant` picks a compiled blur kernel (see blur_variants());
         `tile` picks the one-tile-per-CTA kernel of that output tile;
         neither: each submit picks a 32x32 strip length from its tile count
-        (the results are the same whichever runs). `half_planes` stores the
+        (strips regroup the compensated partial sums, so results agree to
+        rounding, ~1e-7 relative, whichever runs). `half_planes` stores the
         pyramid as binary16 (ssimulacra2.h:41-46)."""
         tw, th = tile if tile else (0, 0)
         v = 0 if variant is None else variant + 1
@@ -664,6 +668,25 @@ class Ssimulacra2Batch:
         ms = (ctypes.c_float * 3)()
         _check(_lib.vqm_cu_ss2_batch_stage_ms(self._b, ms))
         return tuple(ms)
+
+    def device_bytes(self) -> int:
+        """Device memory the batch holds now (reused from submit to submit)."""
+        out = ctypes.c_uint64()
+        _check(_lib.vqm_cu_ss2_batch_device_bytes(self._b, ctypes.byref(out)))
+        return out.value
+
+    def device_bytes_after(self, pairs) -> int:
+        """Device memory the batch will hold once `pairs` are submitted
+        (validated as submit would; nothing is allocated)."""
+        n, origs, dists = self._arrays(pairs)
+        out = ctypes.c_uint64()
+        _check(_lib.vqm_cu_ss2_batch_device_bytes_after(self._b, n, origs, dists,
+                                                         ctypes.byref(out)))
+        return out.value
+
+    def trim(self):
+        """Frees the device memory of an idle batch."""
+        _check(_lib.vqm_cu_ss2_batch_trim(self._b))
 
     @staticmethod
     def _arrays(pairs):
@@ -839,12 +862,17 @@ class Ssimulacra2Server:
 
     ``submit`` queues a pair and returns at once with a ticket; a dispatcher
     thread forms batches from the queue in arrival order whenever one of
-    ``workers`` batch scorers is free, admitting a batch only while its device
-    footprint fits ``memory_budget / workers``; a completion thread finishes
-    batches in order. ``wait`` returns the pair's result and its latency from
-    submit to completion. The images of a request are kept referenced here
-    until its wait returns. A request's result is bit-identical to scoring
-    the pair alone."""
+    ``workers`` batch scorers is free, admitting a batch only while the
+    device memory all workers hold together (counted as allocated) stays
+    within ``memory_budget`` (lowered to the device's free memory less
+    256 MiB if that is smaller), freeing idle workers' memory when the next
+    request needs it; a completion thread finishes batches in order.
+    ``wait`` returns the pair's result and its latency from submit to
+    completion. The images of a request are kept referenced here until its
+    wait returns. A request's result is bit-identical to scoring the pair
+    alone with the same blur kernel (``variant``, as Ssimulacra2Batch's plus
+    one; 0 lets each batch pick a strip length from its size, and results
+    then agree to rounding, ~1e-7 relative)."""
 
     def __init__(self, memory_budget: int = 0, workers: int = 2, max_batch_pairs: int = 64,
                  chroma_filter: int = 0, device: int = -1, variant: int = 0):
