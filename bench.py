@@ -873,7 +873,7 @@ def main(argv=None):
             "step_roofline": {"alg_bytes_per_pair": pair_b,
                               "achieved_gbs": pair_b * value / world / 1e9,
                               "frac": pair_b * value / world / 1e9 / peak},
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": 2 * args.steps,  # prepare + blur (finalize is the blur's epilogue)
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
             "parity": parity,

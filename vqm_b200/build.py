@@ -26,7 +26,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CUDA_SOURCES = ["ss2_prepare.cu", "ss2_blur.cu", "ss2_finalize.cu", "ss2_runtime.cu",
+CUDA_SOURCES = ["ss2_prepare.cu", "ss2_blur.cu", "ss2_runtime.cu",
                 "ss2_noalloc.cu"]
 HOST_SOURCES = ["ss2_host.cc", "ss2_server.cc"]
 HEADERS = ["ss2_device.cuh", "ss2_decode.cuh", "ss2_detmath.h", "ss2_kernels.h", "ss2_host.h",

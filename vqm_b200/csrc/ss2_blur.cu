@@ -21,8 +21,13 @@
 //      again two lanes per instruction, then evaluates the maps of its eight
 //      pixels and keeps six running sums.
 //   4. The CTA's six sums are combined with two-sum compensation into one
-//      partial per CTA (its tile, or its strip of tiles below); the finalize
-//      kernel adds the partials in FP64.
+//      partial per CTA (its tile, or its strip of tiles below).
+//   5. The CTA that writes a segment's last partial adds the segment's
+//      partials in FP64, and the one that completes a pair's last segment
+//      turns the pair's sums into its 108 norms and FP64 score (the
+//      reference's reduce.comp:21-63, ReadResult in vulkan.cc:545-583 and
+//      Score in score.cc:118-163): no separate finalize launch. Counters
+//      decide who is last; no CTA ever waits for another.
 // A persistent form keeps each CTA resident and copies its next tile's
 // window into a second buffer while it computes the current one; a strip
 // form walks a few tiles down one column and reuses the horizontal results
@@ -42,6 +47,8 @@ namespace vqm_b200 {
 namespace {
 
 __constant__ float c_taps[kTaps];
+// score.cc:38-87, flat rows channel * scales + scale.
+__constant__ double c_weights[18][6];
 
 // The last prefix entry <= index (start[0] == 0 <= index < start[count]).
 __device__ __forceinline__ uint32_t FindSlot(const uint32_t* __restrict__ start,
@@ -94,6 +101,7 @@ struct TileRef {
     const float* pb;
     uint32_t pitch;    // floats per row pair
     uint32_t partial;  // index of the tile's partial
+    uint32_t segment;  // index of its segment
     int w, h, x0, y0;
 };
 
@@ -101,7 +109,7 @@ struct TileRef {
 // binary16 elements (typed float* only to share the struct).
 template <int TW, int TH, bool kHalf = false>
 __device__ __forceinline__ TileRef SegmentTile(const DevBatch& batch, const DevSegment& seg,
-                                               uint32_t tx, uint32_t ty) {
+                                               uint32_t si, uint32_t tx, uint32_t ty) {
     const DevPair& P = batch.pair[seg.pair];
     TileRef t;
     if (kHalf) {
@@ -118,6 +126,7 @@ __device__ __forceinline__ TileRef SegmentTile(const DevBatch& batch, const DevS
     t.x0 = static_cast<int>(tx * TW);
     t.y0 = static_cast<int>(ty * TH);
     t.partial = seg.partial_first + ty * seg.tiles_x + tx;
+    t.segment = si;
     return t;
 }
 
@@ -128,7 +137,7 @@ __device__ __forceinline__ TileRef LocateTile(const DevBatch& batch, uint32_t bl
     const DevSegment seg = batch.seg[si];
     const uint32_t tile = blk - __ldg(&batch.blur_start[si]);
     const uint32_t ty = tile / seg.tiles_x;
-    return SegmentTile<TW, TH, kHalf>(batch, seg, tile - ty * seg.tiles_x, ty);
+    return SegmentTile<TW, TH, kHalf>(batch, seg, si, tile - ty * seg.tiles_x, ty);
 }
 
 // Asynchronous 16-byte global-to-shared copy; a source size of 0 writes
@@ -428,9 +437,125 @@ __device__ __forceinline__ void ReducePartials(const float2 (&sum)[6], Scratch r
     __syncthreads();
 }
 
+// score.cc:118-163 in FP64 on the device.
+__device__ __noinline__ double ScoreFromNorms(const double* norms, int scales) {
+    double error = 0.0;
+    for (int c = 0; c < 3; ++c)
+        for (int s = 0; s < scales; ++s) {
+            const double* wt = c_weights[c * scales + s];
+            const double* ssim = norms + s * 18;
+            const double* edge = norms + s * 18 + 6;
+            error += wt[0] * fabs(ssim[c * 2 + 0]);
+            error += wt[1] * fabs(edge[c * 4 + 0]);
+            error += wt[2] * fabs(edge[c * 4 + 2]);
+            error += wt[3] * fabs(ssim[c * 2 + 1]);
+            error += wt[4] * fabs(edge[c * 4 + 1]);
+            error += wt[5] * fabs(edge[c * 4 + 3]);
+        }
+    if (!isfinite(error)) return nan("");
+    const double scaled = error * 0.9562382616834844;
+    const double mapped = 2.326765642916932 * scaled -
+                          0.020884521182843837 * scaled * scaled +
+                          6.248496625763138e-05 * scaled * scaled * scaled;
+    if (!isfinite(mapped)) return nan("");
+    if (mapped > 0.0) return 100.0 - 10.0 * pow(mapped, 0.6276336467831387);
+    return 100.0;
+}
+
+// The pair's 108 norms from its segments' FP64 sums (vulkan.cc:545-583:
+// mean = sum / (W_l H_l), 4-norm = sqrt(sqrt(sum4 / (W_l H_l)))), written
+// straight into its result block (zeros for pruned channels and levels past
+// its scales), then its score and scale count. One thread; out of line, as
+// it runs once per pair and should cost the blur loops no registers.
+__device__ __noinline__ void WritePairResult(const DevBatch& batch, const DevPair& P) {
+    double* out = P.result;
+    for (int i = 0; i < 108; ++i) out[i] = 0.0;
+    for (uint32_t k = 0; k < P.seg_count; ++k) {
+        const uint32_t sk = P.seg_first + k;
+        const DevSegment g = batch.seg[sk];
+        const double inv = 1.0 / (static_cast<double>(P.w[g.level]) *
+                                  static_cast<double>(P.h[g.level]));
+        const double* v = batch.seg_sums + static_cast<size_t>(sk) * 6;
+        double* o = out + g.level * 18;
+        const int c = static_cast<int>(g.channel);
+        o[c * 2 + 0] = inv * __ldcg(v + 0);
+        o[c * 2 + 1] = sqrt(sqrt(inv * __ldcg(v + 1)));
+        o[6 + c * 4 + 0] = inv * __ldcg(v + 2);
+        o[6 + c * 4 + 1] = sqrt(sqrt(inv * __ldcg(v + 3)));
+        o[6 + c * 4 + 2] = inv * __ldcg(v + 4);
+        o[6 + c * 4 + 3] = sqrt(sqrt(inv * __ldcg(v + 5)));
+    }
+    out[kResultScore] = ScoreFromNorms(out, static_cast<int>(P.levels));
+    out[kResultScales] = static_cast<double>(P.levels);
+    out[kResultStatus] = 0.0;
+}
+
+// Called by every thread of a blur CTA once its partial of segment `si` is
+// written (after a barrier). The CTA whose partial completes the segment
+// adds the segment's partials in FP64 in a fixed order (thread t takes
+// partials t, t + NT, ..., then a butterfly and the warps in turn), so a
+// result repeats bit for bit; the CTA whose segment completes the pair
+// writes the pair's result. Each counter is reset by the CTA that finds it
+// complete, so the next launch starts from zero. `scratch` is shared memory
+// for 6 * NT / 32 + 2 doubles that no thread still reads.
+// The CTA that completed segment `si`: its FP64 sum, then the pair's result
+// if the segment completes the pair.
+template <int NT>
+__device__ __forceinline__ void SumSegment(const DevBatch& batch, uint32_t si, double* scratch) {
+    const uint32_t tid = threadIdx.x;
+    volatile uint32_t* flag = reinterpret_cast<volatile uint32_t*>(scratch + 6 * (NT / 32));
+    const DevSegment seg = batch.seg[si];
+    __threadfence();
+    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (uint32_t t = tid; t < seg.partials; t += NT) {
+        const double* p = batch.partials + (static_cast<size_t>(seg.partial_first) + t) * 6;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[k] += __ldcg(p + k);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], off);
+    if (tid % 32 == 0)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) scratch[(tid / 32) * 6 + k] = acc[k];
+    __syncthreads();
+    if (tid < 6) {
+        double sum = 0.0;
+        for (int w = 0; w < NT / 32; ++w) sum += scratch[w * 6 + tid];
+        batch.seg_sums[static_cast<size_t>(si) * 6 + tid] = sum;
+        __threadfence();
+    }
+    __syncthreads();
+    const DevPair& P = batch.pair[seg.pair];
+    if (tid == 0) {
+        batch.seg_done[si] = 0u;
+        flag[1] = atomicAdd(&batch.pair_done[seg.pair], 1u) + 1u == P.seg_count;
+    }
+    __syncthreads();
+    if (!flag[1]) return;
+    __threadfence();
+    if (tid == 0) {
+        WritePairResult(batch, P);
+        batch.pair_done[seg.pair] = 0u;
+    }
+}
+
+template <int NT>
+__device__ __forceinline__ void FinishSegment(const DevBatch& batch, uint32_t si,
+                                              double* scratch) {
+    volatile uint32_t* flag = reinterpret_cast<volatile uint32_t*>(scratch + 6 * (NT / 32));
+    if (threadIdx.x == 0) {
+        __threadfence();  // this CTA's partial, before the count that publishes it
+        flag[0] = atomicAdd(&batch.seg_done[si], 1u) + 1u == __ldg(&batch.seg[si].partials);
+    }
+    __syncthreads();
+    if (flag[0]) SumSegment<NT>(batch, si, scratch);
+}
+
 template <int TW, int TH, int NT>
 __device__ __forceinline__ void ComputeTile(float* src, float* hq, const TileRef& t,
-                                            double* partials) {
+                                            const DevBatch& batch) {
     HorizontalPass<TW, TH, NT>(src, hq);
     __syncthreads();
     float2 sum[6];
@@ -441,7 +566,9 @@ __device__ __forceinline__ void ComputeTile(float* src, float* hq, const TileRef
     else
         VerticalMaps<TW, TH, NT, true>(src, hq, t, sum);
     __syncthreads();  // the reduction overwrites the source window
-    ReducePartials<NT>(sum, LinearScratch<NT>{src}, partials + static_cast<size_t>(t.partial) * 6);
+    ReducePartials<NT>(sum, LinearScratch<NT>{src},
+                       batch.partials + static_cast<size_t>(t.partial) * 6);
+    FinishSegment<NT>(batch, t.segment, reinterpret_cast<double*>(src));
 }
 
 // One output tile per CTA; MB CTAs per SM is the occupancy the shared
@@ -462,7 +589,7 @@ __global__ void __launch_bounds__(NT, MB) Ss2BlurKernel(DevBatch batch) {
         ConvertHalfTile<TW, TH, NT>(smem + T::kSrcBytes, src);
         __syncthreads();
     }
-    ComputeTile<TW, TH, NT>(src, hq, t, batch.partials);
+    ComputeTile<TW, TH, NT>(src, hq, t, batch);
 }
 
 // Persistent: each CTA walks tiles blockIdx.x, + gridDim.x, ... and copies
@@ -492,7 +619,7 @@ __global__ void __launch_bounds__(NT, MB) Ss2BlurPersistentKernel(DevBatch batch
         CpAsyncCommit();   // possibly empty, so the group count stays uniform
         CpAsyncWait<1>();  // everything but the newest group: this tile's
         __syncthreads();
-        ComputeTile<TW, TH, NT>(now, hq, cur, batch.partials);
+        ComputeTile<TW, TH, NT>(now, hq, cur, batch);
         cur = nxt;
         b ^= 1;
     }
@@ -554,7 +681,7 @@ __global__ void __launch_bounds__(NT, MB) Ss2BlurStripKernel(DevBatch batch) {
     const uint32_t tiles_y = seg.tiles / seg.tiles_x;
     const uint32_t ty0 = sy * S;
     const int count = static_cast<int>(min(static_cast<uint32_t>(S), tiles_y - ty0));
-    TileRef t = SegmentTile<TW, TH>(batch, seg, strip - sy * seg.tiles_x, ty0);
+    TileRef t = SegmentTile<TW, TH>(batch, seg, si, strip - sy * seg.tiles_x, ty0);
     IssueTileLoads<TW, TH, NT>(src, t);
     CpAsyncCommit();
     float2 sum[6];
@@ -579,6 +706,7 @@ __global__ void __launch_bounds__(NT, MB) Ss2BlurStripKernel(DevBatch batch) {
     }
     ReducePartials<NT>(sum, HqScratch<TW, TH, NT>{hq},
                        batch.partials + (static_cast<size_t>(seg.partial_first) + strip) * 6);
+    FinishSegment<NT>(batch, si, reinterpret_cast<double*>(src));
 }
 
 // The variants compiled in: {tile width, tile height, threads, persistent,
@@ -699,7 +827,7 @@ cudaError_t Dispatch(const DevBatch& b, int variant, cudaStream_t stream, bool l
 cudaError_t SetConstants(const float* taps13, const double* weights108) {
     cudaError_t e = cudaMemcpyToSymbol(c_taps, taps13, sizeof(float) * kTaps);
     if (e != cudaSuccess) return e;
-    return SetScoreWeights(weights108);
+    return cudaMemcpyToSymbol(c_weights, weights108, sizeof(double) * 108);
 }
 
 cudaError_t LaunchBlur(const DevBatch& b, int variant, cudaStream_t stream) {

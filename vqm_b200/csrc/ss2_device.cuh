@@ -142,9 +142,10 @@ struct DevBatch {
     // order.
     const uint32_t* prep_start;
     const uint32_t* blur_start;  // segments + 1 prefix offsets
-    double* partials;            // 6 doubles per blur tile
+    double* partials;            // 6 doubles per blur partial (segment.partials each)
     double* seg_sums;            // 6 doubles per segment
-    uint32_t* pair_done;         // per pair: segments finalized so far
+    uint32_t* pair_done;         // per pair: segments summed so far (0 between launches)
+    uint32_t* seg_done;          // per segment: partials written so far (0 between launches)
     uint32_t* status;            // nonzero: a kernel found bad input
     uint32_t half;               // 1: pyramid elements are binary16
 };

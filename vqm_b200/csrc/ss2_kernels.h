@@ -10,19 +10,19 @@ namespace vqm_b200 {
 // Gaussian taps (13 floats) and score weights (18 x 6 doubles) into the
 // current device's constant banks; once per device.
 cudaError_t SetConstants(const float* taps13, const double* weights108);
-// The score weights alone (ss2_finalize.cu); SetConstants calls it.
-cudaError_t SetScoreWeights(const double* weights108);
 
 cudaError_t LaunchPrepare(const DevBatch& batch, cudaStream_t stream);
 // `variant` indexes the blur kernels compiled in (BlurTileShape gives each
 // one's output tile); the batch's segments must have been tiled with it.
+// The blur also finishes every pair: its last CTA per segment sums the
+// segment, its last per pair writes the pair's norms and score, so the
+// batch's pair_done and seg_done counters must be zero when it starts (the
+// kernel leaves them zero).
 cudaError_t LaunchBlur(const DevBatch& batch, int variant, cudaStream_t stream);
-cudaError_t LaunchFinalize(const DevBatch& batch, cudaStream_t stream);
 // Load every kernel of each stage on the current device (and set the blur
 // kernels' shared-memory limits), so that no first launch pays for it.
 cudaError_t PreloadPrepare();
 cudaError_t PreloadBlur();
-cudaError_t PreloadFinalize();
 
 // The blur variants compiled into the library and their output tiles.
 int BlurTileCount();
@@ -37,7 +37,8 @@ uint32_t BlurBlocks(int index, uint32_t tiles_x, uint32_t tiles_y);
 // The variant used when a caller does not choose one, for a launch of
 // `tiles` output tiles of the default variant on a device with `sms` SMs:
 // the default itself for small launches, a strip of its tile for large ones.
-// Both reduce each tile alike, so the choice never changes a result.
+// A strip regroups the compensated partial sums, so the choice moves a
+// result by rounding only (~1e-7 relative).
 int AutoBlurVariant(uint64_t tiles, int sms);
 // The one-tile-per-CTA variant with variant's tile shape (the variant
 // itself when it is one), which half planes run; -1 when there is none.

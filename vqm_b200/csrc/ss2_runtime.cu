@@ -77,7 +77,6 @@ void EnsureDevice(int device) {
     // or the first that selects a new blur variant, would pay for it.
     VQM_CK(PreloadPrepare());
     VQM_CK(PreloadBlur());
-    VQM_CK(PreloadFinalize());
     ready[device] = true;
 }
 
@@ -361,7 +360,7 @@ struct BatchMemory {
         return {table_bytes, std::max<size_t>(t.pyramid_floats, 64) * elem_bytes,
                 std::max<size_t>(t.partials, 1) * 6 * sizeof(double),
                 std::max<size_t>(t.segs.size(), 1) * 6 * sizeof(double),
-                std::max<size_t>(t.pairs.size(), 1) * sizeof(uint32_t),
+                (t.pairs.size() + t.segs.size() + 1) * sizeof(uint32_t),
                 std::max<size_t>(t.pairs.size(), 1) * kResultDoubles * sizeof(double)};
     }
     std::array<DeviceBuffer*, 6> Buffers() {
@@ -405,6 +404,7 @@ struct BatchMemory {
         dev.partials = partials.as<double>();
         dev.seg_sums = seg_sums.as<double>();
         dev.pair_done = pair_done.as<uint32_t>();
+        dev.seg_done = pair_done.as<uint32_t>() + t.pairs.size();
         dev.status = nullptr;
         dev.half = elem_bytes == 2 ? 1u : 0u;
         return moved;
@@ -443,14 +443,14 @@ struct BatchMemory {
                                cudaMemcpyHostToDevice, s));
     }
     // ev, when given, holds 4 timing events recorded before prepare and
-    // after each of the three stages.
+    // after prepare, blur and the (fused) finalize: the last two are back
+    // to back, the finalize work being the blur's epilogue.
     void EnqueueKernels(BlurShape shape, cudaStream_t s, cudaEvent_t* ev = nullptr) {
         if (ev) VQM_CK(cudaEventRecord(ev[0], s));
         VQM_CK(LaunchPrepare(dev, s));
         if (ev) VQM_CK(cudaEventRecord(ev[1], s));
         VQM_CK(LaunchBlur(dev, shape.variant, s));
         if (ev) VQM_CK(cudaEventRecord(ev[2], s));
-        VQM_CK(LaunchFinalize(dev, s));
         if (ev) VQM_CK(cudaEventRecord(ev[3], s));
     }
     void EnqueueReadback(cudaStream_t s) {
@@ -1142,7 +1142,8 @@ public:
         mem_.Stage(t);
         if (host_bytes) VQM_CK(cudaEventRecord(copied_, stream_));
         mem_.EnqueueUpload(mem_.table_bytes, stream_);
-        VQM_CK(cudaMemsetAsync(mem_.pair_done.as<void>(), 0, sizeof(uint32_t) * n, stream_));
+        VQM_CK(cudaMemsetAsync(mem_.pair_done.as<void>(), 0,
+                               sizeof(uint32_t) * (n + t.segs.size()), stream_));
         mem_.EnqueueKernels(shape, stream_, timing_ ? stage_ev_ : nullptr);
         timed_ = timing_;
         mem_.EnqueueReadback(stream_);
