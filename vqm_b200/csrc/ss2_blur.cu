@@ -46,7 +46,9 @@
 namespace vqm_b200 {
 namespace {
 
-__constant__ float c_taps[kTaps];
+// The 13 Gaussian taps as (w, w) pairs: the two-lane multiply-adds take a
+// tap for both lanes straight from the constant bank.
+__constant__ float2 c_taps2[kTaps];
 // score.cc:38-87, flat rows channel * scales + scale.
 __constant__ double c_weights[18][6];
 
@@ -294,10 +296,10 @@ __device__ __forceinline__ void HorizontalPass(const float* src, float* hq, int 
                               : __fmul2_rn(A[j], B[j]);
             float2 acc[KH];
 #pragma unroll
-            for (int k = 0; k < KH; ++k) acc[k] = __fmul2_rn(Pack(c_taps[0]), S[k]);
+            for (int k = 0; k < KH; ++k) acc[k] = __fmul2_rn(c_taps2[0], S[k]);
 #pragma unroll
             for (int tap = 1; tap < kTaps; ++tap) {
-                const float2 wt = Pack(c_taps[tap]);
+                const float2 wt = c_taps2[tap];
 #pragma unroll
                 for (int k = 0; k < KH; ++k) acc[k] = __ffma2_rn(wt, S[k + tap], acc[k]);
             }
@@ -334,9 +336,9 @@ __device__ __forceinline__ void VerticalMaps(const float* src, const float* hq, 
                 M[i] = *reinterpret_cast<const float2*>(plane + i * TW + cols[(i >> 1) & 1]);
 #pragma unroll
             for (int j = 0; j < RV; ++j) {
-                float2 acc = __fmul2_rn(Pack(c_taps[0]), M[j]);
+                float2 acc = __fmul2_rn(c_taps2[0], M[j]);
 #pragma unroll
-                for (int k = 1; k < kTaps; ++k) acc = __ffma2_rn(Pack(c_taps[k]), M[j + k], acc);
+                for (int k = 1; k < kTaps; ++k) acc = __ffma2_rn(c_taps2[k], M[j + k], acc);
                 V[q][j] = acc;
             }
         }
@@ -668,15 +670,13 @@ __device__ __forceinline__ void MoveHalo(float* hq) {
     }
 }
 
-template <int TW, int TH, int NT, int MB, int S>
-__global__ void __launch_bounds__(NT, MB) Ss2BlurStripKernel(DevBatch batch) {
-    using T = Tile<TW, TH, NT>;
-    extern __shared__ __align__(16) unsigned char smem[];
-    float* src = reinterpret_cast<float*>(smem);
-    float* hq = reinterpret_cast<float*>(smem + T::kSrcBytes);
-    const uint32_t si = FindSlot(batch.blur_start, batch.segments, blockIdx.x);
+// Strip `block` of the launch (blur_start counts strips).
+template <int TW, int TH, int NT, int S>
+__device__ __forceinline__ void RunStrip(const DevBatch& batch, uint32_t block, float* src,
+                                         float* hq) {
+    const uint32_t si = FindSlot(batch.blur_start, batch.segments, block);
     const DevSegment seg = batch.seg[si];
-    const uint32_t strip = blockIdx.x - __ldg(&batch.blur_start[si]);
+    const uint32_t strip = block - __ldg(&batch.blur_start[si]);
     const uint32_t sy = strip / seg.tiles_x;
     const uint32_t tiles_y = seg.tiles / seg.tiles_x;
     const uint32_t ty0 = sy * S;
@@ -709,7 +709,42 @@ __global__ void __launch_bounds__(NT, MB) Ss2BlurStripKernel(DevBatch batch) {
     FinishSegment<NT>(batch, si, reinterpret_cast<double*>(src));
 }
 
-// The variants compiled in: {tile width, tile height, threads, persistent,
+template <int TW, int TH, int NT, int MB, int S>
+__global__ void __launch_bounds__(NT, MB) Ss2BlurStripKernel(DevBatch batch) {
+    using T = Tile<TW, TH, NT>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    RunStrip<TW, TH, NT, S>(batch, blockIdx.x, reinterpret_cast<float*>(smem),
+                            reinterpret_cast<float*>(smem + T::kSrcBytes));
+}
+
+// A tile queue: as many CTAs as the device holds at once, each taking the
+// next strip from a device counter (batch.blur_queue[0]) until none is left.
+// The strips are the launch's work items in segment order (pair, level,
+// channel); a CTA never waits for another. The last CTA to leave resets the
+// counter and the exit count (blur_queue[1]) for the next launch.
+template <int TW, int TH, int NT, int MB, int S>
+__global__ void __launch_bounds__(NT, MB) Ss2BlurQueueKernel(DevBatch batch) {
+    using T = Tile<TW, TH, NT>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* src = reinterpret_cast<float*>(smem);
+    float* hq = reinterpret_cast<float*>(smem + T::kSrcBytes);
+    __shared__ uint32_t next;
+    for (;;) {
+        if (threadIdx.x == 0) next = atomicAdd(&batch.blur_queue[0], 1u);
+        __syncthreads();
+        const uint32_t block = next;
+        __syncthreads();  // every thread has read `next` before it changes
+        if (block >= batch.blur_blocks) break;
+        RunStrip<TW, TH, NT, S>(batch, block, src, hq);
+    }
+    if (threadIdx.x == 0 && atomicAdd(&batch.blur_queue[1], 1u) + 1u == gridDim.x) {
+        batch.blur_queue[0] = 0u;
+        batch.blur_queue[1] = 0u;
+    }
+}
+
+// The variants compiled in: {tile width, tile height, threads, persistent
+// (1: grid-stride with a second copy buffer, 2: strips from a tile queue),
 // CTAs per SM, tiles per CTA (a strip of that many; 1 = one tile)}.
 struct BlurVariant {
     int w, h, threads, persistent, per_sm, strip;
@@ -718,7 +753,8 @@ constexpr BlurVariant kBlurVariants[] = {
     {32, 32, 128, 0, 5, 1}, {32, 28, 128, 0, 5, 1}, {64, 32, 256, 0, 2, 1},
     {64, 20, 256, 0, 3, 1}, {32, 32, 128, 1, 3, 1}, {32, 20, 128, 1, 5, 1},
     {64, 32, 256, 1, 1, 1}, {32, 32, 128, 0, 5, 2}, {32, 32, 128, 0, 5, 4},
-    {32, 32, 128, 0, 5, 8}, {32, 28, 128, 0, 5, 4},
+    {32, 32, 128, 0, 5, 8}, {32, 28, 128, 0, 5, 4}, {32, 32, 128, 0, 5, 16},
+    {32, 32, 128, 2, 5, 8},
 };
 constexpr int kBlurVariantCount = sizeof(kBlurVariants) / sizeof(kBlurVariants[0]);
 
@@ -794,6 +830,21 @@ cudaError_t LaunchPersistent(const DevBatch& b, cudaStream_t stream, bool launch
 }
 
 template <int TW, int TH, int NT, int MB, int S>
+cudaError_t LaunchQueue(const DevBatch& b, cudaStream_t stream, bool launch) {
+    using T = Tile<TW, TH, NT>;
+    static LaunchCache cache;
+    constexpr size_t smem = T::kSrcBytes + T::kHqBytes;
+    int grid = 0;
+    const cudaError_t e =
+        Prepare(Ss2BlurQueueKernel<TW, TH, NT, MB, S>, smem, cache, NT, true, &grid);
+    if (e != cudaSuccess || !launch) return e;
+    const uint32_t blocks = b.blur_blocks < static_cast<uint32_t>(grid) ? b.blur_blocks
+                                                                        : static_cast<uint32_t>(grid);
+    Ss2BlurQueueKernel<TW, TH, NT, MB, S><<<blocks, NT, smem, stream>>>(b);
+    return cudaGetLastError();
+}
+
+template <int TW, int TH, int NT, int MB, int S>
 cudaError_t LaunchStrips(const DevBatch& b, cudaStream_t stream, bool launch) {
     using T = Tile<TW, TH, NT>;
     static LaunchCache cache;
@@ -818,6 +869,8 @@ cudaError_t Dispatch(const DevBatch& b, int variant, cudaStream_t stream, bool l
         case 8: return LaunchStrips<32, 32, 128, 5, 4>(b, stream, launch);
         case 9: return LaunchStrips<32, 32, 128, 5, 8>(b, stream, launch);
         case 10: return LaunchStrips<32, 28, 128, 5, 4>(b, stream, launch);
+        case 11: return LaunchStrips<32, 32, 128, 5, 16>(b, stream, launch);
+        case 12: return LaunchQueue<32, 32, 128, 5, 8>(b, stream, launch);
     }
     return cudaErrorInvalidValue;
 }
@@ -825,7 +878,9 @@ cudaError_t Dispatch(const DevBatch& b, int variant, cudaStream_t stream, bool l
 }  // namespace
 
 cudaError_t SetConstants(const float* taps13, const double* weights108) {
-    cudaError_t e = cudaMemcpyToSymbol(c_taps, taps13, sizeof(float) * kTaps);
+    float2 pairs[kTaps];
+    for (int i = 0; i < kTaps; ++i) pairs[i] = make_float2(taps13[i], taps13[i]);
+    cudaError_t e = cudaMemcpyToSymbol(c_taps2, pairs, sizeof(pairs));
     if (e != cudaSuccess) return e;
     return cudaMemcpyToSymbol(c_weights, weights108, sizeof(double) * 108);
 }

@@ -146,6 +146,7 @@ struct DevBatch {
     double* seg_sums;            // 6 doubles per segment
     uint32_t* pair_done;         // per pair: segments summed so far (0 between launches)
     uint32_t* seg_done;          // per segment: partials written so far (0 between launches)
+    uint32_t* blur_queue;        // the tile queue's next strip and exit count (0 between launches)
     uint32_t* status;            // nonzero: a kernel found bad input
     uint32_t half;               // 1: pyramid elements are binary16
 };

@@ -71,13 +71,13 @@ struct PairTables {
 static_assert(sizeof(PairTables) < 30000, "kernel parameter space");
 
 // `counters`: the pair's and every segment's completion counter, which the
-// blur's epilogue counts up; they must start at zero whatever the last call
-// left.
+// blur's epilogue counts up, and the blur's tile-queue words; they must
+// start at zero whatever the last call left.
 __global__ void StageTablesKernel(const PairTables tables, PairTables* dst, uint32_t* counters) {
     const uint32_t* from = reinterpret_cast<const uint32_t*>(&tables);
     uint32_t* to = reinterpret_cast<uint32_t*>(dst);
     for (uint32_t i = threadIdx.x; i < sizeof(PairTables) / 4; i += blockDim.x) to[i] = from[i];
-    if (threadIdx.x < 1 + kMaxSegments) counters[threadIdx.x] = 0u;
+    if (threadIdx.x < 3 + kMaxSegments) counters[threadIdx.x] = 0u;
 }
 
 struct DeviceState {
@@ -210,7 +210,7 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
     // partials | pyramid], each 256-byte aligned.
     const size_t off_tables = 0;
     const size_t off_done = Align(off_tables + sizeof(PairTables), 256);
-    const size_t off_sums = Align(off_done + sizeof(uint32_t) * (1 + kMaxSegments), 256);
+    const size_t off_sums = Align(off_done + sizeof(uint32_t) * (3 + kMaxSegments), 256);
     const size_t off_partials = Align(off_sums + sizeof(double) * 6 * kMaxSegments, 256);
     const size_t off_pyramid = Align(off_partials + sizeof(double) * 6 * tiles, 256);
     const size_t need = off_pyramid + sizeof(float) * 2 * floats;
@@ -279,6 +279,7 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
     b.seg_sums = reinterpret_cast<double*>(base + off_sums);
     b.pair_done = pair_done;
     b.seg_done = pair_done + 1;
+    b.blur_queue = pair_done + 1 + kMaxSegments;
     b.status = nullptr;
 
     cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);

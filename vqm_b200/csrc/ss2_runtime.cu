@@ -360,7 +360,7 @@ struct BatchMemory {
         return {table_bytes, std::max<size_t>(t.pyramid_floats, 64) * elem_bytes,
                 std::max<size_t>(t.partials, 1) * 6 * sizeof(double),
                 std::max<size_t>(t.segs.size(), 1) * 6 * sizeof(double),
-                (t.pairs.size() + t.segs.size() + 1) * sizeof(uint32_t),
+                (t.pairs.size() + t.segs.size() + 2) * sizeof(uint32_t),
                 std::max<size_t>(t.pairs.size(), 1) * kResultDoubles * sizeof(double)};
     }
     std::array<DeviceBuffer*, 6> Buffers() {
@@ -405,6 +405,7 @@ struct BatchMemory {
         dev.seg_sums = seg_sums.as<double>();
         dev.pair_done = pair_done.as<uint32_t>();
         dev.seg_done = pair_done.as<uint32_t>() + t.pairs.size();
+        dev.blur_queue = dev.seg_done + t.segs.size();
         dev.status = nullptr;
         dev.half = elem_bytes == 2 ? 1u : 0u;
         return moved;
@@ -1143,7 +1144,7 @@ public:
         if (host_bytes) VQM_CK(cudaEventRecord(copied_, stream_));
         mem_.EnqueueUpload(mem_.table_bytes, stream_);
         VQM_CK(cudaMemsetAsync(mem_.pair_done.as<void>(), 0,
-                               sizeof(uint32_t) * (n + t.segs.size()), stream_));
+                               sizeof(uint32_t) * (n + t.segs.size() + 2), stream_));
         mem_.EnqueueKernels(shape, stream_, timing_ ? stage_ev_ : nullptr);
         timed_ = timing_;
         mem_.EnqueueReadback(stream_);
