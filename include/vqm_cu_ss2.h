@@ -285,6 +285,17 @@ typedef struct vqm_cu_ss2_batch_config {
 #define VQM_CU_SS2_VARIANT_WORDS 5
 int vqm_cu_ss2_blur_variants(uint32_t* count, uint32_t* shapes);
 
+/* A self-check with no counterpart in the reference: the prepare kernels
+ * compute the XYB cube roots by a shorter route than the shared
+ * correctly-rounded cube root the CPU oracle uses (an estimate from the
+ * special-function unit instead of a bit-level one, so one Newton step
+ * instead of three); both must give the same float. This runs both on the
+ * current device for every float whose bit pattern lies in [first_bits,
+ * last_bits] and reports how many differ (*mismatches) and the smallest
+ * such pattern (*first_bad, 0xffffffff when none). Synchronous; allocates a
+ * few bytes of device memory. */
+int vqm_cu_ss2_check_cbrt(uint32_t first_bits, uint32_t last_bits,
+                          uint64_t* mismatches, uint32_t* first_bad);
 /* Which device decode an image of format `format` takes (a diagnostic; no
  * device is touched): VQM_CU_DECODE_GENERIC, _TABLE (8-bit grey/RGB through a
  * per-image table), _TABLE_IN_RANGE (the same, with every linear sample

@@ -161,3 +161,23 @@ def test_round_half_matches_ieee_binary16():
     want = x.astype(np.float16).astype(np.float32)
     got = det(4, x)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_prepare_cube_root_equals_the_shared_one_on_its_whole_range():
+    """The prepare kernels seed x^(-1/3) from the special-function unit and
+    take one Newton step where ss2dm::cbrt takes three from a bit-level
+    seed; both end in the same exact-residual correction and round once.
+    They must give the same float on every input of the band that route
+    takes, [2^-16, 2^24) (335 M values), checked on the device; outside it
+    they part at one hard-to-round mantissa every third octave."""
+    from vqm_b200 import ss2
+    lo = int(np.float32(2.0 ** -16).view(np.uint32))
+    hi = int(np.float32(2.0 ** 24).view(np.uint32)) - 1
+    mismatches, first_bad = ss2.check_cbrt(lo, hi)
+    assert mismatches == 0, hex(first_bad)
+    # Just outside the band the two routes part at 0x7afd13 (the route is
+    # not taken there), which also shows that the check sees differences.
+    below = int(np.float32(2.0 ** -17).view(np.uint32))
+    assert ss2.check_cbrt(below, lo - 1) == (1, below | 0x7AFD13)
+

@@ -32,6 +32,15 @@ constexpr int kRadius = 6;
 constexpr int kNormsPerChannel = 6;
 constexpr int kSumsPerLevel = 18;
 // Per pair result block: 108 norms, the score, the scale count, a status.
+// The prepare kernels' cube root takes its short route (special-function
+// unit estimate, one Newton step) for inputs in [2^-16, 2^24): there it is
+// checked, on every float, to equal the shared correctly rounded cube root.
+// XYB mixes of linear samples in [0, 1.6e7] lie in that band: they are at
+// least the opsin bias 0.0038 and at most the largest sample plus the bias.
+constexpr float kCbrtRouteLo = 1.52587890625e-05f;  // 2^-16
+constexpr float kCbrtRouteHi = 16777216.0f;        // 2^24
+constexpr float kInRangeLinearMax = 1.6e7f;
+
 constexpr int kResultDoubles = 112;
 constexpr int kResultScore = 108;
 constexpr int kResultScales = 109;
@@ -57,9 +66,10 @@ struct DevSource {
     uint8_t identity1, identity2;
     uint8_t chroma_variant;    // subsampled chroma planes present
     uint8_t lut;               // 1: 8-bit RGB, no alpha: decode by table
-    uint8_t in_range;          // 1: table entries finite, >= 0, <= 1e20 and no
-                               // primaries matrix, so every XYB mix of the
-                               // image and its levels lies in [bias, 1e30]
+    uint8_t in_range;          // 1: every linear sample is in [0, 1.6e7] and
+                               // there is no primaries matrix, so every XYB
+                               // mix of the image and its levels lies in
+                               // [kCbrtRouteLo, kCbrtRouteHi) (see below)
     float scale[3], offset[3]; // luma, chroma, alpha
     float m1[9], m2[9];        // encoded->RGB (or ICtCp->LMS), primaries->709
     float kr, kg, kb, to_linear;

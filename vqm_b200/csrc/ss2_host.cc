@@ -440,8 +440,12 @@ void HostBilinearPhase(uint32_t out_pos, float inv_scale, float shift, int centr
 // DevSource's YUV fast-path fields: set when the format qualifies and every
 // block's bilinear phases are those of its parity (checked over block
 // indices across the whole coordinate range).
-void FastYuvConstants(const vqm_cu_format& f, int mode, int tid, uint32_t chroma_filter,
-                      DevSource& d) {
+// Sets the YUV fast path's constants (d.yuv_fast = 1 when it applies) and
+// returns a bound on the magnitude of the YUV matrix's outputs over every
+// sample code (infinity when the path does not apply).
+double FastYuvConstants(const vqm_cu_format& f, int mode, int tid, uint32_t chroma_filter,
+                        DevSource& d) {
+    const double none = HUGE_VAL;
     d.yuv_fast = 0;
     d.chroma_pattern = 0;
     d.gamma = 0.0f;
@@ -449,7 +453,7 @@ void FastYuvConstants(const vqm_cu_format& f, int mode, int tid, uint32_t chroma
     std::memset(d.cweight, 0, sizeof(d.cweight));
     if (!(f.family == 2 && f.type <= 1 && f.alpha == 0 && mode == 0 && tid >= 1 && tid <= 3 &&
           f.subsample_w <= 1 && f.subsample_h <= 1 && (!d.chroma_variant || chroma_filter == 0)))
-        return;
+        return none;
     const float gammas[4] = {0.0f, 2.4f, 2.2f, 2.8f};  // TransferDecode cases 1-3
     d.gamma = gammas[tid];
     float w[2][2][2];  // [axis][parity][tap]
@@ -473,12 +477,12 @@ void FastYuvConstants(const vqm_cu_format& f, int mode, int tid, uint32_t chroma
                     w1_ref = w1;
                 } else if (s0 != s_ref || std::memcmp(&w0, &w0_ref, 4) ||
                            std::memcmp(&w1, &w1_ref, 4)) {
-                    return;
+                    return none;
                 }
             }
             // Slot 2 (an axis that is not subsampled) puts the second tap past
             // the 3x3 window, where the generic decode reads 0.
-            if (s_ref < 0 || s_ref > 2) return;
+            if (s_ref < 0 || s_ref > 2) return none;
             d.cslot[axis][par] = static_cast<int8_t>(s_ref);
             w[axis][par][0] = w0_ref;
             w[axis][par][1] = w1_ref;
@@ -523,14 +527,17 @@ void FastYuvConstants(const vqm_cu_format& f, int mode, int tid, uint32_t chroma
         lim[p] = std::max(std::fabs(static_cast<double>(d.offset[q])),
                           std::fabs(code_max * d.scale[q] + d.offset[q]));
     }
+    double max_bound = 0.0;
     for (int row = 0; row < 3; ++row) {
         double bound = d.identity1 ? lim[row] : 0.0;
         if (!d.identity1)
             for (int j = 0; j < 3; ++j)
                 bound += std::fabs(static_cast<double>(d.m1[3 * row + j])) * lim[j];
-        if (!(bound < 0.5 * ss2dm::kGammaMaxX)) return;
+        if (!(bound < 0.5 * ss2dm::kGammaMaxX)) return none;
+        max_bound = std::max(max_bound, bound);
     }
     d.yuv_fast = 1;
+    return max_bound;
 }
 
 }  // namespace
@@ -612,7 +619,7 @@ void BuildSourceConstants(const vqm_cu_format& f, uint32_t chroma_filter, float 
         d.cl[3] = static_cast<float>(1.0 - Rec709Oetf(kr));
     }
     d.background = background;
-    FastYuvConstants(f, mode, tid, chroma_filter, d);
+    const double yuv_bound = FastYuvConstants(f, mode, tid, chroma_filter, d);
     // 8-bit grey/RGB without alpha: every sample decodes independently of its
     // neighbours, so one table per image holds the whole transfer decode.
     d.lut = (f.type == 0 && (f.family == 0 || f.family == 1) && f.alpha == 0 && mode == 0 &&
@@ -620,8 +627,13 @@ void BuildSourceConstants(const vqm_cu_format& f, uint32_t chroma_filter, float 
                 ? 1
                 : 0;
     // Power-law YUV without a primaries matrix: the transfer maps every
-    // value to >= 0, so every mix is in the cube root's direct range too.
-    d.in_range = d.yuv_fast && d.identity2 ? 1 : 0;
+    // value to >= 0, and the matrix's output bound caps the linear values
+    // (its power, with room for the power's rounding).
+    d.in_range = d.yuv_fast && d.identity2 &&
+                         std::pow(yuv_bound, static_cast<double>(d.gamma)) * (1.0 + 1e-6) <=
+                             static_cast<double>(kInRangeLinearMax)
+                     ? 1
+                     : 0;
     if (!d.lut) {
         std::memset(d.srgb_lut, 0, sizeof(d.srgb_lut));
         return;
@@ -648,7 +660,7 @@ void BuildSourceConstants(const vqm_cu_format& f, uint32_t chroma_filter, float 
     // all-positive opsin rows plus the bias stay in the cube root's direct
     // range; a primaries matrix could make them negative.
     bool in_range = d.identity2 != 0;
-    for (float v : d.srgb_lut) in_range = in_range && v >= 0.0f && v <= 1.0e20f;
+    for (float v : d.srgb_lut) in_range = in_range && v >= 0.0f && v <= kInRangeLinearMax;
     d.in_range = in_range ? 1 : 0;
 }
 

@@ -23,6 +23,11 @@ cudaError_t LaunchBlur(const DevBatch& batch, int variant, cudaStream_t stream);
 // kernels' shared-memory limits), so that no first launch pays for it.
 cudaError_t PreloadPrepare();
 cudaError_t PreloadBlur();
+// Checks the prepare kernels' cube root against ss2dm::cbrt, bit for bit, on
+// every float whose bit pattern lies in [first_bits, last_bits], on the
+// current device; synchronous.
+cudaError_t CheckCbrt(uint32_t first_bits, uint32_t last_bits, uint64_t* mismatches,
+                      uint32_t* first_bad);
 
 // The blur variants compiled into the library and their output tiles.
 int BlurTileCount();

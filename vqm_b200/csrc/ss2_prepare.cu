@@ -64,21 +64,40 @@ constexpr float kCbrtBias = 0.15595419704914093f;
 __device__ __forceinline__ float2 Pack(float v) { return make_float2(v, v); }
 __device__ __forceinline__ float2 Neg(float2 v) { return make_float2(-v.x, -v.y); }
 
-// ss2dm::cbrt of both lanes. For lanes in [1e-20, 1e30] (all that an XYB
-// mix of in-gamut light produces: the mix includes a bias of 0.0038) the
-// function takes its unscaled path, executed here with the same operations in
-// the same order two lanes at a time; any other lane pair calls it per lane.
-// kInRange: the caller knows both lanes are in that range (no check).
+// x^(-1/3) to about 2^-21 relative as 2^(-log2(x) / 3), from the
+// special-function unit's approximate base-2 logarithm and exponential.
+__device__ __forceinline__ float RcbrtEstimate(float x) {
+    float l, r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"(x));
+    l = __fmul_rn(l, -0.333333343267440796f);
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(l));
+    return r;
+}
+
+// The correctly rounded cube root of both lanes, ss2dm::cbrt's value, by a
+// shorter route for lanes in [kCbrtRouteLo, kCbrtRouteHi) = [2^-16, 2^24)
+// (every XYB mix of in-gamut light: the mix includes a bias of 0.0038); any
+// other lane pair calls ss2dm::cbrt per lane. ss2dm::cbrt refines a
+// bit-level estimate of x^(-1/3) (error ~0.04) with three Newton steps;
+// here the estimate comes from the special-function unit (error ~2^-21), so
+// one step brings r to the same float-rounding floor, and the remaining
+// steps are ss2dm::cbrt's own: y0 = x r^2, then one Newton step on the root
+// with its residual x - y0^3 formed exactly, rounded once. Both routes round
+// a value within ~1e-13 of cbrt(x); on every float of the band they give the
+// same float, which the library checks on the device (vqm_cu_ss2_check_cbrt,
+// run by the GPU tests over the whole band). Outside it they can part: one
+// mantissa, 0x7afd13, whose cube root lies almost on a rounding boundary,
+// rounds differently every third octave below 2^-16 and above 2^24.
+// Two lanes per instruction. kInRange: the caller knows both lanes are in
+// the band (the host proves it per image: DevSource::in_range).
 template <bool kInRange = false>
 __device__ __forceinline__ float2 Cbrt2(float2 x) {
-    if (!kInRange &&
-        !(x.x >= 1.0e-20f && x.x <= 1.0e30f && x.y >= 1.0e-20f && x.y <= 1.0e30f))
+    if (!kInRange && !(x.x >= kCbrtRouteLo && x.x < kCbrtRouteHi && x.y >= kCbrtRouteLo &&
+                       x.y < kCbrtRouteHi))
         return make_float2(ss2dm::cbrt(x.x), ss2dm::cbrt(x.y));
-    float2 r = make_float2(__uint_as_float(0x54a21d2au - __float_as_uint(x.x) / 3u),
-                           __uint_as_float(0x54a21d2au - __float_as_uint(x.y) / 3u));
+    float2 r = make_float2(RcbrtEstimate(x.x), RcbrtEstimate(x.y));
     const float2 third = Pack(0.333333343267440796f);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
+    {
         const float2 r3 = __fmul2_rn(__fmul2_rn(r, r), r);
         const float2 t = __ffma2_rn(Neg(x), r3, Pack(1.0f));
         r = __ffma2_rn(__fmul2_rn(r, t), third, r);
@@ -521,6 +540,57 @@ cudaError_t PreloadPrepareOf() {
 cudaError_t PreloadPrepare() {
     const cudaError_t e = PreloadPrepareOf<false>();
     return e == cudaSuccess ? PreloadPrepareOf<true>() : e;
+}
+
+namespace {
+// Compares Cbrt2's in-range route with ss2dm::cbrt on the `count` floats
+// whose bit patterns follow `first`, two per thread step (the odd last one
+// paired with itself); counts the differing patterns and keeps the smallest.
+__global__ void CheckCbrtKernel(uint32_t first, uint32_t count, unsigned long long* mismatches,
+                                uint32_t* first_bad) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t pairs = count / 2 + count % 2;
+    unsigned long long bad = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += stride) {
+        const uint32_t b0 = first + 2 * i;
+        const bool two = 2 * i + 1 < count;
+        const uint32_t b1 = two ? b0 + 1 : b0;
+        const float2 x = make_float2(__uint_as_float(b0), __uint_as_float(b1));
+        const float2 fast = Cbrt2<true>(x);
+        const bool d0 = __float_as_uint(fast.x) != __float_as_uint(ss2dm::cbrt(x.x));
+        const bool d1 = two && __float_as_uint(fast.y) != __float_as_uint(ss2dm::cbrt(x.y));
+        bad += static_cast<unsigned long long>(d0) + static_cast<unsigned long long>(d1);
+        if (d0 || d1) atomicMin(first_bad, d0 ? b0 : b1);
+    }
+    if (bad) atomicAdd(mismatches, bad);
+}
+}  // namespace
+
+cudaError_t CheckCbrt(uint32_t first_bits, uint32_t last_bits, uint64_t* mismatches,
+                      uint32_t* first_bad) {
+    if (last_bits < first_bits || last_bits - first_bits == 0xffffffffu)
+        return cudaErrorInvalidValue;
+    unsigned long long* d_count = nullptr;
+    cudaError_t e = cudaMalloc(&d_count, sizeof(unsigned long long) + sizeof(uint32_t));
+    if (e != cudaSuccess) return e;
+    uint32_t* d_first = reinterpret_cast<uint32_t*>(d_count + 1);
+    const uint32_t none = 0xffffffffu;
+    unsigned long long h_count = 0;
+    uint32_t h_first = none;
+    e = cudaMemset(d_count, 0, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemcpy(d_first, &none, sizeof(none), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        CheckCbrtKernel<<<148 * 8, 256>>>(first_bits, last_bits - first_bits + 1, d_count,
+                                          d_first);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(&h_count, d_count, sizeof(h_count), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&h_first, d_first, sizeof(h_first), cudaMemcpyDeviceToHost);
+    cudaFree(d_count);
+    if (e != cudaSuccess) return e;
+    *mismatches = h_count;
+    *first_bad = h_first;
+    return cudaSuccess;
 }
 
 template <bool kHalf>

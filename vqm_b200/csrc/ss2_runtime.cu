@@ -1321,6 +1321,23 @@ int vqm_cu_ss2_plan_scales(uint32_t width, uint32_t height, uint32_t* sizes12, u
     });
 }
 
+int vqm_cu_ss2_check_cbrt(uint32_t first_bits, uint32_t last_bits, uint64_t* mismatches,
+                          uint32_t* first_bad) {
+    return Guard([&] {
+        NotNull(mismatches, "mismatches");
+        NotNull(first_bad, "first_bad");
+        int device = 0;
+        if (cudaGetDevice(&device) != cudaSuccess) {
+            cudaGetLastError();
+            throw std::runtime_error("cuda: no usable compute device");
+        }
+        vqm_b200::EnsureDevice(device);
+        const cudaError_t e = vqm_b200::CheckCbrt(first_bits, last_bits, mismatches, first_bad);
+        if (e == cudaErrorInvalidValue) throw std::invalid_argument("empty or inverted range");
+        if (e != cudaSuccess) throw std::runtime_error(std::string("cuda: ") + cudaGetErrorString(e));
+    });
+}
+
 int vqm_cu_ss2_channel_pruned(uint32_t channel, uint32_t scale, uint32_t scales, int* pruned) {
     return Guard([&] {
         NotNull(pruned, "pruned");

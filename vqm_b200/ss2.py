@@ -194,6 +194,7 @@ _SIGS = {
     "vqm_cu_validate_format": ([_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p], ctypes.c_int),
     "vqm_cu_ss2_plan_scales": ([ctypes.c_uint32, ctypes.c_uint32, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_channel_pruned": ([ctypes.c_uint32] * 3 + [_P], ctypes.c_int),
+    "vqm_cu_ss2_check_cbrt": ([ctypes.c_uint32, ctypes.c_uint32, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_score": ([_P, ctypes.c_uint32, _P], ctypes.c_int),
     "vqm_cu_ss2_source_constants": ([_P, ctypes.c_uint32, _P], ctypes.c_int),
     "vqm_cu_ss2_create": ([_P, _P], ctypes.c_int),
@@ -445,6 +446,17 @@ def channel_pruned(channel: int, scale: int, scales: int) -> bool:
     out = ctypes.c_int()
     _check(_lib.vqm_cu_ss2_channel_pruned(channel, scale, scales, ctypes.byref(out)))
     return bool(out.value)
+
+
+def check_cbrt(first_bits: int, last_bits: int):
+    """Runs the prepare kernels' cube root and the shared correctly rounded
+    one on every float with a bit pattern in [first_bits, last_bits] on the
+    current device: (how many differ, the smallest differing pattern or
+    0xffffffff)."""
+    n, first = ctypes.c_uint64(), ctypes.c_uint32()
+    _check(_lib.vqm_cu_ss2_check_cbrt(first_bits, last_bits, ctypes.byref(n),
+                                      ctypes.byref(first)))
+    return n.value, first.value
 
 
 def kept_pixels(width: int, height: int) -> int:
