@@ -318,9 +318,12 @@ def test_batch_matches_pipeline():
         assert not helpers.feature_mismatch(single.norms, r.norms, rtol=1e-6, atol=1e-12)
         assert abs(r.device_score - r.score()) <= 1e-9
         check_parity(r, o, d, label=f"batch {o.width}x{o.height}")
-    # A second, smaller batch on the same scorer reuses its memory.
+    # A second, smaller batch on the same scorer reuses its memory (it may
+    # pick a shorter strip, so it agrees to rounding).
     again = b.compute_many(pairs[:2])
-    assert np.array_equal(again[1].norms, results[1].norms)
+    assert not helpers.feature_mismatch(again[1].norms, results[1].norms, rtol=1e-6,
+                                        atol=1e-12)
+    assert np.array_equal(b.compute_many(pairs[:2])[1].norms, again[1].norms)
 
 
 @pytest.mark.parametrize("variant", range(len(ss2.blur_variants())))

@@ -159,23 +159,31 @@ __device__ __forceinline__ void CpAsyncWait() {
 
 // Issues the copies of one tile's two source windows into `buf`: chunk
 // (rp, cp) of the window is the 2x2 block at window column 2cp, row 2rp.
-// Row pairs below `rp_begin` are left as they are.
+// Row pairs below `rp_begin` are left as they are. A thread keeps one chunk
+// column, cp = tid mod CP, and steps down the rows NT / CP at a time, so its
+// column test and addresses are set once and advance by constants.
 template <int TW, int TH, int NT>
 __device__ __forceinline__ void IssueTileLoads(float* buf, const TileRef& t, int rp_begin = 0) {
     using T = Tile<TW, TH, NT>;
-    const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(buf));
+    constexpr int kRowsPerPass = NT / T::CP;
+    static_assert(kRowsPerPass >= 1, "a pass covers at least one row of chunks");
+    const int cp = static_cast<int>(threadIdx.x) % T::CP;
+    const int r = static_cast<int>(threadIdx.x) / T::CP;
+    if (r >= kRowsPerPass) return;
     const uint32_t wp = static_cast<uint32_t>(t.w + 1) >> 1;  // chunks per row pair
     const uint32_t hp = static_cast<uint32_t>(t.h + 1) >> 1;  // row pairs
-    const int cx0 = (t.x0 >> 1) - kRadius / 2, ry0 = (t.y0 >> 1) - kRadius / 2;
-    for (int k = rp_begin * T::CP + threadIdx.x; k < T::RP * T::CP; k += NT) {
-        const int rp = k / T::CP, cp = k - rp * T::CP;
-        const int gy = ry0 + rp, gx = cx0 + cp;
-        const bool in = static_cast<uint32_t>(gy) < hp && static_cast<uint32_t>(gx) < wp;
-        const uint32_t off = in ? static_cast<uint32_t>(gy) * t.pitch + 4u * static_cast<uint32_t>(gx)
-                                : 0u;
-        const uint32_t dst = base + 4u * static_cast<uint32_t>(rp * T::SRS + 4 * cp);
+    const int gx = (t.x0 >> 1) - kRadius / 2 + cp, ry0 = (t.y0 >> 1) - kRadius / 2;
+    const bool column_in = static_cast<uint32_t>(gx) < wp;
+    const uint32_t col_off = 4u * static_cast<uint32_t>(gx);
+    uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(buf)) +
+                   4u * static_cast<uint32_t>((rp_begin + r) * T::SRS + 4 * cp);
+    for (int rp = rp_begin + r; rp < T::RP; rp += kRowsPerPass) {
+        const int gy = ry0 + rp;
+        const bool in = column_in && static_cast<uint32_t>(gy) < hp;
+        const uint32_t off = in ? static_cast<uint32_t>(gy) * t.pitch + col_off : 0u;
         CpAsync16(dst, t.pa + off, in);
         CpAsync16(dst + 4u * T::IMG, t.pb + off, in);
+        dst += 4u * kRowsPerPass * T::SRS;
     }
 }
 
@@ -657,16 +665,18 @@ struct HqScratch {
 
 // Horizontal rows TH..TH+11 of every quantity to rows 0..11. TH is a
 // multiple of 4, so a row and its destination share the store swizzle.
+// A thread moves float4 j of every quantity's halo (j < 96 for 32-wide
+// tiles: one pass for 128 threads), at constant offsets from one address.
 template <int TW, int TH, int NT>
 __device__ __forceinline__ void MoveHalo(float* hq) {
     using T = Tile<TW, TH, NT>;
     constexpr int kRowVec = TW / 4;                   // float4 per row
     constexpr int kPlaneVec = 2 * kRadius * kRowVec;  // float4 per plane's halo
     static_assert(TH % 4 == 0, "swizzle parity");
-    for (int i = threadIdx.x; i < 5 * kPlaneVec; i += NT) {
-        const int q = i / kPlaneVec, j = i - q * kPlaneVec;
-        float4* plane = reinterpret_cast<float4*>(hq + q * T::SH * TW);
-        plane[j] = plane[TH * kRowVec + j];
+    for (int j = threadIdx.x; j < kPlaneVec; j += NT) {
+        float4* at = reinterpret_cast<float4*>(hq) + j;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) at[q * (T::SH * TW / 4)] = at[q * (T::SH * TW / 4) + TH * kRowVec];
     }
 }
 
@@ -923,15 +933,19 @@ int BlurTileStrip(int index) { return kBlurVariants[index].strip; }
 bool BlurTilePersistent(int index) { return kBlurVariants[index].persistent != 0; }
 int AutoBlurVariant(uint64_t tiles, int sms) {
     // The longest 32x32 strip that still gives every CTA slot of the device
-    // 8 CTAs (fewer, and the last wave's idle slots cost more than the
-    // shared rows save: measured on 1080p and 4K pairs, one or many).
+    // 2 CTAs (fewer, and the last wave's idle slots cost more than the
+    // shared rows and the once-per-strip reduction save). Measured blur
+    // times for one pair: 1080p 65.5 us one tile per CTA, 62.0 with strips
+    // of 2 (taken); 4K 163.8 / 149.5 / 143.4 / 147.5 us with strips of
+    // 1 / 2 / 4 / 8 (8 taken); 720p 47.1 us for 1, 2 and 4 (1 taken); large
+    // batches take the longest strip, 16.
     const BlurVariant& base = kBlurVariants[kDefaultBlurVariant];
     const uint64_t slots = static_cast<uint64_t>(sms > 0 ? sms : 1) * base.per_sm;
     int best = kDefaultBlurVariant, strip = 1;
     for (int i = 0; i < kBlurVariantCount; ++i) {
         const BlurVariant& v = kBlurVariants[i];
         if (v.persistent || v.w != base.w || v.h != base.h || v.threads != base.threads) continue;
-        if (v.strip > strip && tiles / static_cast<uint64_t>(v.strip) >= 8 * slots) {
+        if (v.strip > strip && tiles / static_cast<uint64_t>(v.strip) >= 2 * slots) {
             best = i;
             strip = v.strip;
         }

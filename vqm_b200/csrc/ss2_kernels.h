@@ -41,7 +41,8 @@ bool BlurTilePersistent(int index);
 uint32_t BlurBlocks(int index, uint32_t tiles_x, uint32_t tiles_y);
 // The variant used when a caller does not choose one, for a launch of
 // `tiles` output tiles of the default variant on a device with `sms` SMs:
-// the default itself for small launches, a strip of its tile for large ones.
+// the longest strip of its tile that leaves every CTA slot two CTAs (one
+// tile per CTA for small launches).
 // A strip regroups the compensated partial sums, so the choice moves a
 // result by rounding only (~1e-7 relative).
 int AutoBlurVariant(uint64_t tiles, int sms);
