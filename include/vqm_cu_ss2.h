@@ -296,6 +296,15 @@ int vqm_cu_ss2_blur_variants(uint32_t* count, uint32_t* shapes);
  * few bytes of device memory. */
 int vqm_cu_ss2_check_cbrt(uint32_t first_bits, uint32_t last_bits,
                           uint64_t* mismatches, uint32_t* first_bad);
+/* The same self-check for the blur maps' division, which takes the divisor's
+ * reciprocal from the special-function unit and one Newton step where the
+ * shared division takes three from a bit seed (both then correct the
+ * quotient with its exact residual): for every divisor whose bit pattern
+ * lies in [first_bits, last_bits] and sixteen quotient values in [-1, 1.8],
+ * compares the two quotients; *mismatches counts the differing divisions,
+ * *first_bad is the smallest divisor pattern among them. */
+int vqm_cu_ss2_check_division(uint32_t first_bits, uint32_t last_bits,
+                              uint64_t* mismatches, uint32_t* first_bad);
 /* Which device decode an image of format `format` takes (a diagnostic; no
  * device is touched): VQM_CU_DECODE_GENERIC, _TABLE (8-bit grey/RGB through a
  * per-image table), _TABLE_IN_RANGE (the same, with every linear sample

@@ -39,6 +39,7 @@
 #include <cstdint>
 #include <mutex>
 
+#include "ss2_detmath.h"
 #include "ss2_device.cuh"
 #include "ss2_kernels.h"
 #include "ss2_layout.h"
@@ -247,17 +248,33 @@ __device__ __forceinline__ void ConvertHalfTile(const unsigned char* staging, fl
 __device__ __forceinline__ float2 Pack(float v) { return make_float2(v, v); }
 __device__ __forceinline__ float2 Neg(float2 v) { return make_float2(-v.x, -v.y); }
 
-// ss2dm::divf (the maps' division, shared with the CPU checker) of both
-// lanes, two lanes per instruction: the same operations on each lane.
+// The reciprocal of both lanes' divisors for the maps' division: an estimate
+// from the special-function unit (within 1 ulp) and one Newton step
+// r += r (1 - b r), which leaves ~2^-46 of error before its single rounding;
+// ss2dm::recipf takes three steps from a bit seed and leaves ~2^-34, so the
+// two reciprocals differ by an ulp for about 1.6e-4 of divisors.
+__device__ __forceinline__ float RcpEstimate(float b) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
+    return r;
+}
+__device__ __forceinline__ float2 Recip2(float2 b) {
+    const float2 r = make_float2(RcpEstimate(b.x), RcpEstimate(b.y));
+    return __ffma2_rn(r, __ffma2_rn(Neg(b), r, Pack(1.0f)), r);
+}
+
+// The maps' division of both lanes, two lanes per instruction: Recip2 and
+// ss2dm::divf's final step, q0 = a r corrected once with the residual
+// a - b q0 (exact in one fused multiply-add), which absorbs a 1-ulp
+// difference in r: the quotient equals ss2dm::divf's unless it lies within
+// ~2^-46 of a rounding boundary. The library checks every divisor of the
+// maps' band [2^-11, 2^4] (the SSIM' denominator is at least 0.0009, the edge
+// map's at least 1) at sixteen quotient values on the device
+// (vqm_cu_ss2_check_division, run by the GPU tests).
 __device__ __forceinline__ float2 Div2(float2 a, float2 b) {
-    float2 r = make_float2(__uint_as_float(0x7ef311c7u - __float_as_uint(b.x)),
-                           __uint_as_float(0x7ef311c7u - __float_as_uint(b.y)));
-    const float2 nb = Neg(b), one = Pack(1.0f);
-    r = __ffma2_rn(r, __ffma2_rn(nb, r, one), r);
-    r = __ffma2_rn(r, __ffma2_rn(nb, r, one), r);
-    r = __ffma2_rn(r, __ffma2_rn(nb, r, one), r);
+    const float2 r = Recip2(b);
     const float2 q0 = __fmul2_rn(a, r);
-    return __ffma2_rn(__ffma2_rn(nb, q0, a), r, q0);
+    return __ffma2_rn(__ffma2_rn(Neg(b), q0, a), r, q0);
 }
 
 // Horizontal pass (scale.comp:149-207): row pair rp, output columns
@@ -886,6 +903,71 @@ cudaError_t Dispatch(const DevBatch& b, int variant, cudaStream_t stream, bool l
 }
 
 }  // namespace
+
+namespace {
+// Quotient values the division check tries with every divisor: spread over
+// (-1, 1] and beyond, where the maps' quotients lie (the SSIM' map divides
+// its numerator by a denominator at least as large; the edge map's relative
+// difference is at least -1).
+__constant__ float c_check_quotients[16] = {
+    0.0f,       1.0e-7f,   3.3e-5f,   0.00173f, 0.0137f,  0.1f,      0.25f,     0.3333f,
+    0.5f,       0.7731f,   0.9999f,   1.0f,     1.7321f,  -0.2718f,  -0.6667f,  -0.99999f};
+
+// For every divisor whose bit pattern is first + i (i < count) and every
+// quotient value t of the table: the dividend a = b t rounded, then Div2's
+// quotient against ss2dm::divf's (the two lanes hold two divisors); counts
+// the differing divisions and keeps the smallest divisor pattern involved.
+__global__ void CheckDivisionKernel(uint32_t first, uint32_t count,
+                                   unsigned long long* mismatches, uint32_t* first_bad) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t pairs = count / 2 + count % 2;
+    unsigned long long bad = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pairs; i += stride) {
+        const uint32_t b0 = first + 2 * i;
+        const bool two = 2 * i + 1 < count;
+        const uint32_t b1 = two ? b0 + 1 : b0;
+        const float2 b = make_float2(__uint_as_float(b0), __uint_as_float(b1));
+        for (int k = 0; k < 16; ++k) {
+            const float t = c_check_quotients[k];
+            const float2 a = make_float2(__fmul_rn(b.x, t), __fmul_rn(b.y, t));
+            const float2 q = Div2(a, b);
+            const bool d0 = __float_as_uint(q.x) != __float_as_uint(ss2dm::divf(a.x, b.x));
+            const bool d1 =
+                two && __float_as_uint(q.y) != __float_as_uint(ss2dm::divf(a.y, b.y));
+            bad += static_cast<unsigned long long>(d0) + static_cast<unsigned long long>(d1);
+            if (d0 || d1) atomicMin(first_bad, d0 ? b0 : b1);
+        }
+    }
+    if (bad) atomicAdd(mismatches, bad);
+}
+}  // namespace
+
+cudaError_t CheckDivision(uint32_t first_bits, uint32_t last_bits, uint64_t* mismatches,
+                          uint32_t* first_bad) {
+    if (last_bits < first_bits || last_bits - first_bits == 0xffffffffu)
+        return cudaErrorInvalidValue;
+    unsigned long long* d_count = nullptr;
+    cudaError_t e = cudaMalloc(&d_count, sizeof(unsigned long long) + sizeof(uint32_t));
+    if (e != cudaSuccess) return e;
+    uint32_t* d_first = reinterpret_cast<uint32_t*>(d_count + 1);
+    const uint32_t none = 0xffffffffu;
+    unsigned long long h_count = 0;
+    uint32_t h_first = none;
+    e = cudaMemset(d_count, 0, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemcpy(d_first, &none, sizeof(none), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        CheckDivisionKernel<<<148 * 8, 256>>>(first_bits, last_bits - first_bits + 1, d_count,
+                                              d_first);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(&h_count, d_count, sizeof(h_count), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&h_first, d_first, sizeof(h_first), cudaMemcpyDeviceToHost);
+    cudaFree(d_count);
+    if (e != cudaSuccess) return e;
+    *mismatches = h_count;
+    *first_bad = h_first;
+    return cudaSuccess;
+}
 
 cudaError_t SetConstants(const float* taps13, const double* weights108) {
     float2 pairs[kTaps];

@@ -404,11 +404,16 @@ SS2_DM float powf_gamma(float x, float y) {
 // division ("IA-64 and Elementary Functions", 2000). Faithfully rounded, and
 // the correctly rounded a / b unless the quotient lies within ~2^-44 of a
 // rounding boundary (checked against IEEE division by tests/test_detmath.py).
-SS2_DM float divf(float a, float b) {
+// divf's reciprocal of b: the bit seed and its three Newton steps.
+SS2_DM float recipf(float b) {
     float r = from_bits(0x7ef311c7u - bits(b));
     r = fmaf_(r, fmaf_(-b, r, 1.0f), r);
     r = fmaf_(r, fmaf_(-b, r, 1.0f), r);
     r = fmaf_(r, fmaf_(-b, r, 1.0f), r);
+    return r;
+}
+SS2_DM float divf(float a, float b) {
+    const float r = recipf(b);
     const float q0 = a * r;
     return fmaf_(fmaf_(-b, q0, a), r, q0);
 }

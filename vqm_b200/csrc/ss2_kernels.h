@@ -28,6 +28,10 @@ cudaError_t PreloadBlur();
 // current device; synchronous.
 cudaError_t CheckCbrt(uint32_t first_bits, uint32_t last_bits, uint64_t* mismatches,
                       uint32_t* first_bad);
+// The blur maps' division against ss2dm::divf for every divisor whose bit
+// pattern lies in [first_bits, last_bits], at sixteen quotient values each.
+cudaError_t CheckDivision(uint32_t first_bits, uint32_t last_bits, uint64_t* mismatches,
+                          uint32_t* first_bad);
 
 // The blur variants compiled into the library and their output tiles.
 int BlurTileCount();

@@ -1266,6 +1266,26 @@ void NotNull(const void* p, const char* what) {
     if (!p) throw std::invalid_argument(std::string(what) + " is null");
 }
 
+// The self-checks of the kernels' shorter arithmetic routes (CheckCbrt,
+// CheckDivision) on the current device, as C ABI calls.
+template <class Check>
+int RunRouteCheck(Check check, uint32_t first_bits, uint32_t last_bits, uint64_t* mismatches,
+                  uint32_t* first_bad) {
+    return Guard([&] {
+        NotNull(mismatches, "mismatches");
+        NotNull(first_bad, "first_bad");
+        int device = 0;
+        if (cudaGetDevice(&device) != cudaSuccess) {
+            cudaGetLastError();
+            throw std::runtime_error("cuda: no usable compute device");
+        }
+        EnsureDevice(device);
+        const cudaError_t e = check(first_bits, last_bits, mismatches, first_bad);
+        if (e == cudaErrorInvalidValue) throw std::invalid_argument("empty or inverted range");
+        if (e != cudaSuccess) throw std::runtime_error(std::string("cuda: ") + cudaGetErrorString(e));
+    });
+}
+
 }  // namespace
 
 // The message vqm_cu_last_error() returns on this thread, for entry points
@@ -1323,19 +1343,14 @@ int vqm_cu_ss2_plan_scales(uint32_t width, uint32_t height, uint32_t* sizes12, u
 
 int vqm_cu_ss2_check_cbrt(uint32_t first_bits, uint32_t last_bits, uint64_t* mismatches,
                           uint32_t* first_bad) {
-    return Guard([&] {
-        NotNull(mismatches, "mismatches");
-        NotNull(first_bad, "first_bad");
-        int device = 0;
-        if (cudaGetDevice(&device) != cudaSuccess) {
-            cudaGetLastError();
-            throw std::runtime_error("cuda: no usable compute device");
-        }
-        vqm_b200::EnsureDevice(device);
-        const cudaError_t e = vqm_b200::CheckCbrt(first_bits, last_bits, mismatches, first_bad);
-        if (e == cudaErrorInvalidValue) throw std::invalid_argument("empty or inverted range");
-        if (e != cudaSuccess) throw std::runtime_error(std::string("cuda: ") + cudaGetErrorString(e));
-    });
+    return vqm_b200::RunRouteCheck(vqm_b200::CheckCbrt, first_bits, last_bits, mismatches,
+                                   first_bad);
+}
+
+int vqm_cu_ss2_check_division(uint32_t first_bits, uint32_t last_bits, uint64_t* mismatches,
+                              uint32_t* first_bad) {
+    return vqm_b200::RunRouteCheck(vqm_b200::CheckDivision, first_bits, last_bits, mismatches,
+                                   first_bad);
 }
 
 int vqm_cu_ss2_channel_pruned(uint32_t channel, uint32_t scale, uint32_t scales, int* pruned) {

@@ -195,6 +195,7 @@ _SIGS = {
     "vqm_cu_ss2_plan_scales": ([ctypes.c_uint32, ctypes.c_uint32, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_channel_pruned": ([ctypes.c_uint32] * 3 + [_P], ctypes.c_int),
     "vqm_cu_ss2_check_cbrt": ([ctypes.c_uint32, ctypes.c_uint32, _P, _P], ctypes.c_int),
+    "vqm_cu_ss2_check_division": ([ctypes.c_uint32, ctypes.c_uint32, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_score": ([_P, ctypes.c_uint32, _P], ctypes.c_int),
     "vqm_cu_ss2_source_constants": ([_P, ctypes.c_uint32, _P], ctypes.c_int),
     "vqm_cu_ss2_create": ([_P, _P], ctypes.c_int),
@@ -456,6 +457,17 @@ def check_cbrt(first_bits: int, last_bits: int):
     n, first = ctypes.c_uint64(), ctypes.c_uint32()
     _check(_lib.vqm_cu_ss2_check_cbrt(first_bits, last_bits, ctypes.byref(n),
                                       ctypes.byref(first)))
+    return n.value, first.value
+
+
+def check_division(first_bits: int, last_bits: int):
+    """Runs the blur maps' division and the shared one (ss2dm::divf) for
+    every divisor with a bit pattern in [first_bits, last_bits], at sixteen
+    quotient values each, on the current device: (how many divisions differ,
+    the smallest divisor pattern among them or 0xffffffff)."""
+    n, first = ctypes.c_uint64(), ctypes.c_uint32()
+    _check(_lib.vqm_cu_ss2_check_division(first_bits, last_bits, ctypes.byref(n),
+                                          ctypes.byref(first)))
     return n.value, first.value
 
 
