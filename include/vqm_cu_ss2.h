@@ -89,8 +89,18 @@ typedef struct vqm_cu_ss2_config {
     uint32_t streaming_inputs;    /* 1: host-image submit overloads allowed */
     uint64_t input_bytes;         /* pool for allocate_image(); 0 = none */
     int32_t device;               /* CUDA ordinal; -1 = the current device */
-    uint32_t reserved;
+    uint32_t blur;                /* VQM_CU_SS2_BLUR_*; 0 = VQM's */
 } vqm_cu_ss2_config;
+
+/* Blur modes. SAMPLED is VQM's 13-tap sampled Gaussian, sigma 1.5
+ * (pipeline.cc:274-291), the only mode that reproduces VQM's scores.
+ * RECURSIVE (opt-in, no counterpart in VQM) is the third-order recursive
+ * Gaussian, sigma 1.5, that Cloudinary's ssimulacra2 uses and VQM replaced
+ * on purpose (docs/divergence.md:22): 9 nonzero taps of radius 4, zero
+ * padded; everything else is unchanged. Its scores follow that filter's
+ * FP64 evaluation, not VQM. */
+#define VQM_CU_SS2_BLUR_SAMPLED 0
+#define VQM_CU_SS2_BLUR_RECURSIVE 1
 
 /* PipelineMemoryUsage (include/vqm_memory_types.h:24-33), device bytes. */
 typedef struct vqm_cu_memory_usage {
@@ -130,6 +140,11 @@ int vqm_cu_ss2_plan_scales(uint32_t width, uint32_t height, uint32_t* sizes12,
  * 0-2 are X, Y, B; scale < scales <= 6, else VQM_CU_INVALID_ARGUMENT. */
 int vqm_cu_ss2_channel_pruned(uint32_t channel, uint32_t scale, uint32_t scales,
                               int* pruned);
+/* The 13 blur taps (offsets -6..6) a blur mode applies along each axis, as
+ * the kernels hold them: MakeGaussian's (pipeline.cc:274-291) for
+ * VQM_CU_SS2_BLUR_SAMPLED, the recursive Gaussian's impulse response for
+ * VQM_CU_SS2_BLUR_RECURSIVE. VQM_CU_INVALID_ARGUMENT for another mode. */
+int vqm_cu_ss2_blur_taps(uint32_t blur, float* taps13);
 /* Ssimulacra2Result::Score (src/metrics/ssimulacra2/score.cc:118-163), FP64,
  * norms in the layout above. VQM_CU_INVALID_ARGUMENT for more than six
  * scales or nonfinite norms, as the reference throws. */
@@ -276,6 +291,7 @@ typedef struct vqm_cu_ss2_batch_config {
                               ~1e-7 relative), k = compiled variant k - 1 */
     uint32_t half_planes;  /* 1: binary16 pyramid planes, as
                               vqm_cu_ss2_config.half_planes */
+    uint32_t blur;         /* VQM_CU_SS2_BLUR_*; 0 = VQM's */
 } vqm_cu_ss2_batch_config;
 
 /* The blur kernels compiled into the library, for tuning: *count variants,
@@ -386,12 +402,12 @@ typedef struct vqm_cu_ss2_server_config {
     uint32_t chroma_filter;  /* 0 bilinear, 1 bicubic, 2 lanczos */
     int32_t device;          /* CUDA ordinal; -1 = the current device */
     uint32_t variant;        /* blur kernel, as vqm_cu_ss2_batch_config */
-    uint32_t reserved;
+    uint32_t blur;           /* VQM_CU_SS2_BLUR_*; 0 = VQM's */
 } vqm_cu_ss2_server_config;
 
 typedef struct vqm_cu_ss2_server_stats {
     uint64_t submitted, completed, failed;
-    uint64_t batches;          /* three-kernel launches */
+    uint64_t batches;          /* batch launches (prepare, blur) */
     uint64_t largest_batch;    /* pairs in the largest batch formed */
     uint64_t bytes_in_flight;  /* device bytes the admitted, not yet
                                   completed requests need */

@@ -62,6 +62,10 @@ enum class ColorPrimaries : std::uint8_t {
     Bt2020 = 9, St428 = 10, St431_2 = 11, St432_1 = 12, Ebu3213E = 22
 };
 enum class ChromaFilter : std::uint8_t { Bilinear = 0, Bicubic = 1, Lanczos = 2 };
+// The blur (no counterpart in VQM's config): Sampled is VQM's 13-tap
+// Gaussian; Recursive, opt-in, is the recursive Gaussian of Cloudinary's
+// ssimulacra2 (VQM_CU_SS2_BLUR_RECURSIVE), whose scores are not VQM's.
+enum class Ssimulacra2Blur : std::uint32_t { Sampled = 0, Recursive = 1 };
 
 struct ImageFormat {
     PixelType type = PixelType::Float;
@@ -282,6 +286,7 @@ struct Ssimulacra2Config {
     std::size_t input_bytes = 0;
     bool streaming_inputs = true;
     int device = -1;  // CUDA ordinal; -1 = the current device
+    Ssimulacra2Blur blur = Ssimulacra2Blur::Sampled;
 };
 
 // Memory the pipeline holds on the device (PipelineMemoryUsage's role).
@@ -301,6 +306,7 @@ public:
         c.streaming_inputs = config.streaming_inputs ? 1 : 0;
         c.input_bytes = config.input_bytes;
         c.device = config.device;
+        c.blur = static_cast<std::uint32_t>(config.blur);
         vqm_cu_ss2_pipeline* p = nullptr;
         detail::Check(vqm_cu_ss2_create(&c, &p));
         p_.reset(p);
@@ -465,6 +471,8 @@ public:
             c.chroma_filter = static_cast<std::uint32_t>(config.chroma_filter);
             c.device = config.device;
             c.max_pairs = static_cast<std::uint32_t>(chunk_);
+            c.half_planes = config.half_planes ? 1 : 0;
+            c.blur = static_cast<std::uint32_t>(config.blur);
             vqm_cu_ss2_batch* b = nullptr;
             detail::Check(vqm_cu_ss2_batch_create(&c, &b));
             batches_.emplace_back(b);

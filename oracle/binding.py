@@ -120,22 +120,23 @@ def _check(status: int) -> None:
 
 
 def compute(original: Image, distorted: Image, background: float = 0.5,
-            chroma_filter: int = 0, precision: int = 32):
-    """Returns (norms[scales, 18], score) of one pair."""
+            chroma_filter: int = 0, precision: int = 32, blur: int = 0):
+    """Returns (norms[scales, 18], score) of one pair. blur: 0 VQM's sampled
+    Gaussian, 1 the recursive Gaussian."""
     norms = np.zeros(108, dtype=np.float64)
     scales = ctypes.c_uint32()
     score = ctypes.c_double()
     a, b = original.c(), distorted.c()
     _check(lib().ss2o_compute(ctypes.byref(a), ctypes.byref(b),
                               ctypes.c_float(background), chroma_filter,
-                              precision,
+                              precision, blur,
                               norms.ctypes.data_as(ctypes.c_void_p),
                               ctypes.byref(scales), ctypes.byref(score)))
     return norms[: 18 * scales.value].reshape(scales.value, 18), score.value
 
 
 def compute_many(pairs, background: float = 0.5, chroma_filter: int = 0,
-                 precision: int = 32, threads: int | None = None):
+                 precision: int = 32, threads: int | None = None, blur: int = 0):
     """Scores a list of (original, distorted) on host threads; returns
     (norms[n, 108], scales[n], scores[n])."""
     n = len(pairs)
@@ -147,7 +148,7 @@ def compute_many(pairs, background: float = 0.5, chroma_filter: int = 0,
     scores = np.zeros(n, dtype=np.float64)
     _check(lib().ss2o_compute_many(
         n, origs, dists, ctypes.c_float(background), chroma_filter, precision,
-        threads, norms.ctypes.data_as(ctypes.c_void_p),
+        blur, threads, norms.ctypes.data_as(ctypes.c_void_p),
         scales.ctypes.data_as(ctypes.c_void_p),
         scores.ctypes.data_as(ctypes.c_void_p)))
     return norms, scales, scores
@@ -165,6 +166,28 @@ def gaussian() -> np.ndarray:
     taps = np.zeros(13, dtype=np.float32)
     lib().ss2o_gaussian(taps.ctypes.data_as(ctypes.c_void_p))
     return taps
+
+
+def recursive_gaussian():
+    """(radius, freqs[3], beta[3], taps[13] in double) of the recursive
+    Gaussian, sigma 1.5."""
+    radius = ctypes.c_int()
+    freqs, beta, taps = np.zeros(3), np.zeros(3), np.zeros(13)
+    lib().ss2o_recursive_gaussian(ctypes.byref(radius), freqs.ctypes.data_as(ctypes.c_void_p),
+                                  beta.ctypes.data_as(ctypes.c_void_p),
+                                  taps.ctypes.data_as(ctypes.c_void_p))
+    return radius.value, freqs, beta, taps
+
+
+def blur_plane(plane: np.ndarray, blur: int = 0, precision: int = 64) -> np.ndarray:
+    """One plane blurred, zero padded (precision 64: double, the recursive
+    mode by its recursion; 32: float, the 13-tap passes)."""
+    src = np.ascontiguousarray(plane, dtype=np.float64)
+    out = np.zeros_like(src)
+    h, w = src.shape
+    _check(lib().ss2o_blur_plane(blur, precision, src.ctypes.data_as(ctypes.c_void_p), w, h,
+                                 out.ctypes.data_as(ctypes.c_void_p)))
+    return out
 
 
 def channel_pruned(channel: int, scale: int, scales: int) -> bool:

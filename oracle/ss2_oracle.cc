@@ -1118,19 +1118,132 @@ void BuildPyramid(const ss2o_image& img, const Desc& desc, T bg, const Plan& pla
 }
 
 // ---------------------------------------------------------------------------
+// The opt-in recursive Gaussian (no counterpart in VQM): the third-order
+// truncated-cosine recursion of D. Charalampidis, IEEE Trans. Signal
+// Processing 64(14), 2016, sigma 1.5, which Cloudinary's ssimulacra2
+// (81feacf6) applies through libjxl's lib/jxl/gauss_blur.cc (e47d2a2b).
+// Neither project is present here, so this restatement is pinned by the
+// filter's defining properties (unit gain, variance sigma^2, recursion ==
+// convolution), not by their outputs.
+//
+// Derived here from closed forms, independently of the library's numeric
+// sums: with N = round(3.2795 sigma + 0.2546) and w_k = (2k+1) pi / (2N),
+//   sum_{|m|<=N} cos(w_k m)             = (-1)^k / tan(w_k / 2)          (a_k)
+//   sum_{|m|<=N} (N^2 - m^2) cos(w_k m) = (-1)^k / (tan^2(w_k/2) sin w_k) (b_k)
+// and beta solves a . beta = 1, b . beta = N^2 - sigma^2 (unit gain,
+// variance sigma^2) and v . beta = v . rho with v = a x b, the direction the
+// first two leave free, rho_k = exp(-sigma^2 w_k^2 / 2) / N: beta is the
+// point nearest rho on the two constraints.
+// ---------------------------------------------------------------------------
+
+struct RecursiveGauss {
+    int n = 0;
+    double w[3] = {}, beta[3] = {};
+};
+
+RecursiveGauss MakeRecursiveGauss() {
+    constexpr double kPi = 3.14159265358979323846;
+    const double sigma = 1.5;
+    RecursiveGauss g;
+    g.n = static_cast<int>(std::lround(3.2795 * sigma + 0.2546));
+    double a[3], b[3], rho[3];
+    for (int k = 0; k < 3; ++k) {
+        g.w[k] = (2 * k + 1) * kPi / (2.0 * g.n);
+        const double sign = (k & 1) ? -1.0 : 1.0;
+        const double t = std::tan(0.5 * g.w[k]);
+        a[k] = sign / t;
+        b[k] = sign / (t * t * std::sin(g.w[k]));
+        rho[k] = std::exp(-0.5 * sigma * sigma * g.w[k] * g.w[k]) / g.n;
+    }
+    const double v[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2],
+                         a[0] * b[1] - a[1] * b[0]};
+    double m[3][4] = {{a[0], a[1], a[2], 1.0},
+                      {b[0], b[1], b[2], double(g.n) * g.n - sigma * sigma},
+                      {v[0], v[1], v[2], v[0] * rho[0] + v[1] * rho[1] + v[2] * rho[2]}};
+    // Gaussian elimination with partial pivoting on the 3x4 system.
+    for (int c = 0; c < 3; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < 3; ++r)
+            if (std::abs(m[r][c]) > std::abs(m[piv][c])) piv = r;
+        for (int k = 0; k < 4; ++k) std::swap(m[c][k], m[piv][k]);
+        for (int r = 0; r < 3; ++r) {
+            if (r == c) continue;
+            const double f = m[r][c] / m[c][c];
+            for (int k = c; k < 4; ++k) m[r][k] -= f * m[c][k];
+        }
+    }
+    for (int k = 0; k < 3; ++k) g.beta[k] = m[k][3] / m[k][k];
+    return g;
+}
+
+// The impulse response h(m) = sum_k beta_k cos(w_k m), |m| < N, centred in
+// 13 taps (h(+-N) = 0 exactly: cos(w_k N) = 0).
+std::array<double, kTaps> RecursiveTapsDouble() {
+    const RecursiveGauss g = MakeRecursiveGauss();
+    std::array<double, kTaps> h{};
+    for (int m = -(g.n - 1); m <= g.n - 1; ++m) {
+        double v = 0.0;
+        for (int k = 0; k < 3; ++k) v += g.beta[k] * std::cos(g.w[k] * m);
+        h[m + kRadius] = v;
+    }
+    return h;
+}
+
+// The recursion itself, in double, along one line of `len` samples at
+// stride `step`, zero-padded: S_k[n] = 2 cos(w_k) S_k[n-1] - S_k[n-2]
+// + (-1)^k sin(w_k) (x[n+N-1] + x[n-N-1]) from zero state,
+// y[n] = sum_k beta_k S_k[n].
+void RecursiveLine(const RecursiveGauss& g, const double* x, double* y, int len, size_t step) {
+    double c2[3], sn[3], s1[3] = {0, 0, 0}, s2[3] = {0, 0, 0};
+    for (int k = 0; k < 3; ++k) {
+        c2[k] = 2.0 * std::cos(g.w[k]);
+        sn[k] = ((k & 1) ? -1.0 : 1.0) * std::sin(g.w[k]);
+    }
+    auto at = [&](int i) { return (i >= 0 && i < len) ? x[size_t(i) * step] : 0.0; };
+    for (int n = 1 - g.n; n < len; ++n) {
+        const double in = at(n + g.n - 1) + at(n - g.n - 1);
+        double out = 0.0;
+        for (int k = 0; k < 3; ++k) {
+            const double s = c2[k] * s1[k] - s2[k] + sn[k] * in;
+            s2[k] = s1[k];
+            s1[k] = s;
+            out += g.beta[k] * s;
+        }
+        if (n >= 0) y[size_t(n) * step] = out;
+    }
+}
+
+// Rows, then columns, as the reference's blur runs them.
+void RecursiveBlur(const std::vector<double>& src, std::vector<double>& dst, uint32_t w,
+                   uint32_t h) {
+    static const RecursiveGauss g = MakeRecursiveGauss();
+    std::vector<double> tmp(src.size());
+    dst.assign(src.size(), 0.0);
+    for (uint32_t y = 0; y < h; ++y)
+        RecursiveLine(g, &src[size_t(y) * w], &tmp[size_t(y) * w], static_cast<int>(w), 1);
+    for (uint32_t x = 0; x < w; ++x)
+        RecursiveLine(g, &tmp[x], &dst[x], static_cast<int>(h), w);
+}
+
+// ---------------------------------------------------------------------------
 // Blurs, maps and norms (scale.comp) and their reduction (reduce.comp).
 // ---------------------------------------------------------------------------
 
+// blur 0: VQM's sampled Gaussian; 1: the recursive Gaussian's impulse
+// response. The FP32 path rounds the taps to float as the kernels do.
+constexpr int kBlurSampled = 0;
+constexpr int kBlurRecursive = 1;
+
 template <class T>
-std::array<T, kTaps> Taps() {
-    const auto w = GaussianDouble();
+std::array<T, kTaps> Taps(int blur) {
+    const auto w = blur == kBlurRecursive ? RecursiveTapsDouble() : GaussianDouble();
     std::array<T, kTaps> t{};
     for (int i = 0; i < kTaps; ++i) t[i] = static_cast<T>(static_cast<float>(w[i]));
     return t;
 }
 template <>
-std::array<double, kTaps> Taps<double>() {
-    return GaussianDouble();
+std::array<double, kTaps> Taps<double>(int blur) {
+    return blur == kBlurRecursive ? RecursiveTapsDouble() : GaussianDouble();
 }
 
 // scale.comp:149-207: horizontal pass, zero padded, acc = w0*s0 then fused
@@ -1241,9 +1354,25 @@ void Maps4(T mu1, T mu2, T ssum, T s12, T img1, T img2, T out[6]) {
 // invocations sums its column's four rows, a halving ladder adds the 256
 // invocation sums, the tile partial is stored, then reduce adds the partials
 // 256-way strided and halves again.
+// The FP64 recursive mode blurs by the recursion itself; every other mode
+// by the 13-tap passes.
+template <class T>
+void Blur2D(const std::vector<T>& src, std::vector<T>& hq, std::vector<T>& dst, uint32_t w,
+            uint32_t h, const std::array<T, kTaps>& wt, bool recursion) {
+    if constexpr (std::is_same_v<T, double>) {
+        if (recursion) {
+            RecursiveBlur(src, dst, w, h);
+            return;
+        }
+    }
+    BlurH(src, hq, w, h, wt);
+    BlurV(hq, dst, w, h, wt);
+}
+
 template <class T>
 void ChannelSums(const std::vector<T>& a, const std::vector<T>& b, uint32_t w,
-                 uint32_t h, const std::array<T, kTaps>& wt, T sums[6], bool four = false) {
+                 uint32_t h, const std::array<T, kTaps>& wt, T sums[6], bool four = false,
+                 bool recursion = false) {
     std::vector<T> q[5], hq, bq[5];
     const size_t n = size_t(w) * h;
     for (int i = 0; i < 5; ++i) q[i].resize(n);
@@ -1256,8 +1385,7 @@ void ChannelSums(const std::vector<T>& a, const std::vector<T>& b, uint32_t w,
     }
     for (int i = 0; i < 5; ++i) {
         if (four && i == 3) continue;
-        BlurH(q[i], hq, w, h, wt);
-        BlurV(hq, bq[i], w, h, wt);
+        Blur2D(q[i], hq, bq[i], w, h, wt, recursion);
     }
     const uint32_t gx = (w + 31) / 32, gy = (h + 31) / 32;
     const uint32_t groups = gx * gy;
@@ -1309,7 +1437,10 @@ struct PairResult {
 // The whole pair: both pyramids, then every kept (level, channel).
 template <class T>
 PairResult<T> ComputePair(const ss2o_image& o, const ss2o_image& dsrc, float background,
-                          int chroma_filter, bool half = false, bool four = false) {
+                          int chroma_filter, bool half = false, bool four = false,
+                          int blur = kBlurSampled) {
+    if (blur != kBlurSampled && blur != kBlurRecursive)
+        throw std::invalid_argument("unknown blur mode");
     if (o.width != dsrc.width || o.height != dsrc.height)
         throw std::invalid_argument("image sizes differ");
     const Plan plan = PlanScales(o.width, o.height);
@@ -1321,7 +1452,7 @@ PairResult<T> ComputePair(const ss2o_image& o, const ss2o_image& dsrc, float bac
     Pyramid<T> p0, p1;
     BuildPyramid<T>(o, d0, static_cast<T>(background), plan, p0, half);
     BuildPyramid<T>(dsrc, d1, static_cast<T>(background), plan, p1, half);
-    const auto wt = Taps<T>();
+    const auto wt = Taps<T>(blur);
     PairResult<T> r;
     r.scales = plan.count;
     for (int l = 0; l < plan.count; ++l) {
@@ -1330,7 +1461,7 @@ PairResult<T> ComputePair(const ss2o_image& o, const ss2o_image& dsrc, float bac
             if (ChannelPruned(c, l, plan.count)) continue;
             T s[6];
             ChannelSums<T>(p0.planes[l][c], p1.planes[l][c], plan.sizes[l].w,
-                           plan.sizes[l].h, wt, s, four);
+                           plan.sizes[l].h, wt, s, four, blur == kBlurRecursive);
             r.sums[l][c * 2 + 0] = s[0];
             r.sums[l][c * 2 + 1] = s[1];
             r.sums[l][6 + c * 4 + 0] = s[2];
@@ -1366,15 +1497,15 @@ int Fail(const std::exception& e) {
 }
 
 int ComputeOne(const ss2o_image* o, const ss2o_image* d, float bg, int filter,
-               int precision, double* norms, uint32_t* scales, double* score) {
+               int precision, int blur, double* norms, uint32_t* scales, double* score) {
     const Plan plan = PlanScales(o->width, o->height);
     std::fill(norms, norms + 108, 0.0);
     if (precision == 64) {
-        const auto r = ComputePair<double>(*o, *d, bg, filter);
+        const auto r = ComputePair<double>(*o, *d, bg, filter, false, false, blur);
         ReadResult(r, plan, norms);
     } else {
         const auto r = ComputePair<float>(*o, *d, bg, filter, precision == 16,
-                                          precision == 33);
+                                          precision == 33, blur);
         ReadResult(r, plan, norms);
     }
     if (scales) *scales = static_cast<uint32_t>(plan.count);
@@ -1387,11 +1518,11 @@ int ComputeOne(const ss2o_image* o, const ss2o_image* d, float bg, int filter,
 extern "C" {
 
 int ss2o_compute(const ss2o_image* original, const ss2o_image* distorted,
-                 float background, int chroma_filter, int precision,
+                 float background, int chroma_filter, int precision, int blur,
                  double* norms, uint32_t* scales, double* score) {
     try {
         return ComputeOne(original, distorted, background, chroma_filter,
-                          precision, norms, scales, score);
+                          precision, blur, norms, scales, score);
     } catch (const std::exception& e) {
         return Fail(e);
     }
@@ -1399,7 +1530,7 @@ int ss2o_compute(const ss2o_image* original, const ss2o_image* distorted,
 
 int ss2o_compute_many(uint32_t n, const ss2o_image* originals,
                       const ss2o_image* distorteds, float background,
-                      int chroma_filter, int precision, uint32_t threads,
+                      int chroma_filter, int precision, int blur, uint32_t threads,
                       double* norms, uint32_t* scales, double* scores) {
     std::atomic<uint32_t> next{0};
     std::atomic<int> status{SS2O_OK};
@@ -1410,7 +1541,7 @@ int ss2o_compute_many(uint32_t n, const ss2o_image* originals,
             if (i >= n) return;
             try {
                 ComputeOne(&originals[i], &distorteds[i], background, chroma_filter,
-                           precision, norms + size_t(i) * 108,
+                           precision, blur, norms + size_t(i) * 108,
                            scales ? scales + i : nullptr, scores ? scores + i : nullptr);
             } catch (const std::exception& e) {
                 int expected = SS2O_OK;
@@ -1445,6 +1576,40 @@ int ss2o_plan_scales(uint32_t width, uint32_t height, uint32_t* sizes12) {
 void ss2o_gaussian(float* taps13) {
     const auto w = GaussianDouble();
     for (int i = 0; i < kTaps; ++i) taps13[i] = static_cast<float>(w[i]);
+}
+
+void ss2o_recursive_gaussian(int* radius, double* freqs3, double* beta3, double* taps13) {
+    const RecursiveGauss g = MakeRecursiveGauss();
+    const auto h = RecursiveTapsDouble();
+    *radius = g.n;
+    for (int k = 0; k < 3; ++k) {
+        freqs3[k] = g.w[k];
+        beta3[k] = g.beta[k];
+    }
+    for (int i = 0; i < kTaps; ++i) taps13[i] = h[i];
+}
+
+int ss2o_blur_plane(int blur, int precision, const double* in, uint32_t width,
+                    uint32_t height, double* out) {
+    try {
+        if (blur != kBlurSampled && blur != kBlurRecursive)
+            throw std::invalid_argument("unknown blur mode");
+        const size_t n = size_t(width) * height;
+        if (precision == 64) {
+            std::vector<double> src(in, in + n), hq, dst;
+            Blur2D<double>(src, hq, dst, width, height, Taps<double>(blur),
+                           blur == kBlurRecursive);
+            std::copy(dst.begin(), dst.end(), out);
+        } else {
+            std::vector<float> src(n), hq, dst;
+            for (size_t i = 0; i < n; ++i) src[i] = static_cast<float>(in[i]);
+            Blur2D<float>(src, hq, dst, width, height, Taps<float>(blur), false);
+            for (size_t i = 0; i < n; ++i) out[i] = dst[i];
+        }
+        return SS2O_OK;
+    } catch (const std::exception& e) {
+        return Fail(e);
+    }
 }
 
 int ss2o_channel_pruned(uint32_t channel, uint32_t scale, uint32_t scales) {

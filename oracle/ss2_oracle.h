@@ -67,21 +67,32 @@ typedef struct ss2o_image {
  * the same algorithm in FP64, 16 = the FP32 restatement of VQM's half-plane
  * build (pyramid planes and level averages rounded to binary16), 33 = the
  * FP32 restatement with s11 + s22 blurred as one quantity (the CUDA blur's
- * four-quantity mode; not VQM's rounding). Writes 18*scales doubles into
- * norms[108], the scale count into *scales and the score into *score. */
+ * four-quantity mode; not VQM's rounding). blur: 0 = VQM's sampled
+ * Gaussian, 1 = the opt-in recursive Gaussian (FP32: its impulse response
+ * as 13 float taps, the CUDA kernels' evaluation; FP64: the recursion
+ * itself). Writes 18*scales doubles into norms[108], the scale count into
+ * *scales and the score into *score. */
 int ss2o_compute(const ss2o_image* original, const ss2o_image* distorted,
-                 float background, int chroma_filter, int precision,
+                 float background, int chroma_filter, int precision, int blur,
                  double* norms, uint32_t* scales, double* score);
 
 /* Scores n pairs on `threads` host threads (one pair per thread at a time). */
 int ss2o_compute_many(uint32_t n, const ss2o_image* originals,
                       const ss2o_image* distorteds, float background,
-                      int chroma_filter, int precision, uint32_t threads,
+                      int chroma_filter, int precision, int blur, uint32_t threads,
                       double* norms, uint32_t* scales, double* scores);
 
 /* Pieces, exposed so the tests can pin them one by one. */
 int ss2o_plan_scales(uint32_t width, uint32_t height, uint32_t* sizes12);
 void ss2o_gaussian(float* taps13);
+/* The recursive Gaussian (sigma 1.5): window half-width, the three
+ * frequencies and coefficients, and its impulse response in double as 13
+ * taps (offsets -6..6). */
+void ss2o_recursive_gaussian(int* radius, double* freqs3, double* beta3, double* taps13);
+/* One plane blurred, zero padded: precision 64 in double (the recursive
+ * mode by its recursion), 32 in float by the 13-tap passes. */
+int ss2o_blur_plane(int blur, int precision, const double* in, uint32_t width,
+                    uint32_t height, double* out);
 int ss2o_channel_pruned(uint32_t channel, uint32_t scale, uint32_t scales);
 int ss2o_score(const double* norms, uint32_t scales, double* score);
 int ss2o_required_bytes(const ss2o_format* format, uint32_t width,

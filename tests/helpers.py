@@ -122,8 +122,9 @@ def to_oracle(img: ss2.Image) -> ob.Image:
     return ob.Image(img.width, img.height, of, img.data)
 
 
-def oracle_compute(o: ss2.Image, d: ss2.Image, background=0.5, chroma_filter=0, precision=32):
-    return ob.compute(to_oracle(o), to_oracle(d), background, chroma_filter, precision)
+def oracle_compute(o: ss2.Image, d: ss2.Image, background=0.5, chroma_filter=0, precision=32,
+                   blur=0):
+    return ob.compute(to_oracle(o), to_oracle(d), background, chroma_filter, precision, blur)
 
 
 def feature_mismatch(actual: np.ndarray, expected: np.ndarray, rtol=FEATURE_RTOL,

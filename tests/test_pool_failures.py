@@ -25,7 +25,7 @@ class FakeBatch:
 
     log = None
 
-    def __init__(self, max_pairs=0, chroma_filter=0, device=-1):
+    def __init__(self, max_pairs=0, chroma_filter=0, device=-1, half_planes=False, blur=0):
         self.token, self.pending, self.closed = 0, None, False
 
     def submit(self, pairs, background=0.5, borrow=False):

@@ -122,6 +122,14 @@ def test_cli_scores_frames_and_clip_mean(tmp_path):
     lines = out.getvalue().strip().splitlines()
     assert len(lines) == len(pairs) + 1
     assert abs(float(lines[-1]) - doc["score"]) < 1e-7
+    # The opt-in recursive blur scores the same frames against its own oracle.
+    out = io.StringIO()
+    assert cli.run([po, pd, "--json", "--blur", "recursive"], out=out) == 0
+    doc = json.loads(out.getvalue())
+    for s, (o, d) in zip(doc["frame_scores"], pairs):
+        oo, dd = ss2.Image(o.width, o.height, fmt, o.data), ss2.Image(d.width, d.height, fmt, d.data)
+        _, score = helpers.oracle_compute(oo, dd, blur=ss2.Ssimulacra2Blur.RECURSIVE)
+        assert abs(s - score) <= helpers.SCORE_TOL
 
 
 @pytest.mark.gpu

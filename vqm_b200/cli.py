@@ -61,6 +61,7 @@ _PRIMARIES = {
     "smpte432": ss2.ColorPrimaries.St432_1,
 }
 _FILTERS = {"bilinear": 0, "bicubic": 1, "lanczos": 2}
+_BLURS = {"sampled": ss2.Ssimulacra2Blur.SAMPLED, "recursive": ss2.Ssimulacra2Blur.RECURSIVE}
 
 
 def raw_norms(result) -> list[float]:
@@ -92,14 +93,14 @@ class _Scorer:
     """Frame pairs -> results, batched, or one pair per call on two pipelines
     in turn (frame i + 1's upload overlaps frame i's kernels)."""
 
-    def __init__(self, width, height, batch, chroma_filter, device):
+    def __init__(self, width, height, batch, chroma_filter, device, blur=0):
         self.batch = batch
         if batch > 1:
             self.s = [ss2.Ssimulacra2Batch(max_pairs=batch, chroma_filter=chroma_filter,
-                                           device=device)]
+                                           device=device, blur=blur)]
         else:
             self.s = [ss2.Ssimulacra2Pipeline(width, height, chroma_filter=chroma_filter,
-                                              device=device) for _ in range(2)]
+                                              device=device, blur=blur) for _ in range(2)]
 
     def score(self, pairs, background):
         if self.batch > 1:
@@ -144,6 +145,9 @@ def run(argv=None, out=sys.stdout) -> int:
     ap.add_argument("--chroma-filter", choices=list(_FILTERS), default="bilinear")
     ap.add_argument("--batch", type=int, default=8, help="frame pairs per launch (1 = graphs)")
     ap.add_argument("--device", type=int, default=-1)
+    ap.add_argument("--blur", choices=list(_BLURS), default="sampled",
+                    help="sampled: VQM's 13-tap Gaussian; recursive: the recursive Gaussian "
+                         "of Cloudinary's ssimulacra2 (opt-in; not VQM's scores)")
     args = ap.parse_args(argv)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -176,7 +180,7 @@ def run(argv=None, out=sys.stdout) -> int:
             rd.skip(mine.start)
             todo = len(mine)
         scorer = _Scorer(ho.width, ho.height, max(1, args.batch), _FILTERS[args.chroma_filter],
-                         device)
+                         device, _BLURS[args.blur])
         frames = []  # (score, raw norms)
         t0 = time.perf_counter()
         io, idis = iter(ro), iter(rd)

@@ -47,9 +47,6 @@
 namespace vqm_b200 {
 namespace {
 
-// The 13 Gaussian taps as (w, w) pairs: the two-lane multiply-adds take a
-// tap for both lanes straight from the constant bank.
-__constant__ float2 c_taps2[kTaps];
 // score.cc:38-87, flat rows channel * scales + scale.
 __constant__ double c_weights[18][6];
 
@@ -288,7 +285,8 @@ __device__ __forceinline__ float2 Div2(float2 a, float2 b) {
 // 16-byte column block index XORed with 4 on rows whose (row >> 1) is odd,
 // so the quarter warp's stores (rows 2rp and 2rp + 2) do not collide either.
 template <int TW, int TH, int NT>
-__device__ __forceinline__ void HorizontalPass(const float* src, float* hq, int rp_begin = 0) {
+__device__ __forceinline__ void HorizontalPass(const float2 (&taps)[kTaps], const float* src,
+                                               float* hq, int rp_begin = 0) {
     using T = Tile<TW, TH, NT>;
     constexpr int KH = T::KH;
     const int tasks = T::HT - rp_begin * T::NG;
@@ -321,10 +319,10 @@ __device__ __forceinline__ void HorizontalPass(const float* src, float* hq, int 
                               : __fmul2_rn(A[j], B[j]);
             float2 acc[KH];
 #pragma unroll
-            for (int k = 0; k < KH; ++k) acc[k] = __fmul2_rn(c_taps2[0], S[k]);
+            for (int k = 0; k < KH; ++k) acc[k] = __fmul2_rn(taps[0], S[k]);
 #pragma unroll
             for (int tap = 1; tap < kTaps; ++tap) {
-                const float2 wt = c_taps2[tap];
+                const float2 wt = taps[tap];
 #pragma unroll
                 for (int k = 0; k < KH; ++k) acc[k] = __ffma2_rn(wt, S[k + tap], acc[k]);
             }
@@ -341,7 +339,8 @@ __device__ __forceinline__ void HorizontalPass(const float* src, float* hq, int 
 // kEdge, pixels outside the level contribute 0 (their inputs are the zero
 // padding, so every map value is finite before it is dropped).
 template <int TW, int TH, int NT, bool kEdge>
-__device__ __forceinline__ void VerticalMaps(const float* src, const float* hq, const TileRef& t,
+__device__ __forceinline__ void VerticalMaps(const float2 (&taps)[kTaps], const float* src,
+                                             const float* hq, const TileRef& t,
                                              float2 (&sum)[6]) {
     using T = Tile<TW, TH, NT>;
     constexpr int RV = T::RV;
@@ -361,9 +360,9 @@ __device__ __forceinline__ void VerticalMaps(const float* src, const float* hq, 
                 M[i] = *reinterpret_cast<const float2*>(plane + i * TW + cols[(i >> 1) & 1]);
 #pragma unroll
             for (int j = 0; j < RV; ++j) {
-                float2 acc = __fmul2_rn(c_taps2[0], M[j]);
+                float2 acc = __fmul2_rn(taps[0], M[j]);
 #pragma unroll
-                for (int k = 1; k < kTaps; ++k) acc = __ffma2_rn(c_taps2[k], M[j + k], acc);
+                for (int k = 1; k < kTaps; ++k) acc = __ffma2_rn(taps[k], M[j + k], acc);
                 V[q][j] = acc;
             }
         }
@@ -583,15 +582,15 @@ __device__ __forceinline__ void FinishSegment(const DevBatch& batch, uint32_t si
 template <int TW, int TH, int NT>
 __device__ __forceinline__ void ComputeTile(float* src, float* hq, const TileRef& t,
                                             const DevBatch& batch) {
-    HorizontalPass<TW, TH, NT>(src, hq);
+    HorizontalPass<TW, TH, NT>(batch.taps2, src, hq);
     __syncthreads();
     float2 sum[6];
 #pragma unroll
     for (int k = 0; k < 6; ++k) sum[k] = make_float2(0.0f, 0.0f);
     if (t.x0 + TW <= t.w && t.y0 + TH <= t.h)
-        VerticalMaps<TW, TH, NT, false>(src, hq, t, sum);
+        VerticalMaps<TW, TH, NT, false>(batch.taps2, src, hq, t, sum);
     else
-        VerticalMaps<TW, TH, NT, true>(src, hq, t, sum);
+        VerticalMaps<TW, TH, NT, true>(batch.taps2, src, hq, t, sum);
     __syncthreads();  // the reduction overwrites the source window
     ReducePartials<NT>(sum, LinearScratch<NT>{src},
                        batch.partials + static_cast<size_t>(t.partial) * 6);
@@ -717,12 +716,12 @@ __device__ __forceinline__ void RunStrip(const DevBatch& batch, uint32_t block, 
     for (int k = 0; k < count; ++k) {
         CpAsyncWait<0>();
         __syncthreads();
-        HorizontalPass<TW, TH, NT>(src, hq, k == 0 ? 0 : kRadius);
+        HorizontalPass<TW, TH, NT>(batch.taps2, src, hq, k == 0 ? 0 : kRadius);
         __syncthreads();
         if (t.x0 + TW <= t.w && t.y0 + TH <= t.h)
-            VerticalMaps<TW, TH, NT, false>(src, hq, t, sum);
+            VerticalMaps<TW, TH, NT, false>(batch.taps2, src, hq, t, sum);
         else
-            VerticalMaps<TW, TH, NT, true>(src, hq, t, sum);
+            VerticalMaps<TW, TH, NT, true>(batch.taps2, src, hq, t, sum);
         __syncthreads();  // every read of the window and of `hq` is done
         if (k + 1 < count) {
             t.y0 += TH;
@@ -969,11 +968,7 @@ cudaError_t CheckDivision(uint32_t first_bits, uint32_t last_bits, uint64_t* mis
     return cudaSuccess;
 }
 
-cudaError_t SetConstants(const float* taps13, const double* weights108) {
-    float2 pairs[kTaps];
-    for (int i = 0; i < kTaps; ++i) pairs[i] = make_float2(taps13[i], taps13[i]);
-    cudaError_t e = cudaMemcpyToSymbol(c_taps2, pairs, sizeof(pairs));
-    if (e != cudaSuccess) return e;
+cudaError_t SetConstants(const double* weights108) {
     return cudaMemcpyToSymbol(c_weights, weights108, sizeof(double) * 108);
 }
 

@@ -23,6 +23,8 @@
 
 #include <cstdint>
 
+#include <vector_types.h>
+
 namespace vqm_b200 {
 
 constexpr int kMaxLevels = 6;
@@ -159,6 +161,10 @@ struct DevBatch {
     uint32_t* blur_queue;        // the tile queue's next strip and exit count (0 between launches)
     uint32_t* status;            // nonzero: a kernel found bad input
     uint32_t half;               // 1: pyramid elements are binary16
+    // The blur's 13 taps (offsets -6..6) as (w, w) pairs: the blur kernels
+    // take them from the launch's parameter space, a constant bank like
+    // __constant__ memory, so each batch carries its blur mode's filter.
+    float2 taps2[kTaps];
 };
 
 }  // namespace vqm_b200

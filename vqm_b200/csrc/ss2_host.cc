@@ -707,6 +707,77 @@ std::array<float, kTaps> GaussianTaps() {
     return out;
 }
 
+// Cloudinary's ssimulacra2 (github.com/cloudinary/ssimulacra2, 81feacf6)
+// blurs with libjxl's recursive Gaussian (lib/jxl/gauss_blur.cc at libjxl
+// e47d2a2b), the third-order method of D. Charalampidis, "Recursive
+// Implementation of the Gaussian Filter Using Truncated Cosine Functions",
+// IEEE Trans. Signal Processing 64(14), 2016. Restated here from the method:
+//
+// - window half-width N = nearest integer to 3.2795 sigma + 0.2546 (5 for
+//   sigma 1.5) and frequencies w_k = (2k + 1) pi / (2N), k = 0, 1, 2, so
+//   that cos(w_k N) = 0;
+// - impulse response h(m) = sum_k beta_k cos(w_k m) for |m| <= N, 0 outside
+//   (h(+-N) = 0 too, so 2N - 1 = 9 taps are nonzero);
+// - beta: unit gain (sum_m h(m) = 1) and variance sigma^2
+//   (sum_m m^2 h(m) = sigma^2), and of the coefficient vectors that meet both
+//   the one closest to the Gaussian's cosine-series coefficients
+//   rho_k = exp(-sigma^2 w_k^2 / 2) / N.
+//
+// Its recursion runs, for each k, S_k[n] = 2 cos(w_k) S_k[n-1] - S_k[n-2]
+// + (-1)^k sin(w_k) (x[n+N-1] + x[n-N-1]) from zero state over zero-padded
+// input, with y[n] = sum_k beta_k S_k[n]: exactly the zero-padded
+// convolution with h (the windowed cosine times 1 - 2 cos(w) z^-1 + z^-2
+// leaves only the two boundary terms). The kernels evaluate that
+// convolution directly with these taps, rounded to float once as VQM rounds
+// its sampled taps; the oracle's FP64 mode runs the recursion itself.
+std::array<float, kTaps> RecursiveGaussianTaps() {
+    constexpr double kPi = 3.14159265358979323846;
+    const double sigma = 1.5;
+    const int n = static_cast<int>(std::lround(3.2795 * sigma + 0.2546));
+    static_assert(kRadius >= 5, "the recursive Gaussian's support fits the taps");
+    double w[3], rho[3], p[2][3];
+    for (int k = 0; k < 3; ++k) {
+        w[k] = (2 * k + 1) * kPi / (2.0 * n);
+        rho[k] = std::exp(-0.5 * sigma * sigma * w[k] * w[k]) / n;
+        p[0][k] = p[1][k] = 0.0;
+        for (int m = -n; m <= n; ++m) {
+            const double c = std::cos(w[k] * m);
+            p[0][k] += c;
+            p[1][k] += static_cast<double>(m) * m * c;
+        }
+    }
+    // beta = rho + P^T (P P^T)^-1 (g - P rho): the nearest point to rho on
+    // the two constraints P beta = g = (1, sigma^2).
+    const double g[2] = {1.0, sigma * sigma};
+    double r[2], a[2][2];
+    for (int i = 0; i < 2; ++i) {
+        r[i] = g[i];
+        for (int k = 0; k < 3; ++k) r[i] -= p[i][k] * rho[k];
+        for (int j = 0; j < 2; ++j) {
+            a[i][j] = 0.0;
+            for (int k = 0; k < 3; ++k) a[i][j] += p[i][k] * p[j][k];
+        }
+    }
+    const double det = a[0][0] * a[1][1] - a[0][1] * a[1][0];
+    const double l0 = (a[1][1] * r[0] - a[0][1] * r[1]) / det;
+    const double l1 = (a[0][0] * r[1] - a[1][0] * r[0]) / det;
+    double beta[3];
+    for (int k = 0; k < 3; ++k) beta[k] = rho[k] + p[0][k] * l0 + p[1][k] * l1;
+    std::array<float, kTaps> out{};
+    for (int m = -(n - 1); m <= n - 1; ++m) {
+        double h = 0.0;
+        for (int k = 0; k < 3; ++k) h += beta[k] * std::cos(w[k] * m);
+        out[m + kRadius] = static_cast<float>(h);
+    }
+    return out;
+}
+
+std::array<float, kTaps> BlurTaps(uint32_t blur) {
+    if (blur == VQM_CU_SS2_BLUR_SAMPLED) return GaussianTaps();
+    if (blur == VQM_CU_SS2_BLUR_RECURSIVE) return RecursiveGaussianTaps();
+    throw std::invalid_argument("Ssimulacra2Config: unknown blur mode");
+}
+
 const double* ScoreWeights() { return kWeightTable; }
 
 double Score(const double* norms, int scales) {

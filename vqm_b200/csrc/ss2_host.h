@@ -45,6 +45,13 @@ bool ChannelPruned(int channel, int scale, int scales);
 
 // pipeline.cc:274-291: 13 taps, sigma 1.5, normalised in double, as float.
 std::array<float, kTaps> GaussianTaps();
+// The impulse response of the third-order recursive Gaussian (sigma 1.5) of
+// Cloudinary's ssimulacra2, centred in 13 taps (the outer four are 0); see
+// ss2_host.cc.
+std::array<float, kTaps> RecursiveGaussianTaps();
+// The taps of a vqm_cu_ss2 blur mode (VQM_CU_SS2_BLUR_*); throws
+// std::invalid_argument for an unknown mode.
+std::array<float, kTaps> BlurTaps(uint32_t blur);
 // score.cc:38-87 as a flat 108-double table.
 const double* ScoreWeights();
 // score.cc:118-163; throws std::invalid_argument like the reference.

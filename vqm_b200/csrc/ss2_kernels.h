@@ -9,7 +9,7 @@ namespace vqm_b200 {
 
 // Gaussian taps (13 floats) and score weights (18 x 6 doubles) into the
 // current device's constant banks; once per device.
-cudaError_t SetConstants(const float* taps13, const double* weights108);
+cudaError_t SetConstants(const double* weights108);
 
 cudaError_t LaunchPrepare(const DevBatch& batch, cudaStream_t stream);
 // `variant` indexes the blur kernels compiled in (BlurTileShape gives each

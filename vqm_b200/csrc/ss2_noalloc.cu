@@ -100,8 +100,7 @@ unsigned char* ScratchAddress(int device) {
         throw std::runtime_error(std::string("cuda: cudaGetSymbolAddress of the scratch array: ") +
                                  cudaGetErrorString(e));
     }
-    const auto taps = GaussianTaps();
-    const cudaError_t c = SetConstants(taps.data(), ScoreWeights());
+    const cudaError_t c = SetConstants(ScoreWeights());
     if (c != cudaSuccess) {
         cudaGetLastError();
         throw std::runtime_error(std::string("cuda: constant upload: ") + cudaGetErrorString(c));
@@ -281,6 +280,8 @@ void Run(const vqm_cu_image* o, const vqm_cu_image* d, float background, uint32_
     b.seg_done = pair_done + 1;
     b.blur_queue = pair_done + 1 + kMaxSegments;
     b.status = nullptr;
+    const std::array<float, kTaps> taps = GaussianTaps();
+    for (int i = 0; i < kTaps; ++i) b.taps2[i] = make_float2(taps[i], taps[i]);
 
     cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
     StageTablesKernel<<<1, 256, 0, stream>>>(t, dev_tables, pair_done);

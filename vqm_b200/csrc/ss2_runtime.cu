@@ -62,7 +62,7 @@ uint64_t NextIncarnation() {
 constexpr const char* kCapacityError =
     "resident image capacity exhausted; raise gpu_resident_images";
 
-// Per-device one-time constant upload (Gaussian taps, score weights).
+// Per-device one-time constant upload (score weights).
 void EnsureDevice(int device) {
     static std::mutex mu;
     static std::vector<bool> ready;
@@ -71,8 +71,7 @@ void EnsureDevice(int device) {
     if (ready.size() <= static_cast<size_t>(device)) ready.resize(device + 1, false);
     if (ready[device]) return;
     VQM_CK(cudaSetDevice(device));
-    const auto taps = GaussianTaps();
-    VQM_CK(SetConstants(taps.data(), ScoreWeights()));
+    VQM_CK(SetConstants(ScoreWeights()));
     // Kernels load lazily on their first launch otherwise: a first batch,
     // or the first that selects a new blur variant, would pay for it.
     VQM_CK(PreloadPrepare());
@@ -347,6 +346,12 @@ struct BatchMemory {
     uint32_t pair_count = 0;
     size_t elem_bytes = 4;  // pyramid element: float, or binary16 with half planes
 
+    // The blur mode's taps, carried by every launch of this memory's tables.
+    void SetBlur(uint32_t blur) {
+        const std::array<float, kTaps> taps = BlurTaps(blur);
+        for (int i = 0; i < kTaps; ++i) dev.taps2[i] = make_float2(taps[i], taps[i]);
+    }
+
     // Device bytes each buffer needs for `t`, in the order table, pyramid,
     // partials, segment sums, pair counters, results (and the table offsets).
     std::array<size_t, 6> Needs(const Tables& t) {
@@ -581,6 +586,7 @@ public:
         // Half planes (ssimulacra2.h:41-46): binary16 pyramid elements, FP32
         // arithmetic, the level averages rounded like the planes.
         mem_.elem_bytes = cfg.half_planes ? 2 : 4;
+        mem_.SetBlur(cfg.blur);
         device_ = ResolveDevice(cfg.device);
         EnsureDevice(device_);
         VQM_CK(cudaSetDevice(device_));
@@ -1018,6 +1024,7 @@ class Batch {
 public:
     explicit Batch(const vqm_cu_ss2_batch_config& cfg) : cfg_(cfg) {
         if (cfg.chroma_filter > 2) throw std::invalid_argument("invalid chroma filter");
+        mem_.SetBlur(cfg.blur);
         if (cfg.variant) {
             if (cfg.variant > static_cast<uint32_t>(BlurTileCount()))
                 throw std::invalid_argument("cuda: no such blur variant");
@@ -1309,7 +1316,7 @@ struct vqm_cu_ss2_batch {
 extern "C" {
 
 const char* vqm_cu_last_error(void) { return vqm_b200::g_last_error.c_str(); }
-uint32_t vqm_cu_version(void) { return (1u << 16) | 0u; }
+uint32_t vqm_cu_version(void) { return (1u << 16) | 1u; }
 
 int vqm_cu_required_bytes(const vqm_cu_format* format, uint32_t width, uint32_t height,
                           size_t* bytes) {
@@ -1362,6 +1369,14 @@ int vqm_cu_ss2_channel_pruned(uint32_t channel, uint32_t scale, uint32_t scales,
                                           static_cast<int>(scales))
                       ? 1
                       : 0;
+    });
+}
+
+int vqm_cu_ss2_blur_taps(uint32_t blur, float* taps13) {
+    return Guard([&] {
+        NotNull(taps13, "taps13");
+        const std::array<float, vqm_b200::kTaps> taps = vqm_b200::BlurTaps(blur);
+        std::copy(taps.begin(), taps.end(), taps13);
     });
 }
 

@@ -95,6 +95,7 @@ public:
         if (cfg.variant > static_cast<uint32_t>(BlurTileCount()))
             throw std::invalid_argument("cuda: no such blur variant");
         variant_ = cfg.variant ? static_cast<int>(cfg.variant) - 1 : kDefaultBlurVariant;
+        BlurTaps(cfg.blur);  // rejects an unknown blur mode
         ClampToFreeMemory(cfg.device);
         stats_.budget_bytes = budget_;
         for (uint32_t i = 0; i < workers; ++i) {
@@ -103,6 +104,7 @@ public:
             bc.chroma_filter = cfg.chroma_filter;
             bc.device = cfg.device;
             bc.variant = cfg.variant;
+            bc.blur = cfg.blur;
             vqm_cu_ss2_batch* b = nullptr;
             if (vqm_cu_ss2_batch_create(&bc, &b) != VQM_CU_OK) {
                 const std::string msg = vqm_cu_last_error();

@@ -80,6 +80,15 @@ class ChromaFilter:
     Bilinear, Bicubic, Lanczos = 0, 1, 2
 
 
+class Ssimulacra2Blur:
+    """The blur (no counterpart in VQM's config). SAMPLED: VQM's 13-tap
+    sampled Gaussian, sigma 1.5 (pipeline.cc:274-291), VQM's scores.
+    RECURSIVE (opt-in): the third-order recursive Gaussian, sigma 1.5, of
+    Cloudinary's ssimulacra2, which VQM replaced on purpose
+    (docs/divergence.md:22); its scores follow that filter, not VQM."""
+    SAMPLED, RECURSIVE = 0, 1
+
+
 # ---------------------------------------------------------------------------
 # C structs (include/vqm_cu_ss2.h)
 # ---------------------------------------------------------------------------
@@ -144,7 +153,7 @@ class _Config(ctypes.Structure):
         ("streaming_inputs", ctypes.c_uint32),
         ("input_bytes", ctypes.c_uint64),
         ("device", ctypes.c_int32),
-        ("reserved", ctypes.c_uint32),
+        ("blur", ctypes.c_uint32),
     ]
 
 
@@ -158,6 +167,7 @@ class _BatchConfig(ctypes.Structure):
         ("tile_h", ctypes.c_uint32),
         ("variant", ctypes.c_uint32),
         ("half_planes", ctypes.c_uint32),
+        ("blur", ctypes.c_uint32),
     ]
 
 
@@ -169,7 +179,7 @@ class _ServerConfig(ctypes.Structure):
         ("chroma_filter", ctypes.c_uint32),
         ("device", ctypes.c_int32),
         ("variant", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("blur", ctypes.c_uint32),
     ]
 
 
@@ -194,6 +204,7 @@ _SIGS = {
     "vqm_cu_validate_format": ([_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p], ctypes.c_int),
     "vqm_cu_ss2_plan_scales": ([ctypes.c_uint32, ctypes.c_uint32, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_channel_pruned": ([ctypes.c_uint32] * 3 + [_P], ctypes.c_int),
+    "vqm_cu_ss2_blur_taps": ([ctypes.c_uint32, _P], ctypes.c_int),
     "vqm_cu_ss2_check_cbrt": ([ctypes.c_uint32, ctypes.c_uint32, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_check_division": ([ctypes.c_uint32, ctypes.c_uint32, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_score": ([_P, ctypes.c_uint32, _P], ctypes.c_int),
@@ -449,6 +460,14 @@ def channel_pruned(channel: int, scale: int, scales: int) -> bool:
     return bool(out.value)
 
 
+def blur_taps(blur: int = 0) -> np.ndarray:
+    """The 13 float taps (offsets -6..6) the kernels apply along each axis
+    for a blur mode (Ssimulacra2Blur)."""
+    taps = np.zeros(13, dtype=np.float32)
+    _check(_lib.vqm_cu_ss2_blur_taps(int(blur), taps.ctypes.data))
+    return taps
+
+
 def check_cbrt(first_bits: int, last_bits: int):
     """Runs the prepare kernels' cube root and the shared correctly rounded
     one on every float with a bit pattern in [first_bits, last_bits] on the
@@ -507,9 +526,10 @@ class Ssimulacra2Pipeline:
     def __init__(self, width: int, height: int, gpu_resident_images: int = 2,
                  half_planes: bool = False, chroma_filter: int = 0,
                  input_bytes: int = 0, streaming_inputs: bool = True,
-                 device: int = -1):
+                 device: int = -1, blur: int = 0):
+        """`blur`: Ssimulacra2Blur.SAMPLED (VQM's) or RECURSIVE (opt-in)."""
         cfg = _Config(width, height, gpu_resident_images, int(half_planes),
-                      chroma_filter, int(streaming_inputs), input_bytes, device, 0)
+                      chroma_filter, int(streaming_inputs), input_bytes, device, int(blur))
         self._p = ctypes.c_void_p()
         _check(_lib.vqm_cu_ss2_create(ctypes.byref(cfg), ctypes.byref(self._p)))
         self.size = (width, height)
@@ -651,17 +671,18 @@ class Ssimulacra2Batch:
 
     def __init__(self, max_pairs: int = 0, max_pixels: int = 0, chroma_filter: int = 0,
                  device: int = -1, tile: tuple[int, int] | None = None,
-                 variant: int | None = None, half_planes: bool = False):
+                 variant: int | None = None, half_planes: bool = False, blur: int = 0):
         """`variant` picks a compiled blur kernel (see blur_variants());
         `tile` picks the one-tile-per-CTA kernel of that output tile;
         neither: each submit picks a 32x32 strip length from its tile count
         (strips regroup the compensated partial sums, so results agree to
         rounding, ~1e-7 relative, whichever runs). `half_planes` stores the
-        pyramid as binary16 (ssimulacra2.h:41-46)."""
+        pyramid as binary16 (ssimulacra2.h:41-46). `blur`: the filter
+        (Ssimulacra2Blur)."""
         tw, th = tile if tile else (0, 0)
         v = 0 if variant is None else variant + 1
         cfg = _BatchConfig(max_pixels, max_pairs, chroma_filter, device, tw, th, v,
-                           int(half_planes))
+                           int(half_planes), int(blur))
         self._b = ctypes.c_void_p()
         _check(_lib.vqm_cu_ss2_batch_create(ctypes.byref(cfg), ctypes.byref(self._b)))
 
@@ -771,12 +792,13 @@ class Ssimulacra2Pool:
     taken."""
 
     def __init__(self, workers: int = 1, chunk: int = 64, chroma_filter: int = 0,
-                 device: int = -1):
+                 device: int = -1, half_planes: bool = False, blur: int = 0):
         if workers == 0:
             raise InvalidArgument("pool needs at least one worker")
         self._chunk = max(1, chunk)
         self._batches = [Ssimulacra2Batch(max_pairs=self._chunk, chroma_filter=chroma_filter,
-                                          device=device) for _ in range(workers)]
+                                          device=device, half_planes=half_planes, blur=blur)
+                         for _ in range(workers)]
         self._queue = collections.deque()     # (ticket, first, pairs, background) not submitted
         self._inflight = collections.deque()  # (worker, token, ticket, first, pairs) in order
         self._busy = [False] * workers
@@ -899,9 +921,10 @@ class Ssimulacra2Server:
     then agree to rounding, ~1e-7 relative)."""
 
     def __init__(self, memory_budget: int = 0, workers: int = 2, max_batch_pairs: int = 64,
-                 chroma_filter: int = 0, device: int = -1, variant: int = 0):
+                 chroma_filter: int = 0, device: int = -1, variant: int = 0,
+                 blur: int = 0):
         cfg = _ServerConfig(memory_budget, workers, max_batch_pairs, chroma_filter, device,
-                            variant, 0)
+                            variant, int(blur))
         self._s = ctypes.c_void_p()
         _check(_lib.vqm_cu_ss2_server_create(ctypes.byref(cfg), ctypes.byref(self._s)))
         self._keep = {}
