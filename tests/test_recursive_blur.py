@@ -15,8 +15,11 @@ by its defining properties and by its own FP64 evaluation, never by VQM:
   ragged sizes and on an impulse;
 - the FP32 restatement of the whole metric in this mode (the CUDA kernels'
   arithmetic) stays within the stated bound of the FP64 recursion: score
-  within 1e-2, every feature within 1e-2 relative (absolute floor 1e-6);
-  measured on these pairs: at most 1.3e-3 in the score and 6e-3 relative.
+  within 1e-2, every feature within 1e-2 relative plus 5e-5 absolute.
+  Measured on these pairs and the GPU tests' pairs: at most 8.8e-3 in the
+  score (a 1922x1082 10-bit 4:2:0 pair) and 1.3e-5 absolute in a feature;
+  features below 1e-4 can differ by tens of percent, in either blur mode,
+  from the FP32 cancellation in sigma^2 = blur(x^2) - mu^2.
 """
 
 import numpy as np
@@ -29,7 +32,7 @@ from vqm_b200 import ss2
 
 SCORE_TOL64 = 1e-2
 FEATURE_RTOL64 = 1e-2
-FEATURE_ATOL64 = 1e-6
+FEATURE_ATOL64 = 5e-5
 
 
 def test_parameters_and_defining_properties():
@@ -103,6 +106,7 @@ def pairs():
     for w, h, seed in ((333, 187, 1), (640, 360, 2)):
         out.append(synthetic.rgb_pair(w, h, seed)[:2])
     out.append(synthetic.yuv_pair(480, 270, 4)[:2])
+    out.append(synthetic.yuv_pair(1280, 720, 73)[:2])
     return out
 
 
