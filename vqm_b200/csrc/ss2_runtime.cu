@@ -1058,17 +1058,22 @@ public:
         sms_ = DeviceSms(device_);
         VQM_CK(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
         stream_ = own_stream_;
+        VQM_CK(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
         VQM_CK(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming));
         VQM_CK(cudaEventCreateWithFlags(&copied_, cudaEventDisableTiming));
+        VQM_CK(cudaEventCreateWithFlags(&uploaded_, cudaEventDisableTiming));
+        VQM_CK(cudaEventCreateWithFlags(&kernels_done_, cudaEventDisableTiming));
         for (auto& e : stage_ev_) VQM_CK(cudaEventCreate(&e));
     }
     ~Batch() {
         cudaSetDevice(device_);
         if (stream_) cudaStreamSynchronize(stream_);
-        if (done_) cudaEventDestroy(done_);
-        if (copied_) cudaEventDestroy(copied_);
+        if (copy_stream_) cudaStreamSynchronize(copy_stream_);
+        for (cudaEvent_t e : {done_, copied_, uploaded_, kernels_done_})
+            if (e) cudaEventDestroy(e);
         for (auto& e : stage_ev_)
             if (e) cudaEventDestroy(e);
+        if (copy_stream_) cudaStreamDestroy(copy_stream_);
         if (own_stream_) cudaStreamDestroy(own_stream_);
     }
     void SetStream(void* s) {
@@ -1102,6 +1107,7 @@ public:
         if (in_flight_) throw std::logic_error("cuda: a batch is in flight; Finish it first");
         VQM_CK(cudaSetDevice(device_));
         VQM_CK(cudaStreamSynchronize(stream_));
+        VQM_CK(cudaStreamSynchronize(copy_stream_));
         mem_.ReleaseDevice();
         inputs_.reset();
     }
@@ -1149,13 +1155,22 @@ public:
         BuildPrepLists(t, group);
         mem_.Stage(t);
         if (host_bytes) VQM_CK(cudaEventRecord(copied_, stream_));
-        mem_.EnqueueUpload(mem_.table_bytes, stream_);
+        // The tables and counters go up on the batch's copy stream: they
+        // depend on nothing on the launch stream (this batch's previous
+        // submission has finished), so they overlap whatever runs there,
+        // typically another batch's kernels. The results come back on it
+        // too, so the launch stream goes straight on to its next kernels.
         VQM_CK(cudaMemsetAsync(mem_.pair_done.as<void>(), 0,
-                               sizeof(uint32_t) * (n + t.segs.size() + 2), stream_));
+                               sizeof(uint32_t) * (n + t.segs.size() + 2), copy_stream_));
+        mem_.EnqueueUpload(mem_.table_bytes, copy_stream_);
+        VQM_CK(cudaEventRecord(uploaded_, copy_stream_));
+        VQM_CK(cudaStreamWaitEvent(stream_, uploaded_, 0));
         mem_.EnqueueKernels(shape, stream_, timing_ ? stage_ev_ : nullptr);
         timed_ = timing_;
-        mem_.EnqueueReadback(stream_);
-        VQM_CK(cudaEventRecord(done_, stream_));
+        VQM_CK(cudaEventRecord(kernels_done_, stream_));
+        VQM_CK(cudaStreamWaitEvent(copy_stream_, kernels_done_, 0));
+        mem_.EnqueueReadback(copy_stream_);
+        VQM_CK(cudaEventRecord(done_, copy_stream_));
         count_ = n;
         token_ = NextIncarnation();
         in_flight_ = true;
@@ -1231,7 +1246,9 @@ private:
     int sms_ = 0;
     int device_ = 0;
     cudaStream_t own_stream_ = nullptr, stream_ = nullptr;
+    cudaStream_t copy_stream_ = nullptr;  // tables up, results down
     cudaEvent_t done_ = nullptr, copied_ = nullptr;
+    cudaEvent_t uploaded_ = nullptr, kernels_done_ = nullptr;
     cudaEvent_t stage_ev_[4] = {nullptr, nullptr, nullptr, nullptr};
     bool timing_ = false, timed_ = false;
     BatchMemory mem_;
