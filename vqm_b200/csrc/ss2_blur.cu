@@ -88,7 +88,7 @@ struct Tile {
     static constexpr int VT = (TW / 2) * (TH / RV);
     static constexpr size_t kSrcBytes = sizeof(float) * 2 * IMG;
     static constexpr size_t kHqBytes = sizeof(float) * 5 * SH * TW;
-    static_assert(TW % 32 == 0, "the store swizzle flips 16-float column blocks");
+    static_assert(TW % 32 == 0, "whole warps of column pairs in the vertical pass");
     static_assert(TH % RV == 0 && RP % 2 == 0 && NG % 4 == 0, "tile shape");
     static_assert(SRS % 32 == 28, "bank spread of the horizontal loads");
     static_assert(NT % 32 == 0 && NT >= 96, "whole warps, 16 lanes per sum");
@@ -281,9 +281,13 @@ __device__ __forceinline__ float2 Div2(float2 a, float2 b) {
 // Task -> (rp, column group): within every 8 lanes, lanes 0-3 take four
 // column groups of row pair rp and lanes 4-7 the same groups of rp + 1. The
 // source row pair stride is 28 banks mod 32, so the quarter warp's eight
-// 16-byte loads cover all 32 banks once. The results are stored with the
-// 16-byte column block index XORed with 4 on rows whose (row >> 1) is odd,
-// so the quarter warp's stores (rows 2rp and 2rp + 2) do not collide either.
+// 16-byte loads cover all 32 banks once.
+//
+// The horizontal planes are row-pair blocks too: row pair rp is TW / 2
+// 16-byte blocks, block b holding columns 2b, 2b + 1 of row 2rp and then of
+// row 2rp + 1, so the vertical pass reads two rows of its column pair with
+// one load. On odd row pairs block b is stored at b ^ 1, which keeps the
+// quarter warp's stores (row pairs rp and rp + 1, even and odd) apart.
 template <int TW, int TH, int NT>
 __device__ __forceinline__ void HorizontalPass(const float2 (&taps)[kTaps], const float* src,
                                                float* hq, int rp_begin = 0) {
@@ -306,7 +310,8 @@ __device__ __forceinline__ void HorizontalPass(const float2 (&taps)[kTaps], cons
             B[j] = make_float2(vb.x, vb.y);
             B[j + 1] = make_float2(vb.z, vb.w);
         }
-        float* out = hq + (2 * rp) * TW + ((cg ^ ((rp & 1) << 2)) << 2);
+        float* out = hq + rp * 2 * TW + 8 * cg;
+        const int flip = (rp & 1) << 2;  // block 2cg + h at 2cg + (h ^ (rp & 1))
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             float2 S[KH + 12];
@@ -327,9 +332,10 @@ __device__ __forceinline__ void HorizontalPass(const float2 (&taps)[kTaps], cons
                 for (int k = 0; k < KH; ++k) acc[k] = __ffma2_rn(wt, S[k + tap], acc[k]);
             }
             float* plane = out + q * T::SH * TW;
-            *reinterpret_cast<float4*>(plane) = make_float4(acc[0].x, acc[1].x, acc[2].x, acc[3].x);
-            *reinterpret_cast<float4*>(plane + TW) =
-                make_float4(acc[0].y, acc[1].y, acc[2].y, acc[3].y);
+            *reinterpret_cast<float4*>(plane + flip) =
+                make_float4(acc[0].x, acc[1].x, acc[0].y, acc[1].y);
+            *reinterpret_cast<float4*>(plane + (4 ^ flip)) =
+                make_float4(acc[2].x, acc[3].x, acc[2].y, acc[3].y);
         }
     }
 }
@@ -347,17 +353,21 @@ __device__ __forceinline__ void VerticalMaps(const float2 (&taps)[kTaps], const 
     for (int task = threadIdx.x; task < T::VT; task += NT) {
         const int c = (task % (TW / 2)) * 2;
         const int r0 = (task / (TW / 2)) * RV;
-        // Row r0 + i holds column c at c ^ 16 when ((r0 + i) >> 1) is odd,
-        // i.e. when (i >> 1) is odd, r0 being a multiple of 4.
-        const int cols[2] = {c, c ^ 16};
+        // Row pair r0 / 2 + i holds column pair c in block c / 2, at
+        // c / 2 ^ 1 when i is odd (r0 / 2 being even).
+        const int blocks[2] = {2 * c, 2 * (c ^ 2)};
         float2 V[5][RV];
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             const float* plane = hq + q * T::SH * TW + r0 * TW;
             float2 M[RV + 12];
 #pragma unroll
-            for (int i = 0; i < RV + 12; ++i)
-                M[i] = *reinterpret_cast<const float2*>(plane + i * TW + cols[(i >> 1) & 1]);
+            for (int i = 0; i < (RV + 12) / 2; ++i) {
+                const float4 v =
+                    *reinterpret_cast<const float4*>(plane + i * 2 * TW + blocks[i & 1]);
+                M[2 * i] = make_float2(v.x, v.y);
+                M[2 * i + 1] = make_float2(v.z, v.w);
+            }
 #pragma unroll
             for (int j = 0; j < RV; ++j) {
                 float2 acc = __fmul2_rn(taps[0], M[j]);
