@@ -388,12 +388,16 @@ __device__ __forceinline__ void BlockLinearGeneric(const DevSource& s, uint32_t 
 // fast range (x in [2^-30, 2^16), y in [2, 4]; the caller selects the rest),
 // the floating-point steps two lanes per instruction (FFMA2 / FMUL2 / FADD2),
 // each the operation the scalar function performs on that lane: the same
-// values. `logt` and `expt` are copies of the function's two tables (kLogF4,
-// kExpF2) in shared memory: each lane's entry depends on its value, and
-// divergent entries of a shared-memory table cost fewer cycles than the same
-// loads through L1.
-__device__ __forceinline__ float2 PowfGamma2(float2 x, float y, const float4* logt,
-                                             const float2* expt) {
+// values. `pt` is a copy of the function's two tables (kLogF4, kExpF2) in
+// shared memory, one array per field (PowTable): each lane's entry depends
+// on its value, and divergent entries of a shared-memory table cost fewer
+// cycles than the same loads through L1. One field per load puts the two
+// lanes' values straight into the register pair of a two-lane instruction.
+struct PowTable {
+    static constexpr int kInv = 0, kHi = 128, kLo = 256, kExpHi = 384, kExpLo = 448;
+    static constexpr int kFloats = 512;
+};
+__device__ __forceinline__ float2 PowfGamma2(float2 x, float y, const float* pt) {
     using namespace ss2dm;
     const auto P = [](float v) { return make_float2(v, v); };
     const auto N = [](float2 v) { return make_float2(-v.x, -v.y); };
@@ -401,8 +405,7 @@ __device__ __forceinline__ float2 PowfGamma2(float2 x, float y, const float4* lo
     const int i0 = static_cast<int>((ix0 >> 16) & 127u), i1 = static_cast<int>((ix1 >> 16) & 127u);
     const float2 m = make_float2(__uint_as_float((ix0 & 0x007fffffu) | 0x3f800000u),
                                  __uint_as_float((ix1 & 0x007fffffu) | 0x3f800000u));
-    const float4 L0 = logt[i0], L1 = logt[i1];  // inv, hi, lo, 0
-    const float2 inv = make_float2(L0.x, L1.x);
+    const float2 inv = make_float2(pt[PowTable::kInv + i0], pt[PowTable::kInv + i1]);
     const float2 p = __fmul2_rn(m, inv);
     const float2 pe = __ffma2_rn(m, inv, N(p));
     const float2 rh = __fadd2_rn(p, P(-1.0f));
@@ -414,8 +417,8 @@ __device__ __forceinline__ float2 PowfGamma2(float2 x, float y, const float4* lo
     const float2 ef = __fadd2_rn(make_float2(__uint_as_float(0x4b000000u | (ix0 >> 23)),
                                              __uint_as_float(0x4b000000u | (ix1 >> 23))),
                                  P(-8388735.0f));
-    const float2 lh = make_float2(L0.y, L1.y);
-    const float2 ll = make_float2(L0.z, L1.z);
+    const float2 lh = make_float2(pt[PowTable::kHi + i0], pt[PowTable::kHi + i1]);
+    const float2 ll = make_float2(pt[PowTable::kLo + i0], pt[PowTable::kLo + i1]);
     const float2 hi = __fadd2_rn(ef, lh);
     const float2 lo = __fadd2_rn(__fadd2_rn(__fadd2_rn(ef, N(hi)), lh), __fadd2_rn(ll, lr));
     const float2 th = __fmul2_rn(P(y), hi);
@@ -425,13 +428,13 @@ __device__ __forceinline__ float2 PowfGamma2(float2 x, float y, const float4* lo
     // conversion), and the table load issues before z and q are formed.
     const float2 big = __ffma2_rn(th, P(64.0f), P(12582912.0f));
     const uint32_t u0 = __float_as_uint(big.x), u1 = __float_as_uint(big.y);
-    const float2 T0 = expt[u0 & 63u], T1 = expt[u1 & 63u];  // hi, lo of 2^(j/64)
+    const int j0 = static_cast<int>(u0 & 63u), j1 = static_cast<int>(u1 & 63u);
     const float2 kf = __fadd2_rn(big, P(-12582912.0f));
     const float2 z = __ffma2_rn(__ffma2_rn(kf, P(-0.015625f), th), P(kGammaLn2),
                                 __fmul2_rn(tl, P(kGammaLn2)));
     const float2 q = __ffma2_rn(__ffma2_rn(z, P(kGammaSixth), P(0.5f)), __fmul2_rn(z, z), z);
-    const float2 tj = make_float2(T0.x, T1.x);
-    const float2 tjl = make_float2(T0.y, T1.y);
+    const float2 tj = make_float2(pt[PowTable::kExpHi + j0], pt[PowTable::kExpHi + j1]);
+    const float2 tjl = make_float2(pt[PowTable::kExpLo + j0], pt[PowTable::kExpLo + j1]);
     const float2 r = __fadd2_rn(tj, __ffma2_rn(tj, q, tjl));
     // 2^(k >> 6) = bits ((k >> 6) + 127) << 23, with k + 127 * 64 = u -
     // 0x4b3fe040 in [448, 12224] over the fast range (t in [-120, 64)).
@@ -523,7 +526,7 @@ __device__ __forceinline__ void ChromaFixed(const float* stage, int bxs, int bys
 // with the format's branches resolved and the chroma taps read from the
 // staged window at the host's per-parity slots and weights.
 __device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* stage,
-                                               const float4* logt, const float2* expt,
+                                               const float* pow_table,
                                                uint32_t gx, uint32_t gy, uint32_t bx,
                                                uint32_t by, bool aligned4, float rgb[4][3]) {
     const uint32_t x0 = 2 * bx, y0 = 2 * by;
@@ -630,7 +633,7 @@ __device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* 
             const float2 v = q[h][c];
             const bool ia = v.x >= ss2dm::kGammaMinX, ib = v.y >= ss2dm::kGammaMinX;
             const float2 r =
-                PowfGamma2(make_float2(ia ? v.x : 1.0f, ib ? v.y : 1.0f), g, logt, expt);
+                PowfGamma2(make_float2(ia ? v.x : 1.0f, ib ? v.y : 1.0f), g, pow_table);
             q[h][c] = make_float2(ia ? r.x : 0.0f, ib ? r.y : 0.0f);
         }
 #pragma unroll

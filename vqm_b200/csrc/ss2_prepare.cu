@@ -285,8 +285,7 @@ __global__ void __launch_bounds__(kThreads, kGroup == 0   ? 5
     // Both chroma planes' window of the tile, for yuv_fast images, and the
     // power's tables.
     __shared__ float chroma_stage[kYuv ? 2 * kChromaStage : 1];
-    __shared__ float4 pow_log[kYuv ? 128 : 1];
-    __shared__ float2 pow_exp[kYuv ? 64 : 1];
+    __shared__ float pow_table[kYuv ? PowTable::kFloats : 1];
 
     const uint32_t tid = threadIdx.x;
     const uint32_t n_items = batch.prep_items[kGroup];
@@ -309,8 +308,17 @@ __global__ void __launch_bounds__(kThreads, kGroup == 0   ? 5
         constexpr uint32_t words = offsetof(DevSource, srgb_lut) / 4;
         for (uint32_t i = tid; i < words; i += kThreads) to[i] = from[i];
         if (kTable) lut[tid] = P.src[image].srgb_lut[tid];
-        if (kYuv && tid < 128) pow_log[tid] = __ldg(&ss2dm::kLogF4Dev[tid]);
-        if (kYuv && tid < 64) pow_exp[tid] = __ldg(&ss2dm::kExpF2Dev[tid]);
+        if (kYuv && tid < 128) {
+            const float4 l = __ldg(&ss2dm::kLogF4Dev[tid]);  // inv, hi, lo, 0
+            pow_table[PowTable::kInv + tid] = l.x;
+            pow_table[PowTable::kHi + tid] = l.y;
+            pow_table[PowTable::kLo + tid] = l.z;
+        }
+        if (kYuv && tid < 64) {
+            const float2 e = __ldg(&ss2dm::kExpF2Dev[tid]);  // hi, lo
+            pow_table[PowTable::kExpHi + tid] = e.x;
+            pow_table[PowTable::kExpLo + tid] = e.y;
+        }
         if (tid < kMaxLevels * 3) {
             const uint32_t l = tid / 3, c = tid % 3;
             const bool kept = l < P.levels && (P.mask[l] & (1u << c));
@@ -402,7 +410,7 @@ __global__ void __launch_bounds__(kThreads, kGroup == 0   ? 5
                     TableBlock(s, lut, fast, w4, hx, bx, by, lin);
                 } else if constexpr (kYuv) {
                     // Even width and height (PrepGroup): the block is whole.
-                    BlockLinearYuv(s, chroma_stage, pow_log, pow_exp, gx, gy, bx, by,
+                    BlockLinearYuv(s, chroma_stage, pow_table, gx, gy, bx, by,
                                    aligned4 != 0, lin);
                 } else {
                     BlockLinearGeneric(s, bx, by, lin);
