@@ -501,29 +501,36 @@ __device__ __noinline__ double ScoreFromNorms(const double* norms, int scales) {
 // The pair's 108 norms from its segments' FP64 sums (vulkan.cc:545-583:
 // mean = sum / (W_l H_l), 4-norm = sqrt(sqrt(sum4 / (W_l H_l)))), written
 // straight into its result block (zeros for pruned channels and levels past
-// its scales), then its score and scale count. One thread; out of line, as
-// it runs once per pair and should cost the blur loops no registers.
+// its scales), then its score and scale count. Every thread of the CTA that
+// completes the pair takes one norm (a division and two square roots in
+// FP64: one thread doing all of them in turn was most of a small launch's
+// time), then thread 0 the score. Out of line, as it runs once per pair and
+// should cost the blur loops no registers.
+template <int NT>
 __device__ __noinline__ void WritePairResult(const DevBatch& batch, const DevPair& P) {
+    const uint32_t tid = threadIdx.x;
     double* out = P.result;
-    for (int i = 0; i < 108; ++i) out[i] = 0.0;
-    for (uint32_t k = 0; k < P.seg_count; ++k) {
+    for (uint32_t i = tid; i < 108; i += NT) out[i] = 0.0;
+    __syncthreads();
+    for (uint32_t t = tid; t < 6 * P.seg_count; t += NT) {
+        const uint32_t k = t / 6, f = t - 6 * k;  // segment, norm
         const uint32_t sk = P.seg_first + k;
         const DevSegment g = batch.seg[sk];
         const double inv = 1.0 / (static_cast<double>(P.w[g.level]) *
                                   static_cast<double>(P.h[g.level]));
-        const double* v = batch.seg_sums + static_cast<size_t>(sk) * 6;
-        double* o = out + g.level * 18;
-        const int c = static_cast<int>(g.channel);
-        o[c * 2 + 0] = inv * __ldcg(v + 0);
-        o[c * 2 + 1] = sqrt(sqrt(inv * __ldcg(v + 1)));
-        o[6 + c * 4 + 0] = inv * __ldcg(v + 2);
-        o[6 + c * 4 + 1] = sqrt(sqrt(inv * __ldcg(v + 3)));
-        o[6 + c * 4 + 2] = inv * __ldcg(v + 4);
-        o[6 + c * 4 + 3] = sqrt(sqrt(inv * __ldcg(v + 5)));
+        const double v = inv * __ldcg(batch.seg_sums + static_cast<size_t>(sk) * 6 + f);
+        // f: SSIM' mean and 4-norm, ringing mean and 4-norm, blurring mean
+        // and 4-norm.
+        const uint32_t c = g.channel;
+        const uint32_t at = f < 2 ? c * 2 + f : 6 + c * 4 + (f - 2);
+        out[g.level * 18 + at] = (f & 1u) ? sqrt(sqrt(v)) : v;
     }
-    out[kResultScore] = ScoreFromNorms(out, static_cast<int>(P.levels));
-    out[kResultScales] = static_cast<double>(P.levels);
-    out[kResultStatus] = 0.0;
+    __syncthreads();
+    if (tid == 0) {
+        out[kResultScore] = ScoreFromNorms(out, static_cast<int>(P.levels));
+        out[kResultScales] = static_cast<double>(P.levels);
+        out[kResultStatus] = 0.0;
+    }
 }
 
 // Called by every thread of a blur CTA once its partial of segment `si` is
@@ -571,10 +578,8 @@ __device__ __forceinline__ void SumSegment(const DevBatch& batch, uint32_t si, d
     __syncthreads();
     if (!flag[1]) return;
     __threadfence();
-    if (tid == 0) {
-        WritePairResult(batch, P);
-        batch.pair_done[seg.pair] = 0u;
-    }
+    WritePairResult<NT>(batch, P);
+    if (tid == 0) batch.pair_done[seg.pair] = 0u;
 }
 
 template <int NT>
