@@ -473,21 +473,9 @@ __device__ __forceinline__ void ReducePartials(const float2 (&sum)[6], Scratch r
     __syncthreads();
 }
 
-// score.cc:118-163 in FP64 on the device.
-__device__ __noinline__ double ScoreFromNorms(const double* norms, int scales) {
-    double error = 0.0;
-    for (int c = 0; c < 3; ++c)
-        for (int s = 0; s < scales; ++s) {
-            const double* wt = c_weights[c * scales + s];
-            const double* ssim = norms + s * 18;
-            const double* edge = norms + s * 18 + 6;
-            error += wt[0] * fabs(ssim[c * 2 + 0]);
-            error += wt[1] * fabs(edge[c * 4 + 0]);
-            error += wt[2] * fabs(edge[c * 4 + 2]);
-            error += wt[3] * fabs(ssim[c * 2 + 1]);
-            error += wt[4] * fabs(edge[c * 4 + 1]);
-            error += wt[5] * fabs(edge[c * 4 + 3]);
-        }
+// score.cc:118-163 in FP64 on the device, from the weighted sum of the
+// norms' magnitudes (`error`, the sum of w * |norm| over the 108 features).
+__device__ __noinline__ double ScoreFromError(double error) {
     if (!isfinite(error)) return nan("");
     const double scaled = error * 0.9562382616834844;
     const double mapped = 2.326765642916932 * scaled -
@@ -504,14 +492,22 @@ __device__ __noinline__ double ScoreFromNorms(const double* norms, int scales) {
 // its scales), then its score and scale count. Every thread of the CTA that
 // completes the pair takes one norm (a division and two square roots in
 // FP64: one thread doing all of them in turn was most of a small launch's
-// time), then thread 0 the score. Out of line, as it runs once per pair and
-// should cost the blur loops no registers.
+// time) and its weighted magnitude; the weighted sum is a fixed butterfly in
+// each warp and the warps in turn (score.cc's sum in another order: equal to
+// ~1e-15, and the same on every run), and thread 0 maps it to the score.
+// `red` is shared scratch for NT / 32 doubles. Out of line, as it runs once
+// per pair and should cost the blur loops no registers.
 template <int NT>
-__device__ __noinline__ void WritePairResult(const DevBatch& batch, const DevPair& P) {
+__device__ __noinline__ void WritePairResult(const DevBatch& batch, const DevPair& P,
+                                             double* red) {
+    // score.cc's weight slot of each norm f (SSIM' mean and 4-norm, ringing
+    // mean and 4-norm, blurring mean and 4-norm).
+    constexpr uint32_t kWeightSlot = 0x524130u;  // 4 bits per f: 0, 3, 1, 4, 2, 5
     const uint32_t tid = threadIdx.x;
     double* out = P.result;
     for (uint32_t i = tid; i < 108; i += NT) out[i] = 0.0;
     __syncthreads();
+    double term = 0.0;
     for (uint32_t t = tid; t < 6 * P.seg_count; t += NT) {
         const uint32_t k = t / 6, f = t - 6 * k;  // segment, norm
         const uint32_t sk = P.seg_first + k;
@@ -519,15 +515,21 @@ __device__ __noinline__ void WritePairResult(const DevBatch& batch, const DevPai
         const double inv = 1.0 / (static_cast<double>(P.w[g.level]) *
                                   static_cast<double>(P.h[g.level]));
         const double v = inv * __ldcg(batch.seg_sums + static_cast<size_t>(sk) * 6 + f);
-        // f: SSIM' mean and 4-norm, ringing mean and 4-norm, blurring mean
-        // and 4-norm.
         const uint32_t c = g.channel;
         const uint32_t at = f < 2 ? c * 2 + f : 6 + c * 4 + (f - 2);
-        out[g.level * 18 + at] = (f & 1u) ? sqrt(sqrt(v)) : v;
+        const double norm = (f & 1u) ? sqrt(sqrt(v)) : v;
+        out[g.level * 18 + at] = norm;
+        const uint32_t slot = (kWeightSlot >> (4 * f)) & 15u;
+        term += c_weights[c * P.levels + g.level][slot] * fabs(norm);
     }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) term += __shfl_xor_sync(0xffffffffu, term, off);
+    if (tid % 32 == 0) red[tid / 32] = term;
     __syncthreads();
     if (tid == 0) {
-        out[kResultScore] = ScoreFromNorms(out, static_cast<int>(P.levels));
+        double error = 0.0;
+        for (int w = 0; w < NT / 32; ++w) error += red[w];
+        out[kResultScore] = ScoreFromError(error);
         out[kResultScales] = static_cast<double>(P.levels);
         out[kResultStatus] = 0.0;
     }
@@ -540,7 +542,7 @@ __device__ __noinline__ void WritePairResult(const DevBatch& batch, const DevPai
 // result repeats bit for bit; the CTA whose segment completes the pair
 // writes the pair's result. Each counter is reset by the CTA that finds it
 // complete, so the next launch starts from zero. `scratch` is shared memory
-// for 6 * NT / 32 + 2 doubles that no thread still reads.
+// for 7 * NT / 32 + 2 doubles that no thread still reads.
 // The CTA that completed segment `si`: its FP64 sum, then the pair's result
 // if the segment completes the pair.
 template <int NT>
@@ -578,7 +580,7 @@ __device__ __forceinline__ void SumSegment(const DevBatch& batch, uint32_t si, d
     __syncthreads();
     if (!flag[1]) return;
     __threadfence();
-    WritePairResult<NT>(batch, P);
+    WritePairResult<NT>(batch, P, scratch + 6 * (NT / 32) + 2);
     if (tid == 0) batch.pair_done[seg.pair] = 0u;
 }
 
