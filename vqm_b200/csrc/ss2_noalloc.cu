@@ -7,7 +7,8 @@
 // real-time loops where cudaMalloc/cudaFree would synchronize the device and
 // stall unrelated streams, and plug-in hosts that give a plug-in a stream and
 // buffers but no allocation rights. vqm_cu_ss2_compute_noalloc serves them:
-// it runs the same prepare, blur and finalize kernels on the caller's stream,
+// it runs the same prepare and blur kernels (the finalize is the blur's
+// epilogue) on the caller's stream,
 // with every piece of scratch (tables, counters, tile partials, segment sums
 // and the XYB pyramid) placed in one file-scope __device__ array of fixed size
 // that the CUDA module reserves when the library is loaded. The caller passes

@@ -10,7 +10,7 @@
 // not fit, idle workers' memory is freed (vqm_cu_ss2_batch_trim); if it still
 // does not fit, it waits for running batches to finish. The batch scorer
 // copies host inputs (waiting for the copies, so the dispatcher is the only
-// thread feeding PCIe) and launches its three kernels. The completion thread finishes batches in the
+// thread feeding PCIe) and launches its two kernels. The completion thread finishes batches in the
 // order they were submitted (blocking on each batch's completion event),
 // publishes the results and returns the worker. So requests that arrive while
 // batches run are admitted as soon as a worker frees, and up to `workers`
