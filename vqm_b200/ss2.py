@@ -353,6 +353,12 @@ class Image:
         return c
 
 
+def _c_bytes(image) -> bytes:
+    """The vqm_cu_image bytes of any image kind."""
+    f = getattr(image, "_c_bytes", None)
+    return f() if f is not None else bytes(image._c())
+
+
 @dataclass
 class DeviceImage:
     """A caller-owned device buffer (the CUDA counterpart of VulkanBufferView):
@@ -373,12 +379,24 @@ class DeviceImage:
                 planes[p] = base_ptr + geo[0]
         return DeviceImage(width, height, fmt, planes, (0, 0, 0, 0), owner)
 
+    def _c_bytes(self) -> bytes:
+        # The struct's bytes are kept with the fields they came from, so a
+        # buffer scored call after call is converted once (the conversion
+        # was a sizeable part of a one-pair call's host time).
+        key = (self.width, self.height, bytes(self.format), tuple(self.planes),
+               tuple(self.strides))
+        cached = self.__dict__.get("_c_cache")
+        if cached is None or cached[0] != key:
+            c = _CImage(self.width, self.height, self.format, 1)
+            for p in range(4):
+                c.planes[p] = int(self.planes[p]) if self.planes[p] else None
+                c.strides[p] = int(self.strides[p])
+            cached = (key, bytes(c))
+            self.__dict__["_c_cache"] = cached
+        return cached[1]
+
     def _c(self) -> _CImage:
-        c = _CImage(self.width, self.height, self.format, 1)
-        for p in range(4):
-            c.planes[p] = int(self.planes[p]) if self.planes[p] else None
-            c.strides[p] = int(self.strides[p])
-        return c
+        return _CImage.from_buffer_copy(self._c_bytes())
 
 
 @dataclass
@@ -736,8 +754,8 @@ class Ssimulacra2Batch:
     @staticmethod
     def _arrays(pairs):
         n = len(pairs)
-        origs = (_CImage * n)(*[p[0]._c() for p in pairs])
-        dists = (_CImage * n)(*[p[1]._c() for p in pairs])
+        origs = (_CImage * n).from_buffer_copy(b"".join(_c_bytes(p[0]) for p in pairs))
+        dists = (_CImage * n).from_buffer_copy(b"".join(_c_bytes(p[1]) for p in pairs))
         return n, origs, dists
 
     def submit(self, pairs, background: float = 0.5, borrow: bool = False) -> int:
