@@ -663,6 +663,9 @@ __global__ void __launch_bounds__(NT, MB) Ss2BlurPersistentKernel(DevBatch batch
         CpAsyncWait<1>();  // everything but the newest group: this tile's
         __syncthreads();
         ComputeTile<TW, TH, NT>(now, hq, cur, batch);
+        // The segment and pair epilogues use this buffer as scratch; the
+        // next iteration copies a window into it.
+        __syncthreads();
         cur = nxt;
         b ^= 1;
     }
