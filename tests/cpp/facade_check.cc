@@ -109,6 +109,12 @@ void Host() {
     v::MetricsConfig none;
     none.size = {32, 32};
     ExpectThrow<std::invalid_argument>([&] { v::Metrics m(none); }, "no metric selected");
+
+    v::Ssimulacra2Config unknown;
+    unknown.size = {32, 32};
+    unknown.blur = static_cast<v::Ssimulacra2Blur>(7);
+    ExpectThrow<std::invalid_argument>([&] { v::Ssimulacra2Pipeline p(unknown); },
+                                       "unknown blur mode");
 }
 
 void GpuMetrics() {
@@ -167,6 +173,18 @@ void Gpu() {
     const std::vector<v::ImagePair> pairs{{base, base}, {base, d1}, {base, d2}};
     const auto results = pool.ComputeMany(std::span<const v::ImagePair>(pairs));
     for (std::size_t i = 0; i < results.size(); ++i) Print("pool", static_cast<int>(i), results[i]);
+
+    // The opt-in recursive blur, through the pipeline and the pool.
+    v::Ssimulacra2Config rec = config;
+    rec.blur = v::Ssimulacra2Blur::Recursive;
+    v::Ssimulacra2Pipeline rpipe(rec);
+    for (int variant = 1; variant < 3; ++variant)
+        Print("recursive", variant, rpipe.Compute(base, Gradient(variant)));
+    v::Ssimulacra2Pool rpool(rec, 1, 2);
+    const std::vector<v::ImagePair> rpairs{{base, d1}, {base, d2}};
+    const auto rres = rpool.ComputeMany(std::span<const v::ImagePair>(rpairs));
+    for (std::size_t i = 0; i < rres.size(); ++i)
+        Print("recursive_pool", static_cast<int>(i) + 1, rres[i]);
 }
 
 }  // namespace

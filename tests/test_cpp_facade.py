@@ -46,22 +46,27 @@ def test_facade_scores_match_oracle(facade_binary):
     assert r.returncode == 0, r.stderr
     results = [json.loads(line) for line in r.stdout.splitlines() if line.startswith("{")]
     assert [x["path"] for x in results] == (["pipeline"] * 3 + ["uploaded"] + ["pool"] * 3 +
+                                            ["recursive"] * 2 + ["recursive_pool"] * 2 +
                                             ["metrics"] * 3 + ["metrics_image"])
     base = helpers.gradient(0)
-    expected = {}
+    expected, recursive = {}, {}
     for v in range(3):
         expected[v] = helpers.oracle_compute(base, helpers.gradient(v))
+        recursive[v] = helpers.oracle_compute(base, helpers.gradient(v), blur=1)
     # Pool pairs are (base, base), (base, 1), (base, 2).
     for x in results:
-        norms, score = expected[x["variant"]]
+        norms, score = (recursive if x["path"].startswith("recursive") else expected)[x["variant"]]
         if "norms" in x:
             got = np.asarray(x["norms"], dtype=np.float64).reshape(norms.shape)
             bad = helpers.feature_mismatch(got, norms)
             assert not bad, (x["path"], x["variant"], bad[:6])
         assert abs(x["score"] - score) <= helpers.SCORE_TOL, (x["path"], x["score"], score)
+    # The recursive blur moves the scores away from the sampled blur's.
+    for k in (1, 2):
+        assert abs(results[6 + k]["score"] - results[k]["score"]) > 1e-3
     # The unified facade returns the pipeline's score bit for bit.
     for k in range(3):
-        assert results[7 + k]["score"] == results[k]["score"]
-    assert results[10]["score"] == results[1]["score"]
+        assert results[11 + k]["score"] == results[k]["score"]
+    assert results[14]["score"] == results[1]["score"]
     assert results[0]["score"] == 100.0
     assert results[4]["score"] == 100.0
