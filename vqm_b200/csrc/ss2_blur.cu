@@ -36,8 +36,14 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <functional>
 #include <mutex>
+#include <queue>
+#include <unordered_map>
+#include <utility>
+#include <vector>
 
 #include "ss2_detmath.h"
 #include "ss2_device.cuh"
@@ -1028,25 +1034,89 @@ int BlurTileCount() { return kBlurVariantCount; }
 int BlurTileThreads(int index) { return kBlurVariants[index].threads; }
 int BlurTileStrip(int index) { return kBlurVariants[index].strip; }
 bool BlurTilePersistent(int index) { return kBlurVariants[index].persistent != 0; }
-int AutoBlurVariant(uint64_t tiles, int sms) {
-    // The longest 32x32 strip that still gives every CTA slot of the device
-    // 2 CTAs (fewer, and the last wave's idle slots cost more than the
-    // shared rows and the once-per-strip reduction save). Measured blur
-    // times for one pair: 1080p 65.5 us one tile per CTA, 62.0 with strips
-    // of 2 (taken); 4K 163.8 / 149.5 / 143.4 / 147.5 us with strips of
-    // 1 / 2 / 4 / 8 (8 taken); 720p 47.1 us for 1, 2 and 4 (1 taken); large
-    // batches take the longest strip, 16.
+namespace {
+
+// Estimated duration, in tile times, of one launch of strips of S tiles over
+// segments with these tile grids (columns, rows) on `slots` CTA slots. A CTA
+// costs its tiles plus kStripCost (its first tile's extra rows, the strip's
+// reduction and epilogue), fitted to measured one-pair blur times (720p,
+// 1080p, 1440p and 4K, strips of 1 to 16). The device hands CTAs in launch
+// order to the slot that frees first; up to kSimulatedWaves waves that is
+// simulated, beyond it the last wave's share is small and the estimate is
+// the work per slot plus half a CTA.
+constexpr double kStripCost = 0.7;
+constexpr uint64_t kSimulatedWaves = 8;
+
+double StripLaunchCost(const std::vector<std::pair<uint32_t, uint32_t>>& grids, uint32_t S,
+                       uint64_t slots) {
+    uint64_t ctas = 0, tiles = 0;
+    for (const auto& g : grids) {
+        ctas += static_cast<uint64_t>(g.first) * ((g.second + S - 1) / S);
+        tiles += static_cast<uint64_t>(g.first) * g.second;
+    }
+    if (ctas == 0) return 0.0;
+    const double work = static_cast<double>(tiles) + kStripCost * static_cast<double>(ctas);
+    if (ctas > kSimulatedWaves * slots)
+        return work / static_cast<double>(slots) + 0.5 * work / static_cast<double>(ctas);
+    // Launch order: segment by segment, strip rows of all columns in turn.
+    std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
+    for (uint64_t k = 0; k < std::min<uint64_t>(slots, ctas); ++k) free_at.push(0.0);
+    double end = 0.0;
+    for (const auto& g : grids)
+        for (uint32_t y0 = 0; y0 < g.second; y0 += S) {
+            const double d = static_cast<double>(std::min(S, g.second - y0)) + kStripCost;
+            for (uint32_t x = 0; x < g.first; ++x) {
+                const double t = free_at.top() + d;
+                free_at.pop();
+                free_at.push(t);
+                end = std::max(end, t);
+            }
+        }
+    return end;
+}
+
+}  // namespace
+
+int AutoBlurVariant(const std::vector<std::pair<uint32_t, uint32_t>>& grids, int sms) {
+    // The strip length of the default tile with the least estimated time
+    // (StripLaunchCost; on ties the longer strip, with fewer partials).
+    // Large batches take the longest strip, 16; one pair 720p 1 to 4 (equal
+    // times), 1080p 2, 1440p 4 and 4K 4 (4K: 122.9 -> 118.8 us against the
+    // earlier rule, the longest strip leaving every CTA slot 2 CTAs, which
+    // took 8). Memoised per grid list: a batch of the same sizes, or a
+    // pipeline, pays for the estimate once.
     const BlurVariant& base = kBlurVariants[kDefaultBlurVariant];
     const uint64_t slots = static_cast<uint64_t>(sms > 0 ? sms : 1) * base.per_sm;
-    int best = kDefaultBlurVariant, strip = 1;
+    uint64_t key = 1469598103934665603ull ^ static_cast<uint64_t>(sms);
+    for (const auto& g : grids) {
+        key = (key ^ g.first) * 1099511628211ull;
+        key = (key ^ g.second) * 1099511628211ull;
+    }
+    static std::mutex mu;
+    static std::unordered_map<uint64_t, int> memo;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        const auto it = memo.find(key);
+        if (it != memo.end()) return it->second;
+    }
+    int best = kDefaultBlurVariant;
+    double best_cost = StripLaunchCost(grids, 1, slots);
+    int best_strip = 1;
     for (int i = 0; i < kBlurVariantCount; ++i) {
         const BlurVariant& v = kBlurVariants[i];
-        if (v.persistent || v.w != base.w || v.h != base.h || v.threads != base.threads) continue;
-        if (v.strip > strip && tiles / static_cast<uint64_t>(v.strip) >= 2 * slots) {
+        if (v.persistent || v.w != base.w || v.h != base.h || v.threads != base.threads ||
+            v.strip <= 1)
+            continue;
+        const double c = StripLaunchCost(grids, static_cast<uint32_t>(v.strip), slots);
+        if (c < best_cost * (1.0 - 1e-9) || (c <= best_cost * (1.0 + 1e-9) && v.strip > best_strip)) {
             best = i;
-            strip = v.strip;
+            best_cost = c;
+            best_strip = v.strip;
         }
     }
+    std::lock_guard<std::mutex> lock(mu);
+    if (memo.size() >= 4096) memo.clear();
+    memo.emplace(key, best);
     return best;
 }
 

@@ -3,6 +3,10 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+#include <utility>
+#include <vector>
+
 #include "ss2_device.cuh"
 
 namespace vqm_b200 {
@@ -43,13 +47,12 @@ bool BlurTilePersistent(int index);
 // Blocks of variant `index` for a segment of tiles_x x tiles_y tiles: the
 // prefix sums of these are a batch's blur_start.
 uint32_t BlurBlocks(int index, uint32_t tiles_x, uint32_t tiles_y);
-// The variant used when a caller does not choose one, for a launch of
-// `tiles` output tiles of the default variant on a device with `sms` SMs:
-// the longest strip of its tile that leaves every CTA slot two CTAs (one
-// tile per CTA for small launches).
-// A strip regroups the compensated partial sums, so the choice moves a
-// result by rounding only (~1e-7 relative).
-int AutoBlurVariant(uint64_t tiles, int sms);
+// The variant used when a caller does not choose one, for a launch over
+// segments with these tile grids of the default tile (columns, rows, in
+// launch order) on a device with `sms` SMs: the strip length with the least
+// estimated time (ss2_blur.cu). A strip regroups the compensated partial
+// sums, so the choice moves a result by rounding only (~1e-7 relative).
+int AutoBlurVariant(const std::vector<std::pair<uint32_t, uint32_t>>& grids, int sms);
 // The one-tile-per-CTA variant with variant's tile shape (the variant
 // itself when it is one), which half planes run; -1 when there is none.
 int HalfPlaneVariant(int variant);

@@ -279,19 +279,21 @@ Tables BuildTables(const std::vector<std::pair<uint32_t, uint32_t>>& sizes, Blur
 }
 
 // Output tiles of the default blur variant over pairs of the given sizes.
-uint64_t DefaultTileCount(const std::vector<std::pair<uint32_t, uint32_t>>& sizes) {
+// The tile grids (columns, rows) of the default tile over every kept
+// (pair, level, channel), in the blur's launch order.
+std::vector<std::pair<uint32_t, uint32_t>> DefaultTileGrids(
+    const std::vector<std::pair<uint32_t, uint32_t>>& sizes) {
     int tw = 0, th = 0;
     BlurTileShape(kDefaultBlurVariant, &tw, &th);
-    uint64_t tiles = 0;
+    std::vector<std::pair<uint32_t, uint32_t>> grids;
     for (const auto& wh : sizes) {
         const ScalePlan plan = PlanScales(wh.first, wh.second);
         for (int l = 0; l < plan.count; ++l)
             for (int c = 0; c < 3; ++c)
                 if (plan.mask[l] & (1u << c))
-                    tiles += static_cast<uint64_t>((plan.w[l] + tw - 1) / tw) *
-                             ((plan.h[l] + th - 1) / th);
+                    grids.emplace_back((plan.w[l] + tw - 1) / tw, (plan.h[l] + th - 1) / th);
     }
-    return tiles;
+    return grids;
 }
 
 int DeviceSms(int device) {
@@ -596,7 +598,7 @@ public:
         VQM_CK(cudaEventCreateWithFlags(&copied_, cudaEventDisableTiming));
         if (!cfg.half_planes)
             shape_ = BlurShape::Of(
-                AutoBlurVariant(DefaultTileCount({{cfg.width, cfg.height}}), DeviceSms(device_)));
+                AutoBlurVariant(DefaultTileGrids({{cfg.width, cfg.height}}), DeviceSms(device_)));
         tables_ = BuildTables({{cfg.width, cfg.height}}, shape_);
         BuildPrepLists(tables_, {{0, 0}});
         mem_.Layout(tables_);
@@ -1210,7 +1212,7 @@ private:
         return host_bytes;
     }
     BlurShape ShapeFor(const std::vector<std::pair<uint32_t, uint32_t>>& sizes) const {
-        return auto_shape_ ? BlurShape::Of(AutoBlurVariant(DefaultTileCount(sizes), sms_))
+        return auto_shape_ ? BlurShape::Of(AutoBlurVariant(DefaultTileGrids(sizes), sms_))
                            : shape_;
     }
 
