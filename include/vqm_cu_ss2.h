@@ -107,7 +107,7 @@ typedef struct vqm_cu_memory_usage {
     uint64_t pyramid_bytes;  /* XYB planes */
     uint64_t resident_bytes; /* upload() slots */
     uint64_t input_bytes;    /* allocate_image() pool + streaming inputs */
-    uint64_t scratch_bytes;  /* partials, tables, results */
+    uint64_t scratch_bytes;  /* partials, tables, counters */
     uint64_t total_bytes;
 } vqm_cu_memory_usage;
 
@@ -366,7 +366,7 @@ int vqm_cu_ss2_batch_set_timing(vqm_cu_ss2_batch* batch, int enabled);
 int vqm_cu_ss2_batch_stage_ms(vqm_cu_ss2_batch* batch, float* stage_ms3);
 /* The batch's device memory, after PipelineMemoryUsage::total
  * (include/vqm_memory_types.h:24-33): *held = the bytes it holds now
- * (pyramid, tables, partials, results, its copy of host inputs), reused from
+ * (pyramid, tables, partials, counters, its copy of host inputs), reused from
  * submit to submit and never shrunk by a submit. batch_device_bytes_after
  * validates a submission as batch_submit would and gives what the batch
  * will hold once it is submitted (its buffers grown as the submit grows

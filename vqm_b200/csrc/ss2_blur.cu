@@ -496,10 +496,12 @@ __device__ __noinline__ double ScoreFromError(double error) {
 // mean = sum / (W_l H_l), 4-norm = sqrt(sqrt(sum4 / (W_l H_l)))), written
 // straight into its result block (zeros for pruned channels and levels past
 // its scales), then its score and scale count. Every thread of the CTA that
-// completes the pair takes one norm (a division and two square roots in
-// FP64: one thread doing all of them in turn was most of a small launch's
-// time) and its weighted magnitude; the weighted sum is a fixed butterfly in
-// each warp and the warps in turn (score.cc's sum in another order: equal to
+// completes the pair takes one of the 108 slots, each written once (the
+// result block can be host memory the device writes across the bus): the
+// norm of a kept (level, channel), a division and two square roots in FP64
+// (one thread doing all of them in turn was most of a small launch's time),
+// and its weighted magnitude; the weighted sum is a fixed butterfly in each
+// warp and the warps in turn (score.cc's sum in another order: equal to
 // ~1e-15, and the same on every run), and thread 0 maps it to the score.
 // `red` is shared scratch for NT / 32 doubles. Out of line, as it runs once
 // per pair and should cost the blur loops no registers.
@@ -511,22 +513,26 @@ __device__ __noinline__ void WritePairResult(const DevBatch& batch, const DevPai
     constexpr uint32_t kWeightSlot = 0x524130u;  // 4 bits per f: 0, 3, 1, 4, 2, 5
     const uint32_t tid = threadIdx.x;
     double* out = P.result;
-    for (uint32_t i = tid; i < 108; i += NT) out[i] = 0.0;
-    __syncthreads();
     double term = 0.0;
-    for (uint32_t t = tid; t < 6 * P.seg_count; t += NT) {
-        const uint32_t k = t / 6, f = t - 6 * k;  // segment, norm
-        const uint32_t sk = P.seg_first + k;
-        const DevSegment g = batch.seg[sk];
-        const double inv = 1.0 / (static_cast<double>(P.w[g.level]) *
-                                  static_cast<double>(P.h[g.level]));
-        const double v = inv * __ldcg(batch.seg_sums + static_cast<size_t>(sk) * 6 + f);
-        const uint32_t c = g.channel;
-        const uint32_t at = f < 2 ? c * 2 + f : 6 + c * 4 + (f - 2);
-        const double norm = (f & 1u) ? sqrt(sqrt(v)) : v;
-        out[g.level * 18 + at] = norm;
-        const uint32_t slot = (kWeightSlot >> (4 * f)) & 15u;
-        term += c_weights[c * P.levels + g.level][slot] * fabs(norm);
+    for (uint32_t i = tid; i < 108; i += NT) {
+        // Slot i: level l, then Ssimulacra2Scale's order (avg_ssim[c * 2 +
+        // n], then avg_edgediff[c * 4 + n]).
+        const uint32_t l = i / 18, at = i - 18 * l;
+        const uint32_t c = at < 6 ? at / 2 : (at - 6) / 4;
+        const uint32_t f = at < 6 ? at % 2 : 2 + (at - 6) % 4;  // the segment's sum
+        double norm = 0.0;
+        if (l < P.levels && ((P.mask[l] >> c) & 1u)) {
+            // Segments run level by level over the kept channels.
+            uint32_t k = __popc(P.mask[l] & ((1u << c) - 1u));
+            for (uint32_t m = 0; m < l; ++m) k += __popc(P.mask[m] & 7u);
+            const size_t sk = static_cast<size_t>(P.seg_first) + k;
+            const double inv =
+                1.0 / (static_cast<double>(P.w[l]) * static_cast<double>(P.h[l]));
+            const double v = inv * __ldcg(batch.seg_sums + sk * 6 + f);
+            norm = (f & 1u) ? sqrt(sqrt(v)) : v;
+            term += c_weights[c * P.levels + l][(kWeightSlot >> (4 * f)) & 15u] * fabs(norm);
+        }
+        out[i] = norm;
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) term += __shfl_xor_sync(0xffffffffu, term, off);

@@ -335,9 +335,10 @@ void BuildPrepLists(Tables& t, const PrepGroups& group, bool skip_original = fal
 }
 
 // The device tables of one batch: one table allocation, its pinned mirror,
-// the pyramid, partials, segment sums, per-pair counters and results.
+// the pyramid, partials, segment sums and per-pair counters, and the pinned
+// host blocks the results land in.
 struct BatchMemory {
-    DeviceBuffer table, pyramid, partials, seg_sums, pair_done, results;
+    DeviceBuffer table, pyramid, partials, seg_sums, pair_done;
     PinnedBuffer table_host, results_host;
     // Table layout: [pairs | prep items | prep starts | segments | blur
     // starts]. Everything a call can change (pair records, which images take
@@ -355,8 +356,8 @@ struct BatchMemory {
     }
 
     // Device bytes each buffer needs for `t`, in the order table, pyramid,
-    // partials, segment sums, pair counters, results (and the table offsets).
-    std::array<size_t, 6> Needs(const Tables& t) {
+    // partials, segment sums, pair counters (and the table offsets).
+    std::array<size_t, 5> Needs(const Tables& t) {
         off_pairs = 0;
         off_items = AlignUp(off_pairs + sizeof(DevPair) * t.pairs.size(), 16);
         off_prep = AlignUp(off_items + sizeof(DevPrepItem) * t.prep_items.size(), 16);
@@ -367,11 +368,10 @@ struct BatchMemory {
         return {table_bytes, std::max<size_t>(t.pyramid_floats, 64) * elem_bytes,
                 std::max<size_t>(t.partials, 1) * 6 * sizeof(double),
                 std::max<size_t>(t.segs.size(), 1) * 6 * sizeof(double),
-                (t.pairs.size() + t.segs.size() + 2) * sizeof(uint32_t),
-                std::max<size_t>(t.pairs.size(), 1) * kResultDoubles * sizeof(double)};
+                (t.pairs.size() + t.segs.size() + 2) * sizeof(uint32_t)};
     }
-    std::array<DeviceBuffer*, 6> Buffers() {
-        return {&table, &pyramid, &partials, &seg_sums, &pair_done, &results};
+    std::array<DeviceBuffer*, 5> Buffers() {
+        return {&table, &pyramid, &partials, &seg_sums, &pair_done};
     }
     // Device bytes held now.
     size_t DeviceBytes() {
@@ -386,7 +386,7 @@ struct BatchMemory {
     // Sizes and uploads-to-be for `t`; returns true if any address moved.
     bool Layout(const Tables& t) {
         bool moved = false;
-        const std::array<size_t, 6> need = Needs(t);
+        const std::array<size_t, 5> need = Needs(t);
         moved |= table.ensure(need[0]);
         moved |= table_host.ensure(table_bytes);
         moved |= pyramid.ensure(need[1]);
@@ -396,7 +396,6 @@ struct BatchMemory {
             moved = true;
             VQM_CK(cudaMemset(pair_done.as<void>(), 0, pair_done.bytes()));
         }
-        moved |= results.ensure(need[5]);
         moved |= results_host.ensure(std::max<size_t>(t.pairs.size(), 1) * kResultDoubles * sizeof(double));
         pair_count = static_cast<uint32_t>(t.pairs.size());
         uint8_t* base = table.as<uint8_t>();
@@ -423,7 +422,10 @@ struct BatchMemory {
         for (size_t i = 0; i < t.pairs.size(); ++i) {
             t.pairs[i].pyramid =
                 reinterpret_cast<float*>(pyramid.as<uint8_t>() + t.pyramid_first[i] * elem_bytes);
-            t.pairs[i].result = results.as<double>() + i * kResultDoubles;
+            // Pinned host memory, which the device reaches at the same
+            // address: the blur's epilogue writes each result across the
+            // bus once, and no copy follows the kernels.
+            t.pairs[i].result = results_host.as<double>() + i * kResultDoubles;
         }
         uint8_t* h = table_host.as<uint8_t>();
         std::memcpy(h + off_pairs, t.pairs.data(), sizeof(DevPair) * t.pairs.size());
@@ -460,11 +462,6 @@ struct BatchMemory {
         VQM_CK(LaunchBlur(dev, shape.variant, s));
         if (ev) VQM_CK(cudaEventRecord(ev[2], s));
         if (ev) VQM_CK(cudaEventRecord(ev[3], s));
-    }
-    void EnqueueReadback(cudaStream_t s) {
-        VQM_CK(cudaMemcpyAsync(results_host.as<void>(), results.as<void>(),
-                               sizeof(double) * kResultDoubles * pair_count,
-                               cudaMemcpyDeviceToHost, s));
     }
 };
 
@@ -902,7 +899,7 @@ public:
         for (const auto& s : slots_) u->resident_bytes += s.memory.bytes();
         u->input_bytes = pool_.bytes() + stream_in_[0].bytes() + stream_in_[1].bytes();
         u->scratch_bytes = mem_.table.bytes() + mem_.partials.bytes() + mem_.seg_sums.bytes() +
-                           mem_.pair_done.bytes() + mem_.results.bytes();
+                           mem_.pair_done.bytes();
         u->total_bytes = u->pyramid_bytes + u->resident_bytes + u->input_bytes + u->scratch_bytes;
     }
 
@@ -973,7 +970,6 @@ private:
                 try {
                     mem_.EnqueueUpload(upload, stream_);
                     mem_.EnqueueKernels(shape_, stream_);
-                    mem_.EnqueueReadback(stream_);
                 } catch (...) {
                     cudaStreamEndCapture(stream_, &graph);
                     if (graph) cudaGraphDestroy(graph);
@@ -988,7 +984,6 @@ private:
         } else {
             mem_.EnqueueUpload(upload, stream_);
             mem_.EnqueueKernels(shape_, stream_);
-            mem_.EnqueueReadback(stream_);
         }
         VQM_CK(cudaEventRecord(done_, stream_));
         token_ = NextIncarnation();
@@ -1064,14 +1059,13 @@ public:
         VQM_CK(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming));
         VQM_CK(cudaEventCreateWithFlags(&copied_, cudaEventDisableTiming));
         VQM_CK(cudaEventCreateWithFlags(&uploaded_, cudaEventDisableTiming));
-        VQM_CK(cudaEventCreateWithFlags(&kernels_done_, cudaEventDisableTiming));
         for (auto& e : stage_ev_) VQM_CK(cudaEventCreate(&e));
     }
     ~Batch() {
         cudaSetDevice(device_);
         if (stream_) cudaStreamSynchronize(stream_);
         if (copy_stream_) cudaStreamSynchronize(copy_stream_);
-        for (cudaEvent_t e : {done_, copied_, uploaded_, kernels_done_})
+        for (cudaEvent_t e : {done_, copied_, uploaded_})
             if (e) cudaEventDestroy(e);
         for (auto& e : stage_ev_)
             if (e) cudaEventDestroy(e);
@@ -1083,7 +1077,7 @@ public:
         stream_ = s ? static_cast<cudaStream_t>(s) : own_stream_;
     }
 
-    // Device bytes the batch holds now (pyramid, tables, partials, results
+    // Device bytes the batch holds now (pyramid, tables, partials, counters
     // and its copy of host inputs), reused from submit to submit.
     size_t DeviceBytes() { return mem_.DeviceBytes() + inputs_.bytes(); }
 
@@ -1096,10 +1090,10 @@ public:
         Tables t = BuildTables(sizes, ShapeFor(sizes));
         BatchMemory probe;  // offsets only; the sizes come from mem_
         probe.elem_bytes = mem_.elem_bytes;
-        const std::array<size_t, 6> need = probe.Needs(t);
-        const std::array<DeviceBuffer*, 6> buf = mem_.Buffers();
+        const std::array<size_t, 5> need = probe.Needs(t);
+        const std::array<DeviceBuffer*, 5> buf = mem_.Buffers();
         size_t bytes = inputs_.grown(std::max<size_t>(host_bytes, 256));
-        for (int i = 0; i < 6; ++i) bytes += buf[i]->grown(need[i]);
+        for (int i = 0; i < 5; ++i) bytes += buf[i]->grown(need[i]);
         return bytes;
     }
 
@@ -1160,8 +1154,8 @@ public:
         // The tables and counters go up on the batch's copy stream: they
         // depend on nothing on the launch stream (this batch's previous
         // submission has finished), so they overlap whatever runs there,
-        // typically another batch's kernels. The results come back on it
-        // too, so the launch stream goes straight on to its next kernels.
+        // typically another batch's kernels. The results need no copy: the
+        // blur writes them into pinned host memory.
         VQM_CK(cudaMemsetAsync(mem_.pair_done.as<void>(), 0,
                                sizeof(uint32_t) * (n + t.segs.size() + 2), copy_stream_));
         mem_.EnqueueUpload(mem_.table_bytes, copy_stream_);
@@ -1169,10 +1163,7 @@ public:
         VQM_CK(cudaStreamWaitEvent(stream_, uploaded_, 0));
         mem_.EnqueueKernels(shape, stream_, timing_ ? stage_ev_ : nullptr);
         timed_ = timing_;
-        VQM_CK(cudaEventRecord(kernels_done_, stream_));
-        VQM_CK(cudaStreamWaitEvent(copy_stream_, kernels_done_, 0));
-        mem_.EnqueueReadback(copy_stream_);
-        VQM_CK(cudaEventRecord(done_, copy_stream_));
+        VQM_CK(cudaEventRecord(done_, stream_));
         count_ = n;
         token_ = NextIncarnation();
         in_flight_ = true;
@@ -1248,9 +1239,9 @@ private:
     int sms_ = 0;
     int device_ = 0;
     cudaStream_t own_stream_ = nullptr, stream_ = nullptr;
-    cudaStream_t copy_stream_ = nullptr;  // tables up, results down
+    cudaStream_t copy_stream_ = nullptr;  // tables and counter resets
     cudaEvent_t done_ = nullptr, copied_ = nullptr;
-    cudaEvent_t uploaded_ = nullptr, kernels_done_ = nullptr;
+    cudaEvent_t uploaded_ = nullptr;
     cudaEvent_t stage_ev_[4] = {nullptr, nullptr, nullptr, nullptr};
     bool timing_ = false, timed_ = false;
     BatchMemory mem_;
