@@ -326,6 +326,22 @@ def test_batch_matches_pipeline():
     assert np.array_equal(b.compute_many(pairs[:2])[1].norms, again[1].norms)
 
 
+def test_table_prepare_of_large_launches_is_bit_exact():
+    """Large launches of the 8-bit table decode run 128-thread CTAs, small
+    ones 256-thread CTAs; both write the same planes, so with the same blur
+    kernel a pair scores bit for bit the same alone and in a batch of
+    three 1080p pairs (3,060 tiles of 64x64, the 128-thread form on any
+    device of up to 306 SMs)."""
+    pairs = [synthetic.rgb_pair(1920, 1080, 60 + i)[:2] for i in range(3)]
+    b = ss2.Ssimulacra2Batch(variant=0)
+    together = b.compute_many(pairs)
+    for (o, d), r in zip(pairs, together):
+        alone = b.compute_many([(o, d)])[0]
+        assert np.array_equal(alone.norms, r.norms) and alone.device_score == r.device_score
+        check_parity(r, o, d, label="1080p in a batch of three")
+    b.close()
+
+
 @pytest.mark.parametrize("variant", range(len(ss2.blur_variants())))
 def test_every_blur_variant(variant):
     """Every compiled blur kernel gives the oracle's features; they differ

@@ -2,13 +2,13 @@
 // 2x2-box pyramid of one image's 64x64 base tile, per CTA
 // (reference: src/metrics/ssimulacra2/shaders/prepare.comp).
 //
-// A CTA is 256 threads over the tile's 32x32 base 2x2 blocks: thread
-// (tx, ty) = (t & 15, t >> 4) owns blocks (2tx + hx, ty + 16vy), hx, vy in
-// {0, 1}, i.e. four base pixels in a row of two rows, twice. Levels 0 and 1
-// come from the thread's own samples; level 1 goes through a shared-memory
-// ladder from which levels 2.. are averaged, each level with a barrier among
-// the threads it still needs. Because the 2x2 box nests exactly, no CTA ever
-// needs a neighbour's samples.
+// A CTA is NT threads (128 or 256) over the tile's 32x32 base 2x2 blocks:
+// thread (tx, ty) = (t & 15, t >> 4) owns blocks (2tx + hx, ty + (NT / 16) vy),
+// hx in {0, 1}, vy < 32 / (NT / 16), i.e. four base pixels in a row of two
+// rows, two or four times. Levels 0 and 1 come from the thread's own samples;
+// level 1 goes through a shared-memory ladder from which levels 2.. are
+// averaged, each level with a barrier among the threads it still needs.
+// Because the 2x2 box nests exactly, no CTA ever needs a neighbour's samples.
 //
 // Two kernels: 8-bit grey/RGB without alpha decode through the image's
 // 256-entry table in shared memory, reading four samples of a row with one
@@ -27,6 +27,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <mutex>
 #include <type_traits>
 
 #include "ss2_decode.cuh"
@@ -38,8 +39,12 @@
 namespace vqm_b200 {
 namespace {
 
-constexpr int kThreads = 256;
 constexpr uint32_t kBlocks = kPrepTile / 2;  // base 2x2 blocks per tile side
+
+// CTAs per SM of a prepare kernel with NT threads (ten of 128, for the
+// table decode of large launches; otherwise five or four of 256, see
+// PrepareKernel).
+constexpr int kTableCtas128 = 10;
 
 // The last prefix entry <= index (start[0] == 0 <= index < start[count]).
 __device__ __forceinline__ uint32_t FindSlot(const uint32_t* __restrict__ start, uint32_t count,
@@ -254,8 +259,9 @@ __device__ __forceinline__ void TableBlock(const DevSource& s, const float* lut,
     }
 }
 
-// CTAs per SM: five (40 warps) for the table and YUV decodes, four for the
-// generic one. The decodes' long dependency chains (the YUV power's table
+// CTAs per SM: five of 256 threads (40 warps) for the table and YUV
+// decodes, four for the generic one; the table decode also runs as ten CTAs
+// of 128 threads (see LaunchPrepareOf). The decodes' long dependency chains (the YUV power's table
 // loads, the generic FP64 transfers) want the warps more than the registers
 // (measured on 136 uneven pairs: the YUV kernel at 5 CTAs with some spilling
 // took 8.48 ms, at 4 9.33 ms; the generic decode at 4 beats 2 by a
@@ -267,11 +273,15 @@ __device__ __forceinline__ void TableBlock(const DevSource& s, const float* lut,
 #ifndef VQM_YUV_PREPARE_CTAS
 #define VQM_YUV_PREPARE_CTAS 5
 #endif
-template <int kGroup, bool kHalf>
-__global__ void __launch_bounds__(kThreads, kGroup == 0   ? 5
-                                            : kGroup == 1 ? VQM_YUV_PREPARE_CTAS
-                                                          : VQM_GENERIC_PREPARE_CTAS)
+template <int kGroup, bool kHalf, int kNT>
+__global__ void __launch_bounds__(kNT, kNT == 128     ? kTableCtas128
+                                       : kGroup == 0 ? 5
+                                       : kGroup == 1 ? VQM_YUV_PREPARE_CTAS
+                                                     : VQM_GENERIC_PREPARE_CTAS)
     PrepareKernel(DevBatch batch) {
+    constexpr uint32_t kThreads = kNT;
+    constexpr uint32_t kRows = kThreads / 16;         // block rows per pass
+    constexpr uint32_t kRowPasses = kBlocks / kRows;  // 2 or 4
     constexpr bool kTable = kGroup == 0;  // 8-bit RGB/grey by table
     constexpr bool kYuv = kGroup == 1;    // yuv_fast images
     // Level-1 tile (32x32) of each channel, then the levels after it in two
@@ -307,7 +317,8 @@ __global__ void __launch_bounds__(kThreads, kGroup == 0   ? 5
         uint32_t* to = reinterpret_cast<uint32_t*>(&src_s);
         constexpr uint32_t words = offsetof(DevSource, srgb_lut) / 4;
         for (uint32_t i = tid; i < words; i += kThreads) to[i] = from[i];
-        if (kTable) lut[tid] = P.src[image].srgb_lut[tid];
+        if (kTable)
+            for (uint32_t i = tid; i < 256; i += kThreads) lut[i] = P.src[image].srgb_lut[i];
         if (kYuv && tid < 128) {
             const float4 l = __ldg(&ss2dm::kLogF4Dev[tid]);  // inv, hi, lo, 0
             pow_table[PowTable::kInv + tid] = l.x;
@@ -368,8 +379,8 @@ __global__ void __launch_bounds__(kThreads, kGroup == 0   ? 5
         if (lv.mask[l]) last = l;
 
 #pragma unroll 1
-    for (uint32_t vy = 0; vy < 2; ++vy) {
-        const uint32_t by = gy * kBlocks + ty + 16 * vy;
+    for (uint32_t vy = 0; vy < kRowPasses; ++vy) {
+        const uint32_t by = gy * kBlocks + ty + kRows * vy;
         const uint32_t bx0 = gx * kBlocks + 2 * tx;
         // Both blocks' samples of each plane as two 32-bit words when the
         // four columns and two rows are inside and aligned.
@@ -476,7 +487,7 @@ __global__ void __launch_bounds__(kThreads, kGroup == 0   ? 5
                 StorePixel<kHalf>(lv, 1, bx0 + 1, by, xyb[0].y, xyb[1].y, xyb[2].y);
             }
             if (last >= 2) {
-                const uint32_t at = (ty + 16 * vy) * kBlocks + 2 * tx;  // even
+                const uint32_t at = (ty + kRows * vy) * kBlocks + 2 * tx;  // even
 #pragma unroll
                 for (int c = 0; c < 3; ++c)
                     *reinterpret_cast<float2*>(&ladder_a[c][at]) = make_float2(l1[0][c], l1[1][c]);
@@ -486,47 +497,59 @@ __global__ void __launch_bounds__(kThreads, kGroup == 0   ? 5
     if (last < 2) return;
     __syncthreads();
 
-    // Levels 2..last: the first side^2 threads (256, 64, 16, 4) average the
-    // previous level's 2x2 blocks from the ladder (prepare.comp:149-168,
-    // clamped to the previous level's last column and row); threads that no
-    // longer take part leave, and the rest meet at a barrier of their own.
+    // Levels 2..last: the first min(side^2, NT) threads average the
+    // previous level's 2x2 blocks from the ladder (side^2 = 256, 64, 16, 4
+    // pixels; prepare.comp:149-168, clamped to the previous level's last
+    // column and row); threads that no longer take part leave, and the rest
+    // meet at a barrier of their own.
 #pragma unroll 1
     for (uint32_t level = 2; level <= last; ++level) {
         const uint32_t shift = 6 - level;             // side = 64 >> level
         const uint32_t side = 1u << shift;
         const uint32_t active = side * side;
-        if (tid >= active) return;
-        const uint32_t jx = tid & (side - 1);
-        const uint32_t jy = tid >> shift;
+        const uint32_t workers = active < kThreads ? active : kThreads;
+        if (tid >= workers) return;
         const uint32_t prev_side = side * 2;
         const uint32_t pw = lv.w[level - 1], ph = lv.h[level - 1];
         const uint32_t ox = min(gx * prev_side, pw - 1);
         const uint32_t oy = min(gy * prev_side, ph - 1);
         const uint32_t lx = pw - 1 - ox, ly = ph - 1 - oy;
-        const uint32_t cx0 = min(2 * jx, lx), cx1 = min(2 * jx + 1, lx);
-        const uint32_t cy0 = min(2 * jy, ly), cy1 = min(2 * jy + 1, ly);
         const float* prev0 = (level & 1u) ? &ladder_b[0][0] : &ladder_a[0][0];
         const uint32_t prev_stride = (level & 1u) ? kBlocks * kBlocks / 4 : kBlocks * kBlocks;
-        float v[3];
+        float* next0 = (level & 1u) ? &ladder_a[0][0] : &ladder_b[0][0];
+        const uint32_t next_stride = (level & 1u) ? kBlocks * kBlocks : kBlocks * kBlocks / 4;
+        const auto pixel = [&](uint32_t px) {
+            const uint32_t jx = px & (side - 1);
+            const uint32_t jy = px >> shift;
+            const uint32_t cx0 = min(2 * jx, lx), cx1 = min(2 * jx + 1, lx);
+            const uint32_t cy0 = min(2 * jy, ly), cy1 = min(2 * jy + 1, ly);
+            float v[3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const float* p = prev0 + c * prev_stride;
-            v[c] = BoxAverage<kHalf>(p[cy0 * prev_side + cx0], p[cy0 * prev_side + cx1],
-                                     p[cy1 * prev_side + cx0], p[cy1 * prev_side + cx1]);
+            for (int c = 0; c < 3; ++c) {
+                const float* p = prev0 + c * prev_stride;
+                v[c] = BoxAverage<kHalf>(p[cy0 * prev_side + cx0], p[cy0 * prev_side + cx1],
+                                         p[cy1 * prev_side + cx0], p[cy1 * prev_side + cx1]);
+            }
+            float xyb[3];
+            Xyb<kInRange>(v[0], v[1], v[2], lv.mask[level], xyb);
+            StorePixel<kHalf>(lv, level, gx * side + jx, gy * side + jy, xyb[0], xyb[1],
+                              xyb[2]);
+            if (level < last) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) next0[c * next_stride + px] = v[c];
+            }
+        };
+        if constexpr (kThreads >= 256) {
+            pixel(tid);  // at most 256 pixels a level: one each
+        } else {
+            for (uint32_t px = tid; px < active; px += kThreads) pixel(px);
         }
-        float xyb[3];
-        Xyb<kInRange>(v[0], v[1], v[2], lv.mask[level], xyb);
-        StorePixel<kHalf>(lv, level, gx * side + jx, gy * side + jy, xyb[0], xyb[1], xyb[2]);
         if (level < last) {
-            float* next0 = (level & 1u) ? &ladder_a[0][0] : &ladder_b[0][0];
-            const uint32_t next_stride = (level & 1u) ? kBlocks * kBlocks : kBlocks * kBlocks / 4;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) next0[c * next_stride + tid] = v[c];
-            if (active > 32) {
-                // 256 or 64 threads: whole warps from warp 0.
-                asm volatile("bar.sync 1, %0;" ::"r"(active) : "memory");
+            if (workers > 32) {
+                // 256, 128 or 64 threads: whole warps from warp 0.
+                asm volatile("bar.sync 1, %0;" ::"r"(workers) : "memory");
             } else {
-                __syncwarp((1u << active) - 1u);
+                __syncwarp((1u << workers) - 1u);
             }
         }
     }
@@ -540,9 +563,10 @@ __global__ void __launch_bounds__(kThreads, kGroup == 0   ? 5
 template <bool kHalf>
 cudaError_t PreloadPrepareOf() {
     cudaFuncAttributes a;
-    cudaError_t e = cudaFuncGetAttributes(&a, PrepareKernel<0, kHalf>);
-    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, PrepareKernel<1, kHalf>);
-    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, PrepareKernel<2, kHalf>);
+    cudaError_t e = cudaFuncGetAttributes(&a, PrepareKernel<0, kHalf, 256>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, PrepareKernel<0, kHalf, 128>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, PrepareKernel<1, kHalf, 256>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, PrepareKernel<2, kHalf, 256>);
     return e;
 }
 cudaError_t PreloadPrepare() {
@@ -601,11 +625,40 @@ cudaError_t CheckCbrt(uint32_t first_bits, uint32_t last_bits, uint64_t* mismatc
     return cudaSuccess;
 }
 
+// SMs of the current device, looked up once per device.
+static uint32_t DeviceSmCount() {
+    static std::mutex mu;
+    static int cached[64] = {};
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) {
+        cudaGetLastError();
+        return 148;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (cached[device] == 0 &&
+        cudaDeviceGetAttribute(&cached[device], cudaDevAttrMultiProcessorCount, device) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        return 148;
+    }
+    return static_cast<uint32_t>(cached[device]);
+}
+
 template <bool kHalf>
 void LaunchPrepareOf(const DevBatch& b, cudaStream_t stream) {
-    if (b.prep_blocks[0]) PrepareKernel<0, kHalf><<<b.prep_blocks[0], kThreads, 0, stream>>>(b);
-    if (b.prep_blocks[1]) PrepareKernel<1, kHalf><<<b.prep_blocks[1], kThreads, 0, stream>>>(b);
-    if (b.prep_blocks[2]) PrepareKernel<2, kHalf><<<b.prep_blocks[2], kThreads, 0, stream>>>(b);
+    // The table decode of a launch of at least two waves of 256-thread CTAs
+    // runs as ten CTAs of 128 threads per SM: 64 1080p pairs 1.149 -> 1.075
+    // ms. Smaller launches keep 256 threads, which finish a CTA's tile
+    // sooner (one 1080p pair 27.0 against 28.7 us, one 256x256 pair 12.3
+    // against 17.0 us).
+    if (b.prep_blocks[0]) {
+        if (b.prep_blocks[0] >= 2u * 5u * DeviceSmCount())
+            PrepareKernel<0, kHalf, 128><<<b.prep_blocks[0], 128, 0, stream>>>(b);
+        else
+            PrepareKernel<0, kHalf, 256><<<b.prep_blocks[0], 256, 0, stream>>>(b);
+    }
+    if (b.prep_blocks[1]) PrepareKernel<1, kHalf, 256><<<b.prep_blocks[1], 256, 0, stream>>>(b);
+    if (b.prep_blocks[2]) PrepareKernel<2, kHalf, 256><<<b.prep_blocks[2], 256, 0, stream>>>(b);
 }
 cudaError_t LaunchPrepare(const DevBatch& b, cudaStream_t stream) {
     if (b.half)
