@@ -261,12 +261,12 @@ __device__ __forceinline__ void TableBlock(const DevSource& s, const float* lut,
 
 // CTAs per SM: five of 256 threads (40 warps) for the table and YUV
 // decodes, four for the generic one; the table decode also runs as ten CTAs
-// of 128 threads (see LaunchPrepareOf). The decodes' long dependency chains (the YUV power's table
-// loads, the generic FP64 transfers) want the warps more than the registers
-// (measured on 136 uneven pairs: the YUV kernel at 5 CTAs with some spilling
-// took 8.48 ms, at 4 9.33 ms; the generic decode at 4 beats 2 by a
-// quarter; the table kernel on 64 1080p pairs takes 1.366 ms at 5, 1.374 ms
-// at 6 and 1.399 ms at 4).
+// of 128 threads (see LaunchPrepareOf). The decodes' long dependency chains
+// (the YUV power's table loads, the generic FP64 transfers) want the warps
+// more than the registers (measured on 136 uneven pairs: the YUV kernel at
+// 5 CTAs with some spilling took 8.48 ms, at 4 9.33 ms; the generic decode
+// at 4 beats 2 by a quarter; the table kernel of 256 threads on 64 1080p
+// pairs took 1.366 ms at 5, 1.374 ms at 6 and 1.399 ms at 4).
 #ifndef VQM_GENERIC_PREPARE_CTAS
 #define VQM_GENERIC_PREPARE_CTAS 4
 #endif

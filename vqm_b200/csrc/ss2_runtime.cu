@@ -278,7 +278,6 @@ Tables BuildTables(const std::vector<std::pair<uint32_t, uint32_t>>& sizes, Blur
     return t;
 }
 
-// Output tiles of the default blur variant over pairs of the given sizes.
 // The tile grids (columns, rows) of the default tile over every kept
 // (pair, level, channel), in the blur's launch order.
 std::vector<std::pair<uint32_t, uint32_t>> DefaultTileGrids(
@@ -394,7 +393,10 @@ struct BatchMemory {
         moved |= seg_sums.ensure(need[3]);
         if (pair_done.ensure(need[4])) {
             moved = true;
+            // New counters start at zero; wait for it, as launches run on
+            // streams that do not wait for the legacy stream's memset.
             VQM_CK(cudaMemset(pair_done.as<void>(), 0, pair_done.bytes()));
+            VQM_CK(cudaStreamSynchronize(nullptr));
         }
         moved |= results_host.ensure(std::max<size_t>(t.pairs.size(), 1) * kResultDoubles * sizeof(double));
         pair_count = static_cast<uint32_t>(t.pairs.size());
