@@ -300,6 +300,12 @@ typedef struct vqm_cu_ss2_batch_config {
  * one tile per CTA) and 1 if its CTAs stay resident over many tiles. */
 #define VQM_CU_SS2_VARIANT_WORDS 5
 int vqm_cu_ss2_blur_variants(uint32_t* count, uint32_t* shapes);
+/* A host-only diagnostic with no counterpart in the reference: the blur
+ * variant a batch created without one takes for `n` pairs of the sizes in
+ * `sizes` (width, height interleaved) on a device of `sms` SMs (the strip
+ * length with the least estimated time). */
+int vqm_cu_ss2_auto_blur_variant(const uint32_t* sizes, uint32_t n, uint32_t sms,
+                                 uint32_t* variant);
 
 /* A self-check with no counterpart in the reference: the prepare kernels
  * compute the XYB cube roots by a shorter route than the shared

@@ -154,3 +154,23 @@ def test_pipeline_without_device_raises_runtime_error():
         ss2.Ssimulacra2Pipeline(64, 64)
     with pytest.raises(ss2.InvalidArgument, match="8x8"):
         ss2.Ssimulacra2Pipeline(4, 8)
+
+
+def test_automatic_strip_length():
+    """The blur kernel a batch without a variant takes: for one pair, the
+    strip length whose measured blur time on a B200 was least (1080p 2,
+    1440p and 4K 4), for large batches the longest strip."""
+    shapes = ss2.blur_variants()
+    strip = lambda sizes: shapes[ss2.auto_blur_variant(sizes, sms=148)][3]  # noqa: E731
+    assert strip([(1920, 1080)]) == 2
+    assert strip([(2560, 1440)]) == 4
+    assert strip([(3840, 2160)]) == 4
+    assert strip([(1920, 1080)] * 64) == 16
+    assert strip([(3840, 2160)] * 8) == 16
+    assert strip([(256, 256)]) == 1
+    # Every choice is a plain strip kernel of the default tile.
+    for sizes in ([(1280, 720)], [(640, 360)] * 3, [(333, 187), (3840, 2160)]):
+        w, h, threads, _, persistent = shapes[ss2.auto_blur_variant(sizes)]
+        assert (w, h, threads, persistent) == (32, 32, 128, 0)
+    with pytest.raises(ss2.InvalidArgument):
+        ss2.auto_blur_variant([(4, 4)])

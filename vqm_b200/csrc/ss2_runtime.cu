@@ -1694,6 +1694,23 @@ int vqm_cu_ss2_blur_variants(uint32_t* count, uint32_t* shapes) {
     });
 }
 
+int vqm_cu_ss2_auto_blur_variant(const uint32_t* sizes, uint32_t n, uint32_t sms,
+                                 uint32_t* variant) {
+    return Guard([&] {
+        NotNull(variant, "variant");
+        if (n == 0 || sms == 0) throw std::invalid_argument("no pairs or no SMs");
+        NotNull(sizes, "sizes");
+        std::vector<std::pair<uint32_t, uint32_t>> wh(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            wh[i] = {sizes[2 * i], sizes[2 * i + 1]};
+            if (wh[i].first < vqm_b200::kMinDimension || wh[i].second < vqm_b200::kMinDimension)
+                throw std::invalid_argument("pair smaller than 8x8");
+        }
+        *variant = static_cast<uint32_t>(
+            vqm_b200::AutoBlurVariant(vqm_b200::DefaultTileGrids(wh), static_cast<int>(sms)));
+    });
+}
+
 int vqm_cu_ss2_batch_set_timing(vqm_cu_ss2_batch* b, int enabled) {
     return Guard([&] {
         NotNull(b, "batch");

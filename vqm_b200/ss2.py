@@ -205,6 +205,7 @@ _SIGS = {
     "vqm_cu_ss2_plan_scales": ([ctypes.c_uint32, ctypes.c_uint32, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_channel_pruned": ([ctypes.c_uint32] * 3 + [_P], ctypes.c_int),
     "vqm_cu_ss2_blur_taps": ([ctypes.c_uint32, _P], ctypes.c_int),
+    "vqm_cu_ss2_auto_blur_variant": ([_P, ctypes.c_uint32, ctypes.c_uint32, _P], ctypes.c_int),
     "vqm_cu_ss2_check_cbrt": ([ctypes.c_uint32, ctypes.c_uint32, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_check_division": ([ctypes.c_uint32, ctypes.c_uint32, _P, _P], ctypes.c_int),
     "vqm_cu_ss2_score": ([_P, ctypes.c_uint32, _P], ctypes.c_int),
@@ -476,6 +477,17 @@ def channel_pruned(channel: int, scale: int, scales: int) -> bool:
     out = ctypes.c_int()
     _check(_lib.vqm_cu_ss2_channel_pruned(channel, scale, scales, ctypes.byref(out)))
     return bool(out.value)
+
+
+def auto_blur_variant(sizes, sms: int = 148) -> int:
+    """The blur variant (index into blur_variants()) a batch created without
+    one takes for pairs of these (width, height) sizes on a device of `sms`
+    SMs. Host only."""
+    flat = np.asarray(list(sizes), dtype=np.uint32).reshape(-1)
+    out = ctypes.c_uint32()
+    _check(_lib.vqm_cu_ss2_auto_blur_variant(flat.ctypes.data, flat.size // 2, sms,
+                                             ctypes.byref(out)))
+    return out.value
 
 
 def blur_taps(blur: int = 0) -> np.ndarray:
