@@ -37,6 +37,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <functional>
 #include <mutex>
@@ -1048,10 +1049,10 @@ namespace {
 // reduction and epilogue), fitted to measured one-pair blur times (720p,
 // 1080p, 1440p and 4K, strips of 1 to 16). The device hands CTAs in launch
 // order to the slot that frees first; up to kSimulatedWaves waves that is
-// simulated, beyond it the last wave's share is small and the estimate is
-// the work per slot plus half a CTA.
+// simulated, beyond it the estimate is the work per slot plus the last
+// wave's idle share of an average CTA.
 constexpr double kStripCost = 0.7;
-constexpr uint64_t kSimulatedWaves = 8;
+constexpr uint64_t kSimulatedWaves = 4;
 
 double StripLaunchCost(const std::vector<std::pair<uint32_t, uint32_t>>& grids, uint32_t S,
                        uint64_t slots) {
@@ -1062,8 +1063,11 @@ double StripLaunchCost(const std::vector<std::pair<uint32_t, uint32_t>>& grids, 
     }
     if (ctas == 0) return 0.0;
     const double work = static_cast<double>(tiles) + kStripCost * static_cast<double>(ctas);
-    if (ctas > kSimulatedWaves * slots)
-        return work / static_cast<double>(slots) + 0.5 * work / static_cast<double>(ctas);
+    if (ctas > kSimulatedWaves * slots) {
+        const double waves = static_cast<double>(ctas) / static_cast<double>(slots);
+        return work / static_cast<double>(slots) +
+               (std::ceil(waves) - waves) * work / static_cast<double>(ctas);
+    }
     // Launch order: segment by segment, strip rows of all columns in turn.
     std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
     for (uint64_t k = 0; k < std::min<uint64_t>(slots, ctas); ++k) free_at.push(0.0);
@@ -1089,12 +1093,15 @@ int AutoBlurVariant(const std::vector<std::pair<uint32_t, uint32_t>>& grids, int
     // Large batches take the longest strip, 16; one pair 720p 1 to 4 (equal
     // times), 1080p 2, 1440p 4 and 4K 4 (4K: 122.9 -> 118.8 us against the
     // earlier rule, the longest strip leaving every CTA slot 2 CTAs, which
-    // took 8). Memoised per grid list: a batch of the same sizes, or a
-    // pipeline, pays for the estimate once.
+    // took 8). Memoised per set of grids (sorted, so a batch of the same
+    // sizes in another order is the same entry): a batch of the same sizes,
+    // or a pipeline, pays for the estimate once.
     const BlurVariant& base = kBlurVariants[kDefaultBlurVariant];
     const uint64_t slots = static_cast<uint64_t>(sms > 0 ? sms : 1) * base.per_sm;
+    std::vector<std::pair<uint32_t, uint32_t>> sorted(grids);
+    std::sort(sorted.begin(), sorted.end());
     uint64_t key = 1469598103934665603ull ^ static_cast<uint64_t>(sms);
-    for (const auto& g : grids) {
+    for (const auto& g : sorted) {
         key = (key ^ g.first) * 1099511628211ull;
         key = (key ^ g.second) * 1099511628211ull;
     }
@@ -1106,14 +1113,14 @@ int AutoBlurVariant(const std::vector<std::pair<uint32_t, uint32_t>>& grids, int
         if (it != memo.end()) return it->second;
     }
     int best = kDefaultBlurVariant;
-    double best_cost = StripLaunchCost(grids, 1, slots);
+    double best_cost = StripLaunchCost(sorted, 1, slots);
     int best_strip = 1;
     for (int i = 0; i < kBlurVariantCount; ++i) {
         const BlurVariant& v = kBlurVariants[i];
         if (v.persistent || v.w != base.w || v.h != base.h || v.threads != base.threads ||
             v.strip <= 1)
             continue;
-        const double c = StripLaunchCost(grids, static_cast<uint32_t>(v.strip), slots);
+        const double c = StripLaunchCost(sorted, static_cast<uint32_t>(v.strip), slots);
         if (c < best_cost * (1.0 - 1e-9) || (c <= best_cost * (1.0 + 1e-9) && v.strip > best_strip)) {
             best = i;
             best_cost = c;
