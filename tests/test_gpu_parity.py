@@ -342,6 +342,37 @@ def test_table_prepare_of_large_launches_is_bit_exact():
     b.close()
 
 
+def test_yuv_prepare_of_large_launches_is_bit_exact():
+    """Large YUV launches whose images all have 4:2:0 chroma run 128-thread
+    CTAs with a 4:2:0 chroma window; other YUV launches run 256-thread CTAs
+    with a window for any subsampling. Both write the same planes: 720p
+    pairs score bit for bit the same alone (480 tiles, 256 threads) and
+    beside a 4K pair (5,040 tiles, 128 threads), and a 4:2:2 image keeps its
+    launch on the 256-thread kernel (the 4K pair then scores as before) and
+    matches the oracle."""
+    big = synthetic.yuv_pair(3840, 2160, 80)[:2]
+    small = [synthetic.yuv_pair(1280, 720, 81 + i)[:2] for i in range(2)]
+    b = ss2.Ssimulacra2Batch(variant=0)
+    try:
+        together = b.compute_many(small + [big])
+        for (o, d), r in zip(small, together[:2]):
+            alone = b.compute_many([(o, d)])[0]
+            assert np.array_equal(alone.norms, r.norms) and alone.device_score == r.device_score
+            check_parity(r, o, d, label="720p 4:2:0 beside a 4K pair")
+        check_parity(together[2], *big, label="4K 4:2:0 in a large launch")
+        fmt = _variants()["yuv422_bt601"]
+        w, h = 640, 360
+        ov = _values(fmt, w, h, 82)
+        dv = [None if v is None else np.clip(v * 0.97 + 0.01, -0.5 if i in (1, 2) else 0, 1)
+              for i, v in enumerate(ov)]
+        o422, d422 = helpers.pack_planes(fmt, w, h, ov), helpers.pack_planes(fmt, w, h, dv)
+        mixed = b.compute_many([big, (o422, d422)])
+        assert np.array_equal(mixed[0].norms, together[2].norms)
+        check_parity(mixed[1], o422, d422, label="4:2:2 in a large YUV launch")
+    finally:
+        b.close()
+
+
 @pytest.mark.parametrize("variant", range(len(ss2.blur_variants())))
 def test_every_blur_variant(variant):
     """Every compiled blur kernel gives the oracle's features; they differ

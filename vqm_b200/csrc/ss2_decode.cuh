@@ -446,10 +446,12 @@ __device__ __forceinline__ float2 PowfGamma2(float2 x, float y, const float* pt)
 // planes staged once in shared memory (kPrepTile >> sub samples per axis plus
 // one on each side, edge-clamped: for the one-past-the-edge positions a block
 // can touch that is the reference's mirror index), already scaled like
-// RawSample. kChromaStage floats per plane.
+// RawSample. `plane` floats per plane: kChromaStage covers every
+// subsampling the path takes, kChromaStage420 4:2:0 alone.
 constexpr int kChromaStage = ((kPrepTile >> 1) + 2) * (kPrepTile + 2);
+constexpr int kChromaStage420 = ((kPrepTile >> 1) + 2) * ((kPrepTile >> 1) + 2);
 __device__ __forceinline__ void StageChroma(const DevSource& s, uint32_t gx, uint32_t gy,
-                                            float* stage) {
+                                            float* stage, int plane) {
     const uint32_t sw = (kPrepTile >> s.sub_w) + 2, sh = (kPrepTile >> s.sub_h) + 2;
     const int c0x = static_cast<int>((gx * kPrepTile) >> s.sub_w) - 1;
     const int c0y = static_cast<int>((gy * kPrepTile) >> s.sub_h) - 1;
@@ -472,7 +474,7 @@ __device__ __forceinline__ void StageChroma(const DevSource& s, uint32_t gx, uin
         const uint32_t y = static_cast<uint32_t>(min(max(c0y + static_cast<int>(j), 0), dy - 1));
         const float u = sample(1, y), v = sample(2, y);
         stage[j * sw + i] = __fmaf_rn(u, s.scale[1], s.offset[1]);
-        stage[kChromaStage + j * sw + i] = __fmaf_rn(v, s.scale[1], s.offset[1]);
+        stage[plane + j * sw + i] = __fmaf_rn(v, s.scale[1], s.offset[1]);
     }
 }
 
@@ -493,7 +495,8 @@ struct AxisPhase {
     }
 };
 template <int kX, int kY>
-__device__ __forceinline__ void ChromaFixed(const float* stage, int bxs, int bys, float e[4][3]) {
+__device__ __forceinline__ void ChromaFixed(const float* stage, int plane, int bxs, int bys,
+                                            float e[4][3]) {
     using X = AxisPhase<kX>;
     using Y = AxisPhase<kY>;
     constexpr int sw = (kPrepTile >> 1) + 2;
@@ -501,7 +504,7 @@ __device__ __forceinline__ void ChromaFixed(const float* stage, int bxs, int bys
     // the scalar chain.
 #pragma unroll
     for (int p = 0; p < 2; ++p) {
-        const float* base = stage + p * kChromaStage + bys * sw + bxs;
+        const float* base = stage + p * plane + bys * sw + bxs;
 #pragma unroll
         for (int yp = 0; yp < 2; ++yp) {
             const float* t0 = base + Y::Slot(yp) * sw + X::Slot(0);
@@ -526,7 +529,7 @@ __device__ __forceinline__ void ChromaFixed(const float* stage, int bxs, int bys
 // with the format's branches resolved and the chroma taps read from the
 // staged window at the host's per-parity slots and weights.
 __device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* stage,
-                                               const float* pow_table,
+                                               int plane, const float* pow_table,
                                                uint32_t gx, uint32_t gy, uint32_t bx,
                                                uint32_t by, bool aligned4, float rgb[4][3]) {
     const uint32_t x0 = 2 * bx, y0 = 2 * by;
@@ -574,10 +577,10 @@ __device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* 
         const int bxs = static_cast<int>((x0 >> 1) - ((gx * kPrepTile) >> 1));
         const int bys = static_cast<int>((y0 >> 1) - ((gy * kPrepTile) >> 1));
         switch (s.chroma_pattern) {
-            case 1: ChromaFixed<0, 0>(stage, bxs, bys, e); break;
-            case 2: ChromaFixed<1, 0>(stage, bxs, bys, e); break;
-            case 3: ChromaFixed<0, 1>(stage, bxs, bys, e); break;
-            default: ChromaFixed<1, 1>(stage, bxs, bys, e); break;
+            case 1: ChromaFixed<0, 0>(stage, plane, bxs, bys, e); break;
+            case 2: ChromaFixed<1, 0>(stage, plane, bxs, bys, e); break;
+            case 3: ChromaFixed<0, 1>(stage, plane, bxs, bys, e); break;
+            default: ChromaFixed<1, 1>(stage, plane, bxs, bys, e); break;
         }
     } else if (s.chroma_variant) {
         const uint32_t sw = (kPrepTile >> s.sub_w) + 2;
@@ -591,7 +594,7 @@ __device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* 
             for (int i = 0; i < 4; ++i) {
                 const int xp = i & 1, yp = i >> 1;
                 const float* t =
-                    stage + p * kChromaStage + (bys + s.cslot[1][yp]) * static_cast<int>(sw) +
+                    stage + p * plane + (bys + s.cslot[1][yp]) * static_cast<int>(sw) +
                     bxs + s.cslot[0][xp];
                 const float* w = s.cweight[yp][xp];
                 // A first slot of 2 puts the second tap past the window: 0.

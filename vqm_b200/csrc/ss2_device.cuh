@@ -140,6 +140,11 @@ inline int PrepGroup(const DevSource& s) {
     if (s.lut) return 0;
     return s.yuv_fast && s.width % 2 == 0 && s.height % 2 == 0 ? 1 : 2;
 }
+// Whether an image fits the 4:2:0 chroma window of the 128-thread YUV
+// prepare kernel (4:2:0 chroma, or none subsampled).
+inline bool Yuv420Window(const DevSource& s) {
+    return !s.chroma_variant || (s.sub_w == 1 && s.sub_h == 1);
+}
 
 struct DevBatch {
     uint32_t pairs;
@@ -161,6 +166,8 @@ struct DevBatch {
     uint32_t* blur_queue;        // the tile queue's next strip and exit count (0 between launches)
     uint32_t* status;            // nonzero: a kernel found bad input
     uint32_t half;               // 1: pyramid elements are binary16
+    uint32_t yuv420;             // 1: every image of the YUV prepare group
+                                 // has 4:2:0 chroma or none subsampled
     // The blur's 13 taps (offsets -6..6) as (w, w) pairs: the blur kernels
     // take them from the launch's parameter space, a constant bank like
     // __constant__ memory, so each batch carries its blur mode's filter.

@@ -958,7 +958,14 @@ private:
         const DevPair* hp = mem_.HostPair(0);
         const uint8_t g0 = static_cast<uint8_t>(PrepGroup(hp->src[0]));
         const uint8_t g1 = static_cast<uint8_t>(PrepGroup(hp->src[1]));
-        const int key = g0 + kPrepGroups * (g1 + kPrepGroups * (skip_original ? 1 : 0));
+        // The YUV prepare kernel (and its window) depends on the images'
+        // chroma subsampling too.
+        bool yuv420 = true;
+        for (int k = skip_original ? 1 : 0; k < 2; ++k)
+            if (PrepGroup(hp->src[k]) == 1 && !Yuv420Window(hp->src[k])) yuv420 = false;
+        mem_.dev.yuv420 = yuv420 ? 1u : 0u;
+        const int key = g0 + kPrepGroups * (g1 + kPrepGroups * ((skip_original ? 1 : 0) +
+                                                                 2 * (yuv420 ? 1 : 0)));
         BuildPrepLists(tables_, {{g0, g1}}, skip_original);
         mem_.StagePrep(tables_);
         const size_t upload = mem_.head_bytes;
@@ -999,7 +1006,7 @@ private:
     int device_ = 0;
     cudaStream_t own_stream_ = nullptr, stream_ = nullptr;
     cudaEvent_t done_ = nullptr, copied_ = nullptr;
-    cudaGraphExec_t graph_exec_[2 * kPrepGroups * kPrepGroups] = {};
+    cudaGraphExec_t graph_exec_[4 * kPrepGroups * kPrepGroups] = {};
     bool reference_valid_ = false;
     uint64_t reference_handle_ = 0;
     float reference_background_ = 0.0f;
@@ -1147,9 +1154,14 @@ public:
             }
         }
         PrepGroups group(n);
-        for (uint32_t i = 0; i < n; ++i)
+        bool yuv420 = true;
+        for (uint32_t i = 0; i < n; ++i) {
             group[i] = {static_cast<uint8_t>(PrepGroup(t.pairs[i].src[0])),
                         static_cast<uint8_t>(PrepGroup(t.pairs[i].src[1]))};
+            for (int k = 0; k < 2; ++k)
+                if (group[i][k] == 1 && !Yuv420Window(t.pairs[i].src[k])) yuv420 = false;
+        }
+        mem_.dev.yuv420 = yuv420 ? 1u : 0u;
         BuildPrepLists(t, group);
         mem_.Stage(t);
         if (host_bytes) VQM_CK(cudaEventRecord(copied_, stream_));
