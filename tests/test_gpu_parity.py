@@ -330,9 +330,10 @@ def test_table_prepare_of_large_launches_is_bit_exact():
     """Large launches of the 8-bit table decode run 128-thread CTAs, small
     ones 256-thread CTAs; both write the same planes, so with the same blur
     kernel a pair scores bit for bit the same alone and in a batch of
-    three 1080p pairs (3,060 tiles of 64x64, the 128-thread form on any
-    device of up to 306 SMs)."""
-    pairs = [synthetic.rgb_pair(1920, 1080, 60 + i)[:2] for i in range(3)]
+    three ~1080p pairs, one of odd size (3,060 tiles of 64x64, the
+    128-thread form on any device of up to 306 SMs)."""
+    pairs = [synthetic.rgb_pair(1920, 1080, 60 + i)[:2] for i in range(2)]
+    pairs.append(synthetic.rgb_pair(1919, 1077, 62)[:2])  # partial tiles, odd sizes
     b = ss2.Ssimulacra2Batch(variant=0)
     together = b.compute_many(pairs)
     for (o, d), r in zip(pairs, together):
