@@ -1,6 +1,8 @@
 """Accuracy of the deterministic functions that the kernels, the host decode
 tables and the oracle share (vqm_b200/csrc/ss2_detmath.h), against
-double-precision libm.
+double-precision libm, and on samples against exact rational and 40-digit
+decimal arithmetic (no libm in the checker: the oracle shares these
+functions with the kernels, so they are pinned independently here).
 
 pow, cbrt, exp and sin(pi x) evaluate to ~3e-13 and round once, so they must
 land on the correctly rounded float in all but a tiny fraction of cases, and
@@ -196,3 +198,43 @@ def test_blur_division_equals_the_shared_one_across_its_band():
     hi = int(np.float32(2.0 ** 4).view(np.uint32))
     mismatches, first_bad = ss2.check_division(lo, hi)
     assert mismatches == 0, (mismatches, hex(first_bad))
+
+
+def test_cbrt_correctly_rounded_by_exact_arithmetic():
+    """The cube root's correct rounding checked without libm: for float x
+    and the returned float y with ulp u, exact rational arithmetic confirms
+    (y - u/2)^3 <= x <= (y + u/2)^3 on 60,000 random floats of [1, 8) and of
+    the whole normal range."""
+    from fractions import Fraction
+    rng = np.random.default_rng(31)
+    lo, hi = np.float32(1.0).view(np.uint32), np.float32(8.0).view(np.uint32)
+    x = np.concatenate([
+        rng.integers(lo, hi, 30_000, dtype=np.uint32).view(np.float32),
+        samples(1.2e-38, 3e38, n=30_000, seed=32)])
+    y = det(0, x)
+    for xi, yi in zip(x.tolist(), y.tolist()):
+        m, e = np.frexp(np.float32(yi))  # yi = m 2^e, m in [0.5, 1)
+        half_ulp = Fraction(2) ** (int(e) - 25)
+        fy, fx = Fraction(yi), Fraction(xi)
+        assert (fy - half_ulp) ** 3 <= fx <= (fy + half_ulp) ** 3, (xi, yi)
+
+
+def test_powers_faithful_by_decimal_arithmetic():
+    """pow and the transfers' powf_gamma checked without libm: each result
+    is one of the two floats around the exact power, computed in 40-digit
+    decimal arithmetic, on 4,000 random arguments per exponent."""
+    import decimal
+    ctx = decimal.Context(prec=40)
+    for fn, y, lo, hi in ((5, 2.4, 2.0 ** -30, 65535.9), (5, 2.2, 1e-6, 1.5),
+                          (1, 1 / 0.45, 1e-6, 1.5), (1, 1 / 78.84375, 1e-6, 1.0),
+                          (1, 1 / 0.1593017578125, 1e-3, 1.0)):
+        yf = np.float32(y)
+        x = samples(lo, hi, n=4_000, seed=int(1e3 * y))
+        got = det(fn, x, yf)
+        for xi, gi in zip(x.tolist(), got.tolist()):
+            exact = ctx.power(decimal.Decimal(xi), decimal.Decimal(float(yf)))
+            below = np.float32(float(exact))
+            if decimal.Decimal(float(below)) > exact:
+                below = np.nextafter(below, np.float32(0))
+            above = np.nextafter(below, np.float32(np.inf))
+            assert gi in (float(below), float(above)), (fn, y, xi, gi, exact)
