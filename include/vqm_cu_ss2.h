@@ -247,6 +247,12 @@ int vqm_cu_ss2_set_graphs(vqm_cu_ss2_pipeline* pipeline, int enabled);
  * submission's skips the original's decode and pyramid. *count receives how
  * many submissions have done so. */
 int vqm_cu_ss2_reference_reuses(vqm_cu_ss2_pipeline* pipeline, uint64_t* count);
+/* VulkanRuntime::pending() (src/vulkan/vulkan_runtime.h:275-285): *in_flight
+ * receives 1 from a successful submit until finish takes its token, else 0.
+ * VQM reports a call made while a submission is in flight before it looks at
+ * the call's images; the facades check image sizes on the host, so they ask
+ * this before reporting such an error. */
+int vqm_cu_ss2_in_flight(const vqm_cu_ss2_pipeline* pipeline, uint32_t* in_flight);
 
 /* ---- scoring without allocation --------------------------------------- */
 

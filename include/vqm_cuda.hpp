@@ -339,9 +339,13 @@ public:
     }
 
     [[nodiscard]] std::uint64_t Submit(const Image& o, const Image& d, float background = 0.5f) {
-        Geometry(o.size, "original");
-        Geometry(d.size, "distorted");
-        const vqm_cu_image a = detail::ToC(o, "original"), b = detail::ToC(d, "distorted");
+        vqm_cu_image a{}, b{};
+        IdleFirst([&] {
+            Geometry(o.size, "original");
+            Geometry(d.size, "distorted");
+            a = detail::ToC(o, "original");
+            b = detail::ToC(d, "distorted");
+        });
         return SubmitC(a, b, background);
     }
     [[nodiscard]] std::uint64_t Submit(const ImageView& o, const ImageView& d,
@@ -356,8 +360,11 @@ public:
     }
     [[nodiscard]] std::uint64_t Submit(const UploadedImage& o, const Image& d,
                                        float background = 0.5f) {
-        Geometry(d.size, "distorted");
-        const vqm_cu_image b = detail::ToC(d, "distorted");
+        vqm_cu_image b{};
+        IdleFirst([&] {
+            Geometry(d.size, "distorted");
+            b = detail::ToC(d, "distorted");
+        });
         std::uint64_t token = 0;
         detail::Check(vqm_cu_ss2_submit_resident_image(p_.get(), o.slot, &b, background, &token));
         return token;
@@ -391,8 +398,11 @@ public:
     }
 
     [[nodiscard]] UploadedImage Upload(const Image& image) {
-        Geometry(image.size, "image");
-        const vqm_cu_image c = detail::ToC(image, "image");
+        vqm_cu_image c{};
+        IdleFirst([&] {
+            Geometry(image.size, "image");
+            c = detail::ToC(image, "image");
+        });
         std::uint64_t handle = 0;
         detail::Check(vqm_cu_ss2_upload(p_.get(), &c, &handle));
         return UploadedImage{handle, image.size};
@@ -431,6 +441,22 @@ private:
         if (!(s == config_.size))
             throw std::invalid_argument(std::string(name) +
                                         ": image size does not match the pipeline geometry");
+    }
+    // The host-side image checks (geometry, data size) run before the
+    // library sees the call; VQM reports a call made while a submission is
+    // in flight first (vulkan_runtime.h:275-285), so a failed check defers
+    // to that.
+    template <class F>
+    void IdleFirst(F&& checks) const {
+        try {
+            checks();
+        } catch (const std::invalid_argument&) {
+            std::uint32_t busy = 0;
+            if (vqm_cu_ss2_in_flight(p_.get(), &busy) == VQM_CU_OK && busy)
+                throw std::logic_error(
+                    "cuda: a submission is already in flight; Finish it first");
+            throw;
+        }
     }
     std::uint64_t SubmitC(const vqm_cu_image& a, const vqm_cu_image& b, float background) {
         std::uint64_t token = 0;

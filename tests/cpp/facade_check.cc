@@ -167,6 +167,16 @@ void Gpu() {
     ExpectThrow<std::invalid_argument>([&] { (void)pipeline.Compute(base, small); },
                                        "size mismatch");
     ExpectThrow<std::invalid_argument>([&] { (void)pipeline.Finish(12345); }, "unknown token");
+    // While a submission is in flight that is reported before a bad image
+    // (pipeline_test.cc:385-395).
+    const std::uint64_t token = pipeline.Submit(base, Gradient(1));
+    ExpectThrow<std::logic_error>([&] { (void)pipeline.Submit(base, small); },
+                                  "in flight before a bad image");
+    ExpectThrow<std::logic_error>([&] { (void)pipeline.Upload(small); },
+                                  "in flight before a bad upload");
+    (void)pipeline.Finish(token);
+    ExpectThrow<std::invalid_argument>([&] { (void)pipeline.Submit(base, small); },
+                                       "bad image once idle");
 
     v::Ssimulacra2Pool pool(config, 2, 2);
     const v::Image d1 = Gradient(1), d2 = Gradient(2);

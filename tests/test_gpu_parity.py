@@ -474,6 +474,164 @@ def test_reference_pyramid_reuse():
         assert p.reference_reuses() == 3
 
 
+def test_mixed_resident_reference_with_alpha():
+    """pipeline_test.cc:47-118 (the SSIMULACRA 2 half): a resident original
+    with straight alpha against streamed distorted images at two
+    backgrounds. With alpha the background changes the planes, so a cached
+    reference pyramid must be re-prepared when it changes; every resident
+    result equals the streamed one bit for bit (VQM: within 1e-12)."""
+    o = helpers.ramp_image(32, 32, True, ss2.PixelType.Byte)
+    d_data = o.data.copy()
+    d_data[:32 * 32] = 0
+    other_data = o.data.copy()
+    other_data[32 * 32:2 * 32 * 32] = 0
+    d = ss2.Image(32, 32, o.format, d_data)
+    other = ss2.Image(32, 32, o.format, other_data)
+    with ss2.Ssimulacra2Pipeline(32, 32) as p:
+        dark = p.compute(o, d, 0.1)
+        bright = p.compute(o, d, 0.9)
+        other_dark = p.compute(o, other, 0.1)
+        assert dark.score() != bright.score()  # the background matters here
+        ref = p.upload(o)
+        assert np.array_equal(p.compute(ref, d, 0.1).norms, dark.norms)
+        assert np.array_equal(p.compute(ref, d, 0.1).norms, dark.norms)
+        assert np.array_equal(p.compute(ref, other, 0.1).norms, other_dark.norms)
+        assert np.array_equal(p.compute(ref, d, 0.9).norms, bright.norms)
+        tok = p.submit(ref, d)
+        with pytest.raises(ss2.LogicError):
+            p.submit(ref, d)
+        p.finish(tok)
+        short = ss2.Image(32, 32, o.format, d.data[:-1])
+        with pytest.raises(ss2.InvalidArgument):
+            p.submit(ref, short)
+        p.release(ref)
+        with pytest.raises(ss2.InvalidArgument):
+            p.compute(ref, d)
+        replacement = p.upload(d)
+        assert np.array_equal(p.compute(replacement, d).norms, p.compute(d, d).norms)
+    for bg, want in ((0.1, dark), (0.9, bright)):
+        _, score = helpers.oracle_compute(o, d, bg)
+        assert abs(want.score() - score) <= helpers.SCORE_TOL
+    with ss2.Ssimulacra2Pipeline(32, 32, streaming_inputs=False) as p:
+        ref = p.upload(o)
+        with pytest.raises(ss2.InvalidArgument):
+            p.compute(ref, d)
+
+
+def test_invalid_formats_rejected_on_every_path():
+    """pipeline_test.cc:218-274 (the SSIMULACRA 2 half): a format VQM rejects
+    raises InvalidArgument from compute on packed images and on plane views,
+    from upload and from allocate_image, and takes nothing from the
+    caller-owned input pool."""
+    base = ss2.ImageFormat()
+    for w, h in ((32, 32), (33, 17)):
+        image_bytes = ss2.required_bytes(base, w, h)
+        invalid = [base.copy(subsample_w=1),  # RGB with subsampled planes
+                   base.copy(family=ss2.ColorFamily.Yuv)]  # YUV with the RGB matrix
+        if w % 2 or h % 2:
+            invalid.append(base.copy(family=ss2.ColorFamily.Yuv,
+                                     matrix=ss2.MatrixCoefficients.Bt709,
+                                     subsample_w=1, subsample_h=1))
+        invalid += [base.copy(range=255), base.copy(alpha=255)]
+        with ss2.Ssimulacra2Pipeline(w, h, input_bytes=2 * image_bytes + 63) as p:
+            for bad in invalid:
+                packed = ss2.Image(w, h, bad, np.zeros(image_bytes, np.uint8))
+                planes = [np.zeros(4 * w * h, np.uint8) for _ in range(4)]
+                view = ss2.HostImage(w, h, bad, planes)
+                with pytest.raises(ss2.InvalidArgument):
+                    p.compute(packed, packed)
+                with pytest.raises(ss2.InvalidArgument):
+                    p.compute(view, view)
+                with pytest.raises(ss2.InvalidArgument):
+                    p.upload(packed)
+                with pytest.raises(ss2.InvalidArgument):
+                    p.allocate_image(bad)
+            a, b = p.allocate_image(base), p.allocate_image(base)
+            assert a.bytes + b.bytes == 2 * image_bytes
+
+
+def test_streaming_submission_validation():
+    """pipeline_test.cc:359-446 (the SSIMULACRA 2 half): bad streamed inputs
+    raise InvalidArgument; while a submission is in flight every call that
+    would touch the pipeline's inputs raises LogicError and the pending pair
+    is left as it was; after Finish, handle 0 (a default handle) raises
+    InvalidArgument in a submission and releases as a no-op."""
+    o, d = helpers.gradient(0), helpers.gradient(1)
+    w, h = o.width, o.height
+    oversized = ss2.Image(w, h, d.format, np.zeros(20 * w * h, np.uint8))
+    short = ss2.Image(w, h, o.format, o.data[:1])
+    wrong_size = ss2.Image(w - 1, h, o.format,
+                           np.zeros(ss2.required_bytes(o.format, w - 1, h), np.uint8))
+    no_image = ss2.UploadedImage(0, (w, h))
+    no_buffer = ss2.ImageBuffer(0, (w, h), 0)
+    with ss2.Ssimulacra2Pipeline(w, h) as p:
+        resident, resident_d = p.upload(o), p.upload(d)
+        with pytest.raises(ss2.InvalidArgument):
+            p.upload(o)  # both resident slots are taken
+        for bad in ((o, oversized), (short, d), (wrong_size, d)):
+            with pytest.raises(ss2.InvalidArgument):
+                p.submit(*bad)
+        expected = p.compute(o, d)
+        tok = p.submit(o, d)
+        in_flight = [
+            lambda: p.submit(o, o), lambda: p.submit(o, oversized),
+            lambda: p.compute(o, oversized), lambda: p.upload(o),
+            lambda: p.upload(oversized), lambda: p.release(resident),
+            lambda: p.release(no_image), lambda: p.submit(resident, resident_d),
+            lambda: p.submit(no_image, resident), lambda: p.compute(no_image, resident),
+            lambda: p.allocate_image(o.format), lambda: p.map_image(no_buffer),
+            lambda: p.release(no_buffer), lambda: p.submit(no_buffer, no_buffer),
+            lambda: p.compute(no_buffer, no_buffer)]
+        for call in in_flight:
+            with pytest.raises(ss2.LogicError):
+                call()
+        assert np.array_equal(p.finish(tok).norms, expected.norms)
+        with pytest.raises(ss2.InvalidArgument):
+            p.finish(tok)
+        with pytest.raises(ss2.InvalidArgument):
+            p.submit(no_image, resident)
+        with pytest.raises(ss2.InvalidArgument):
+            p.submit(no_buffer, no_buffer)
+        p.release(no_image)
+        p.release(no_buffer)
+        p.release(resident)
+        p.release(resident_d)
+
+
+def test_resident_handle_contracts():
+    """pipeline_test.cc:478-513: a released handle does not alias the image
+    that reuses its slot, and a replacement scores like its pixels."""
+    o, d = helpers.gradient(0), helpers.gradient(1)
+    with ss2.Ssimulacra2Pipeline(o.width, o.height) as p:
+        old, other = p.upload(o), p.upload(d)
+        before = p.compute(old, other).score()
+        with pytest.raises(ss2.InvalidArgument):
+            p.upload(o)
+        wrong = ss2.UploadedImage(other.slot, (o.width - 1, o.height))
+        wrong_img = ss2.Image(o.width - 1, o.height, d.format,
+                              np.zeros(ss2.required_bytes(d.format, o.width - 1, o.height),
+                                       np.uint8))
+        with pytest.raises(ss2.InvalidArgument):
+            p.submit(old, wrong_img)
+        p.release(old)
+        replacement = p.upload(d)
+        with pytest.raises(ss2.InvalidArgument):
+            p.submit(old, other)
+        expected = p.compute(d, d).score()
+        after = p.compute(replacement, other).score()
+        assert after == expected == 100.0
+        assert abs(before - after) > 1e-5
+        del wrong
+    # One slot: a second upload has nowhere to go until the first is released
+    # (pipeline_test.cc:451-476).
+    with ss2.Ssimulacra2Pipeline(o.width, o.height, gpu_resident_images=1) as single:
+        first = single.upload(o)
+        with pytest.raises(ss2.InvalidArgument):
+            single.upload(d)
+        single.release(first)
+        single.upload(d)
+
+
 def test_submit_finish_contracts():
     o, d = helpers.plain_256_pair()
     with ss2.Ssimulacra2Pipeline(256, 256) as p:

@@ -624,6 +624,7 @@ public:
     void* GetStream() const { return stream_; }
     // Submissions that reused the cached original's pyramid.
     uint64_t ReferenceReuses() const { return reference_reuses_; }
+    bool InFlight() const { return in_flight_; }
     void SetGraphs(bool on) {
         RequireIdle();
         graphs_ = on;
@@ -1340,7 +1341,7 @@ struct vqm_cu_ss2_batch {
 extern "C" {
 
 const char* vqm_cu_last_error(void) { return vqm_b200::g_last_error.c_str(); }
-uint32_t vqm_cu_version(void) { return (1u << 16) | 1u; }
+uint32_t vqm_cu_version(void) { return (1u << 16) | 2u; }
 
 int vqm_cu_required_bytes(const vqm_cu_format* format, uint32_t width, uint32_t height,
                           size_t* bytes) {
@@ -1485,6 +1486,14 @@ int vqm_cu_ss2_reference_reuses(vqm_cu_ss2_pipeline* p, uint64_t* count) {
         NotNull(p, "pipeline");
         NotNull(count, "count");
         *count = p->impl.ReferenceReuses();
+    });
+}
+
+int vqm_cu_ss2_in_flight(const vqm_cu_ss2_pipeline* p, uint32_t* in_flight) {
+    return Guard([&] {
+        NotNull(p, "pipeline");
+        NotNull(in_flight, "in_flight");
+        *in_flight = p->impl.InFlight() ? 1u : 0u;
     });
 }
 

@@ -216,6 +216,7 @@ _SIGS = {
     "vqm_cu_ss2_get_stream": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_set_graphs": ([_P, ctypes.c_int], ctypes.c_int),
     "vqm_cu_ss2_reference_reuses": ([_P, _P], ctypes.c_int),
+    "vqm_cu_ss2_in_flight": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_submit": ([_P, _P, _P, ctypes.c_float, _P], ctypes.c_int),
     "vqm_cu_ss2_submit_resident": ([_P, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float, _P], ctypes.c_int),
     "vqm_cu_ss2_submit_resident_image": ([_P, ctypes.c_uint64, _P, ctypes.c_float, _P], ctypes.c_int),
@@ -604,14 +605,14 @@ class Ssimulacra2Pipeline:
             _check(_lib.vqm_cu_ss2_submit_resident(self._p, original.slot, distorted.slot,
                                                    background, ctypes.byref(tok)))
         elif isinstance(original, UploadedImage):
-            d = distorted._c()
+            d = self._idle_first(distorted._c)
             _check(_lib.vqm_cu_ss2_submit_resident_image(self._p, original.slot, ctypes.byref(d),
                                                          background, ctypes.byref(tok)))
         elif isinstance(original, ImageBuffer) and isinstance(distorted, ImageBuffer):
             _check(_lib.vqm_cu_ss2_submit_buffers(self._p, original.slot, distorted.slot,
                                                   background, ctypes.byref(tok)))
         else:
-            o, d = original._c(), distorted._c()
+            o, d = self._idle_first(lambda: (original._c(), distorted._c()))
             _check(_lib.vqm_cu_ss2_submit(self._p, ctypes.byref(o), ctypes.byref(d),
                                           background, ctypes.byref(tok)))
         return tok.value
@@ -625,8 +626,20 @@ class Ssimulacra2Pipeline:
     def compute(self, original, distorted, background: float = 0.5) -> Ssimulacra2Result:
         return self.finish(self.submit(original, distorted, background))
 
+    def _idle_first(self, checks):
+        """Runs the host-side image checks; when one fails while a submission
+        is in flight, reports the submission first, as VQM does
+        (vulkan_runtime.h:275-285)."""
+        try:
+            return checks()
+        except InvalidArgument:
+            busy = ctypes.c_uint32()
+            if _lib.vqm_cu_ss2_in_flight(self._p, ctypes.byref(busy)) == 0 and busy.value:
+                raise LogicError("cuda: a submission is already in flight; Finish it first")
+            raise
+
     def upload(self, image) -> UploadedImage:
-        c = image._c()
+        c = self._idle_first(image._c)
         h = ctypes.c_uint64()
         _check(_lib.vqm_cu_ss2_upload(self._p, ctypes.byref(c), ctypes.byref(h)))
         return UploadedImage(h.value, (image.width, image.height))
