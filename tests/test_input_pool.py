@@ -1,0 +1,144 @@
+"""Handles and the caller-owned input pool of one pipeline, as VQM's tests
+state them (tests/metrics/ssimulacra2/pipeline_test.cc:515-720): handles
+belong to the pipeline that made them, the pool's buffers have the exact
+size of their format and 64-byte aligned starts, a released span is reused
+first-fit, a pipeline holds at most 4095 live buffers, and a stale handle
+never matches a later buffer however many allocations come between.
+
+Moves (the C++ half of VQM's ownership test) are covered by the C++ facade,
+whose pipeline owns its handle through a unique_ptr.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from tests import helpers
+from tests.test_gpu_parity import _cudart
+from vqm_b200 import ss2
+
+pytestmark = pytest.mark.gpu
+
+BYTE_RGB = helpers.pinned_format(type=ss2.PixelType.Byte)
+
+
+def test_handles_belong_to_their_pipeline():
+    """pipeline_test.cc:515-546: a handle of one pipeline is rejected by
+    another, a foreign release is ignored, tokens are distinct and a foreign
+    token cannot be finished."""
+    o, d = helpers.gradient(0), helpers.gradient(1)
+    with ss2.Ssimulacra2Pipeline(o.width, o.height) as first, \
+            ss2.Ssimulacra2Pipeline(o.width, o.height) as second:
+        a, b = first.upload(o), second.upload(d)
+        assert a.slot != b.slot
+        with pytest.raises(ss2.InvalidArgument):
+            second.compute(a, b)
+        second.release(a)  # ignored: not this pipeline's handle
+        identity = second.compute(b, b).score()
+        token_a = first.submit(a, a)
+        token_b = second.submit(b, b)
+        assert token_a != token_b
+        with pytest.raises(ss2.InvalidArgument):
+            second.finish(token_a)
+        assert second.finish(token_b).score() == identity == 100.0
+        original_identity = first.finish(token_a).score()
+        assert first.compute(a, a).score() == original_identity == 100.0
+        with pytest.raises(ss2.InvalidArgument):
+            first.compute(b, b)
+        first.release(a)
+
+
+def test_input_pool_exact_size_and_ownership():
+    """pipeline_test.cc:567-611."""
+    w, h = 33, 17
+    nbytes = ss2.required_bytes(BYTE_RGB, w, h)
+    assert nbytes == 1692
+    with ss2.Ssimulacra2Pipeline(w, h, input_bytes=nbytes) as first, \
+            ss2.Ssimulacra2Pipeline(w, h, input_bytes=nbytes) as second:
+        a = first.allocate_image(BYTE_RGB)
+        b = second.allocate_image(BYTE_RGB)
+        assert a.bytes == nbytes and b.bytes == nbytes
+        assert a.slot != b.slot
+        assert first.map_image(a)
+        with pytest.raises(ss2.InvalidArgument):
+            second.map_image(a)
+        with pytest.raises(ss2.InvalidArgument):
+            second.submit(a, b)
+        second.release(a)  # ignored
+        assert second.map_image(b)
+        with pytest.raises(ss2.InvalidArgument):
+            first.allocate_image(BYTE_RGB)  # the pool holds one image
+        assert first.map_image(a)
+        first.release(a)
+        second.release(b)
+
+
+def test_input_handle_beyond_old_generation_limit():
+    """pipeline_test.cc:613-645: 2^20 allocations and releases later, the
+    first (released) handle still matches no buffer."""
+    with ss2.Ssimulacra2Pipeline(8, 8, gpu_resident_images=0, streaming_inputs=False,
+                                 input_bytes=ss2.required_bytes(BYTE_RGB, 8, 8)) as p:
+        stale = p.allocate_image(BYTE_RGB)
+        p.release(stale)
+        fmt = ctypes.byref(BYTE_RGB)
+        handle, size = ctypes.c_uint64(), ctypes.c_size_t()
+        allocate, release = ss2._lib.vqm_cu_ss2_allocate_image, ss2._lib.vqm_cu_ss2_release_image
+        n = 1 << 20
+        for i in range(n):
+            assert allocate(p._p, fmt, ctypes.byref(handle), ctypes.byref(size)) == 0
+            if i + 1 != n:
+                assert release(p._p, handle.value) == 0
+        current = ss2.ImageBuffer(handle.value, (8, 8), size.value)
+        assert current.slot != stale.slot
+        assert p.map_image(current)
+        with pytest.raises(ss2.InvalidArgument):
+            p.map_image(stale)
+        p.release(current)
+
+
+def test_input_pool_aligns_starts_and_reuses_gaps():
+    """pipeline_test.cc:647-682: the second buffer starts at the first's size
+    rounded up to 64 bytes; a released span is reused at the same address,
+    and the neighbour's bytes are left alone."""
+    w, h = 33, 17
+    nbytes = ss2.required_bytes(BYTE_RGB, w, h)
+    second_offset = (nbytes + 63) // 64 * 64
+    rt = _cudart()
+    with ss2.Ssimulacra2Pipeline(w, h, input_bytes=second_offset + nbytes) as p:
+        first = p.allocate_image(BYTE_RGB)
+        second = p.allocate_image(BYTE_RGB)
+        first_at, second_at = p.map_image(first), p.map_image(second)
+        assert second_at - first_at == second_offset
+        assert rt.cudaMemset(ctypes.c_void_p(second_at), 0x5A, ctypes.c_size_t(nbytes)) == 0
+        with pytest.raises(ss2.InvalidArgument):
+            p.allocate_image(BYTE_RGB)
+        p.release(first)
+        replacement = p.allocate_image(BYTE_RGB)
+        assert p.map_image(replacement) == first_at
+        back = np.zeros(nbytes, np.uint8)
+        assert rt.cudaMemcpy(ctypes.c_void_p(back.ctypes.data),
+                             ctypes.c_void_p(p.map_image(second)), ctypes.c_size_t(nbytes), 2) == 0
+        assert np.all(back == 0x5A)
+        p.release(replacement)
+        p.release(second)
+
+
+def test_input_handle_capacity():
+    """pipeline_test.cc:684-720: 4095 live buffers at most; a released
+    handle does not name its replacement."""
+    grey = BYTE_RGB.copy(family=ss2.ColorFamily.Grey, matrix=ss2.MatrixCoefficients.Unspecified)
+    nbytes = ss2.required_bytes(grey, 8, 8)
+    assert nbytes == 64
+    with ss2.Ssimulacra2Pipeline(8, 8, gpu_resident_images=0, streaming_inputs=False,
+                                 input_bytes=nbytes * 4096) as p:
+        buffers = [p.allocate_image(grey) for _ in range(4095)]
+        with pytest.raises(ss2.InvalidArgument):
+            p.allocate_image(grey)
+        old = buffers[1024]
+        p.release(old)
+        replacement = p.allocate_image(grey)
+        assert replacement.slot != old.slot
+        with pytest.raises(ss2.InvalidArgument):
+            p.map_image(old)
+        assert p.map_image(replacement)
