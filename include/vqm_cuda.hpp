@@ -504,10 +504,32 @@ public:
             batches_.emplace_back(b);
         }
     }
+    // A moved-from pool has no workers and refuses work (pool.cc:118-122).
+    Ssimulacra2Pool(Ssimulacra2Pool&& other) noexcept
+        : chroma_filter_(other.chroma_filter_),
+          chunk_(other.chunk_),
+          batches_(std::move(other.batches_)),
+          poisoned_(other.poisoned_) {
+        other.batches_.clear();
+        other.moved_from_ = true;
+    }
+    Ssimulacra2Pool& operator=(Ssimulacra2Pool&& other) noexcept {
+        if (this != &other) {
+            chroma_filter_ = other.chroma_filter_;
+            chunk_ = other.chunk_;
+            batches_ = std::move(other.batches_);
+            poisoned_ = other.poisoned_;
+            moved_from_ = other.moved_from_;
+            other.batches_.clear();
+            other.moved_from_ = true;
+        }
+        return *this;
+    }
     [[nodiscard]] std::size_t Workers() const noexcept { return batches_.size(); }
 
     [[nodiscard]] std::vector<Ssimulacra2Result> ComputeMany(std::span<const ImagePair> pairs,
                                                              float background = 0.5f) {
+        Ready();
         std::vector<vqm_cu_image> o, d;
         for (const auto& p : pairs) {
             o.push_back(detail::ToC(p.original, "original"));
@@ -517,6 +539,7 @@ public:
     }
     [[nodiscard]] std::vector<Ssimulacra2Result> ComputeMany(std::span<const ImageViewPair> pairs,
                                                              float background = 0.5f) {
+        Ready();
         std::vector<vqm_cu_image> o, d;
         for (const auto& p : pairs) {
             o.push_back(detail::ToC(p.original));
@@ -526,6 +549,7 @@ public:
     }
     [[nodiscard]] std::vector<Ssimulacra2Result> ComputeMany(std::span<const CudaBufferPair> pairs,
                                                              float background = 0.5f) {
+        Ready();
         std::vector<vqm_cu_image> o, d;
         for (const auto& p : pairs) {
             o.push_back(detail::ToC(p.original));
@@ -544,9 +568,13 @@ private:
     struct Deleter {
         void operator()(vqm_cu_ss2_batch* b) const noexcept { vqm_cu_ss2_batch_destroy(b); }
     };
+    void Ready() const {
+        if (moved_from_) throw std::logic_error("pool has been moved from");
+        if (poisoned_) throw std::logic_error("pool cannot be reused after a failed drain");
+    }
     std::vector<Ssimulacra2Result> Run(const std::vector<vqm_cu_image>& o,
                                        const std::vector<vqm_cu_image>& d, float background) {
-        if (poisoned_) throw std::logic_error("pool cannot be reused after a failed drain");
+        Ready();
         const std::size_t n = o.size();
         std::vector<Ssimulacra2Result> out(n);
         std::vector<std::pair<std::uint64_t, std::size_t>> pending(batches_.size(), {0, 0});
@@ -604,6 +632,7 @@ private:
     std::size_t chunk_;
     std::vector<std::unique_ptr<vqm_cu_ss2_batch, Deleter>> batches_;
     bool poisoned_ = false;
+    bool moved_from_ = false;
 };
 
 // ---- vqm_metrics.h (SSIMULACRA 2 only) ---------------------------------------

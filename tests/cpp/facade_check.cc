@@ -183,6 +183,26 @@ void Gpu() {
     const std::vector<v::ImagePair> pairs{{base, base}, {base, d1}, {base, d2}};
     const auto results = pool.ComputeMany(std::span<const v::ImagePair>(pairs));
     for (std::size_t i = 0; i < results.size(); ++i) Print("pool", static_cast<int>(i), results[i]);
+    // pool_test.cc:17-61: no workers is an error; an empty list gives no
+    // results; ScoreMany matches ComputeMany; a moved-from pool has no
+    // workers and refuses work, the pool it moved into keeps scoring.
+    ExpectThrow<std::invalid_argument>([&] { v::Ssimulacra2Pool none(config, 0); },
+                                       "pool of zero workers");
+    Expect(pool.ComputeMany(std::span<const v::ImagePair>{}).empty(), "empty list");
+    const auto scores = pool.ScoreMany(std::span<const v::ImagePair>(pairs));
+    for (std::size_t i = 0; i < pairs.size(); ++i)
+        Expect(scores[i] == results[i].Score(), "ScoreMany equals ComputeMany");
+    const std::span<const v::ImagePair> first_pair(pairs.data(), 1);
+    v::Ssimulacra2Pool moved(std::move(pool));
+    Expect(pool.Workers() == 0 && moved.Workers() == 2, "workers after a move");
+    ExpectThrow<std::logic_error>([&] { (void)pool.ScoreMany(first_pair); }, "moved-from pool");
+    Expect(moved.ScoreMany(first_pair)[0] == results[0].Score(), "moved pool scores");
+    v::Ssimulacra2Pool assigned(config, 1, 2);
+    assigned = std::move(moved);
+    Expect(assigned.Workers() == 2 && moved.Workers() == 0, "workers after assignment");
+    Expect(assigned.ScoreMany(first_pair)[0] == results[0].Score(), "assigned pool scores");
+    ExpectThrow<std::logic_error>([&] { (void)moved.ComputeMany(first_pair); },
+                                  "moved-from pool after assignment");
 
     // The opt-in recursive blur, through the pipeline and the pool.
     v::Ssimulacra2Config rec = config;

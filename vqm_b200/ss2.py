@@ -836,7 +836,7 @@ class Ssimulacra2Pool:
 
     def __init__(self, workers: int = 1, chunk: int = 64, chroma_filter: int = 0,
                  device: int = -1, half_planes: bool = False, blur: int = 0):
-        if workers == 0:
+        if workers < 1:
             raise InvalidArgument("pool needs at least one worker")
         self._chunk = max(1, chunk)
         self._batches = [Ssimulacra2Batch(max_pairs=self._chunk, chroma_filter=chroma_filter,
