@@ -467,6 +467,24 @@ private:
     std::unique_ptr<vqm_cu_ss2_pipeline, Deleter> p_;
 };
 
+// ---- vqm_alpha.h --------------------------------------------------------------
+
+// ComputeWorstBackground (include/vqm_alpha.h:12-28), the CLI's alpha policy
+// for callers: a pair with no alpha on either side is scored once at the
+// default background; otherwise it is scored over a dark (0.1) and a bright
+// (0.9) background and the lower score's result is returned. Frame is any
+// image kind the pipeline's Compute takes (Image, ImageView, CudaBufferView).
+template <typename Frame>
+[[nodiscard]] Ssimulacra2Result ComputeWorstBackground(Ssimulacra2Pipeline& pipeline,
+                                                       const Frame& original,
+                                                       const Frame& distorted) {
+    if (original.format.alpha == AlphaType::None && distorted.format.alpha == AlphaType::None)
+        return pipeline.Compute(original, distorted);
+    Ssimulacra2Result dark = pipeline.Compute(original, distorted, 0.1f);
+    Ssimulacra2Result bright = pipeline.Compute(original, distorted, 0.9f);
+    return bright.Score() < dark.Score() ? bright : dark;
+}
+
 // ---- vqm_pool.h ---------------------------------------------------------------
 
 struct ImagePair {

@@ -4,6 +4,7 @@
 //   facade_check gpu    scores the 32x32 gradient pairs (tests/support.h
 //                       MakeGradient) through Pipeline, Upload and Pool and
 //                       prints one JSON object per result on stdout
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -177,6 +178,20 @@ void Gpu() {
     (void)pipeline.Finish(token);
     ExpectThrow<std::invalid_argument>([&] { (void)pipeline.Submit(base, small); },
                                        "bad image once idle");
+    // vqm_alpha.h: an opaque pair once at the default background; with alpha
+    // on either side, the lower of the dark and bright scores.
+    const v::Image check = Gradient(1);
+    Expect(v::ComputeWorstBackground(pipeline, base, check).Score() ==
+               pipeline.Compute(base, check).Score(),
+           "worst background of an opaque pair");
+    v::Image translucent = Gradient(1);
+    translucent.format.alpha = v::AlphaType::Straight;
+    translucent.data.resize(4 * 32 * 32, 96);
+    const double dark = pipeline.Compute(base, translucent, 0.1f).Score();
+    const double bright = pipeline.Compute(base, translucent, 0.9f).Score();
+    Expect(dark != bright, "the background matters with alpha");
+    Expect(v::ComputeWorstBackground(pipeline, base, translucent).Score() == std::min(dark, bright),
+           "worst background with alpha on one side");
 
     v::Ssimulacra2Pool pool(config, 2, 2);
     const v::Image d1 = Gradient(1), d2 = Gradient(2);

@@ -551,6 +551,20 @@ class ImageBuffer:
     bytes: int
 
 
+def compute_worst_background(pipeline, original, distorted) -> "Ssimulacra2Result":
+    """ComputeWorstBackground (include/vqm_alpha.h:12-28): a pair with no
+    alpha on either side is scored once at the default background; otherwise
+    over a dark (0.1) and a bright (0.9) background, returning the result
+    with the lower score. `pipeline` is a Ssimulacra2Pipeline; the images are
+    any kind its compute takes."""
+    if (original.format.alpha == AlphaType.None_
+            and distorted.format.alpha == AlphaType.None_):
+        return pipeline.compute(original, distorted)
+    dark = pipeline.compute(original, distorted, 0.1)
+    bright = pipeline.compute(original, distorted, 0.9)
+    return bright if bright.score() < dark.score() else dark
+
+
 class Ssimulacra2Pipeline:
     """Ssimulacra2Pipeline (include/ssimulacra2.h:83-215) on a CUDA device."""
 
