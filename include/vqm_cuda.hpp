@@ -697,12 +697,14 @@ public:
     }
 
     [[nodiscard]] std::optional<MetricsResult> Compute(const Image& o, const Image& d) {
-        return Run([&] { return pipeline_->Compute(o, d, config_.background); }, o.size,
-                   o.format, d.size, d.format, true);
+        return Run([&] { return pipeline_->Compute(o, d, config_.background); },
+                   [&] { Storage(o, "original"), Storage(d, "distorted"); }, o.size, o.format,
+                   d.size, d.format, true);
     }
     [[nodiscard]] std::optional<MetricsResult> Compute(const ImageView& o, const ImageView& d) {
-        return Run([&] { return pipeline_->Compute(o, d, config_.background); }, o.size,
-                   o.format, d.size, d.format, true);
+        return Run([&] { return pipeline_->Compute(o, d, config_.background); },
+                   [&] { Storage(o, "original"), Storage(d, "distorted"); }, o.size, o.format,
+                   d.size, d.format, true);
     }
     // Tightly packed planes in the configured formats, exactly RequiredBytes
     // each.
@@ -714,8 +716,9 @@ public:
     }
     [[nodiscard]] std::optional<MetricsResult> Compute(const CudaBufferView& o,
                                                        const CudaBufferView& d) {
-        return Run([&] { return pipeline_->Compute(o, d, config_.background); }, o.size,
-                   o.format, d.size, d.format, false);
+        return Run([&] { return pipeline_->Compute(o, d, config_.background); },
+                   [&] { Storage(o, "original"), Storage(d, "distorted"); }, o.size, o.format,
+                   d.size, d.format, false);
     }
 
     [[nodiscard]] MetricsResult ComputeImage(const Image& o, const Image& d) {
@@ -759,9 +762,9 @@ private:
                a.depth == b.depth;
     }
     Image Packed(std::span<const std::byte> bytes, const ImageFormat& f, const char* name) const {
+        (void)name;
         if (bytes.size() != RequiredBytes(f, config_.size))
-            throw std::invalid_argument(std::string(name) +
-                                        ": data size does not match the image format");
+            throw std::invalid_argument("metrics: packed input has incorrect size");
         Image img;
         img.size = config_.size;
         img.format = f;
@@ -769,9 +772,19 @@ private:
         std::memcpy(img.data.data(), bytes.data(), bytes.size());
         return img;
     }
-    template <class F>
-    std::optional<MetricsResult> Run(F&& compute, Size os, const ImageFormat& of, Size ds,
-                                     const ImageFormat& df, bool host) {
+    // Checks of the inputs' storage (metrics.cc:46-58): made before the
+    // frame is attempted, so a rejected input does not fail the sequence.
+    static void Storage(const Image& img, const char* name) {
+        ValidateFormat(img.format, img.size, name);
+        (void)detail::ToC(img, name);
+    }
+    template <class View>
+    static void Storage(const View& v, const char* name) {
+        ValidateFormat(v.format, v.size, name);
+    }
+    template <class F, class S>
+    std::optional<MetricsResult> Run(F&& compute, S&& storage, Size os, const ImageFormat& of,
+                                     Size ds, const ImageFormat& df, bool host) {
         if (failed_) throw std::logic_error("metrics: previous call failed; call Reset");
         if (finished_) throw std::logic_error("metrics: sequence finished; call Reset");
         if (next_index_ == ~std::uint64_t{0})
@@ -780,6 +793,7 @@ private:
             throw std::invalid_argument("metrics: image size differs from configured size");
         if (!SameFormat(of, config_.original_format) || !SameFormat(df, config_.distorted_format))
             throw std::invalid_argument("metrics: image format differs from configured format");
+        storage();
         if (host && !config_.streaming_inputs)
             throw std::invalid_argument("metrics: streaming inputs are disabled");
         try {

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <span>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -148,6 +149,36 @@ void GpuMetrics() {
     grey.data.resize(32 * 32);
     ExpectThrow<std::invalid_argument>([&] { (void)metrics.Compute(grey, grey); },
                                        "format differs from configured");
+    // metrics_test.cc:439-475, 555-574: a rejected input does not consume a
+    // frame or fail the sequence; packed spans must have the exact size.
+    metrics.Reset();
+    v::Image wrong = Gradient(1);
+    wrong.format.transfer = v::TransferCharacteristics::Bt709;
+    ExpectThrow<std::invalid_argument>([&] { (void)metrics.Compute(base, wrong); },
+                                       "transfer differs from configured");
+    v::Image narrow = Gradient(1);
+    narrow.size.width -= 1;
+    ExpectThrow<std::invalid_argument>([&] { (void)metrics.Compute(base, narrow); },
+                                       "size differs from configured");
+    v::Image short_data = Gradient(1);
+    short_data.data.pop_back();
+    ExpectThrow<std::invalid_argument>([&] { (void)metrics.Compute(base, short_data); },
+                                       "short image data");
+    const auto frame0 = metrics.Compute(base, Gradient(1));
+    Expect(frame0 && frame0->frame_index == 0, "rejected inputs consume no frame");
+    metrics.Reset();
+    const v::Image d1 = Gradient(1);
+    const auto ob = std::as_bytes(std::span(base.data));
+    const auto db = std::as_bytes(std::span(d1.data));
+    ExpectThrow<std::invalid_argument>(
+        [&] { (void)metrics.Compute(ob.first(ob.size() - 1), db); }, "short packed original");
+    ExpectThrow<std::invalid_argument>(
+        [&] { (void)metrics.Compute(ob, db.first(db.size() - 1)); }, "short packed distorted");
+    const auto packed = metrics.ComputeImage(ob, db);
+    const auto image = metrics.ComputeImage(base, d1);
+    Expect(packed.frame_index == 0 && image.frame_index == 0 &&
+               *packed.ssimulacra2 == *image.ssimulacra2,
+           "packed spans and images agree");
 }
 
 void Gpu() {
