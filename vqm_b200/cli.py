@@ -1,12 +1,14 @@
-"""SSIMULACRA 2.1 of two Y4M sequences, frame by frame, on the GPU.
+"""SSIMULACRA 2.1 of two Y4M sequences or PNG/JPEG images, on the GPU.
 
     python -m vqm_b200.cli original.y4m distorted.y4m [--raw] [--json] [-v]
+    python -m vqm_b200.cli original.png distorted.png
 
 The sequence path of VQM's CLI for this metric (cli/video.cc:175-348,
 cli/report.cc:197-248, docs/ssimulacra2.md:3-6): both clips must have the
 same frame size, frame count and frame rate; every frame pair is scored
 independently and the clip score is the mean of the frame scores, printed
-with eight decimals as the last line. Inputs with alpha are scored over the
+with eight decimals as the last line. A PNG or JPEG file is a one-frame
+sequence without a frame rate (`stills.py`, VQM's still formats). Inputs with alpha are scored over the
 dark and bright backgrounds (0.1 and 0.9) and the worse score is kept
 (include/vqm_alpha.h:17-28). --raw prints each frame's 108 norms in the
 channel-major order of the reference tool's tuning build (report.cc:234-248)
@@ -35,30 +37,38 @@ import statistics
 import sys
 import time
 
-from . import replicas, ss2, y4m
+from . import replicas, ss2, stills, y4m
 
+# The names of VQM's --input-* flags (tools/image_io/io.cc:706-762).
 _MATRICES = {
     "rgb": ss2.MatrixCoefficients.Rgb, "bt709": ss2.MatrixCoefficients.Bt709,
     "fcc": ss2.MatrixCoefficients.Fcc, "bt470bg": ss2.MatrixCoefficients.Bt470Bg,
-    "smpte170m": ss2.MatrixCoefficients.St170M, "smpte240m": ss2.MatrixCoefficients.St240M,
-    "ycgco": ss2.MatrixCoefficients.YCgCo, "bt2020nc": ss2.MatrixCoefficients.Bt2020Ncl,
-    "bt2020c": ss2.MatrixCoefficients.Bt2020Cl, "ictcp": ss2.MatrixCoefficients.Bt2100ICtCp,
+    "st170m": ss2.MatrixCoefficients.St170M, "st240m": ss2.MatrixCoefficients.St240M,
+    "ycgco": ss2.MatrixCoefficients.YCgCo, "bt2020ncl": ss2.MatrixCoefficients.Bt2020Ncl,
+    "bt2020cl": ss2.MatrixCoefficients.Bt2020Cl,
+    "chromaticity-derived-ncl": ss2.MatrixCoefficients.ChromaticityDerivedNcl,
+    "chromaticity-derived-cl": ss2.MatrixCoefficients.ChromaticityDerivedCl,
+    "ictcp": ss2.MatrixCoefficients.Bt2100ICtCp,
 }
 _TRANSFERS = {
-    "bt709": ss2.TransferCharacteristics.Bt709, "bt470m": ss2.TransferCharacteristics.Bt470M,
-    "bt470bg": ss2.TransferCharacteristics.Bt470Bg, "smpte170m": ss2.TransferCharacteristics.Bt601,
-    "smpte240m": ss2.TransferCharacteristics.St240M, "linear": ss2.TransferCharacteristics.Linear,
-    "srgb": ss2.TransferCharacteristics.Srgb, "bt2020-10": ss2.TransferCharacteristics.Bt2020_10,
+    "bt709": ss2.TransferCharacteristics.Bt709, "bt601": ss2.TransferCharacteristics.Bt601,
+    "bt470m": ss2.TransferCharacteristics.Bt470M, "bt470bg": ss2.TransferCharacteristics.Bt470Bg,
+    "st240m": ss2.TransferCharacteristics.St240M, "linear": ss2.TransferCharacteristics.Linear,
+    "log100": ss2.TransferCharacteristics.Log100, "log316": ss2.TransferCharacteristics.Log316,
+    "xvycc": ss2.TransferCharacteristics.Iec61966_2_4,
+    "bt1361": ss2.TransferCharacteristics.Bt1361, "srgb": ss2.TransferCharacteristics.Srgb,
+    "bt2020-10": ss2.TransferCharacteristics.Bt2020_10,
     "bt2020-12": ss2.TransferCharacteristics.Bt2020_12,
-    "smpte2084": ss2.TransferCharacteristics.St2084,
-    "arib-std-b67": ss2.TransferCharacteristics.AribB67,
+    "st2084": ss2.TransferCharacteristics.St2084, "st428": ss2.TransferCharacteristics.St428,
+    "arib-b67": ss2.TransferCharacteristics.AribB67,
 }
 _PRIMARIES = {
     "bt709": ss2.ColorPrimaries.Bt709, "bt470m": ss2.ColorPrimaries.Bt470M,
-    "bt470bg": ss2.ColorPrimaries.Bt470Bg, "smpte170m": ss2.ColorPrimaries.St170M,
-    "smpte240m": ss2.ColorPrimaries.St240M, "film": ss2.ColorPrimaries.Film,
-    "bt2020": ss2.ColorPrimaries.Bt2020, "smpte431": ss2.ColorPrimaries.St431_2,
-    "smpte432": ss2.ColorPrimaries.St432_1,
+    "bt470bg": ss2.ColorPrimaries.Bt470Bg, "st170m": ss2.ColorPrimaries.St170M,
+    "st240m": ss2.ColorPrimaries.St240M, "film": ss2.ColorPrimaries.Film,
+    "bt2020": ss2.ColorPrimaries.Bt2020, "st428": ss2.ColorPrimaries.St428,
+    "st431-2": ss2.ColorPrimaries.St431_2, "st432-1": ss2.ColorPrimaries.St432_1,
+    "ebu3213e": ss2.ColorPrimaries.Ebu3213E,
 }
 _FILTERS = {"bilinear": 0, "bicubic": 1, "lanczos": 2}
 _BLURS = {"sampled": ss2.Ssimulacra2Blur.SAMPLED, "recursive": ss2.Ssimulacra2Blur.RECURSIVE}
@@ -160,7 +170,12 @@ def run(argv=None, out=sys.stdout) -> int:
         # One GPU per rank; ranks beyond the GPU count share them (their
         # work is independent).
         device = int(os.environ.get("LOCAL_RANK", str(rank))) % max(1, torch.cuda.device_count())
-    ro, rd = y4m.Reader(args.original), y4m.Reader(args.distorted)
+    ro = stills.open_sequence(args.original)
+    try:
+        rd = stills.open_sequence(args.distorted)
+    except Exception:
+        ro.close()
+        raise
     try:
         ho, hd = ro.header, rd.header
         if (ho.width, ho.height) != (hd.width, hd.height):
