@@ -106,7 +106,8 @@ typedef struct vqm_cu_ss2_config {
 typedef struct vqm_cu_memory_usage {
     uint64_t pyramid_bytes;  /* XYB planes */
     uint64_t resident_bytes; /* upload() slots */
-    uint64_t input_bytes;    /* allocate_image() pool + streaming inputs */
+    uint64_t input_bytes;    /* allocate_image() pool (pinned host memory)
+                                + streaming inputs (device) */
     uint64_t scratch_bytes;  /* partials, tables, counters */
     uint64_t total_bytes;
 } vqm_cu_memory_usage;
@@ -221,14 +222,16 @@ int vqm_cu_ss2_upload(vqm_cu_ss2_pipeline* pipeline, const vqm_cu_image* image,
  * handles are ignored. */
 int vqm_cu_ss2_release(vqm_cu_ss2_pipeline* pipeline, uint64_t handle);
 /* AllocateImage / MapImage / Release(ImageBuffer) (ssimulacra2.h:161-176):
- * device memory carved from config.input_bytes, RequiredBytes(format) long,
- * 64-byte aligned, in vqm::Image's packed layout. *device_ptr is a CUDA
- * device address the caller fills (cudaMemcpy or its own kernels). */
+ * spans of a pinned host pool of config.input_bytes, RequiredBytes(format)
+ * long, 64-byte aligned, in vqm::Image's packed layout. *host_ptr is a host
+ * address the caller writes (memcpy, as into VQM's mapped arena, or
+ * cudaMemcpy with cudaMemcpyDefault); the prepare kernels read the span in
+ * place over the bus (unified addressing), so nothing is copied at submit. */
 int vqm_cu_ss2_allocate_image(vqm_cu_ss2_pipeline* pipeline,
                               const vqm_cu_format* format, uint64_t* handle,
                               size_t* bytes);
 int vqm_cu_ss2_map_image(vqm_cu_ss2_pipeline* pipeline, uint64_t handle,
-                         void** device_ptr);
+                         void** host_ptr);
 int vqm_cu_ss2_release_image(vqm_cu_ss2_pipeline* pipeline, uint64_t handle);
 /* GetMemoryUsage (ssimulacra2.h:204-205). */
 int vqm_cu_ss2_memory_usage(vqm_cu_ss2_pipeline* pipeline,

@@ -416,11 +416,12 @@ public:
         detail::Check(vqm_cu_ss2_allocate_image(p_.get(), &f, &handle, &bytes));
         return ImageBuffer{handle, config_.size, bytes};
     }
-    // A CUDA device address (fill it with cudaMemcpy or a kernel).
-    [[nodiscard]] void* MapImage(ImageBuffer buffer) {
+    // The buffer's bytes in pinned host memory, written with memcpy as in
+    // VQM (ssimulacra2.h:174-176) and read by the kernels in place.
+    [[nodiscard]] std::byte* MapImage(ImageBuffer buffer) {
         void* ptr = nullptr;
         detail::Check(vqm_cu_ss2_map_image(p_.get(), buffer.slot, &ptr));
-        return ptr;
+        return static_cast<std::byte*>(ptr);
     }
     void Release(ImageBuffer buffer) {
         detail::Check(vqm_cu_ss2_release_image(p_.get(), buffer.slot));

@@ -224,6 +224,39 @@ void Gpu() {
     Expect(v::ComputeWorstBackground(pipeline, base, translucent).Score() == std::min(dark, bright),
            "worst background with alpha on one side");
 
+    {
+        // pipeline_test.cc:179-216: caller-owned buffers written through
+        // the mapping score like the packed images; while a submission is
+        // in flight the pool cannot change; two buffers fill this pool.
+        v::Ssimulacra2Config owned = config;
+        const std::size_t per_image = v::RequiredBytes(base.format, base.size);
+        owned.input_bytes = 2 * per_image;
+        v::Ssimulacra2Pipeline p(owned);
+        const v::Image dist = Gradient(2);
+        const double expected = p.Compute(base, dist).Score();
+        const v::ImageBuffer a = p.AllocateImage(base.format);
+        const v::ImageBuffer b = p.AllocateImage(dist.format);
+        Expect(a.bytes == per_image && b.bytes == per_image, "buffer sizes");
+        std::memcpy(p.MapImage(a), base.data.data(), base.data.size());
+        std::memcpy(p.MapImage(b), dist.data.data(), dist.data.size());
+        Expect(p.Compute(a, b).Score() == expected, "caller-owned buffers");
+        const std::uint64_t token = p.Submit(a, b);
+        ExpectThrow<std::logic_error>([&] { p.Release(a); }, "Release in flight");
+        ExpectThrow<std::logic_error>([&] { (void)p.MapImage(a); }, "MapImage in flight");
+        ExpectThrow<std::logic_error>([&] { (void)p.AllocateImage(base.format); },
+                                      "AllocateImage in flight");
+        Expect(p.Finish(token).Score() == expected, "submitted buffers");
+        p.Release(a);
+        ExpectThrow<std::invalid_argument>([&] { (void)p.Compute(a, b); }, "released buffer");
+        p.Release(b);
+        const v::ImageBuffer c = p.AllocateImage(base.format);
+        const v::ImageBuffer d = p.AllocateImage(base.format);
+        ExpectThrow<std::invalid_argument>([&] { (void)p.AllocateImage(base.format); },
+                                           "a third buffer");
+        p.Release(c);
+        p.Release(d);
+    }
+
     v::Ssimulacra2Pool pool(config, 2, 2);
     const v::Image d1 = Gradient(1), d2 = Gradient(2);
     const std::vector<v::ImagePair> pairs{{base, base}, {base, d1}, {base, d2}};

@@ -695,11 +695,16 @@ def test_device_buffers_and_caller_pool():
         assert a.bytes == nbytes and b.bytes == nbytes
         with pytest.raises(ss2.InvalidArgument):
             p.allocate_image(o.format)  # pool full
-        rt = _cudart()
-        for buf, t in ((a, to), (b, td)):
-            assert rt.cudaMemcpy(ctypes.c_void_p(p.map_image(buf)), ctypes.c_void_p(t.data_ptr()),
-                                 ctypes.c_size_t(nbytes), 3) == 0
+        # Written like VQM's mapped arena: a host copy into the mapping.
+        for buf, img in ((a, o), (b, d)):
+            ctypes.memmove(p.map_image(buf), img.data.ctypes.data, nbytes)
         assert np.array_equal(p.compute(a, b).norms, want.norms)
+        # Or by the copy engine from device memory (unified addressing).
+        rt = _cudart()
+        for buf, t in ((a, td), (b, to)):
+            assert rt.cudaMemcpy(ctypes.c_void_p(p.map_image(buf)), ctypes.c_void_p(t.data_ptr()),
+                                 ctypes.c_size_t(nbytes), 4) == 0
+        assert np.array_equal(p.compute(b, a).norms, want.norms)
         tok = p.submit(a, b)
         with pytest.raises(ss2.LogicError):
             p.release(a)

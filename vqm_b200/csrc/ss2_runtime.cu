@@ -163,6 +163,7 @@ public:
     }
     template <class T>
     T* as() const { return static_cast<T*>(ptr_); }
+    size_t bytes() const { return bytes_; }
 
 private:
     void* ptr_ = nullptr;
@@ -1016,7 +1017,10 @@ private:
     Tables tables_;
     BatchMemory mem_;
     DeviceBuffer stream_in_[2];
-    DeviceBuffer pool_;
+    // The AllocateImage pool: pinned host memory the caller writes through
+    // MapImage (as into VQM's host-visible arena) and the prepare kernels
+    // read in place over the bus (unified addressing maps it on the device).
+    PinnedBuffer pool_;
     std::vector<Slot> slots_;
     std::vector<InputAlloc> inputs_;
     bool in_flight_ = false;

@@ -672,7 +672,9 @@ class Ssimulacra2Pipeline:
         return ImageBuffer(h.value, self.size, b.value)
 
     def map_image(self, buffer: ImageBuffer) -> int:
-        """Device address of the buffer (fill it with cudaMemcpy or a kernel)."""
+        """Host address of the buffer's bytes in the pinned pool: write them
+        (ctypes.memmove, or cudaMemcpy with cudaMemcpyDefault) before the
+        submission; the kernels read them in place."""
         ptr = ctypes.c_void_p()
         _check(_lib.vqm_cu_ss2_map_image(self._p, buffer.slot, ctypes.byref(ptr)))
         return ptr.value
