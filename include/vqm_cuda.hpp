@@ -184,7 +184,32 @@ inline void ValidateFormat(const ImageFormat& format, Size size, const char* nam
 
 namespace detail {
 
-// Plane addresses of a packed Image (input.cc:114-145 layout).
+// Plane p of vqm::Image's packed layout (input.cc:114-145): whether it is
+// present, its offset, samples per row and rows, and bytes per sample.
+struct PlaneGeometry {
+    bool present = false;
+    std::size_t offset = 0, width = 0, height = 0, sample_bytes = 0;
+};
+inline std::array<PlaneGeometry, 4> Layout(const ImageFormat& f, Size size) {
+    std::array<PlaneGeometry, 4> out{};
+    const std::size_t sb = f.type == PixelType::Byte ? 1 : f.type == PixelType::Float ? 4 : 2;
+    std::size_t cursor = 0;
+    for (int p = 0; p < 4; ++p) {
+        const bool chroma = p == 1 || p == 2;
+        PlaneGeometry& g = out[p];
+        g.present = p == 0 || (chroma && f.family != ColorFamily::Grey) ||
+                    (p == 3 && f.alpha != AlphaType::None);
+        if (!g.present) continue;
+        g.width = chroma ? size.width >> f.subsample_w : size.width;
+        g.height = chroma ? size.height >> f.subsample_h : size.height;
+        g.sample_bytes = sb;
+        g.offset = cursor;
+        cursor = (cursor + g.width * g.height * sb + 3) / 4 * 4;
+    }
+    return out;
+}
+
+// Plane addresses of a packed Image.
 inline vqm_cu_image ToC(const Image& img, const char* name) {
     const std::size_t expected = RequiredBytes(img.format, img.size);
     if (img.data.size() != expected)
@@ -196,24 +221,36 @@ inline vqm_cu_image ToC(const Image& img, const char* name) {
     c.height = Dim(img.size.height);
     c.format = ToC(img.format);
     c.memory = VQM_CU_MEMORY_HOST;
-    const std::size_t sb = img.format.type == PixelType::Byte ? 1
-                         : img.format.type == PixelType::Float ? 4 : 2;
-    const std::size_t cw = img.size.width >> img.format.subsample_w;
-    const std::size_t ch = img.size.height >> img.format.subsample_h;
-    std::size_t cursor = 0;
-    for (int p = 0; p < 4; ++p) {
-        const bool chroma = p == 1 || p == 2;
-        const bool present = p == 0 || (chroma && img.format.family != ColorFamily::Grey) ||
-                             (p == 3 && img.format.alpha != AlphaType::None);
-        if (!present) continue;
-        c.planes[p] = img.data.data() + cursor;
-        const std::size_t n = chroma ? cw * ch : img.size.width * img.size.height;
-        cursor = (cursor + n * sb + 3) / 4 * 4;
-    }
+    const auto layout = Layout(img.format, img.size);
+    for (int p = 0; p < 4; ++p)
+        if (layout[p].present) c.planes[p] = img.data.data() + layout[p].offset;
     return c;
 }
 
+// DescribeImageView (src/image_view.cc:16-45): a non-empty size, a valid
+// format, and every present plane with data and a stride of at least a row.
+inline std::array<PlaneGeometry, 4> CheckView(const ImageView& v) {
+    if (v.size.width == 0 || v.size.height == 0)
+        throw std::invalid_argument("image view: size must be non-zero");
+    const vqm_cu_format f = ToC(v.format);
+    Check(vqm_cu_validate_format(&f, Dim(v.size.width), Dim(v.size.height), "image view"));
+    const auto layout = Layout(v.format, v.size);
+    for (int p = 0; p < 4; ++p) {
+        const PlaneGeometry& g = layout[p];
+        if (!g.present) continue;
+        const std::size_t row = g.width * g.sample_bytes;
+        if (v.planes[p].data == nullptr || v.planes[p].stride_bytes < row)
+            throw std::invalid_argument("image view: missing plane or short stride");
+        const auto max_offset = static_cast<std::size_t>(PTRDIFF_MAX);
+        if (row > max_offset ||
+            (g.height > 1 && v.planes[p].stride_bytes > (max_offset - row) / (g.height - 1)))
+            throw std::overflow_error("image view: plane stride is too large");
+    }
+    return layout;
+}
+
 inline vqm_cu_image ToC(const ImageView& v) {
+    (void)CheckView(v);
     vqm_cu_image c{};
     c.width = Dim(v.size.width);
     c.height = Dim(v.size.height);
@@ -350,7 +387,12 @@ public:
     }
     [[nodiscard]] std::uint64_t Submit(const ImageView& o, const ImageView& d,
                                        float background = 0.5f) {
-        return SubmitC(detail::ToC(o), detail::ToC(d), background);
+        vqm_cu_image a{}, b{};
+        IdleFirst([&] {
+            a = detail::ToC(o);
+            b = detail::ToC(d);
+        });
+        return SubmitC(a, b, background);
     }
     [[nodiscard]] std::uint64_t Submit(const UploadedImage& o, const UploadedImage& d,
                                        float background = 0.5f) {
@@ -467,6 +509,36 @@ private:
     Ssimulacra2Config config_;
     std::unique_ptr<vqm_cu_ss2_pipeline, Deleter> p_;
 };
+
+// ---- vqm_views.h helpers --------------------------------------------------------
+
+// CopyImage (include/vqm_views.h:36, src/image_view.cc:82-90): the view's
+// planes packed into a vqm::Image, each plane's trailing bytes up to a 4-byte
+// boundary zero.
+[[nodiscard]] inline Image CopyImage(const ImageView& view) {
+    const auto layout = detail::CheckView(view);
+    Image image;
+    image.size = view.size;
+    image.format = view.format;
+    image.data.assign(RequiredBytes(view.format, view.size), 0);
+    for (int p = 0; p < 4; ++p) {
+        const auto& g = layout[p];
+        if (!g.present) continue;
+        const std::size_t row = g.width * g.sample_bytes;
+        for (std::size_t y = 0; y < g.height; ++y)
+            std::memcpy(image.data.data() + g.offset + y * row,
+                        view.planes[p].data + y * view.planes[p].stride_bytes, row);
+    }
+    return image;
+}
+
+// Score (include/vqm_views.h:37-41, src/image_view.cc:92-100).
+[[nodiscard]] inline double Score(Ssimulacra2Pipeline& pipeline, const ImageView& original,
+                                  const ImageView& distorted, float background = 0.5f) {
+    if (!(original.size == distorted.size))
+        throw std::invalid_argument("image views must have the same size");
+    return pipeline.Compute(original, distorted, background).Score();
+}
 
 // ---- vqm_alpha.h --------------------------------------------------------------
 
@@ -779,8 +851,8 @@ private:
         ValidateFormat(img.format, img.size, name);
         (void)detail::ToC(img, name);
     }
-    template <class View>
-    static void Storage(const View& v, const char* name) {
+    static void Storage(const ImageView& v, const char*) { (void)detail::CheckView(v); }
+    static void Storage(const CudaBufferView& v, const char* name) {
         ValidateFormat(v.format, v.size, name);
     }
     template <class F, class S>

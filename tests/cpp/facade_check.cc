@@ -5,6 +5,7 @@
 //                       MakeGradient) through Pipeline, Upload and Pool and
 //                       prints one JSON object per result on stdout
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -82,7 +83,63 @@ void Print(const char* path, int variant, const v::Ssimulacra2Result& r) {
     std::printf("]}\n");
 }
 
+// image_view_test.cc:17-83: CopyImage packs padded planes, each plane's
+// tail zero up to a 4-byte boundary.
+void Views() {
+    std::array<std::array<std::byte, 10>, 3> planes{};
+    for (std::size_t p = 0; p < 3; ++p)
+        for (std::size_t y = 0; y < 2; ++y)
+            for (std::size_t x = 0; x < 3; ++x)
+                planes[p][y * 5 + x] = static_cast<std::byte>(p * 20 + y * 3 + x + 1);
+    v::ImageView view;
+    view.size = {3, 2};
+    view.format = Srgb8();
+    for (std::size_t p = 0; p < 3; ++p) view.planes[p] = {planes[p].data(), 5};
+    const v::Image image = v::CopyImage(view);
+    Expect(image.size == view.size &&
+               image.data == std::vector<std::uint8_t>({1, 2, 3, 4, 5, 6, 0, 0, 21, 22, 23, 24,
+                                                        25, 26, 0, 0, 41, 42, 43, 44, 45, 46,
+                                                        0, 0}),
+           "CopyImage of padded planes");
+    std::array<std::byte, 24> y{}, alpha{};
+    std::array<std::byte, 8> u{}, w{};
+    for (std::size_t r = 0; r < 4; ++r)
+        for (std::size_t c = 0; c < 4; ++c) {
+            y[r * 6 + c] = static_cast<std::byte>(r * 4 + c);
+            alpha[r * 6 + c] = static_cast<std::byte>(200 + r * 4 + c);
+        }
+    for (std::size_t r = 0; r < 2; ++r)
+        for (std::size_t c = 0; c < 2; ++c) {
+            u[r * 4 + c] = static_cast<std::byte>(30 + r * 2 + c);
+            w[r * 4 + c] = static_cast<std::byte>(60 + r * 2 + c);
+        }
+    v::ImageView yuv;
+    yuv.size = {4, 4};
+    yuv.format.type = v::PixelType::Byte;
+    yuv.format.family = v::ColorFamily::Yuv;
+    yuv.format.alpha = v::AlphaType::Straight;
+    yuv.format.matrix = v::MatrixCoefficients::Bt709;
+    yuv.format.subsample_w = yuv.format.subsample_h = 1;
+    yuv.planes = {{{y.data(), 6}, {u.data(), 4}, {w.data(), 4}, {alpha.data(), 6}}};
+    std::vector<std::uint8_t> want;
+    for (int i = 0; i < 16; ++i) want.push_back(static_cast<std::uint8_t>(i));
+    for (int i : {30, 31, 32, 33, 60, 61, 62, 63}) want.push_back(static_cast<std::uint8_t>(i));
+    for (int i = 0; i < 16; ++i) want.push_back(static_cast<std::uint8_t>(200 + i));
+    Expect(v::CopyImage(yuv).data == want, "CopyImage of subsampled planes and alpha");
+    v::ImageView short_stride = view;
+    short_stride.planes[1].stride_bytes = 2;
+    ExpectThrow<std::invalid_argument>([&] { (void)v::CopyImage(short_stride); },
+                                       "a short stride");
+    v::ImageView missing = view;
+    missing.planes[2].data = nullptr;
+    ExpectThrow<std::invalid_argument>([&] { (void)v::CopyImage(missing); }, "a missing plane");
+    v::ImageView empty = view;
+    empty.size = {0, 2};
+    ExpectThrow<std::invalid_argument>([&] { (void)v::CopyImage(empty); }, "an empty view");
+}
+
 void Host() {
+    Views();
     Expect(v::RequiredBytes(Srgb8(), {32, 32}) == 3 * 32 * 32, "RequiredBytes srgb8");
     v::ImageFormat yuv;
     yuv.type = v::PixelType::Word;
@@ -255,6 +312,45 @@ void Gpu() {
                                            "a third buffer");
         p.Release(c);
         p.Release(d);
+    }
+
+    {
+        // vqm_views.h Score, and padded views through the pool with one
+        // invalid view in the list (pool_test.cc:112-182).
+        const v::Image dist = Gradient(2);
+        std::array<std::vector<std::byte>, 3> ob, db;
+        const auto padded = [](const v::Image& img, std::array<std::vector<std::byte>, 3>& st) {
+            v::ImageView view;
+            view.size = img.size;
+            view.format = img.format;
+            for (std::size_t p = 0; p < 3; ++p) {
+                st[p].assign(39 * 32, std::byte{0});
+                for (std::size_t r = 0; r < 32; ++r)
+                    std::memcpy(st[p].data() + r * 39, img.data.data() + p * 1024 + r * 32, 32);
+                view.planes[p] = {st[p].data(), 39};
+            }
+            return view;
+        };
+        const v::ImageView vo = padded(base, ob), vd = padded(dist, db);
+        const double expected = pipeline.Compute(base, dist).Score();
+        Expect(v::Score(pipeline, vo, vd) == expected, "Score of padded views");
+        v::ImageView other = vd;
+        other.size = {16, 16};
+        ExpectThrow<std::invalid_argument>([&] { (void)v::Score(pipeline, vo, other); },
+                                           "views of different sizes");
+        v::Ssimulacra2Pool views(config, 2, 1);
+        const std::vector<v::ImageViewPair> vp{{vo, vd}, {vd, vo}};
+        const auto scores = views.ScoreMany(std::span<const v::ImageViewPair>(vp));
+        Expect(scores[0] == expected && scores[1] == pipeline.Compute(dist, base).Score(),
+               "pool of padded views");
+        v::ImageView invalid = vd;
+        invalid.planes[0].stride_bytes = 1;
+        const std::vector<v::ImageViewPair> bad{{vo, vd}, {vd, vo}, {vo, invalid}};
+        ExpectThrow<std::invalid_argument>(
+            [&] { (void)views.ComputeMany(std::span<const v::ImageViewPair>(bad)); },
+            "an invalid view in a pool list");
+        Expect(views.ScoreMany(std::span<const v::ImageViewPair>(vp).first(1))[0] == expected,
+               "the pool after an invalid view");
     }
 
     v::Ssimulacra2Pool pool(config, 2, 2);
