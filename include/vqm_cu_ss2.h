@@ -122,6 +122,19 @@ const char* vqm_cu_last_error(void);
 /* ABI version: (major << 16) | minor. */
 uint32_t vqm_cu_version(void);
 
+/* ---- devices (include/vqm_device.h) --------------------------------- */
+
+/* ListDevices: the CUDA devices in ordinal order. vqm_cu_device_info fills
+ * device `index`'s name (NUL-terminated, cut to name_bytes), its 16-byte
+ * UUID and its kind as VQM's DeviceType (1 integrated, 2 discrete GPU). */
+int vqm_cu_device_count(uint32_t* count);
+int vqm_cu_device_info(uint32_t index, char* name, size_t name_bytes,
+                       uint8_t* uuid16, uint32_t* type);
+/* SetDefaultDevice: from now on, process-wide, a config whose device is -1
+ * uses the device with this UUID (before any call, -1 is the calling
+ * thread's current device). VQM_CU_INVALID_ARGUMENT for an unknown UUID. */
+int vqm_cu_set_default_device(const uint8_t* uuid16);
+
 /* ---- formats (src/input.cc) ----------------------------------------- */
 
 /* RequiredBytes (include/vqm_image.h:360-363; src/input.cc:244-255). */

@@ -510,6 +510,37 @@ private:
     std::unique_ptr<vqm_cu_ss2_pipeline, Deleter> p_;
 };
 
+// ---- vqm_device.h -------------------------------------------------------------
+
+using DeviceUuid = std::array<std::uint8_t, 16>;
+enum class DeviceType { Other, IntegratedGpu, DiscreteGpu, VirtualGpu, Cpu };
+struct DeviceInfo {
+    DeviceUuid uuid;
+    std::string name;
+    DeviceType type;
+};
+
+// ListDevices / SetDefaultDevice (include/vqm_device.h): CUDA devices in
+// ordinal order; the default device is the one a config's device = -1 uses.
+[[nodiscard]] inline std::vector<DeviceInfo> ListDevices() {
+    std::uint32_t n = 0;
+    detail::Check(vqm_cu_device_count(&n));
+    std::vector<DeviceInfo> out;
+    for (std::uint32_t i = 0; i < n; ++i) {
+        char name[256];
+        DeviceInfo d{};
+        std::uint32_t type = 0;
+        detail::Check(vqm_cu_device_info(i, name, sizeof(name), d.uuid.data(), &type));
+        d.name = name;
+        d.type = static_cast<DeviceType>(type);
+        out.push_back(std::move(d));
+    }
+    return out;
+}
+inline void SetDefaultDevice(const DeviceUuid& uuid) {
+    detail::Check(vqm_cu_set_default_device(uuid.data()));
+}
+
 // ---- vqm_views.h helpers --------------------------------------------------------
 
 // CopyImage (include/vqm_views.h:36, src/image_view.cc:82-90): the view's

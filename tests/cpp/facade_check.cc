@@ -239,6 +239,13 @@ void GpuMetrics() {
 }
 
 void Gpu() {
+    // vqm_device.h: the devices, and the default device by UUID.
+    const auto devices = v::ListDevices();
+    Expect(!devices.empty() && !devices[0].name.empty(), "ListDevices");
+    if (!devices.empty()) v::SetDefaultDevice(devices[0].uuid);
+    v::DeviceUuid unknown{};
+    unknown.fill(0xEE);
+    ExpectThrow<std::invalid_argument>([&] { v::SetDefaultDevice(unknown); }, "an unknown UUID");
     v::Ssimulacra2Config config;
     config.size = {32, 32};
     v::Ssimulacra2Pipeline pipeline(config);

@@ -137,3 +137,17 @@ def test_input_handle_capacity():
         with pytest.raises(ss2.InvalidArgument):
             p.map_image(old)
         assert p.map_image(replacement)
+
+
+def test_devices_and_default_device():
+    """vqm_device.h: ListDevices gives each CUDA device's name, UUID and kind;
+    SetDefaultDevice makes a config's device -1 that device; an unknown UUID
+    is rejected."""
+    devices = ss2.list_devices()
+    assert devices and all(len(d.uuid) == 16 and d.name for d in devices)
+    assert devices[0].type in (1, 2)
+    ss2.set_default_device(devices[0].uuid)
+    with ss2.Ssimulacra2Pipeline(32, 32) as p:
+        assert p.compute(helpers.gradient(0), helpers.gradient(0)).score() == 100.0
+    with pytest.raises(ss2.InvalidArgument, match="device UUID"):
+        ss2.set_default_device(bytes(16) if devices[0].uuid != bytes(16) else b"\xff" * 16)

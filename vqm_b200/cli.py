@@ -311,25 +311,19 @@ def read_pairs(path):
 
 
 def list_devices(out) -> None:
-    """One line per CUDA device: index, name, kind and UUID (VQM's
-    --list-devices lists Vulkan devices the same way, cli/main.cc:71-88)."""
-    import torch
-    n = torch.cuda.device_count() if torch.cuda.is_available() else 0
-    if not n:
+    """One line per CUDA device: index, name, kind and UUID, as VQM's
+    --list-devices lists its Vulkan devices (cli/main.cc:71-88)."""
+    devices = ss2.list_devices()
+    if not devices:
         print("No CUDA devices found.", file=out)
         return
-    for i in range(n):
-        props = torch.cuda.get_device_properties(i)
-        text = str(props.uuid)
-        digits = "".join(c for c in (text[4:] if text.startswith("GPU-") else text)
-                         if c in "0123456789abcdef")
-        uuid = "-".join((digits[:8], digits[8:12], digits[12:16], digits[16:20], digits[20:32]))
-        print(f"{i}  {props.name}  (discrete GPU)  {uuid}", file=out)
+    kinds = {1: "integrated GPU", 2: "discrete GPU"}
+    for i, d in enumerate(devices):
+        print(f"{i}  {d.name}  ({kinds.get(d.type, 'other')})  {d.uuid_text()}", file=out)
 
 
 def _device_count() -> int:
-    import torch
-    return torch.cuda.device_count() if torch.cuda.is_available() else 0
+    return len(ss2.list_devices())
 
 
 # ---- scoring (cli/video.cc:419-506) -------------------------------------------

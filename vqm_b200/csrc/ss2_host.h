@@ -59,5 +59,8 @@ double Score(const double* norms, int scales);
 
 // Sets the calling thread's vqm_cu_last_error() message.
 void SetLastErrorMessage(const char* message);
+// A config's device ordinal: `requested` when >= 0, else the default device
+// vqm_cu_set_default_device chose, else the thread's current device.
+int ResolveDeviceOrdinal(int32_t requested);
 
 }  // namespace vqm_b200

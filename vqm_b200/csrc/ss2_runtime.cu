@@ -79,12 +79,17 @@ void EnsureDevice(int device) {
     ready[device] = true;
 }
 
+// The device a config's device = -1 names once SetDefaultDevice chose one
+// (process-wide, as VQM's default device is); -1: the thread's current one.
+std::atomic<int> g_default_device{-1};
+
 int ResolveDevice(int32_t requested) {
     int count = 0;
     const cudaError_t e = cudaGetDeviceCount(&count);
     if (e != cudaSuccess || count == 0)
         throw std::runtime_error("cuda: no usable compute device");
     int device = requested;
+    if (device < 0) device = g_default_device.load();
     if (device < 0) VQM_CK(cudaGetDevice(&device));
     if (device >= count) throw std::invalid_argument("cuda: invalid device ordinal");
     return device;
@@ -1324,6 +1329,8 @@ int RunRouteCheck(Check check, uint32_t first_bits, uint32_t last_bits, uint64_t
 
 }  // namespace
 
+int ResolveDeviceOrdinal(int32_t requested) { return ResolveDevice(requested); }
+
 // The message vqm_cu_last_error() returns on this thread, for entry points
 // defined in other translation units.
 void SetLastErrorMessage(const char* message) { g_last_error = message ? message : ""; }
@@ -1345,7 +1352,64 @@ struct vqm_cu_ss2_batch {
 extern "C" {
 
 const char* vqm_cu_last_error(void) { return vqm_b200::g_last_error.c_str(); }
-uint32_t vqm_cu_version(void) { return (1u << 16) | 2u; }
+uint32_t vqm_cu_version(void) { return (1u << 16) | 3u; }
+
+int vqm_cu_device_count(uint32_t* count) {
+    return vqm_b200::Guard([&] {
+        vqm_b200::NotNull(count, "count");
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess) {
+            cudaGetLastError();
+            n = 0;
+        }
+        *count = static_cast<uint32_t>(n);
+    });
+}
+
+int vqm_cu_device_info(uint32_t index, char* name, size_t name_bytes, uint8_t* uuid16,
+                       uint32_t* type) {
+    return vqm_b200::Guard([&] {
+        vqm_b200::NotNull(uuid16, "uuid");
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess) {
+            cudaGetLastError();
+            n = 0;
+        }
+        if (index >= static_cast<uint32_t>(n))
+            throw std::invalid_argument("cuda: no device " + std::to_string(index));
+        cudaDeviceProp prop{};
+        const cudaError_t e = cudaGetDeviceProperties(&prop, static_cast<int>(index));
+        if (e != cudaSuccess) throw std::runtime_error(std::string("cuda: ") + cudaGetErrorString(e));
+        if (name && name_bytes) {
+            std::strncpy(name, prop.name, name_bytes - 1);
+            name[name_bytes - 1] = '\0';
+        }
+        std::memcpy(uuid16, prop.uuid.bytes, 16);
+        if (type) *type = prop.integrated ? 1u : 2u;
+    });
+}
+
+int vqm_cu_set_default_device(const uint8_t* uuid16) {
+    return vqm_b200::Guard([&] {
+        vqm_b200::NotNull(uuid16, "uuid");
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess) {
+            cudaGetLastError();
+            n = 0;
+        }
+        for (int i = 0; i < n; ++i) {
+            cudaDeviceProp prop{};
+            const cudaError_t e = cudaGetDeviceProperties(&prop, i);
+            if (e != cudaSuccess)
+                throw std::runtime_error(std::string("cuda: ") + cudaGetErrorString(e));
+            if (std::memcmp(prop.uuid.bytes, uuid16, 16) == 0) {
+                vqm_b200::g_default_device.store(i);
+                return;
+            }
+        }
+        throw std::invalid_argument("device UUID is not available");
+    });
+}
 
 int vqm_cu_required_bytes(const vqm_cu_format* format, uint32_t width, uint32_t height,
                           size_t* bytes) {

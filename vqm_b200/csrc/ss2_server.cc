@@ -210,7 +210,7 @@ private:
             cudaGetLastError();
             throw std::runtime_error("cuda: no device");
         }
-        const int want = device < 0 ? current : device;
+        const int want = ResolveDeviceOrdinal(device);
         size_t free_bytes = 0, total = 0;
         const bool ok = cudaSetDevice(want) == cudaSuccess &&
                         cudaMemGetInfo(&free_bytes, &total) == cudaSuccess;

@@ -217,6 +217,10 @@ _SIGS = {
     "vqm_cu_ss2_set_graphs": ([_P, ctypes.c_int], ctypes.c_int),
     "vqm_cu_ss2_reference_reuses": ([_P, _P], ctypes.c_int),
     "vqm_cu_ss2_in_flight": ([_P, _P], ctypes.c_int),
+    "vqm_cu_device_count": ([_P], ctypes.c_int),
+    "vqm_cu_device_info": ([ctypes.c_uint32, ctypes.c_char_p, ctypes.c_size_t, _P, _P],
+                           ctypes.c_int),
+    "vqm_cu_set_default_device": ([_P], ctypes.c_int),
     "vqm_cu_ss2_submit": ([_P, _P, _P, ctypes.c_float, _P], ctypes.c_int),
     "vqm_cu_ss2_submit_resident": ([_P, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float, _P], ctypes.c_int),
     "vqm_cu_ss2_submit_resident_image": ([_P, ctypes.c_uint64, _P, ctypes.c_float, _P], ctypes.c_int),
@@ -549,6 +553,39 @@ class ImageBuffer:
     slot: int
     size: tuple
     bytes: int
+
+
+@dataclass(frozen=True)
+class DeviceInfo:
+    """vqm::DeviceInfo (include/vqm_device.h): a 16-byte UUID, the name and
+    the kind (DeviceType: 1 integrated, 2 discrete GPU)."""
+    uuid: bytes
+    name: str
+    type: int
+
+    def uuid_text(self) -> str:
+        h = self.uuid.hex()
+        return f"{h[:8]}-{h[8:12]}-{h[12:16]}-{h[16:20]}-{h[20:]}"
+
+
+def list_devices() -> list:
+    """ListDevices: the CUDA devices in ordinal order."""
+    n = ctypes.c_uint32()
+    _check(_lib.vqm_cu_device_count(ctypes.byref(n)))
+    out = []
+    for i in range(n.value):
+        name = ctypes.create_string_buffer(256)
+        uuid = (ctypes.c_uint8 * 16)()
+        kind = ctypes.c_uint32()
+        _check(_lib.vqm_cu_device_info(i, name, 256, uuid, ctypes.byref(kind)))
+        out.append(DeviceInfo(bytes(uuid), name.value.decode(errors="replace"), kind.value))
+    return out
+
+
+def set_default_device(uuid: bytes) -> None:
+    """SetDefaultDevice: the device a config's device = -1 uses from now on."""
+    buf = (ctypes.c_uint8 * 16).from_buffer_copy(bytes(uuid))
+    _check(_lib.vqm_cu_set_default_device(buf))
 
 
 def compute_worst_background(pipeline, original, distorted) -> "Ssimulacra2Result":
