@@ -110,6 +110,9 @@ typedef struct vqm_cu_memory_usage {
                                 + streaming inputs (device) */
     uint64_t scratch_bytes;  /* partials, tables, counters */
     uint64_t total_bytes;
+    uint64_t host_bytes;     /* of total_bytes, pinned host memory (the
+                                allocate_image() pool); the rest is device
+                                memory */
 } vqm_cu_memory_usage;
 
 typedef struct vqm_cu_ss2_pipeline vqm_cu_ss2_pipeline;

@@ -326,8 +326,24 @@ struct Ssimulacra2Config {
     Ssimulacra2Blur blur = Ssimulacra2Blur::Sampled;
 };
 
-// Memory the pipeline holds on the device (PipelineMemoryUsage's role).
-using PipelineMemoryUsage = vqm_cu_memory_usage;
+// vqm_memory_types.h:17-33. The arena is the device memory a pipeline
+// holds; staging is the pinned host memory of its AllocateImage pool, which
+// the kernels read in place. Memory types and heaps are 0 (device) and 1
+// (host). The five byte counts break the same memory down by use.
+struct MemoryAllocation {
+    std::uint64_t buffer_bytes = 0;
+    std::uint64_t allocation_bytes = 0;
+    std::uint32_t memory_type = 0;
+    std::uint32_t heap = 0;
+};
+struct PipelineMemoryUsage {
+    bool uses_staging = false;
+    MemoryAllocation arena;
+    MemoryAllocation staging;
+    std::vector<MemoryAllocation> auxiliary = {};
+    std::uint64_t pyramid_bytes = 0, resident_bytes = 0, input_bytes = 0, scratch_bytes = 0,
+                  total_bytes = 0;
+};
 
 class Ssimulacra2Pipeline {
 public:
@@ -470,8 +486,18 @@ public:
     }
 
     [[nodiscard]] PipelineMemoryUsage GetMemoryUsage() const {
-        PipelineMemoryUsage u{};
-        detail::Check(vqm_cu_ss2_memory_usage(p_.get(), &u));
+        vqm_cu_memory_usage c{};
+        detail::Check(vqm_cu_ss2_memory_usage(p_.get(), &c));
+        PipelineMemoryUsage u;
+        const std::uint64_t device = c.total_bytes - c.host_bytes;
+        u.arena = {device, device, 0, 0};
+        u.staging = {c.host_bytes, c.host_bytes, 1, 1};
+        u.uses_staging = c.host_bytes != 0;
+        u.pyramid_bytes = c.pyramid_bytes;
+        u.resident_bytes = c.resident_bytes;
+        u.input_bytes = c.input_bytes;
+        u.scratch_bytes = c.scratch_bytes;
+        u.total_bytes = c.total_bytes;
         return u;
     }
     void SetStream(void* stream) { detail::Check(vqm_cu_ss2_set_stream(p_.get(), stream)); }

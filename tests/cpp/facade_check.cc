@@ -301,6 +301,12 @@ void Gpu() {
         const v::ImageBuffer a = p.AllocateImage(base.format);
         const v::ImageBuffer b = p.AllocateImage(dist.format);
         Expect(a.bytes == per_image && b.bytes == per_image, "buffer sizes");
+        const v::PipelineMemoryUsage usage = p.GetMemoryUsage();
+        Expect(usage.uses_staging && usage.staging.allocation_bytes >= 2 * per_image &&
+                   usage.arena.allocation_bytes >= usage.pyramid_bytes &&
+                   usage.arena.allocation_bytes + usage.staging.allocation_bytes ==
+                       usage.total_bytes,
+               "memory usage: device arena and pinned pool");
         std::memcpy(p.MapImage(a), base.data.data(), base.data.size());
         std::memcpy(p.MapImage(b), dist.data.data(), dist.data.size());
         Expect(p.Compute(a, b).Score() == expected, "caller-owned buffers");

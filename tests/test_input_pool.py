@@ -59,6 +59,9 @@ def test_input_pool_exact_size_and_ownership():
         b = second.allocate_image(BYTE_RGB)
         assert a.bytes == nbytes and b.bytes == nbytes
         assert a.slot != b.slot
+        u = first.get_memory_usage()  # the pool is pinned host memory
+        assert u.host_bytes == nbytes and u.input_bytes >= nbytes
+        assert u.total_bytes - u.host_bytes >= u.pyramid_bytes > 0
         assert first.map_image(a)
         with pytest.raises(ss2.InvalidArgument):
             second.map_image(a)

@@ -910,6 +910,7 @@ public:
         u->scratch_bytes = mem_.table.bytes() + mem_.partials.bytes() + mem_.seg_sums.bytes() +
                            mem_.pair_done.bytes();
         u->total_bytes = u->pyramid_bytes + u->resident_bytes + u->input_bytes + u->scratch_bytes;
+        u->host_bytes = pool_.bytes();
     }
 
 private:
@@ -1352,7 +1353,7 @@ struct vqm_cu_ss2_batch {
 extern "C" {
 
 const char* vqm_cu_last_error(void) { return vqm_b200::g_last_error.c_str(); }
-uint32_t vqm_cu_version(void) { return (1u << 16) | 3u; }
+uint32_t vqm_cu_version(void) { return (1u << 16) | 4u; }
 
 int vqm_cu_device_count(uint32_t* count) {
     return vqm_b200::Guard([&] {

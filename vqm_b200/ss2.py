@@ -192,7 +192,7 @@ class ServerStats(ctypes.Structure):
 class MemoryUsage(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in (
         "pyramid_bytes", "resident_bytes", "input_bytes", "scratch_bytes",
-        "total_bytes")]
+        "total_bytes", "host_bytes")]
 
 
 _P = ctypes.c_void_p
