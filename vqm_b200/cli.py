@@ -328,7 +328,18 @@ def _device_count() -> int:
 
 # ---- scoring (cli/video.cc:419-506) -------------------------------------------
 
-def _score_clip(o, original, distorted, device, world, rank):
+def _scorer(cache, o, width, height, device):
+    """The scorer for this frame size, kept across pairs and iterations (VQM
+    keeps its metric pipelines per input key, cli/video.cc:300-385): a batch
+    scorer takes any size, one-pair pipelines are per size."""
+    key = (width, height) if o["batch"] <= 1 else None
+    if key not in cache:
+        cache[key] = _Scorer(width, height, max(1, o["batch"]), o["chroma_filter"], device,
+                             _BLURS[o["blur"]], o["half_planes"])
+    return cache[key]
+
+
+def _score_clip(o, original, distorted, device, world, rank, cache):
     """One clip of a pair: (frames as (score, raw norms), core seconds,
     decode seconds), this rank's frames gathered on rank 0."""
     t = time.perf_counter()
@@ -360,37 +371,33 @@ def _score_clip(o, original, distorted, device, world, rank):
             ro.skip(mine.start)
             rd.skip(mine.start)
             todo, first = len(mine), mine.start
-        scorer = _Scorer(ho.width, ho.height, max(1, o["batch"]), o["chroma_filter"], device,
-                         _BLURS[o["blur"]], o["half_planes"])
-        try:
-            io_, id_ = iter(ro), iter(rd)
-            while todo is None or len(frames) < todo:
-                t = time.perf_counter()
-                chunk = []
-                want = o["batch"] if todo is None else min(o["batch"], todo - len(frames))
-                for _ in range(max(1, want)):
-                    a, b = next(io_, None), next(id_, None)
-                    if (a is None) != (b is None):
-                        raise ss2.InvalidArgument("inputs have unequal frame counts")
-                    if a is None:
-                        break
-                    chunk.append((a, b))
-                decode += time.perf_counter() - t
-                if not chunk:
+        scorer = _scorer(cache, o, ho.width, ho.height, device)
+        io_, id_ = iter(ro), iter(rd)
+        while todo is None or len(frames) < todo:
+            t = time.perf_counter()
+            chunk = []
+            want = o["batch"] if todo is None else min(o["batch"], todo - len(frames))
+            for _ in range(max(1, want)):
+                a, b = next(io_, None), next(id_, None)
+                if (a is None) != (b is None):
+                    raise ss2.InvalidArgument("inputs have unequal frame counts")
+                if a is None:
                     break
-                t = time.perf_counter()
-                if alpha:
-                    # The worse of the dark and bright backgrounds
-                    # (include/vqm_alpha.h:17-28).
-                    dark = scorer.score(chunk, 0.1)
-                    bright = scorer.score(chunk, 0.9)
-                    picked = [x if x.score() <= y.score() else y for x, y in zip(dark, bright)]
-                else:
-                    picked = scorer.score(chunk, 0.5)
-                core += time.perf_counter() - t
-                frames += [(r.score(), raw_norms(r) if o["raw"] else None) for r in picked]
-        finally:
-            scorer.close()
+                chunk.append((a, b))
+            decode += time.perf_counter() - t
+            if not chunk:
+                break
+            t = time.perf_counter()
+            if alpha:
+                # The worse of the dark and bright backgrounds
+                # (include/vqm_alpha.h:17-28).
+                dark = scorer.score(chunk, 0.1)
+                bright = scorer.score(chunk, 0.9)
+                picked = [x if x.score() <= y.score() else y for x, y in zip(dark, bright)]
+            else:
+                picked = scorer.score(chunk, 0.5)
+            core += time.perf_counter() - t
+            frames += [(r.score(), raw_norms(r) if o["raw"] else None) for r in picked]
     finally:
         ro.close()
         rd.close()
@@ -471,13 +478,14 @@ def run(argv=None, out=sys.stdout) -> int:
     elif o["device"] is not None and o["device"] >= _device_count():
         raise ss2.InvalidArgument(f"--device {o['device']} is unavailable. Run --list-devices "
                                   "to see available indexes.")
+    cache = {}
     try:
         pairs = (read_pairs(o["pairs_file"]) if o["pairs_file"] is not None
                  else [("pair", o["original"], o["distorted"])])
         for sample_id, original, distorted in pairs:
             for _ in range(o["warmup"]):
-                _score_clip(o, original, distorted, device, world, rank)
-            runs = sorted((_score_clip(o, original, distorted, device, world, rank)
+                _score_clip(o, original, distorted, device, world, rank, cache)
+            runs = sorted((_score_clip(o, original, distorted, device, world, rank, cache)
                            for _ in range(o["iterations"])), key=lambda r: r[1])
             frames, core, decode = runs[len(runs) // 2]
             if not frames:
@@ -485,6 +493,8 @@ def run(argv=None, out=sys.stdout) -> int:
             if rank == 0:
                 _print_clip(o, sample_id, frames, core, decode, out)
     finally:
+        for scorer in cache.values():
+            scorer.close()
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
