@@ -83,6 +83,17 @@ def test_png_formats(tmp_path):
     for c in range(3):
         assert np.array_equal(p[c], lut[index, c])
     assert np.array_equal(p[3], np.array([255, 0, 128, 255], np.uint8)[index])
+    # A colour key (tRNS of a grey or RGB image) becomes an alpha plane, as
+    # libpng's png_set_tRNS_to_alpha gives it to VQM.
+    PIL.fromarray(grey, "L").save(tmp_path / "grey_key.png", transparency=int(grey[0, 0]))
+    img, f = fmt("grey_key.png")
+    assert (f.family, f.alpha) == (ss2.ColorFamily.Grey, ss2.AlphaType.Straight)
+    assert np.array_equal(_planes(img)[3], np.where(grey == grey[0, 0], 0, 255))
+    key = tuple(int(v) for v in rgb[2, 3])
+    PIL.fromarray(rgb, "RGB").save(tmp_path / "rgb_key.png", transparency=key)
+    img, f = fmt("rgb_key.png")
+    assert (f.family, f.alpha) == (ss2.ColorFamily.Rgb, ss2.AlphaType.Straight)
+    assert np.array_equal(_planes(img)[3], np.where((rgb == key).all(-1), 0, 255))
 
 
 def test_jpeg_and_readers(tmp_path):

@@ -34,6 +34,29 @@ def _png_color_type(path: str) -> int | None:
     return head[25]
 
 
+def _png_transparent_key(path: str):
+    """(bit depth, colour type, key samples) of a grey or RGB PNG's tRNS
+    chunk, or None. OpenCV keeps the colour key out of its output, while
+    libpng (png_set_tRNS_to_alpha) turns it into an alpha plane for VQM."""
+    with open(path, "rb") as f:
+        data = f.read()
+    if data[:8] != PNG_MAGIC:
+        return None
+    depth, ctype = data[24], data[25]
+    at = 8
+    while at + 8 <= len(data):
+        n = int.from_bytes(data[at:at + 4], "big")
+        kind = data[at + 4:at + 8]
+        if kind in (b"IDAT", b"IEND"):
+            return None
+        if kind == b"tRNS" and ctype in (0, 2):
+            body = data[at + 8:at + 8 + n]
+            key = [int.from_bytes(body[i:i + 2], "big") for i in range(0, len(body) - 1, 2)]
+            return depth, ctype, key
+        at += 12 + n
+    return None
+
+
 def load(path: str) -> ss2.Image:
     """A PNG or JPEG file as a packed ss2.Image in VQM's still format."""
     try:
@@ -54,12 +77,24 @@ def load(path: str) -> ss2.Image:
         planes = [pixels[..., 2], pixels[..., 1], pixels[..., 0]] if c >= 3 else [pixels[..., 0]]
         if c == 4:
             planes.append(pixels[..., 3])
-        # OpenCV widens grey + alpha to four channels; the file's two
-        # channels are one grey plane and alpha.
-        if c == 4 and _png_color_type(path) == 4:
+        # OpenCV widens grey + alpha (PNG colour type 4, or grey with a tRNS
+        # chunk) to four channels; libpng gives VQM one grey plane and alpha.
+        if c == 4 and _png_color_type(path) in (0, 4):
             planes = [pixels[..., 0], pixels[..., 3]]
     if pixels.dtype not in (np.uint8, np.uint16):
         raise y4m.Y4mError(f"{path}: unsupported sample type {pixels.dtype}")
+    key = _png_transparent_key(path) if len(planes) in (1, 3) else None
+    if key is not None:
+        depth, ctype, values = key
+        need = 1 if ctype == 0 else 3
+        if len(values) >= need and len(planes) == need:
+            # Samples below 8 bits come out of the decoder scaled to 8 bits.
+            scale = 255 // ((1 << depth) - 1) if depth < 8 else 1
+            hit = np.ones(planes[0].shape, bool)
+            for plane, v in zip(planes, values[:need]):
+                hit &= plane == v * scale
+            top = 65535 if pixels.dtype == np.uint16 else 255
+            planes.append(np.where(hit, 0, top).astype(pixels.dtype))
     wide = pixels.dtype == np.uint16
     grey = len(planes) <= 2
     alpha = len(planes) in (2, 4)
