@@ -90,7 +90,17 @@ typedef struct vqm_cu_ss2_config {
     uint64_t input_bytes;         /* pool for allocate_image(); 0 = none */
     int32_t device;               /* CUDA ordinal; -1 = the current device */
     uint32_t blur;                /* VQM_CU_SS2_BLUR_*; 0 = VQM's */
+    uint32_t memory_policy;       /* VQM_CU_MEMORY_POLICY_* (MemoryPolicy,
+                                     vqm_memory_types.h:12-14) */
 } vqm_cu_ss2_config;
+
+/* Where the kernels read the allocate_image() pool from. DIRECT (and
+ * AUTOMATIC, which picks it): the pinned host pool in place, over the bus.
+ * STAGED: a device copy of the two spans made on the stream at submit, so
+ * the prepare kernels read HBM; the pool keeps a device mirror. */
+#define VQM_CU_MEMORY_POLICY_AUTOMATIC 0
+#define VQM_CU_MEMORY_POLICY_DIRECT 1
+#define VQM_CU_MEMORY_POLICY_STAGED 2
 
 /* Blur modes. SAMPLED is VQM's 13-tap sampled Gaussian, sigma 1.5
  * (pipeline.cc:274-291), the only mode that reproduces VQM's scores.
@@ -113,6 +123,8 @@ typedef struct vqm_cu_memory_usage {
     uint64_t host_bytes;     /* of total_bytes, pinned host memory (the
                                 allocate_image() pool); the rest is device
                                 memory */
+    uint32_t uses_staging;   /* 1: the STAGED memory policy is in force */
+    uint32_t reserved;
 } vqm_cu_memory_usage;
 
 typedef struct vqm_cu_ss2_pipeline vqm_cu_ss2_pipeline;

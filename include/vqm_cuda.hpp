@@ -315,6 +315,11 @@ struct Ssimulacra2Result {
     }
 };
 
+// vqm_memory_types.h:12-14: Automatic and Direct read the AllocateImage pool
+// in place from pinned host memory; Staged copies its spans to a device
+// mirror at submit.
+enum class MemoryPolicy : std::uint8_t { Automatic, Direct, Staged };
+
 struct Ssimulacra2Config {
     Size size;
     std::size_t gpu_resident_images = 2;
@@ -322,6 +327,7 @@ struct Ssimulacra2Config {
     ChromaFilter chroma_filter = ChromaFilter::Bilinear;
     std::size_t input_bytes = 0;
     bool streaming_inputs = true;
+    MemoryPolicy memory_policy = MemoryPolicy::Automatic;
     int device = -1;  // CUDA ordinal; -1 = the current device
     Ssimulacra2Blur blur = Ssimulacra2Blur::Sampled;
 };
@@ -360,6 +366,7 @@ public:
         c.input_bytes = config.input_bytes;
         c.device = config.device;
         c.blur = static_cast<std::uint32_t>(config.blur);
+        c.memory_policy = static_cast<std::uint32_t>(config.memory_policy);
         vqm_cu_ss2_pipeline* p = nullptr;
         detail::Check(vqm_cu_ss2_create(&c, &p));
         p_.reset(p);
@@ -492,7 +499,7 @@ public:
         const std::uint64_t device = c.total_bytes - c.host_bytes;
         u.arena = {device, device, 0, 0};
         u.staging = {c.host_bytes, c.host_bytes, 1, 1};
-        u.uses_staging = c.host_bytes != 0;
+        u.uses_staging = c.uses_staging != 0;
         u.pyramid_bytes = c.pyramid_bytes;
         u.resident_bytes = c.resident_bytes;
         u.input_bytes = c.input_bytes;

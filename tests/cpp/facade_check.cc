@@ -295,6 +295,7 @@ void Gpu() {
         v::Ssimulacra2Config owned = config;
         const std::size_t per_image = v::RequiredBytes(base.format, base.size);
         owned.input_bytes = 2 * per_image;
+        owned.memory_policy = v::MemoryPolicy::Staged;
         v::Ssimulacra2Pipeline p(owned);
         const v::Image dist = Gradient(2);
         const double expected = p.Compute(base, dist).Score();
@@ -303,6 +304,7 @@ void Gpu() {
         Expect(a.bytes == per_image && b.bytes == per_image, "buffer sizes");
         const v::PipelineMemoryUsage usage = p.GetMemoryUsage();
         Expect(usage.uses_staging && usage.staging.allocation_bytes >= 2 * per_image &&
+                   usage.input_bytes >= 4 * per_image &&
                    usage.arena.allocation_bytes >= usage.pyramid_bytes &&
                    usage.arena.allocation_bytes + usage.staging.allocation_bytes ==
                        usage.total_bytes,

@@ -154,3 +154,27 @@ def test_devices_and_default_device():
         assert p.compute(helpers.gradient(0), helpers.gradient(0)).score() == 100.0
     with pytest.raises(ss2.InvalidArgument, match="device UUID"):
         ss2.set_default_device(bytes(16) if devices[0].uuid != bytes(16) else b"\xff" * 16)
+
+
+@pytest.mark.parametrize("policy", [ss2.MemoryPolicy.AUTOMATIC, ss2.MemoryPolicy.DIRECT,
+                                    ss2.MemoryPolicy.STAGED])
+def test_memory_policies_score_alike(policy):
+    """Every memory policy scores the pool's buffers like the packed images
+    (the same planes either way: read in place, or from the device copy
+    STAGED makes at submit); STAGED reports its staging and device mirror."""
+    o, d = helpers.plain_256_pair()
+    nbytes = o.data.nbytes
+    with ss2.Ssimulacra2Pipeline(256, 256, input_bytes=2 * ((nbytes + 63) // 64 * 64),
+                                 memory_policy=policy) as p:
+        want = p.compute(o, d)
+        a, b = p.allocate_image(o.format), p.allocate_image(d.format)
+        for buf, img in ((a, o), (b, d)):
+            ctypes.memmove(p.map_image(buf), img.data.ctypes.data, nbytes)
+        assert np.array_equal(p.compute(a, b).norms, want.norms)
+        ctypes.memmove(p.map_image(a), d.data.ctypes.data, nbytes)  # rewritten between calls
+        assert p.compute(a, b).score() == 100.0
+        u = p.get_memory_usage()
+        assert u.uses_staging == (policy == ss2.MemoryPolicy.STAGED)
+        assert u.input_bytes >= u.host_bytes * (2 if policy == ss2.MemoryPolicy.STAGED else 1)
+    with pytest.raises(ss2.InvalidArgument, match="memory policy"):
+        ss2.Ssimulacra2Pipeline(32, 32, memory_policy=3)

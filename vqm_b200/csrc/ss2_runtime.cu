@@ -594,6 +594,9 @@ public:
         // arithmetic, the level averages rounded like the planes.
         mem_.elem_bytes = cfg.half_planes ? 2 : 4;
         mem_.SetBlur(cfg.blur);
+        if (cfg.memory_policy > VQM_CU_MEMORY_POLICY_STAGED)
+            throw std::invalid_argument("cuda: invalid memory policy");
+        staged_ = cfg.memory_policy == VQM_CU_MEMORY_POLICY_STAGED;
         device_ = ResolveDevice(cfg.device);
         EnsureDevice(device_);
         VQM_CK(cudaSetDevice(device_));
@@ -612,6 +615,7 @@ public:
                           cudaMemcpyHostToDevice));
         slots_.resize(cfg.gpu_resident_images);
         if (cfg.input_bytes) pool_.ensure(cfg.input_bytes);
+        if (cfg.input_bytes && staged_) pool_device_.ensure(cfg.input_bytes);
     }
     ~Pipeline() {
         cudaSetDevice(device_);
@@ -735,8 +739,16 @@ public:
         const InputAlloc& ia = RequireInput(a);
         const InputAlloc& ib = RequireInput(b);
         VQM_CK(cudaSetDevice(device_));
-        SourceFromDevice(0, ia.format, pool_.as<uint8_t>() + ia.offset, bg);
-        SourceFromDevice(1, ib.format, pool_.as<uint8_t>() + ib.offset, bg);
+        const uint8_t* base = pool_.as<uint8_t>();
+        if (staged_) {
+            // The two spans to the device mirror, ahead of the kernels.
+            for (const InputAlloc* in : {&ia, &ib})
+                VQM_CK(cudaMemcpyAsync(pool_device_.as<uint8_t>() + in->offset, base + in->offset,
+                                       in->bytes, cudaMemcpyHostToDevice, stream_));
+            base = pool_device_.as<uint8_t>();
+        }
+        SourceFromDevice(0, ia.format, base + ia.offset, bg);
+        SourceFromDevice(1, ib.format, base + ib.offset, bg);
         return Launch();
     }
 
@@ -906,11 +918,13 @@ public:
         std::memset(u, 0, sizeof(*u));
         u->pyramid_bytes = mem_.pyramid.bytes();
         for (const auto& s : slots_) u->resident_bytes += s.memory.bytes();
-        u->input_bytes = pool_.bytes() + stream_in_[0].bytes() + stream_in_[1].bytes();
+        u->input_bytes = pool_.bytes() + pool_device_.bytes() + stream_in_[0].bytes() +
+                         stream_in_[1].bytes();
         u->scratch_bytes = mem_.table.bytes() + mem_.partials.bytes() + mem_.seg_sums.bytes() +
                            mem_.pair_done.bytes();
         u->total_bytes = u->pyramid_bytes + u->resident_bytes + u->input_bytes + u->scratch_bytes;
         u->host_bytes = pool_.bytes();
+        u->uses_staging = staged_ ? 1u : 0u;
     }
 
 private:
@@ -1027,6 +1041,9 @@ private:
     // MapImage (as into VQM's host-visible arena) and the prepare kernels
     // read in place over the bus (unified addressing maps it on the device).
     PinnedBuffer pool_;
+    // The STAGED memory policy's device mirror of the pool.
+    DeviceBuffer pool_device_;
+    bool staged_ = false;
     std::vector<Slot> slots_;
     std::vector<InputAlloc> inputs_;
     bool in_flight_ = false;
@@ -1353,7 +1370,7 @@ struct vqm_cu_ss2_batch {
 extern "C" {
 
 const char* vqm_cu_last_error(void) { return vqm_b200::g_last_error.c_str(); }
-uint32_t vqm_cu_version(void) { return (1u << 16) | 4u; }
+uint32_t vqm_cu_version(void) { return (1u << 16) | 5u; }
 
 int vqm_cu_device_count(uint32_t* count) {
     return vqm_b200::Guard([&] {

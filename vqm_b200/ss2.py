@@ -94,6 +94,11 @@ class Ssimulacra2Blur:
 # ---------------------------------------------------------------------------
 
 
+class MemoryPolicy:
+    """vqm::MemoryPolicy (vqm_memory_types.h:12-14)."""
+    AUTOMATIC, DIRECT, STAGED = 0, 1, 2
+
+
 class ImageFormat(ctypes.Structure):
     """vqm::ImageFormat; the defaults are the reference's (8-bit needs type)."""
 
@@ -154,6 +159,7 @@ class _Config(ctypes.Structure):
         ("input_bytes", ctypes.c_uint64),
         ("device", ctypes.c_int32),
         ("blur", ctypes.c_uint32),
+        ("memory_policy", ctypes.c_uint32),
     ]
 
 
@@ -192,7 +198,8 @@ class ServerStats(ctypes.Structure):
 class MemoryUsage(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in (
         "pyramid_bytes", "resident_bytes", "input_bytes", "scratch_bytes",
-        "total_bytes", "host_bytes")]
+        "total_bytes", "host_bytes")] + [("uses_staging", ctypes.c_uint32),
+                                        ("reserved", ctypes.c_uint32)]
 
 
 _P = ctypes.c_void_p
@@ -608,10 +615,14 @@ class Ssimulacra2Pipeline:
     def __init__(self, width: int, height: int, gpu_resident_images: int = 2,
                  half_planes: bool = False, chroma_filter: int = 0,
                  input_bytes: int = 0, streaming_inputs: bool = True,
-                 device: int = -1, blur: int = 0):
-        """`blur`: Ssimulacra2Blur.SAMPLED (VQM's) or RECURSIVE (opt-in)."""
+                 device: int = -1, blur: int = 0, memory_policy: int = 0):
+        """`blur`: Ssimulacra2Blur.SAMPLED (VQM's) or RECURSIVE (opt-in).
+        `memory_policy`: MemoryPolicy.AUTOMATIC/DIRECT read the allocate_image
+        pool in place from pinned host memory, STAGED copies its spans to the
+        device at submit."""
         cfg = _Config(width, height, gpu_resident_images, int(half_planes),
-                      chroma_filter, int(streaming_inputs), input_bytes, device, int(blur))
+                      chroma_filter, int(streaming_inputs), input_bytes, device, int(blur),
+                      int(memory_policy))
         self._p = ctypes.c_void_p()
         _check(_lib.vqm_cu_ss2_create(ctypes.byref(cfg), ctypes.byref(self._p)))
         self.size = (width, height)
