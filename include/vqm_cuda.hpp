@@ -797,21 +797,40 @@ struct MetricsConfig {
     ImageFormat original_format{};
     ImageFormat distorted_format{};
     bool streaming_inputs = true;
+    MemoryPolicy memory_policy = MemoryPolicy::Automatic;
     float background = 0.5f;
     // The one metric this library computes; leaving it empty is the
     // reference's "select at least one metric" error.
     std::optional<Ssimulacra2Config> ssimulacra2 = std::nullopt;
 };
 
+// vqm_metrics.h:50-61; the other metrics' fields stay empty here.
 struct MetricsResult {
     std::uint64_t frame_index = 0;
     std::optional<double> ssimulacra2;
+    std::optional<double> butteraugli;
+    std::optional<double> vmaf_v0;
+    std::optional<double> vmaf_v1;
+    std::optional<double> cvvdp;
+    std::optional<double> psnr_hvs;
 };
 
 struct MetricsFinalResult {
     std::optional<MetricsResult> last_frame;
     std::uint64_t frames = 0;
     std::optional<MetricsResult> penultimate_frame;
+};
+
+// vqm_metrics.h:63-75: `scratch` holds the pipeline's memory (its device
+// arena and pinned pool); `spatial`, the SSIMULACRA 2 entry, holds what it
+// keeps beside that, which is nothing; the other metrics' entries are empty.
+struct MetricsMemoryUsage {
+    std::optional<PipelineMemoryUsage> spatial;
+    std::optional<PipelineMemoryUsage> vmaf_v0;
+    std::optional<PipelineMemoryUsage> vmaf_v1;
+    std::optional<PipelineMemoryUsage> cvvdp;
+    std::optional<PipelineMemoryUsage> psnr_hvs;
+    std::optional<PipelineMemoryUsage> scratch;
 };
 
 // Metrics (include/vqm_metrics.h:147-217, src/metrics/metrics.cc:83-396) with
@@ -828,6 +847,7 @@ public:
         Ssimulacra2Config c = *config_.ssimulacra2;
         c.size = config_.size;
         c.streaming_inputs = config_.streaming_inputs;
+        c.memory_policy = config_.memory_policy;
         c.gpu_resident_images = 0;
         c.input_bytes = 0;
         pipeline_.emplace(c);
@@ -888,7 +908,12 @@ public:
         failed_ = false;
         finished_ = false;
     }
-    [[nodiscard]] PipelineMemoryUsage GetMemoryUsage() const { return pipeline_->GetMemoryUsage(); }
+    [[nodiscard]] MetricsMemoryUsage GetMemoryUsage() const {
+        MetricsMemoryUsage u;
+        u.scratch = pipeline_->GetMemoryUsage();
+        u.spatial = PipelineMemoryUsage{};
+        return u;
+    }
 
 private:
     static bool SameFormat(const ImageFormat& a, const ImageFormat& b) {

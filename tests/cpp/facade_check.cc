@@ -183,6 +183,25 @@ void GpuMetrics() {
     mc.ssimulacra2 = v::Ssimulacra2Config{};
     v::Metrics metrics(mc);
     const v::Image base = Gradient(0);
+    // metrics_test.cc:376-411: SSIMULACRA 2 alone; the pipeline's memory
+    // is the scratch entry, the other metrics have none.
+    {
+        const v::MetricsMemoryUsage usage = metrics.GetMemoryUsage();
+        v::Ssimulacra2Config single;
+        single.size = mc.size;
+        single.gpu_resident_images = 0;
+        v::Ssimulacra2Pipeline standalone(single);
+        Expect(usage.spatial && usage.scratch && !usage.vmaf_v0 && !usage.vmaf_v1 &&
+                   usage.scratch->arena.allocation_bytes ==
+                       standalone.GetMemoryUsage().arena.allocation_bytes,
+               "metrics memory usage");
+        const auto r = metrics.Compute(base, Gradient(1));
+        Expect(r && r->ssimulacra2 && !r->butteraugli && !r->vmaf_v0 && !r->vmaf_v1 &&
+                   *r->ssimulacra2 == standalone.Compute(base, Gradient(1)).Score(),
+               "SSIMULACRA 2 alone through Metrics");
+        Expect(!metrics.Flush(), "nothing left to flush");
+        metrics.Reset();
+    }
     for (int variant = 0; variant < 3; ++variant) {
         const auto r = metrics.Compute(base, Gradient(variant));
         Expect(r.has_value() && r->frame_index == static_cast<std::uint64_t>(variant),
