@@ -331,12 +331,12 @@ void Gpu() {
         std::memcpy(p.MapImage(a), base.data.data(), base.data.size());
         std::memcpy(p.MapImage(b), dist.data.data(), dist.data.size());
         Expect(p.Compute(a, b).Score() == expected, "caller-owned buffers");
-        const std::uint64_t token = p.Submit(a, b);
+        const std::uint64_t pending = p.Submit(a, b);
         ExpectThrow<std::logic_error>([&] { p.Release(a); }, "Release in flight");
         ExpectThrow<std::logic_error>([&] { (void)p.MapImage(a); }, "MapImage in flight");
         ExpectThrow<std::logic_error>([&] { (void)p.AllocateImage(base.format); },
                                       "AllocateImage in flight");
-        Expect(p.Finish(token).Score() == expected, "submitted buffers");
+        Expect(p.Finish(pending).Score() == expected, "submitted buffers");
         p.Release(a);
         ExpectThrow<std::invalid_argument>([&] { (void)p.Compute(a, b); }, "released buffer");
         p.Release(b);
