@@ -14,6 +14,7 @@
 // alias a live one.
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <atomic>
@@ -58,6 +59,17 @@ uint64_t NextIncarnation() {
     if (v > kIncarnationMax) throw std::overflow_error("handle identifiers exhausted");
     return v;
 }
+
+// An NVTX range (a named span on the Nsight Systems timeline) over a scope:
+// the host side of a submission, or the wait for its results. Without a tool
+// attached, NVTX v3 calls return at once.
+class TraceRange {
+public:
+    explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange&) = delete;
+    TraceRange& operator=(const TraceRange&) = delete;
+};
 
 constexpr const char* kCapacityError =
     "resident image capacity exhausted; raise gpu_resident_images";
@@ -755,6 +767,7 @@ public:
     void Finish(uint64_t token, double* norms, uint32_t* scales) {
         if (!in_flight_ || token != token_)
             throw std::invalid_argument("cuda: no submission with that token");
+        TraceRange trace("ss2 pipeline finish");
         VQM_CK(cudaSetDevice(device_));
         const cudaError_t e = cudaEventSynchronize(done_);
         in_flight_ = false;
@@ -974,6 +987,7 @@ private:
     // graph replay when graphs are on. `skip_original` leaves the original's
     // prepare out (its pyramid is cached).
     uint64_t Launch(bool skip_original = false) {
+        TraceRange trace("ss2 pipeline launch");
         if (!skip_original) reference_valid_ = false;
         // Each image's prepare group, and whether the original is prepared,
         // decide the prepare launches; one graph per combination.
@@ -1150,6 +1164,7 @@ public:
     uint64_t Submit(uint32_t n, const vqm_cu_image* o, const vqm_cu_image* d, float bg,
                     bool wait_copies = true) {
         if (in_flight_) throw std::logic_error("cuda: a batch is in flight; Finish it first");
+        TraceRange trace("ss2 batch submit");
         std::vector<std::pair<uint32_t, uint32_t>> sizes;
         const size_t host_bytes = ValidatePairs(n, o, d, sizes);
         VQM_CK(cudaSetDevice(device_));
@@ -1259,6 +1274,7 @@ public:
     void Finish(uint64_t token, double* norms, uint32_t* scales, double* scores) {
         if (!in_flight_ || token != token_)
             throw std::invalid_argument("cuda: no submission with that token");
+        TraceRange trace("ss2 batch finish");
         VQM_CK(cudaSetDevice(device_));
         const cudaError_t e = cudaEventSynchronize(done_);
         in_flight_ = false;
