@@ -23,7 +23,7 @@
 
 namespace vqm_b200 {
 
-__device__ __forceinline__ float RawSample(const DevSource& s, int plane,
+__device__ __forceinline__ float RawSample(const DevSourceHead& s, int plane,
                                            uint32_t x, uint32_t y) {
     const uint8_t* row = s.plane[plane] + static_cast<size_t>(y) * s.row_bytes[plane];
     float v;
@@ -67,7 +67,7 @@ __device__ __forceinline__ float AribInvOetf(float x) {
                                            0.28466892f),
                                  12.0f);
 }
-__device__ __forceinline__ float TransferDecode(const DevSource& s, float v) {
+__device__ __forceinline__ float TransferDecode(const DevSourceHead& s, float v) {
     switch (s.transfer) {
         case 0: return v;
         case 1: return v < 0.0f ? 0.0f : ss2dm::powf_gamma(v, 2.4f);
@@ -94,7 +94,7 @@ __device__ __forceinline__ float TransferDecode(const DevSource& s, float v) {
     return v;
 }
 // color.glsl:181-205.
-__device__ __forceinline__ void TransferRgb(const DevSource& s, float c[3]) {
+__device__ __forceinline__ void TransferRgb(const DevSourceHead& s, float c[3]) {
     if (s.transfer == 11) {
         for (int i = 0; i < 3; ++i) c[i] = AribInvOetf(c[i]);
         const float luma =
@@ -132,7 +132,7 @@ __device__ __forceinline__ void ApplyMatrix2(const float* m, float2 v[3]) {
     v[2] = r[2];
 }
 // color.glsl:223-236.
-__device__ __forceinline__ void ClToRgb(const DevSource& s, float e[3]) {
+__device__ __forceinline__ void ClToRgb(const DevSourceHead& s, float e[3]) {
     const float u = e[1], v = e[2];
     const float kbv = u < 0.0f ? s.cl[0] : s.cl[1];
     const float krv = v < 0.0f ? s.cl[2] : s.cl[3];
@@ -219,7 +219,7 @@ __device__ __forceinline__ float BilinearTap(const WinRows& r, int s, float xw0,
 }
 
 // color.glsl:324-367: bilinear chroma of the block's four samples.
-__device__ __forceinline__ void ChromaBilinear(const DevSource& s, int plane, const uint32_t px[4],
+__device__ __forceinline__ void ChromaBilinear(const DevSourceHead& s, int plane, const uint32_t px[4],
                                                const uint32_t py[4], float out[4]) {
     const uint32_t dx = s.plane_w[plane], dy = s.plane_h[plane];
     const int cx = static_cast<int>(px[0] >> s.sub_w);
@@ -276,7 +276,7 @@ __device__ __forceinline__ void ChromaBilinear(const DevSource& s, int plane, co
 }
 
 // color.glsl:371-432: bicubic (4 taps) or Lanczos-3 (6 taps) chroma.
-__device__ void AxisTaps(const DevSource& s, uint32_t out_pos, float scale, float shift,
+__device__ void AxisTaps(const DevSourceHead& s, uint32_t out_pos, float scale, float shift,
                          uint32_t dim, int taps, float* w, int* idx) {
     const float pos =
         __fadd_rn(__fdiv_rn(__fadd_rn(static_cast<float>(out_pos), 0.5f), scale), shift);
@@ -293,7 +293,7 @@ __device__ void AxisTaps(const DevSource& s, uint32_t out_pos, float scale, floa
         idx[j] = MirrorIndex(__fadd_rn(base, static_cast<float>(j)), dim);
     }
 }
-__device__ void ChromaTaps(const DevSource& s, int plane, const uint32_t px[4],
+__device__ void ChromaTaps(const DevSourceHead& s, int plane, const uint32_t px[4],
                            const uint32_t py[4], float out[4]) {
     const int taps = s.filter == 1 ? 4 : 6;
     const float scx = static_cast<float>(1u << s.sub_w);
@@ -325,7 +325,7 @@ __device__ void ChromaTaps(const DevSource& s, int plane, const uint32_t px[4],
 
 // color.glsl:447-541: the block's four samples, linear Rec.709, in
 // (0,0), (1,0), (0,1), (1,1) order. The generic path: any format.
-__device__ __forceinline__ void BlockLinearGeneric(const DevSource& s, uint32_t bx, uint32_t by,
+__device__ __forceinline__ void BlockLinearGeneric(const DevSourceHead& s, uint32_t bx, uint32_t by,
                                    float rgb[4][3]) {
     const uint32_t lx = s.width - 1, ly = s.height - 1;
     const uint32_t px[4] = {min(2 * bx, lx), min(2 * bx + 1, lx), min(2 * bx, lx),
@@ -450,7 +450,7 @@ __device__ __forceinline__ float2 PowfGamma2(float2 x, float y, const float* pt)
 // subsampling the path takes, kChromaStage420 4:2:0 alone.
 constexpr int kChromaStage = ((kPrepTile >> 1) + 2) * (kPrepTile + 2);
 constexpr int kChromaStage420 = ((kPrepTile >> 1) + 2) * ((kPrepTile >> 1) + 2);
-__device__ __forceinline__ void StageChroma(const DevSource& s, uint32_t gx, uint32_t gy,
+__device__ __forceinline__ void StageChroma(const DevSourceHead& s, uint32_t gx, uint32_t gy,
                                             float* stage, int plane) {
     const uint32_t sw = (kPrepTile >> s.sub_w) + 2, sh = (kPrepTile >> s.sub_h) + 2;
     const int c0x = static_cast<int>((gx * kPrepTile) >> s.sub_w) - 1;
@@ -528,7 +528,7 @@ __device__ __forceinline__ void ChromaFixed(const float* stage, int plane, int b
 // (gx, gy) whose two columns and rows are inside the image: the same values,
 // with the format's branches resolved and the chroma taps read from the
 // staged window at the host's per-parity slots and weights.
-__device__ __forceinline__ void BlockLinearYuv(const DevSource& s, const float* stage,
+__device__ __forceinline__ void BlockLinearYuv(const DevSourceHead& s, const float* stage,
                                                int plane, const float* pow_table,
                                                uint32_t gx, uint32_t gy, uint32_t bx,
                                                uint32_t by, bool aligned4, float rgb[4][3]) {

@@ -52,7 +52,10 @@ constexpr int kResultStatus = 110;
 // SourceDesc (src/vulkan/vulkan_support.h:104-120) with device pointers and
 // byte strides in place of arena word offsets, so caller-owned padded device
 // buffers are read in place.
-struct DevSource {
+// Everything about one image the prepare kernels read per CTA (staged in
+// shared memory); DevSource adds the 8-bit byte table, which the table
+// kernels stage separately, so the CTAs do not hold its 1 KB twice.
+struct DevSourceHead {
     const uint8_t* plane[4];   // device address of each plane's first row
     uint32_t row_bytes[4];     // row stride of each plane, bytes
     uint32_t plane_w[4];       // samples per row of each plane
@@ -92,8 +95,11 @@ struct DevSource {
     int8_t cslot[2][2];        // [0 = x, 1 = y][parity]: first window slot
     float gamma;               // the transfer exponent
     float cweight[2][2][4];    // [y parity][x parity]: w00, w10, w01, w11
+};
+struct DevSource : DevSourceHead {
     float srgb_lut[256];       // transfer(raw * scale + offset) per byte code
 };
+static_assert(sizeof(DevSourceHead) % 4 == 0, "the head is copied in words");
 
 // One pair of a batch.
 struct DevPair {

@@ -225,7 +225,7 @@ __device__ __forceinline__ void PutBlock(void* plane, size_t at, float a, float 
 // entries, in (0,0), (1,0), (0,1), (1,1) order, edge-clamped like
 // prepare.comp's loads. `w4[c]` holds the 32-bit words of rows 2by and
 // 2by + 1 at column 4 * (bx / 2) when `fast`.
-__device__ __forceinline__ void TableBlock(const DevSource& s, const float* lut, bool fast,
+__device__ __forceinline__ void TableBlock(const DevSourceHead& s, const float* lut, bool fast,
                                            const uint32_t (&w4)[3][2], uint32_t hx, uint32_t bx,
                                            uint32_t by, float lin[4][3]) {
     const bool grey = s.family == 0;
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(kNT, kNT == 128     ? (kGroup == 0 ? kTableCta
     __shared__ __align__(16) float ladder_a[3][kBlocks * kBlocks];
     __shared__ float ladder_b[3][kBlocks * kBlocks / 4];
     __shared__ float lut[kTable ? 256 : 1];
-    __shared__ DevSource src_s;
+    __shared__ DevSourceHead src_s;  // (the byte table goes to `lut`)
     __shared__ LevelInfo lv;
     __shared__ uint32_t aligned4;
     // Both chroma planes' window of the tile, for yuv_fast images, and the
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(kNT, kNT == 128     ? (kGroup == 0 ? kTableCta
     {
         const uint32_t* from = reinterpret_cast<const uint32_t*>(&P.src[image]);
         uint32_t* to = reinterpret_cast<uint32_t*>(&src_s);
-        constexpr uint32_t words = offsetof(DevSource, srgb_lut) / 4;
+        constexpr uint32_t words = sizeof(DevSourceHead) / 4;
         for (uint32_t i = tid; i < words; i += kThreads) to[i] = from[i];
         if (kTable)
             for (uint32_t i = tid; i < 256; i += kThreads) lut[i] = P.src[image].srgb_lut[i];
@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(kNT, kNT == 128     ? (kGroup == 0 ? kTableCta
     // the cube root's direct range (kInRange) or not.
     const auto body = [=](auto in_range) {
     constexpr bool kInRange = decltype(in_range)::value;
-    const DevSource& s = src_s;
+    const DevSourceHead& s = src_s;
     if constexpr (kYuv) {
         if (s.chroma_variant) {
             // A window larger than the stage would overrun it: such an image
