@@ -798,6 +798,12 @@ class Ssimulacra2Batch:
             _check(_lib.vqm_cu_ss2_batch_destroy(self._b))
             self._b = ctypes.c_void_p()
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
     def __del__(self):
         try:
             self.close()
@@ -920,6 +926,12 @@ class Ssimulacra2Pool:
     def close(self):
         for b in self._batches:
             b.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
     def _pump(self):
         """Submits queued chunks while the next worker in turn is free."""
